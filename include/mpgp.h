@@ -1,0 +1,333 @@
+/*
+ * mpgp.h -- C ABI of the B200-native global-placement engine (libmpgp.so).
+ *
+ * The engine evaluates MyPlacement's `adaptive + neumann + course_eplace_v1`
+ * global-placement objective on one NVIDIA B200 (sm_100a) and can run the
+ * whole adaptive controller with its state resident on the device.
+ *
+ * Conventions
+ *   - Every entry point returns an int status (MPGP_OK == 0) and never throws.
+ *     The message of the most recent failure on the calling thread is
+ *     available from mpgp_last_error().
+ *   - All arrays are caller-owned host memory, plain pointers plus counts.
+ *     Positions and gradients are interleaved (x0, y0, x1, y1, ...) doubles,
+ *     exactly the layout of std::vector<myplacement::Vec2>.
+ *   - A handle is confined to one host thread; its work runs on one CUDA
+ *     stream owned by the handle.
+ *   - Status codes map onto the reference's error conventions:
+ *     MPGP_ERR_INVALID_ARGUMENT  <-> std::invalid_argument
+ *     MPGP_ERR_RUNTIME / _CUDA / _NON_FINITE / _BUDGET <-> std::runtime_error
+ *     MPGP_ERR_UNAVAILABLE       <-> tryCreateCudaPlacementBackend returning
+ *                                    nullptr with a populated reason.
+ */
+#ifndef MPGP_H
+#define MPGP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPGP_ABI_VERSION 1
+
+enum {
+    MPGP_OK = 0,
+    MPGP_ERR_INVALID_ARGUMENT = 1,
+    MPGP_ERR_RUNTIME = 2,
+    MPGP_ERR_CUDA = 3,
+    MPGP_ERR_BUDGET = 4,
+    MPGP_ERR_NON_FINITE = 5,
+    MPGP_ERR_UNAVAILABLE = 6,
+    MPGP_ERR_TIMEOUT = 7
+};
+
+/* Module flag bits (PlacementDatabase.hpp Module::is_terminal / is_fixed). */
+enum { MPGP_MODULE_TERMINAL = 1, MPGP_MODULE_FIXED = 2 };
+
+/* Density layers of a particle (CudaPlacementBackend.cu:789-800: 0/1/2). */
+enum { MPGP_LAYER_STANDARD = 0, MPGP_LAYER_MACRO = 1, MPGP_LAYER_FILLER = 2 };
+
+/* Compute backend (GlobalPlacer.hpp:19 ComputeBackend). */
+enum { MPGP_BACKEND_CPU = 0, MPGP_BACKEND_CUDA = 1, MPGP_BACKEND_AUTO = 2 };
+
+/* RUDY penalty (Rudy.hpp:16 RudyPenaltyModel). */
+enum { MPGP_RUDY_DISABLED = 0, MPGP_RUDY_HINGE_L2 = 1, MPGP_RUDY_SOFTPLUS_L2 = 2, MPGP_RUDY_HINGE_L4 = 3 };
+
+/*
+ * A flattened PlacementDatabase (include/myplacement/model/PlacementDatabase.hpp:
+ * Module :30-51, Pin :23-28, Net :53-57, SiteRow :59-69).  Pins are listed net
+ * by net: the pins of net n are [net_pin_start[n], net_pin_start[n+1]).  Module
+ * centres are the `center` field; pin offsets are relative to the centre
+ * before the module orientation is applied (transformOffset, PlacementDatabase.cpp:55-68).
+ */
+typedef struct mpgp_design {
+    int32_t module_count;
+    const double* module_width;
+    const double* module_height;
+    const double* module_x;
+    const double* module_y;
+    const int32_t* module_flags;       /* MPGP_MODULE_* bits */
+    const int32_t* module_orientation; /* Orientation enum order N,S,E,W,FN,FS,FE,FW; NULL = all N */
+    int32_t net_count;
+    const double* net_weight;
+    const int64_t* net_pin_start; /* net_count + 1 entries */
+    int64_t pin_count;
+    const int32_t* pin_module;
+    const double* pin_offset_x;
+    const double* pin_offset_y;
+    int32_t row_count;
+    const double* row_bottom;
+    const double* row_height;
+    const double* row_site_width;
+    const double* row_site_spacing;
+    const double* row_x_start;
+    const int64_t* row_site_count;
+} mpgp_design;
+
+/* GlobalPlacementOptions (include/myplacement/placement/GlobalPlacer.hpp:26-80),
+ * field for field; mpgp_options_default() fills the reference defaults. */
+typedef struct mpgp_options {
+    int32_t iterations;
+    int32_t bins_x;
+    int32_t bins_y;
+    int32_t report_interval;
+    double target_density;
+    double maximum_bin_overflow;
+    double initial_smoothing;
+    double final_smoothing;
+    double maximum_movement_in_bins;
+    double penalty_growth;
+    int32_t optimizer; /* 1 = adaptive (the only one this engine implements) */
+    int32_t maximum_backtracks;
+    double backtracking_ratio;
+    double armijo_coefficient;
+    double maximum_momentum;
+    double initial_movement_in_bins;
+    double objective_increase_for_density;
+    double hpwl_growth_restart_threshold;
+    double density_stall_threshold;
+    double density_penalty_increase;
+    double density_penalty_decrease;
+    double minimum_density_penalty;
+    double maximum_density_penalty;
+    double smoothing_overflow_exponent;
+    int32_t feasible_refinement_iterations;
+    int32_t pad0;
+    uint64_t maximum_fillers;
+    uint64_t seed;
+    /* RudyOptions (Rudy.hpp:21-40) and the routability schedule. */
+    int32_t rudy_columns;
+    int32_t rudy_rows;
+    double rudy_minimum_span_in_bins;
+    double rudy_capacity_factor;
+    double rudy_softplus_temperature;
+    int32_t rudy_penalty_model;
+    int32_t rudy_validation_bins;
+    double rudy_validation_capacity_factor;
+    double routability_start_overflow;
+    double routability_weight_scale;
+    int32_t routability_ramp_iterations;
+    int32_t density_field_boundary; /* 1 = Neumann (the only boundary the engine implements) */
+    int32_t compute_backend;        /* MPGP_BACKEND_* */
+    int32_t cuda_device;
+    uint64_t maximum_cuda_memory_bytes;
+} mpgp_options;
+
+/* DensityMetrics (include/myplacement/metrics/Metrics.hpp:38-47). */
+typedef struct mpgp_density_metrics {
+    double total_overflow_area;
+    double normalized_overflow;
+    double maximum_density;
+    double average_density;
+    double total_charge_area;
+    double normalization_area;
+    double placeable_area;
+    double dark_area;
+} mpgp_density_metrics;
+
+/* CudaPlacementEvaluation without the gradient vectors
+ * (src/placement/CudaPlacementBackend.hpp:15-23); gradients go to caller arrays. */
+typedef struct mpgp_evaluation {
+    double hpwl;
+    double smooth_wirelength;
+    double electrostatic_energy;
+    mpgp_density_metrics optimizer_density;
+    mpgp_density_metrics design_density;
+} mpgp_evaluation;
+
+/* GlobalPlacementIteration (GlobalPlacer.hpp:82-105); the global_history.csv row. */
+typedef struct mpgp_history_row {
+    int32_t iteration;
+    int32_t backtracks;
+    double hpwl;
+    double overflow;
+    double design_overflow;
+    double smooth_wirelength;
+    double density_energy;
+    double objective;
+    double penalty;
+    double smoothing;
+    double step_size;
+    double maximum_displacement;
+    double gradient_norm;
+    double curvature;
+    double rudy_energy;
+    double rudy_proxy_overflow;
+    double rudy_maximum_utilization;
+    double rudy_weight;
+    int32_t momentum_restarted;
+    int32_t accepted;
+    int32_t best_checkpoint;
+    int32_t rudy_active;
+} mpgp_history_row;
+
+/* GlobalPlacementResult (GlobalPlacer.hpp:107-129) minus the history vector. */
+typedef struct mpgp_result {
+    double hpwl_before;
+    double hpwl_after;
+    double overflow_before;
+    double overflow_after;
+    int32_t completed_iterations;
+    int32_t accepted_iterations;
+    int32_t momentum_restarts;
+    int32_t rejected_candidates;
+    int32_t best_checkpoint_iteration;
+    int32_t restored_best_checkpoint;
+    double best_checkpoint_hpwl;
+    double best_checkpoint_overflow;
+    double elapsed_seconds;
+    int32_t compute_backend_used;
+    int32_t cuda_device_used;
+    uint64_t cuda_reserved_memory_bytes;
+    int32_t history_count;
+    int32_t evaluations; /* gradient + candidate evaluations performed */
+    double rudy_energy_after;
+} mpgp_result;
+
+/*
+ * The flattened backend layout: what tryCreateCudaPlacementBackend receives
+ * (CudaPlacementBackend.hpp:45-48) after buildHostLayout
+ * (CudaPlacementBackend.cu:784-839).  Particles are the movable modules in
+ * PlacementDatabase::movableModules() order followed by the fillers.  A pin
+ * with pin_particle[i] >= 0 sits at particle centre + (pin_x, pin_y) (offset
+ * already orientation-transformed); a pin with pin_particle[i] < 0 is static
+ * at the absolute position (pin_x, pin_y).  Static bin layers are row-major
+ * [row * bins_x + column] physical areas (DensityBin::fixed_area / dark_area).
+ */
+typedef struct mpgp_layout {
+    int64_t particle_count;
+    int64_t movable_count;
+    const double* particle_width;
+    const double* particle_height;
+    const int32_t* particle_layer; /* MPGP_LAYER_* */
+    const int32_t* particle_pin_count; /* Module::pins.size(); 0 for fillers (preconditioner) */
+    int32_t net_count;
+    int32_t pad0;
+    const double* net_weight;
+    const int64_t* net_pin_start;
+    int64_t pin_count;
+    const int32_t* pin_particle;
+    const double* pin_x;
+    const double* pin_y;
+    int32_t bins_x;
+    int32_t bins_y;
+    double region_llx;
+    double region_lly;
+    double region_urx;
+    double region_ury;
+    double target_density;
+    const double* static_fixed_area;
+    const double* static_dark_area;
+} mpgp_layout;
+
+typedef struct mpgp_backend mpgp_backend;
+typedef struct mpgp_session mpgp_session;
+
+/* ---- library ---------------------------------------------------------------- */
+
+/* Replaces cudaPlacementBackendCompiled() (CudaPlacementBackend.hpp:44,
+ * CudaPlacementBackend.cu:1152-1154).  Returns 1. */
+int mpgp_compiled(void);
+
+/* ABI version of the loaded library (MPGP_ABI_VERSION). */
+int mpgp_abi_version(void);
+
+/* Message of the last failure on this thread ("" when none). */
+const char* mpgp_last_error(void);
+
+/* Fills the reference defaults of GlobalPlacementOptions (GlobalPlacer.hpp:26-80). */
+void mpgp_options_default(mpgp_options* options);
+
+/* ---- drop-in backend: one evaluation per call ---------------------------------- */
+
+/* Replaces tryCreateCudaPlacementBackend (CudaPlacementBackend.hpp:45-48,
+ * CudaPlacementBackend.cu:1156-1216).  On a recoverable failure returns
+ * MPGP_ERR_UNAVAILABLE and writes the reason (the reference's nullptr + reason). */
+int mpgp_backend_create(const mpgp_layout* layout, int device, uint64_t maximum_bytes, mpgp_backend** out,
+                        char* reason, size_t reason_capacity);
+
+/* Replaces CudaPlacementBackend::evaluate (CudaPlacementBackend.hpp:32-33,
+ * CudaPlacementBackend.cu:921-950).  `positions` holds particle_count (x, y)
+ * pairs.  When calculate_gradient != 0 the wire and density gradients (each
+ * particle_count (x, y) pairs) are written to the caller's arrays. */
+int mpgp_backend_evaluate(mpgp_backend* backend, const double* positions, double smoothing,
+                          int calculate_gradient, mpgp_evaluation* out, double* wire_gradient,
+                          double* density_gradient);
+
+/* Replaces CudaPlacementBackend::device() (CudaPlacementBackend.hpp:34). */
+int mpgp_backend_device(const mpgp_backend* backend);
+
+/* Replaces CudaPlacementBackend::reservedBytes() (CudaPlacementBackend.hpp:35). */
+uint64_t mpgp_backend_reserved_bytes(const mpgp_backend* backend);
+
+/* Replaces ~CudaPlacementBackend (CudaPlacementBackend.hpp:27). */
+void mpgp_backend_destroy(mpgp_backend* backend);
+
+/* Parity hook with no behavioural counterpart: copies the three fixed-point
+ * dynamic density layers of the last evaluation (movable, macro, filler; each
+ * bins_x*bins_y int64 in units of bin_area * 2^-32) to host arrays. */
+int mpgp_backend_density_layers(mpgp_backend* backend, int64_t* movable, int64_t* macro, int64_t* filler);
+
+/* Parity hook: solves the Neumann field of `deviation` (bins_x*bins_y doubles)
+ * with the engine's DCT contractions, matching ElectrostaticField::solve
+ * (ElectrostaticField.cpp:119-133, 205-237).  Any output may be NULL. */
+int mpgp_backend_field_solve(mpgp_backend* backend, const double* deviation, double* potential, double* field_x,
+                             double* field_y);
+
+/* ---- host setup restated from the reference ----------------------------------- */
+
+/* randomPlacement (src/placement/InitialPlacer.cpp:102-121): writes the module
+ * centres (module_count each) after seeding movables uniformly in the core. */
+int mpgp_random_placement(const mpgp_design* design, uint64_t seed, double* module_x, double* module_y);
+
+/* ---- device-resident adaptive global placement ---------------------------------- */
+
+/* Replaces GlobalPlacer::run (GlobalPlacer.cpp:134-146) ->
+ * runAdaptiveGlobalPlacement (AdaptiveGlobalPlacer.cpp:652-953) for
+ * compute_backend cuda.  module_x/module_y hold every module centre on input and
+ * receive the placed centres.  Up to history_capacity rows are written. */
+int mpgp_global_place(const mpgp_design* design, const mpgp_options* options, double* module_x, double* module_y,
+                      mpgp_result* result, mpgp_history_row* history, int32_t history_capacity);
+
+/* The same run split into steps, for callers that interleave work or time
+ * iterations: create (setup + the two initial evaluations,
+ * AdaptiveGlobalPlacer.cpp:656-733), step (up to `iterations` controller
+ * iterations; *done becomes 1 after the budget or the early stop), finish
+ * (checkpoint restore + final metrics, :930-952). */
+int mpgp_session_create(const mpgp_design* design, const mpgp_options* options, mpgp_session** out);
+int mpgp_session_step(mpgp_session* session, int32_t iterations, int32_t* completed, int32_t* done);
+int mpgp_session_finish(mpgp_session* session, double* module_x, double* module_y, mpgp_result* result,
+                        mpgp_history_row* history, int32_t history_capacity);
+/* Number of engine kernel launches issued by this session so far. */
+int64_t mpgp_session_kernel_launches(const mpgp_session* session);
+/* The CUDA stream the session's work runs on (a cudaStream_t). */
+void* mpgp_session_stream(const mpgp_session* session);
+void mpgp_session_destroy(mpgp_session* session);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPGP_H */
