@@ -244,6 +244,7 @@ typedef struct mpgp_layout {
 
 typedef struct mpgp_backend mpgp_backend;
 typedef struct mpgp_session mpgp_session;
+typedef struct mpgp_setup mpgp_setup;
 
 /* ---- library ---------------------------------------------------------------- */
 
@@ -302,6 +303,20 @@ int mpgp_backend_field_solve(mpgp_backend* backend, const double* deviation, dou
  * centres (module_count each) after seeding movables uniformly in the core. */
 int mpgp_random_placement(const mpgp_design* design, uint64_t seed, double* module_x, double* module_y);
 
+/* The host part of GlobalPlacementSession's constructor (AdaptiveGlobalPlacer.cpp:
+ * 114-126): static density (initializeStaticDensity, GlobalPlacementSupport.cpp:21-30),
+ * fillers (createDensityFillers, :52-103) and the preconditioner
+ * (initializePreconditioner, AdaptiveGlobalPlacer.cpp:358-375).  Host only: it
+ * needs no GPU, and mpgp_session_create runs the same code.  Particle queries
+ * are in session order (movable modules, then fillers); movable modules report
+ * position 0 (their positions are the caller's).  With NULL arrays only the
+ * counts are written. */
+int mpgp_setup_create(const mpgp_design* design, const mpgp_options* options, mpgp_setup** out);
+int mpgp_setup_particles(const mpgp_setup* setup, int64_t* particle_count, int64_t* movable_count, double* x,
+                         double* y, double* width, double* height, int32_t* layer, double* preconditioner);
+int mpgp_setup_static_density(const mpgp_setup* setup, double* fixed, double* dark);
+void mpgp_setup_destroy(mpgp_setup* setup);
+
 /* ---- device-resident adaptive global placement ---------------------------------- */
 
 /* Replaces GlobalPlacer::run (GlobalPlacer.cpp:134-146) ->
@@ -320,6 +335,8 @@ int mpgp_session_create(const mpgp_design* design, const mpgp_options* options, 
 int mpgp_session_step(mpgp_session* session, int32_t iterations, int32_t* completed, int32_t* done);
 int mpgp_session_finish(mpgp_session* session, double* module_x, double* module_y, mpgp_result* result,
                         mpgp_history_row* history, int32_t history_capacity);
+/* Current particle positions (particle_count (x, y) pairs). */
+int mpgp_session_positions(const mpgp_session* session, double* positions);
 /* Number of engine kernel launches issued by this session so far. */
 int64_t mpgp_session_kernel_launches(const mpgp_session* session);
 /* The CUDA stream the session's work runs on (a cudaStream_t). */

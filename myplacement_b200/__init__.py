@@ -1,0 +1,17 @@
+"""B200-native global placement for MyPlacement's adaptive + neumann + course_eplace_v1 method.
+
+The engine is the native library ``libmpgp.so`` (C ABI in include/mpgp.h,
+hand-written sm_100a CUDA kernels); this package is its host-side mirror of the
+reference's GlobalPlacer / CudaPlacementBackend interface plus the seeded
+synthetic designs the engine is measured on.
+"""
+from ._abi import EngineError, load_library
+from .design import Design, synthetic_design, workload
+from .placer import (BackendLayout, CudaPlacementBackend, GlobalPlacer, PlacementResult, Session, build_layout,
+                     default_options, host_setup, random_placement, try_create_backend)
+
+__all__ = [
+    "BackendLayout", "CudaPlacementBackend", "Design", "EngineError", "GlobalPlacer", "PlacementResult", "Session",
+    "build_layout", "default_options", "host_setup", "load_library", "random_placement", "synthetic_design", "try_create_backend",
+    "workload",
+]

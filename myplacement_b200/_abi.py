@@ -250,6 +250,11 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "mpgp_session_create": (C.c_int, [C.POINTER(Design), C.POINTER(Options), C.POINTER(vp)]),
         "mpgp_session_step": (C.c_int, [vp, C.c_int32, _i32, _i32]),
         "mpgp_session_finish": (C.c_int, [vp, _d, _d, C.POINTER(Result), C.POINTER(HistoryRow), C.c_int32]),
+        "mpgp_setup_create": (C.c_int, [C.POINTER(Design), C.POINTER(Options), C.POINTER(vp)]),
+        "mpgp_setup_particles": (C.c_int, [vp, _i64, _i64, _d, _d, _d, _d, _i32, _d]),
+        "mpgp_setup_static_density": (C.c_int, [vp, _d, _d]),
+        "mpgp_setup_destroy": (None, [vp]),
+        "mpgp_session_positions": (C.c_int, [vp, _d]),
         "mpgp_session_kernel_launches": (C.c_int64, [vp]),
         "mpgp_session_stream": (vp, [vp]),
         "mpgp_session_destroy": (None, [vp]),

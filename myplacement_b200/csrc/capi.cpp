@@ -1,0 +1,309 @@
+// extern "C" entry points of libmpgp.so (include/mpgp.h).  No exception crosses
+// this boundary: each call catches, records the message for mpgp_last_error()
+// and returns the status of the failure.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.cuh"
+#include "mpgp.h"
+#include "session.hpp"
+#include "setup.hpp"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int record(const std::exception& error) {
+    g_last_error = error.what();
+    if (const auto* e = dynamic_cast<const mpgp::Error*>(&error)) return e->status();
+    if (dynamic_cast<const std::bad_alloc*>(&error) != nullptr) return MPGP_ERR_RUNTIME;
+    if (dynamic_cast<const std::invalid_argument*>(&error) != nullptr) return MPGP_ERR_INVALID_ARGUMENT;
+    return MPGP_ERR_RUNTIME;
+}
+
+template <typename F>
+int guarded(F&& body) {
+    try {
+        g_last_error.clear();
+        body();
+        return MPGP_OK;
+    } catch (const std::exception& error) {
+        return record(error);
+    } catch (...) {
+        g_last_error = "unknown failure";
+        return MPGP_ERR_RUNTIME;
+    }
+}
+
+}  // namespace
+
+struct mpgp_backend {
+    std::unique_ptr<mpgp::Engine> engine;
+    double2* wire = nullptr;
+    double2* density = nullptr;
+    int64_t particles = 0;
+    std::vector<double2> host;
+};
+
+struct mpgp_session {
+    std::unique_ptr<mpgp::Session> session;
+};
+
+struct mpgp_setup {
+    mpgp::DerivedDesign derived;
+    mpgp::Problem problem;
+    std::vector<mpgp::Filler> fillers;
+};
+
+extern "C" {
+
+int mpgp_compiled(void) { return 1; }
+
+int mpgp_abi_version(void) { return MPGP_ABI_VERSION; }
+
+const char* mpgp_last_error(void) { return g_last_error.c_str(); }
+
+void mpgp_options_default(mpgp_options* options) {
+    if (options != nullptr) mpgp::defaultOptions(*options);
+}
+
+int mpgp_backend_create(const mpgp_layout* layout, int device, uint64_t maximum_bytes, mpgp_backend** out,
+                        char* reason, size_t reason_capacity) {
+    const auto write_reason = [&](const std::string& text) {
+        if (reason != nullptr && reason_capacity > 0) {
+            const std::size_t n = std::min(text.size(), reason_capacity - 1);
+            std::memcpy(reason, text.data(), n);
+            reason[n] = '\0';
+        }
+    };
+    write_reason("");
+    if (out == nullptr || layout == nullptr) {
+        g_last_error = "mpgp_backend_create requires a layout and an output handle.";
+        write_reason(g_last_error);
+        return MPGP_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    // The factory's recoverable failures (CudaPlacementBackend.cu:1156-1216): no
+    // device, an absent requested device, or a zero budget give a reason.
+    int device_count = 0;
+    const cudaError_t status = cudaGetDeviceCount(&device_count);
+    if (status != cudaSuccess || device_count <= 0) {
+        g_last_error = std::string("CUDA device discovery failed: ") + cudaGetErrorString(status);
+        write_reason(g_last_error);
+        return MPGP_ERR_UNAVAILABLE;
+    }
+    if (device < 0 || device >= device_count) {
+        g_last_error = "Requested CUDA device does not exist on this host.";
+        write_reason(g_last_error);
+        return MPGP_ERR_UNAVAILABLE;
+    }
+    if (maximum_bytes == 0) {
+        g_last_error = "CUDA memory limit leaves no allocatable device memory.";
+        write_reason(g_last_error);
+        return MPGP_ERR_UNAVAILABLE;
+    }
+    const int rc = guarded([&] {
+        auto backend = std::make_unique<mpgp_backend>();
+        const mpgp::Problem problem = mpgp::problemFromLayout(*layout);
+        backend->engine = std::make_unique<mpgp::Engine>(problem, device, maximum_bytes);
+        backend->particles = problem.particle_count;
+        backend->wire = backend->engine->newParticleArray("wire gradients");
+        backend->density = backend->engine->newParticleArray("density gradients");
+        backend->host.resize(static_cast<std::size_t>(problem.particle_count));
+        *out = backend.release();
+    });
+    if (rc != MPGP_OK) {
+        write_reason(g_last_error);
+        // A creation failure is recoverable for the caller (auto falls back to the CPU).
+        return rc == MPGP_ERR_INVALID_ARGUMENT ? rc : MPGP_ERR_UNAVAILABLE;
+    }
+    return MPGP_OK;
+}
+
+int mpgp_backend_evaluate(mpgp_backend* b, const double* positions, double smoothing, int calculate_gradient,
+                          mpgp_evaluation* out, double* wire_gradient, double* density_gradient) {
+    return guarded([&] {
+        mpgp::require(b != nullptr && out != nullptr, "mpgp_backend_evaluate requires a backend and an output.");
+        mpgp::require(std::isfinite(smoothing) && smoothing > 0.0,
+                      "CUDA global placement requires positive finite smoothing.");
+        mpgp::require(b->particles == 0 || positions != nullptr, "CUDA placement positions are missing.");
+        mpgp::require(!calculate_gradient || b->particles == 0 || (wire_gradient != nullptr && density_gradient != nullptr),
+                      "Gradient outputs are missing.");
+        mpgp::Engine& e = *b->engine;
+        mpgp::checkCuda(cudaSetDevice(e.device()), "Select CUDA device for evaluation");
+        const std::size_t bytes = sizeof(double2) * static_cast<std::size_t>(b->particles);
+        for (int64_t i = 0; i < 2 * b->particles; ++i) {
+            if (!std::isfinite(positions[i])) {
+                mpgp::fail(MPGP_ERR_NON_FINITE, "CUDA placement positions must be finite.");
+            }
+        }
+        if (b->particles > 0) {
+            mpgp::checkCuda(cudaMemcpyAsync(e.scratchPositions(), positions, bytes, cudaMemcpyHostToDevice, e.stream()),
+                      "Upload CUDA particle positions");
+        }
+        mpgp::EvalRequest q;
+        q.mode = mpgp::kGiven;
+        q.positions = e.scratchPositions();
+        q.smoothing = smoothing;
+        q.gradient = calculate_gradient != 0;
+        q.wire_out = b->wire;
+        q.density_out = b->density;
+        const mpgp::EvalScalars& s = e.evaluate(q);
+        out->hpwl = s.v[mpgp::kHpwl];
+        out->smooth_wirelength = s.v[mpgp::kSmooth];
+        out->electrostatic_energy = e.energy(s);
+        e.densityMetrics(s, true, out->optimizer_density);
+        e.densityMetrics(s, false, out->design_density);
+        if (calculate_gradient && b->particles > 0) {
+            mpgp::checkCuda(cudaMemcpyAsync(wire_gradient, b->wire, bytes, cudaMemcpyDeviceToHost, e.stream()),
+                      "Download CUDA wire gradients");
+            mpgp::checkCuda(cudaMemcpyAsync(density_gradient, b->density, bytes, cudaMemcpyDeviceToHost, e.stream()),
+                      "Download CUDA density gradients");
+            mpgp::checkCuda(cudaStreamSynchronize(e.stream()), "Synchronize CUDA placement evaluation");
+        }
+        if (!std::isfinite(out->smooth_wirelength) || !std::isfinite(out->hpwl) ||
+            !std::isfinite(out->electrostatic_energy)) {
+            mpgp::fail(MPGP_ERR_NON_FINITE, "CUDA global-placement evaluation produced a non-finite metric.");
+        }
+    });
+}
+
+int mpgp_backend_device(const mpgp_backend* b) { return b != nullptr ? b->engine->device() : -1; }
+
+uint64_t mpgp_backend_reserved_bytes(const mpgp_backend* b) { return b != nullptr ? b->engine->reservedBytes() : 0; }
+
+void mpgp_backend_destroy(mpgp_backend* b) {
+    if (b == nullptr) return;
+    cudaSetDevice(b->engine->device());
+    delete b;
+}
+
+int mpgp_backend_density_layers(mpgp_backend* b, int64_t* movable, int64_t* macro, int64_t* filler) {
+    return guarded([&] {
+        mpgp::require(b != nullptr, "A backend is required.");
+        mpgp::checkCuda(cudaSetDevice(b->engine->device()), "Select CUDA device");
+        b->engine->depositLayers(b->engine->scratchPositions(), movable, macro, filler);
+    });
+}
+
+int mpgp_backend_field_solve(mpgp_backend* b, const double* deviation, double* potential, double* field_x,
+                             double* field_y) {
+    return guarded([&] {
+        mpgp::require(b != nullptr && deviation != nullptr, "A backend and a deviation map are required.");
+        mpgp::checkCuda(cudaSetDevice(b->engine->device()), "Select CUDA device");
+        b->engine->fieldSolve(deviation, potential, field_x, field_y);
+    });
+}
+
+int mpgp_random_placement(const mpgp_design* design, uint64_t seed, double* module_x, double* module_y) {
+    return guarded([&] {
+        mpgp::require(design != nullptr && module_x != nullptr && module_y != nullptr, "Arguments are required.");
+        mpgp::validateDesign(*design);
+        const mpgp::DerivedDesign derived = mpgp::deriveDesign(*design);
+        mpgp::randomPlacement(*design, derived, seed, module_x, module_y);
+    });
+}
+
+int mpgp_session_create(const mpgp_design* design, const mpgp_options* options, mpgp_session** out) {
+    return guarded([&] {
+        mpgp::require(design != nullptr && options != nullptr && out != nullptr, "Arguments are required.");
+        *out = nullptr;
+        auto s = std::make_unique<mpgp_session>();
+        s->session = std::make_unique<mpgp::Session>(*design, *options);
+        *out = s.release();
+    });
+}
+
+int mpgp_session_step(mpgp_session* s, int32_t iterations, int32_t* completed, int32_t* done) {
+    return guarded([&] {
+        mpgp::require(s != nullptr && iterations >= 0, "A session and a non-negative iteration count are required.");
+        const bool finished = s->session->step(iterations, completed);
+        if (done != nullptr) *done = finished ? 1 : 0;
+    });
+}
+
+int mpgp_session_finish(mpgp_session* s, double* module_x, double* module_y, mpgp_result* result,
+                        mpgp_history_row* history, int32_t history_capacity) {
+    return guarded([&] {
+        mpgp::require(s != nullptr, "A session is required.");
+        s->session->finish(module_x, module_y, result, history, history_capacity);
+    });
+}
+
+int mpgp_setup_create(const mpgp_design* design, const mpgp_options* options, mpgp_setup** out) {
+    return guarded([&] {
+        mpgp::require(design != nullptr && options != nullptr && out != nullptr, "Arguments are required.");
+        *out = nullptr;
+        mpgp::validateDesign(*design);
+        mpgp::validateOptions(*options);
+        auto setup = std::make_unique<mpgp_setup>();
+        setup->derived = mpgp::deriveDesign(*design);
+        setup->problem = mpgp::buildProblem(*design, setup->derived, *options, setup->fillers);
+        *out = setup.release();
+    });
+}
+
+int mpgp_setup_particles(const mpgp_setup* s, int64_t* particle_count, int64_t* movable_count, double* x, double* y,
+                         double* width, double* height, int32_t* layer, double* preconditioner) {
+    return guarded([&] {
+        mpgp::require(s != nullptr, "A setup is required.");
+        const mpgp::Problem& p = s->problem;
+        if (particle_count != nullptr) *particle_count = p.particle_count;
+        if (movable_count != nullptr) *movable_count = p.movable_count;
+        const std::size_t movable = static_cast<std::size_t>(p.movable_count);
+        for (int64_t i = 0; i < p.particle_count; ++i) {
+            const std::size_t k = static_cast<std::size_t>(i);
+            if (x != nullptr) x[i] = k < movable ? 0.0 : s->fillers[k - movable].x;
+            if (y != nullptr) y[i] = k < movable ? 0.0 : s->fillers[k - movable].y;
+            if (width != nullptr) width[i] = p.width[k];
+            if (height != nullptr) height[i] = p.height[k];
+            if (layer != nullptr) layer[i] = p.layer[k];
+            if (preconditioner != nullptr) preconditioner[i] = p.precond_base[k];
+        }
+    });
+}
+
+int mpgp_setup_static_density(const mpgp_setup* s, double* fixed, double* dark) {
+    return guarded([&] {
+        mpgp::require(s != nullptr, "A setup is required.");
+        if (fixed != nullptr) std::copy(s->problem.static_fixed.begin(), s->problem.static_fixed.end(), fixed);
+        if (dark != nullptr) std::copy(s->problem.static_dark.begin(), s->problem.static_dark.end(), dark);
+    });
+}
+
+void mpgp_setup_destroy(mpgp_setup* s) { delete s; }
+
+int mpgp_session_positions(const mpgp_session* s, double* positions) {
+    return guarded([&] {
+        mpgp::require(s != nullptr && positions != nullptr, "A session and an output array are required.");
+        s->session->currentPositions(positions);
+    });
+}
+
+int64_t mpgp_session_kernel_launches(const mpgp_session* s) { return s != nullptr ? s->session->launches() : 0; }
+
+void* mpgp_session_stream(const mpgp_session* s) { return s != nullptr ? s->session->stream() : nullptr; }
+
+void mpgp_session_destroy(mpgp_session* s) { delete s; }
+
+int mpgp_global_place(const mpgp_design* design, const mpgp_options* options, double* module_x, double* module_y,
+                      mpgp_result* result, mpgp_history_row* history, int32_t history_capacity) {
+    return guarded([&] {
+        mpgp::require(design != nullptr && options != nullptr && module_x != nullptr && module_y != nullptr,
+                      "Arguments are required.");
+        mpgp::Session session(*design, *options);
+        while (!session.step(64, nullptr)) {
+        }
+        session.finish(module_x, module_y, result, history, history_capacity);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,95 @@
+// Shared definitions of the B200 global-placement engine (device and host).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "mpgp.h"
+
+namespace mpgp {
+
+// Engine failure carrying the C-ABI status it maps to.
+class Error : public std::runtime_error {
+public:
+    Error(int status, const std::string& message) : std::runtime_error(message), status_(status) {}
+    [[nodiscard]] int status() const { return status_; }
+
+private:
+    int status_;
+};
+
+[[noreturn]] inline void fail(int status, const std::string& message) { throw Error(status, message); }
+
+inline void checkCuda(cudaError_t status, const char* what) {
+    if (status != cudaSuccess) {
+        fail(MPGP_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(status));
+    }
+}
+
+inline void require(bool condition, const std::string& message) {
+    if (!condition) fail(MPGP_ERR_INVALID_ARGUMENT, message);
+}
+
+constexpr double kEpsilon = 1e-9;  // Geometry.hpp:8
+constexpr double kPi = 3.141592653589793238462643383279502884;
+constexpr int kThreads = 256;
+constexpr float kFixedOne = 4294967296.0f;  // 2^32: one bin area in fixed-point density units
+constexpr double kFixedUnit = 1.0 / 4294967296.0;
+
+inline int ceilDiv(long long value, long long divisor) {
+    return static_cast<int>((value + divisor - 1) / divisor);
+}
+
+// ---- device helpers -------------------------------------------------------------------
+
+#ifdef __CUDACC__
+
+__device__ __forceinline__ double warpSum(double value) {
+#pragma unroll
+    for (int offset = 16; offset > 0; offset >>= 1) value += __shfl_xor_sync(0xffffffffu, value, offset);
+    return value;
+}
+
+__device__ __forceinline__ double warpMax(double value) {
+#pragma unroll
+    for (int offset = 16; offset > 0; offset >>= 1) value = fmax(value, __shfl_xor_sync(0xffffffffu, value, offset));
+    return value;
+}
+
+// Deterministic block reduction of K doubles (sum, or max where `is_max[k]`);
+// thread 0 returns the result in `values`.  blockDim.x must be a multiple of 32, <= 1024.
+template <int K>
+__device__ __forceinline__ void blockReduce(double (&values)[K], const bool (&is_max)[K]) {
+    __shared__ double scratch[K][32];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int warps = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        values[k] = is_max[k] ? warpMax(values[k]) : warpSum(values[k]);
+        if (lane == 0) scratch[k][warp] = values[k];
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double v = lane < warps ? scratch[k][lane] : (is_max[k] ? -1.0e308 : 0.0);
+            values[k] = is_max[k] ? warpMax(v) : warpSum(v);
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ long long warpSumI64(long long value) {
+#pragma unroll
+    for (int offset = 16; offset > 0; offset >>= 1) value += __shfl_xor_sync(0xffffffffu, value, offset);
+    return value;
+}
+
+#endif
+
+}  // namespace mpgp

@@ -1,0 +1,213 @@
+// Course-ePlace density: fixed-point scatter and the per-bin metrics pass.
+//
+// scatter: restates DensityMap::addRectangle (Metrics.cpp:74-99) for every
+// particle (depositDynamicDensity, GlobalPlacementSupport.cpp:32-40; the
+// reference CUDA depositParticlesKernel, CudaPlacementBackend.cu:339-375).  The
+// overlap of a particle with each covered bin is computed in FP32 bin units and
+// quantized to int64 in units of bin_area * 2^-32, then added with integer
+// atomics, so the map is bit-exact run to run and equal to the fixed-point CPU
+// oracle (oracle/density_fixed.c).  Every floating-point operation uses an
+// explicitly rounded intrinsic, so no fused multiply-add can change a bit.
+// The same pass optionally forms the particle positions first: the
+// backtracking proposal (proposeStep, AdaptiveGlobalPlacer.cpp:494-519) or the
+// Nesterov lookahead (:776-780), both clamped to the core
+// (clampCenterToRegion, GlobalPlacementSupport.cpp:11-19).
+//
+// metrics: restates buildDensityMetricsKernel + collectDensityMetrics
+// (CudaPlacementBackend.cu:377-398, 1022-1038) and DensityMap::metrics
+// (Metrics.cpp:101-119), reads-and-clears the fixed-point layers and writes the
+// mean-free FP32 source of the Poisson solve (ElectrostaticField.cpp:119-133);
+// the mean comes from the exact integer layer totals of the scatter.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace mpgp {
+namespace {
+
+__device__ __forceinline__ double clampIndex(double value, int upper) {
+    return value < 0.0 ? 0.0 : (value > static_cast<double>(upper) ? static_cast<double>(upper) : value);
+}
+
+__device__ __forceinline__ double clampCenter(double value, double size, double low, double high) {
+    const double lo = __dadd_rn(low, __dmul_rn(size, 0.5));
+    const double hi = __dsub_rn(high, __dmul_rn(size, 0.5));
+    return lo <= hi ? fmax(lo, fmin(value, hi)) : __dmul_rn(__dadd_rn(low, high), 0.5);
+}
+
+__global__ void __launch_bounds__(kThreads) scatterKernel(ScatterArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double predicted = 0.0;
+    double displacement = 0.0;
+    long long totals[3] = {0, 0, 0};
+    if (i < a.particle_count) {
+        double2 c;
+        const double2 size = a.size[i];
+        if (a.mode == kGiven) {
+            c = a.positions[i];
+        } else {
+            const double2 base = a.base[i];
+            const double2 dir = a.direction[i];
+            double dx, dy;
+            if (a.mode == kPropose) {
+                dx = dir.x * (-a.step);
+                dy = dir.y * (-a.step);
+                const double norm = sqrt(dx * dx + dy * dy);
+                if (norm > a.max_displacement) {
+                    const double s = a.max_displacement / norm;
+                    dx = dx * s;
+                    dy = dy * s;
+                }
+            } else {
+                dx = dir.x * a.step;
+                dy = dir.y * a.step;
+            }
+            c.x = clampCenter(base.x + dx, size.x, a.llx, a.urx);
+            c.y = clampCenter(base.y + dy, size.y, a.lly, a.ury);
+            a.out_positions[i] = c;
+            if (a.mode == kPropose) {
+                const double2 raw = a.raw[i];
+                const double ax = base.x - c.x;
+                const double ay = base.y - c.y;
+                predicted = raw.x * ax + raw.y * ay;
+                displacement = sqrt(ax * ax + ay * ay);
+            }
+        }
+        // Fixed-point deposit (oracle/density_fixed.c).
+        const double half_w = __dmul_rn(size.x, 0.5);
+        const double half_h = __dmul_rn(size.y, 0.5);
+        const double l = fmax(a.llx, __dsub_rn(c.x, half_w));
+        const double r = fmin(a.urx, __dadd_rn(c.x, half_w));
+        const double b = fmax(a.lly, __dsub_rn(c.y, half_h));
+        const double t = fmin(a.ury, __dadd_rn(c.y, half_h));
+        if (__dmul_rn(fmax(0.0, __dsub_rn(r, l)), fmax(0.0, __dsub_rn(t, b))) > 1e-9) {
+            const double gl = __ddiv_rn(__dsub_rn(l, a.llx), a.bin_w);
+            const double gr = __ddiv_rn(__dsub_rn(r, a.llx), a.bin_w);
+            const double gb = __ddiv_rn(__dsub_rn(b, a.lly), a.bin_h);
+            const double gt = __ddiv_rn(__dsub_rn(t, a.lly), a.bin_h);
+            const int c0 = static_cast<int>(clampIndex(floor(gl), a.bins_x - 1));
+            const int c1 = static_cast<int>(clampIndex(__dsub_rn(ceil(gr), 1.0), a.bins_x - 1));
+            const int r0 = static_cast<int>(clampIndex(floor(gb), a.bins_y - 1));
+            const int r1 = static_cast<int>(clampIndex(__dsub_rn(ceil(gt), 1.0), a.bins_y - 1));
+            const float fl = __double2float_rn(__dsub_rn(gl, static_cast<double>(c0)));
+            const float fr = __double2float_rn(__dsub_rn(gr, static_cast<double>(c0)));
+            const float fb = __double2float_rn(__dsub_rn(gb, static_cast<double>(r0)));
+            const float ft = __double2float_rn(__dsub_rn(gt, static_cast<double>(r0)));
+            const int code = a.layer[i];
+            unsigned long long* target = a.layers + static_cast<size_t>(code) * a.bins_x * a.bins_y;
+            long long sum = 0;
+            for (int row = r0; row <= r1; ++row) {
+                const float fi = static_cast<float>(row - r0);
+                const float oy = fmaxf(0.0f, __fsub_rn(fminf(ft, __fadd_rn(fi, 1.0f)), fmaxf(fb, fi)));
+                for (int column = c0; column <= c1; ++column) {
+                    const float fj = static_cast<float>(column - c0);
+                    const float ox = fmaxf(0.0f, __fsub_rn(fminf(fr, __fadd_rn(fj, 1.0f)), fmaxf(fl, fj)));
+                    const long long q = __float2ll_rn(__fmul_rn(__fmul_rn(ox, oy), kFixedOne));
+                    if (q != 0) {
+                        atomicAdd(target + static_cast<size_t>(row) * a.bins_x + column,
+                                  static_cast<unsigned long long>(q));
+                        sum += q;
+                    }
+                }
+            }
+            totals[code] = sum;
+        }
+    }
+    // Exact integer totals of each layer (for the mean removal) and the proposal scalars.
+    __shared__ long long block_totals[3];
+    if (threadIdx.x < 3) block_totals[threadIdx.x] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const long long w = warpSumI64(totals[k]);
+        if ((threadIdx.x & 31) == 0 && w != 0) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(&block_totals[k]), static_cast<unsigned long long>(w));
+        }
+    }
+    double values[2] = {predicted, displacement};
+    const bool is_max[2] = {false, true};
+    blockReduce<2>(values, is_max);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (block_totals[k] != 0) atomicAdd(a.totals + k, static_cast<unsigned long long>(block_totals[k]));
+        }
+        if (a.partials != nullptr) {
+            a.partials[2 * blockIdx.x + 0] = values[0];
+            a.partials[2 * blockIdx.x + 1] = values[1];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) metricsKernel(MetricsArgs a) {
+    const double t = a.target_density;
+    const double unit = a.bin_area * kFixedUnit;
+    const double capacity = t * a.bin_area;
+    // Mean of the density deviation from the exact layer totals.
+    const double movable_sum = static_cast<double>(static_cast<long long>(a.totals[0])) * unit;
+    const double macro_sum = static_cast<double>(static_cast<long long>(a.totals[1])) * unit;
+    const double filler_sum = static_cast<double>(static_cast<long long>(a.totals[2])) * unit;
+    const double charge_total = movable_sum + t * (a.static_fixed_sum + macro_sum + a.static_dark_sum + filler_sum);
+    const double mean = charge_total / (a.bin_area * static_cast<double>(a.bin_count)) - t;
+
+    double v[9] = {0, 0, 0, 0, 0, 0, 0, -1.0e308, -1.0e308};
+    const size_t bins = static_cast<size_t>(a.bin_count);
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < a.bin_count; b += gridDim.x * blockDim.x) {
+        const long long qm = static_cast<long long>(a.layers[b]);
+        const long long qc = static_cast<long long>(a.layers[bins + b]);
+        const long long qf = static_cast<long long>(a.layers[2 * bins + b]);
+        a.layers[b] = 0ULL;
+        a.layers[bins + b] = 0ULL;
+        a.layers[2 * bins + b] = 0ULL;
+        const double movable = static_cast<double>(qm) * unit;
+        const double macro = static_cast<double>(qc) * unit;
+        const double filler = static_cast<double>(qf) * unit;
+        const double fixed = a.fixed[b];
+        const double dark = a.dark[b];
+        const double without = movable + t * (fixed + macro + dark + 0.0);  // DensityBin::chargeArea(t, false)
+        const double with = movable + t * (fixed + macro + dark + filler);  // DensityBin::chargeArea(t, true)
+        const double density_with = with / a.bin_area;
+        const double density_without = without / a.bin_area;
+        v[0] += fmax(0.0, with - capacity);
+        v[1] += fmax(0.0, without - capacity);
+        v[2] += with;
+        v[3] += without;
+        v[4] += movable + t * macro;  // DensityBin::normalizationArea
+        v[5] += density_with;
+        v[6] += density_without;
+        v[7] = fmax(v[7], density_with);
+        v[8] = fmax(v[8], density_without);
+        a.source[b] = static_cast<float>((density_with - t) - mean);
+    }
+    const bool is_max[9] = {false, false, false, false, false, false, false, true, true};
+    blockReduce<9>(v, is_max);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) a.partials[9 * blockIdx.x + k] = v[k];
+    }
+}
+
+__global__ void velocityKernel(const double2* next, const double2* previous, double2* velocity, int count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const double2 n = next[i];
+    const double2 p = previous[i];
+    velocity[i] = make_double2(n.x - p.x, n.y - p.y);
+}
+
+}  // namespace
+
+void launchScatter(const ScatterArgs& args, int blocks, cudaStream_t stream) {
+    if (blocks <= 0) return;
+    scatterKernel<<<blocks, kThreads, 0, stream>>>(args);
+}
+
+void launchMetrics(const MetricsArgs& args, int blocks, cudaStream_t stream) {
+    metricsKernel<<<blocks, kThreads, 0, stream>>>(args);
+}
+
+void launchVelocity(const double2* next, const double2* previous, double2* velocity, int count, cudaStream_t stream) {
+    if (count <= 0) return;
+    velocityKernel<<<ceilDiv(count, kThreads), kThreads, 0, stream>>>(next, previous, velocity, count);
+}
+
+}  // namespace mpgp

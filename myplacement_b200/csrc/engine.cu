@@ -1,0 +1,554 @@
+// Device engine: allocation, static upload, and the launch sequence of one evaluation.
+//
+// One evaluation replaces CudaPlacementBackendImpl::evaluate
+// (CudaPlacementBackend.cu:921-950) with, on one stream:
+//   scatter (+ proposal / lookahead)  ->  wirelength  ->  metrics + source
+//   -> DCT forward (2 contractions, spectral epilogue, Parseval energy)
+//   [gradient: -> 2 x 2 inverse contractions -> fused field gather + combine]
+//   -> scalar reduction
+// and one 168-byte scalar read-back, instead of 14 blocking reductions and the
+// position / gradient round trips of the reference.
+#include "engine.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "common.cuh"
+
+namespace mpgp {
+
+DeviceArena::~DeviceArena() {
+    for (void* p : blocks_) cudaFree(p);
+}
+
+void* DeviceArena::allocate(std::size_t bytes, const char* what) {
+    bytes = std::max<std::size_t>(bytes, 16);
+    bytes = (bytes + 255) & ~static_cast<std::size_t>(255);
+    if (bytes > limit_ - std::min(limit_, reserved_)) {
+        fail(MPGP_ERR_BUDGET, std::string("CUDA allocation budget exceeded while reserving ") + what +
+                                  " (requested " + std::to_string(bytes) + " bytes, reserved " +
+                                  std::to_string(reserved_) + " bytes, limit " + std::to_string(limit_) + " bytes).");
+    }
+    void* p = nullptr;
+    checkCuda(cudaMalloc(&p, bytes), what);
+    blocks_.push_back(p);
+    reserved_ += bytes;
+    return p;
+}
+
+namespace {
+
+template <typename T>
+void upload(T* device, const std::vector<T>& host, cudaStream_t stream) {
+    if (!host.empty()) {
+        checkCuda(cudaMemcpyAsync(device, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice, stream),
+                  "upload");
+    }
+}
+
+// cos(pi * m / (2n)) for an integer m, reduced exactly modulo 4n.
+double cosQuarter(long long m, int n) {
+    m %= 4LL * n;
+    return std::cos(kPi * static_cast<double>(m) / (2.0 * n));
+}
+double sinQuarter(long long m, int n) {
+    m %= 4LL * n;
+    return std::sin(kPi * static_cast<double>(m) / (2.0 * n));
+}
+
+}  // namespace
+
+Engine::Engine(const Problem& p, int device, uint64_t budget_bytes) : device_(device), arena_(budget_bytes) {
+    checkCuda(cudaSetDevice(device_), "Select CUDA device");
+    checkCuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "Create engine stream");
+    particle_count_ = p.particle_count;
+    movable_count_ = p.movable_count;
+    bins_x_ = p.bins_x;
+    bins_y_ = p.bins_y;
+    bin_count_ = bins_x_ * bins_y_;
+    region_ = p.region;
+    target_density_ = p.target_density;
+    bin_w_ = region_.width() / static_cast<double>(bins_x_);
+    bin_h_ = region_.height() / static_cast<double>(bins_y_);
+    bin_area_ = (std::max(0.0, region_.width()) * std::max(0.0, region_.height())) / static_cast<double>(bin_count_);
+    uploadStatic(p);
+    buildNetLayout(p);
+    buildBasis();
+    checkCuda(cudaMallocHost(reinterpret_cast<void**>(&host_scalars_), sizeof(EvalScalars)), "pinned scalars");
+    std::memset(host_scalars_, 0, sizeof(EvalScalars));
+    checkCuda(cudaStreamSynchronize(stream_), "Engine setup");
+}
+
+Engine::~Engine() {
+    if (stream_ != nullptr) {
+        cudaStreamSynchronize(stream_);
+        cudaStreamDestroy(stream_);
+    }
+    if (host_scalars_ != nullptr) cudaFreeHost(host_scalars_);
+}
+
+double2* Engine::newParticleArray(const char* what) {
+    double2* p = arena_.array<double2>(static_cast<std::size_t>(std::max<int64_t>(1, particle_count_)), what);
+    checkCuda(cudaMemsetAsync(p, 0, sizeof(double2) * std::max<int64_t>(1, particle_count_), stream_), what);
+    return p;
+}
+
+void Engine::uploadStatic(const Problem& p) {
+    const std::size_t n = static_cast<std::size_t>(std::max<int64_t>(1, particle_count_));
+    std::vector<double2> size(static_cast<std::size_t>(particle_count_));
+    std::vector<unsigned char> layer(static_cast<std::size_t>(particle_count_));
+    for (int64_t i = 0; i < particle_count_; ++i) {
+        size[i] = make_double2(p.width[i], p.height[i]);
+        layer[i] = static_cast<unsigned char>(p.layer[i]);
+    }
+    size_ = arena_.array<double2>(n, "particle sizes");
+    layer_ = arena_.array<unsigned char>(n, "particle layers");
+    charge_ = arena_.array<double>(n, "particle charge areas");
+    precond_ = arena_.array<double>(n, "preconditioner");
+    scratch_positions_ = arena_.array<double2>(n, "uploaded positions");
+    upload(size_, size, stream_);
+    upload(layer_, layer, stream_);
+    upload(charge_, p.charge, stream_);
+    if (!p.precond_base.empty()) upload(precond_, p.precond_base, stream_);
+
+    const std::size_t bins = static_cast<std::size_t>(bin_count_);
+    layers_ = arena_.array<unsigned long long>(3 * bins, "fixed-point density layers");
+    totals_ = arena_.array<unsigned long long>(4, "density layer totals");
+    fixed_ = arena_.array<double>(bins, "fixed density layer");
+    dark_ = arena_.array<double>(bins, "dark density layer");
+    source_ = arena_.array<float>(bins, "density source");
+    checkCuda(cudaMemsetAsync(layers_, 0, 3 * bins * sizeof(unsigned long long), stream_), "clear layers");
+    checkCuda(cudaMemsetAsync(totals_, 0, 4 * sizeof(unsigned long long), stream_), "clear totals");
+    upload(fixed_, p.static_fixed, stream_);
+    upload(dark_, p.static_dark, stream_);
+    // Static sums in bin order: DensityMap::metrics (Metrics.cpp:101-119) uses each
+    // bin's own rectangle area for the placeable area.
+    for (int row = 0; row < bins_y_; ++row) {
+        for (int column = 0; column < bins_x_; ++column) {
+            const std::size_t b = static_cast<std::size_t>(row) * bins_x_ + column;
+            const double left = region_.llx + static_cast<double>(column) * bin_w_;
+            const double bottom = region_.lly + static_cast<double>(row) * bin_h_;
+            const double area = std::max(0.0, (left + bin_w_) - left) * std::max(0.0, (bottom + bin_h_) - bottom);
+            static_fixed_sum_ += p.static_fixed[b];
+            static_dark_sum_ += p.static_dark[b];
+            static_placeable_sum_ += area - p.static_dark[b];
+        }
+    }
+    scatter_blocks_ = ceilDiv(std::max<int64_t>(1, particle_count_), kThreads);
+    gather_blocks_ = scatter_blocks_;
+    metrics_blocks_ = std::min(ceilDiv(bin_count_, kThreads), 148 * 8);
+    partials_sc_ = arena_.array<double>(2 * static_cast<std::size_t>(scatter_blocks_), "scatter partials");
+    partials_m_ = arena_.array<double>(9 * static_cast<std::size_t>(metrics_blocks_), "metric partials");
+    partials_g_ = arena_.array<double>(7 * static_cast<std::size_t>(gather_blocks_), "gather partials");
+    scalars_ = arena_.array<double>(kScalarCount, "evaluation scalars");
+    checkCuda(cudaMemsetAsync(scalars_, 0, kScalarCount * sizeof(double), stream_), "clear scalars");
+}
+
+void Engine::buildNetLayout(const Problem& p) {
+    const int net_count = static_cast<int>(p.net_weight.size());
+    // Degree buckets: G lanes per net for degree <= G, a warp loop above 32.
+    const int kGroups[6] = {2, 4, 8, 16, 32, 0};
+    std::vector<std::vector<int>> bucket(6);
+    for (int n = 0; n < net_count; ++n) {
+        const int64_t degree = p.net_pin_start[n + 1] - p.net_pin_start[n];
+        if (degree < 2) continue;  // nets with fewer than two pins contribute nothing
+        const int b = degree <= 2 ? 0 : degree <= 4 ? 1 : degree <= 8 ? 2 : degree <= 16 ? 3 : degree <= 32 ? 4 : 5;
+        bucket[b].push_back(n);
+    }
+    std::vector<int> pin_particle;
+    std::vector<float2> pin_offset;
+    std::vector<double2> static_pins;
+    std::vector<int> net_start{0};
+    std::vector<float> net_weight;
+    std::vector<int4> work;
+    for (int b = 0; b < 6; ++b) {
+        const int group = kGroups[b];
+        const int nets_per_block = group == 0 ? 32 : (kThreads / group) * 4;
+        const int first_net = static_cast<int>(net_weight.size());
+        for (const int n : bucket[b]) {
+            for (int64_t pin = p.net_pin_start[n]; pin < p.net_pin_start[n + 1]; ++pin) {
+                const int particle = p.pin_particle[pin];
+                if (particle >= 0) {
+                    pin_particle.push_back(particle);
+                    pin_offset.push_back(make_float2(static_cast<float>(p.pin_x[pin]), static_cast<float>(p.pin_y[pin])));
+                } else {
+                    pin_particle.push_back(-static_cast<int>(static_pins.size()) - 1);
+                    pin_offset.push_back(make_float2(0.0f, 0.0f));
+                    static_pins.push_back(make_double2(p.pin_x[pin], p.pin_y[pin]));
+                }
+            }
+            net_start.push_back(static_cast<int>(pin_particle.size()));
+            net_weight.push_back(static_cast<float>(p.net_weight[n]));
+        }
+        const int count = static_cast<int>(bucket[b].size());
+        for (int off = 0; off < count; off += nets_per_block) {
+            work.push_back(make_int4(group, first_net + off, std::min(nets_per_block, count - off), 0));
+        }
+    }
+    wl_blocks_ = static_cast<int>(work.size());
+    const std::size_t pins = std::max<std::size_t>(1, pin_particle.size());
+    pin_particle_ = arena_.array<int>(pins, "pin particles");
+    pin_offset_ = arena_.array<float2>(pins, "pin offsets");
+    static_pins_ = arena_.array<double2>(std::max<std::size_t>(1, static_pins.size()), "static pins");
+    net_start_ = arena_.array<int>(net_start.size(), "net offsets");
+    net_weight_ = arena_.array<float>(std::max<std::size_t>(1, net_weight.size()), "net weights");
+    block_work_ = arena_.array<int4>(std::max<std::size_t>(1, work.size()), "wirelength work");
+    pin_gradient_ = arena_.array<float2>(pins, "pin gradients");
+    partials_wl_ = arena_.array<double>(2 * std::max<std::size_t>(1, work.size()), "wirelength partials");
+    upload(pin_particle_, pin_particle, stream_);
+    upload(pin_offset_, pin_offset, stream_);
+    upload(static_pins_, static_pins, stream_);
+    upload(net_start_, net_start, stream_);
+    upload(net_weight_, net_weight, stream_);
+    upload(block_work_, work, stream_);
+    checkCuda(cudaMemsetAsync(pin_gradient_, 0, pins * sizeof(float2), stream_), "clear pin gradients");
+
+    // Per-particle pin lists (bucketed pin indices, ascending) for the deterministic gather.
+    const std::size_t movable = static_cast<std::size_t>(movable_count_);
+    std::vector<int> count(movable + 1, 0);
+    for (std::size_t i = 0; i < pin_particle.size(); ++i) {
+        const int particle = pin_particle[i];
+        if (particle >= 0 && static_cast<std::size_t>(particle) < movable) ++count[particle + 1];
+    }
+    for (std::size_t i = 0; i < movable; ++i) count[i + 1] += count[i];
+    std::vector<int> list(static_cast<std::size_t>(count[movable]));
+    std::vector<int> fill(count.begin(), count.end() - 1);
+    for (std::size_t i = 0; i < pin_particle.size(); ++i) {
+        const int particle = pin_particle[i];
+        if (particle >= 0 && static_cast<std::size_t>(particle) < movable) list[fill[particle]++] = static_cast<int>(i);
+    }
+    particle_pin_start_ = arena_.array<int>(count.size(), "particle pin offsets");
+    particle_pins_ = arena_.array<int>(std::max<std::size_t>(1, list.size()), "particle pins");
+    upload(particle_pin_start_, count, stream_);
+    upload(particle_pins_, list, stream_);
+    checkCuda(cudaStreamSynchronize(stream_), "net layout upload");
+}
+
+void Engine::buildBasis() {
+    const int nx = bins_x_, ny = bins_y_;
+    const double width = region_.width(), height = region_.height();
+    std::vector<float> cx_t(static_cast<std::size_t>(nx) * nx), dx_t(cx_t.size()), sx_w(cx_t.size());
+    std::vector<float> cy(static_cast<std::size_t>(ny) * ny), dy(cy.size()), sy_w(cy.size());
+    for (int c = 0; c < nx; ++c) {
+        for (int k = 0; k < nx; ++k) {
+            const long long m = static_cast<long long>(k) * (2 * c + 1);
+            const double wave = kPi * static_cast<double>(k) / width;
+            cx_t[static_cast<std::size_t>(c) * nx + k] = static_cast<float>(2.0 * cosQuarter(m, nx));
+            dx_t[static_cast<std::size_t>(k) * nx + c] = static_cast<float>(k == 0 ? 1.0 : 2.0 * cosQuarter(m, nx));
+            sx_w[static_cast<std::size_t>(k) * nx + c] = static_cast<float>(k == 0 ? 0.0 : wave * 2.0 * sinQuarter(m, nx));
+        }
+    }
+    for (int r = 0; r < ny; ++r) {
+        for (int l = 0; l < ny; ++l) {
+            const long long m = static_cast<long long>(l) * (2 * r + 1);
+            const double wave = kPi * static_cast<double>(l) / height;
+            cy[static_cast<std::size_t>(l) * ny + r] = static_cast<float>(2.0 * cosQuarter(m, ny));
+            dy[static_cast<std::size_t>(r) * ny + l] = static_cast<float>(l == 0 ? 1.0 : 2.0 * cosQuarter(m, ny));
+            sy_w[static_cast<std::size_t>(r) * ny + l] = static_cast<float>(l == 0 ? 0.0 : wave * 2.0 * sinQuarter(m, ny));
+        }
+    }
+    // Spectral divide (ElectrostaticField.cpp:212-221): 1/(4 Nx Ny) / (kx^2 + ky^2), DC removed.
+    std::vector<float> scale(static_cast<std::size_t>(ny) * nx);
+    const double normalization = 1.0 / (4.0 * static_cast<double>(nx) * static_cast<double>(ny));
+    for (int l = 0; l < ny; ++l) {
+        const double wave_y = kPi * static_cast<double>(l) / height;
+        for (int k = 0; k < nx; ++k) {
+            const double wave_x = kPi * static_cast<double>(k) / width;
+            const double denominator = wave_x * wave_x + wave_y * wave_y;
+            scale[static_cast<std::size_t>(l) * nx + k] =
+                denominator <= kEpsilon ? 0.0f : static_cast<float>(normalization / denominator);
+        }
+    }
+    std::vector<float> wy(static_cast<std::size_t>(ny), 1.0f), wx(static_cast<std::size_t>(nx), 1.0f);
+    wy[0] = 0.5f;
+    wx[0] = 0.5f;
+    const std::size_t bins = static_cast<std::size_t>(bin_count_);
+    basis_cx_t_ = arena_.array<float>(cx_t.size(), "DCT basis");
+    basis_dx_t_ = arena_.array<float>(dx_t.size(), "DCT basis");
+    basis_sx_w_ = arena_.array<float>(sx_w.size(), "DST basis");
+    basis_cy_ = arena_.array<float>(cy.size(), "DCT basis");
+    basis_dy_ = arena_.array<float>(dy.size(), "DCT basis");
+    basis_sy_w_ = arena_.array<float>(sy_w.size(), "DST basis");
+    spectral_scale_ = arena_.array<float>(bins, "spectral scale");
+    weight_y_ = arena_.array<float>(wy.size(), "Parseval weights");
+    weight_x_ = arena_.array<float>(wx.size(), "Parseval weights");
+    stage_a_ = arena_.array<float>(bins, "DCT stage");
+    phi_hat_ = arena_.array<float>(bins, "potential coefficients");
+    stage_t_ = arena_.array<float>(bins, "DCT stage");
+    stage_u_ = arena_.array<float>(bins, "DCT stage");
+    field_ = arena_.array<float2>(bins, "electric field");
+    potential_ = arena_.array<float>(bins, "potential");
+    upload(basis_cx_t_, cx_t, stream_);
+    upload(basis_dx_t_, dx_t, stream_);
+    upload(basis_sx_w_, sx_w, stream_);
+    upload(basis_cy_, cy, stream_);
+    upload(basis_dy_, dy, stream_);
+    upload(basis_sy_w_, sy_w, stream_);
+    upload(spectral_scale_, scale, stream_);
+    upload(weight_y_, wy, stream_);
+    upload(weight_x_, wx, stream_);
+    GemmTask probe{};
+    probe.m = ny;
+    probe.n = nx;
+    energy_blocks_ = gemmBlocks(probe);
+    partials_e_ = arena_.array<double>(static_cast<std::size_t>(energy_blocks_), "energy partials");
+    checkCuda(cudaStreamSynchronize(stream_), "basis upload");
+}
+
+void Engine::launch(const EvalRequest& q) {
+    const int nx = bins_x_, ny = bins_y_;
+    const double2* positions = q.mode == kGiven ? q.positions : q.out_positions;
+    require(positions != nullptr, "An evaluation needs positions.");
+    require(q.smoothing > 0.0 && std::isfinite(q.smoothing), "Global placement requires positive finite smoothing.");
+
+    ScatterArgs sa{};
+    sa.mode = q.mode;
+    sa.particle_count = static_cast<int>(particle_count_);
+    sa.positions = q.positions;
+    sa.base = q.base;
+    sa.direction = q.direction;
+    sa.raw = q.raw_direction;
+    sa.step = q.step;
+    sa.max_displacement = q.max_displacement;
+    sa.out_positions = q.out_positions;
+    sa.size = size_;
+    sa.layer = layer_;
+    sa.llx = region_.llx;
+    sa.lly = region_.lly;
+    sa.urx = region_.urx;
+    sa.ury = region_.ury;
+    sa.bin_w = bin_w_;
+    sa.bin_h = bin_h_;
+    sa.bins_x = nx;
+    sa.bins_y = ny;
+    sa.layers = layers_;
+    sa.totals = totals_;
+    sa.partials = partials_sc_;
+    launchScatter(sa, particle_count_ > 0 ? scatter_blocks_ : 0, stream_);
+
+    WirelengthArgs wa{};
+    wa.positions = positions;
+    wa.pin_particle = pin_particle_;
+    wa.pin_offset = pin_offset_;
+    wa.static_pins = static_pins_;
+    wa.net_start = net_start_;
+    wa.net_weight = net_weight_;
+    wa.block_work = block_work_;
+    wa.gamma = static_cast<float>(std::max(q.smoothing, kEpsilon));
+    wa.inv_gamma = static_cast<float>(1.0 / std::max(q.smoothing, kEpsilon));
+    wa.pin_gradient = pin_gradient_;
+    wa.gradient = q.gradient ? 1 : 0;
+    wa.partials = partials_wl_;
+    launchWirelength(wa, wl_blocks_, stream_);
+
+    MetricsArgs ma{};
+    ma.layers = layers_;
+    ma.totals = totals_;
+    ma.fixed = fixed_;
+    ma.dark = dark_;
+    ma.static_fixed_sum = static_fixed_sum_;
+    ma.static_dark_sum = static_dark_sum_;
+    ma.target_density = target_density_;
+    ma.bin_area = bin_area_;
+    ma.bin_count = bin_count_;
+    ma.source = source_;
+    ma.partials = partials_m_;
+    launchMetrics(ma, metrics_blocks_, stream_);
+
+    // Forward DCT-II in both axes; epilogue: spectral divide + Parseval energy.
+    GemmTask f1{};
+    f1.a = source_; f1.b = basis_cx_t_; f1.c = stage_a_;
+    f1.m = ny; f1.n = nx; f1.k = nx; f1.lda = nx; f1.ldb = nx; f1.ldc = nx; f1.c_step = 1;
+    launchGemm(&f1, 1, stream_);
+    GemmTask f2{};
+    f2.a = basis_cy_; f2.b = stage_a_; f2.c = phi_hat_;
+    f2.m = ny; f2.n = nx; f2.k = ny; f2.lda = ny; f2.ldb = nx; f2.ldc = nx; f2.c_step = 1;
+    f2.scale = spectral_scale_; f2.weight_r = weight_y_; f2.weight_c = weight_x_; f2.energy_partials = partials_e_;
+    launchGemm(&f2, 1, stream_);
+    int kernels = 6;
+
+    if (q.gradient) {
+        GemmTask inv1[2]{};
+        inv1[0].a = basis_dy_; inv1[0].b = phi_hat_; inv1[0].c = stage_t_;
+        inv1[0].m = ny; inv1[0].n = nx; inv1[0].k = ny; inv1[0].lda = ny; inv1[0].ldb = nx; inv1[0].ldc = nx; inv1[0].c_step = 1;
+        inv1[1].a = phi_hat_; inv1[1].b = basis_dx_t_; inv1[1].c = stage_u_;
+        inv1[1].m = ny; inv1[1].n = nx; inv1[1].k = nx; inv1[1].lda = nx; inv1[1].ldb = nx; inv1[1].ldc = nx; inv1[1].c_step = 1;
+        launchGemm(inv1, 2, stream_);
+        GemmTask inv2[2]{};
+        inv2[0].a = stage_t_; inv2[0].b = basis_sx_w_; inv2[0].c = reinterpret_cast<float*>(field_);
+        inv2[0].m = ny; inv2[0].n = nx; inv2[0].k = nx; inv2[0].lda = nx; inv2[0].ldb = nx; inv2[0].ldc = 2 * nx; inv2[0].c_step = 2;
+        inv2[1].a = basis_sy_w_; inv2[1].b = stage_u_; inv2[1].c = reinterpret_cast<float*>(field_) + 1;
+        inv2[1].m = ny; inv2[1].n = nx; inv2[1].k = ny; inv2[1].lda = ny; inv2[1].ldb = nx; inv2[1].ldc = 2 * nx; inv2[1].c_step = 2;
+        launchGemm(inv2, 2, stream_);
+        kernels += 2;
+        if (q.want_potential) {
+            GemmTask pot{};
+            pot.a = stage_t_; pot.b = basis_dx_t_; pot.c = potential_;
+            pot.m = ny; pot.n = nx; pot.k = nx; pot.lda = nx; pot.ldb = nx; pot.ldc = nx; pot.c_step = 1;
+            launchGemm(&pot, 1, stream_);
+            kernels += 1;
+        }
+        GatherArgs ga{};
+        ga.particle_count = static_cast<int>(particle_count_);
+        ga.movable_count = static_cast<int>(movable_count_);
+        ga.positions = positions;
+        ga.particle_pin_start = particle_pin_start_;
+        ga.particle_pins = particle_pins_;
+        ga.pin_gradient = pin_gradient_;
+        ga.field = field_;
+        ga.charge = charge_;
+        ga.precond_base = q.wire_out != nullptr ? nullptr : precond_;
+        ga.llx = region_.llx;
+        ga.lly = region_.lly;
+        ga.urx = region_.urx;
+        ga.ury = region_.ury;
+        ga.bin_w = bin_w_;
+        ga.bin_h = bin_h_;
+        ga.bins_x = nx;
+        ga.bins_y = ny;
+        ga.penalty = q.penalty;
+        ga.precond_scale = q.precond_scale;
+        ga.raw = q.raw;
+        ga.pre = q.pre;
+        ga.wire_out = q.wire_out;
+        ga.density_out = q.density_out;
+        ga.prev_positions = q.prev_positions;
+        ga.prev_gradient = q.prev_gradient;
+        ga.velocity = q.velocity;
+        ga.partials = partials_g_;
+        launchGather(ga, particle_count_ > 0 ? gather_blocks_ : 0, stream_);
+        kernels += 1;
+    }
+
+    ReduceArgs ra{};
+    int s = 0;
+    const auto add = [&](const double* partials, int rows, int stride, int column, bool is_max, int target) {
+        ra.sources[s++] = ReduceSource{partials, rows, stride, column, is_max ? 1 : 0, target};
+    };
+    add(partials_wl_, wl_blocks_, 2, 0, false, kSmooth);
+    add(partials_wl_, wl_blocks_, 2, 1, false, kHpwl);
+    const int scatter_rows = particle_count_ > 0 ? scatter_blocks_ : 0;
+    add(partials_sc_, q.mode == kPropose ? scatter_rows : 0, 2, 0, false, kPredicted);
+    add(partials_sc_, q.mode == kPropose ? scatter_rows : 0, 2, 1, true, kMaxDisplacement);
+    for (int k = 0; k < 9; ++k) add(partials_m_, metrics_blocks_, 9, k, k >= 7, kOverflowWith + k);
+    add(partials_e_, energy_blocks_, 1, 0, false, kEnergy);
+    if (q.gradient) {
+        const int rows = particle_count_ > 0 ? gather_blocks_ : 0;
+        for (int k = 0; k < 7; ++k) add(partials_g_, rows, 7, k, false, kWireL1 + k);
+    }
+    ra.source_count = s;
+    ra.scalars = scalars_;
+    ra.totals = totals_;
+    launchReduce(ra, stream_);
+    checkCuda(cudaMemcpyAsync(host_scalars_, scalars_, sizeof(EvalScalars), cudaMemcpyDeviceToHost, stream_),
+              "Download evaluation scalars");
+    launches_ += kernels;
+    last_gradient_ = q.gradient;
+    last_propose_ = q.mode == kPropose;
+}
+
+const EvalScalars& Engine::sync() {
+    checkCuda(cudaStreamSynchronize(stream_), "Synchronize placement evaluation");
+    return *host_scalars_;
+}
+
+void Engine::densityMetrics(const EvalScalars& s, bool with, mpgp_density_metrics& out) const {
+    out.total_overflow_area = with ? s.v[kOverflowWith] : s.v[kOverflowWithout];
+    out.total_charge_area = with ? s.v[kChargeWith] : s.v[kChargeWithout];
+    out.normalization_area = s.v[kNormalization];
+    out.maximum_density = std::max(0.0, with ? s.v[kDensityMaxWith] : s.v[kDensityMaxWithout]);
+    out.average_density = (with ? s.v[kDensitySumWith] : s.v[kDensitySumWithout]) /
+                          static_cast<double>(std::max(1, bin_count_));
+    out.dark_area = static_dark_sum_;
+    out.placeable_area = static_placeable_sum_;
+    out.normalized_overflow = out.total_overflow_area / std::max(out.normalization_area, kEpsilon);
+}
+
+double Engine::energy(const EvalScalars& s) const { return std::max(0.0, 0.5 * bin_area_ * s.v[kEnergy]); }
+
+void Engine::fieldSolve(const double* deviation, double* potential, double* field_x, double* field_y) {
+    // Upload the deviation into the source buffer with its FP64 mean removed
+    // (ElectrostaticField.cpp:119-133), then run the same contractions.
+    const std::size_t bins = static_cast<std::size_t>(bin_count_);
+    double mean = 0.0;
+    for (std::size_t i = 0; i < bins; ++i) mean += deviation[i];
+    mean /= static_cast<double>(bins);
+    std::vector<float> source(bins);
+    for (std::size_t i = 0; i < bins; ++i) source[i] = static_cast<float>(deviation[i] - mean);
+    upload(source_, source, stream_);
+    const int nx = bins_x_, ny = bins_y_;
+    GemmTask f1{};
+    f1.a = source_; f1.b = basis_cx_t_; f1.c = stage_a_;
+    f1.m = ny; f1.n = nx; f1.k = nx; f1.lda = nx; f1.ldb = nx; f1.ldc = nx; f1.c_step = 1;
+    launchGemm(&f1, 1, stream_);
+    GemmTask f2{};
+    f2.a = basis_cy_; f2.b = stage_a_; f2.c = phi_hat_;
+    f2.m = ny; f2.n = nx; f2.k = ny; f2.lda = ny; f2.ldb = nx; f2.ldc = nx; f2.c_step = 1;
+    f2.scale = spectral_scale_; f2.weight_r = weight_y_; f2.weight_c = weight_x_; f2.energy_partials = partials_e_;
+    launchGemm(&f2, 1, stream_);
+    GemmTask inv1[2]{};
+    inv1[0].a = basis_dy_; inv1[0].b = phi_hat_; inv1[0].c = stage_t_;
+    inv1[0].m = ny; inv1[0].n = nx; inv1[0].k = ny; inv1[0].lda = ny; inv1[0].ldb = nx; inv1[0].ldc = nx; inv1[0].c_step = 1;
+    inv1[1].a = phi_hat_; inv1[1].b = basis_dx_t_; inv1[1].c = stage_u_;
+    inv1[1].m = ny; inv1[1].n = nx; inv1[1].k = nx; inv1[1].lda = nx; inv1[1].ldb = nx; inv1[1].ldc = nx; inv1[1].c_step = 1;
+    launchGemm(inv1, 2, stream_);
+    GemmTask inv2[2]{};
+    inv2[0].a = stage_t_; inv2[0].b = basis_sx_w_; inv2[0].c = reinterpret_cast<float*>(field_);
+    inv2[0].m = ny; inv2[0].n = nx; inv2[0].k = nx; inv2[0].lda = nx; inv2[0].ldb = nx; inv2[0].ldc = 2 * nx; inv2[0].c_step = 2;
+    inv2[1].a = basis_sy_w_; inv2[1].b = stage_u_; inv2[1].c = reinterpret_cast<float*>(field_) + 1;
+    inv2[1].m = ny; inv2[1].n = nx; inv2[1].k = ny; inv2[1].lda = ny; inv2[1].ldb = nx; inv2[1].ldc = 2 * nx; inv2[1].c_step = 2;
+    launchGemm(inv2, 2, stream_);
+    GemmTask pot{};
+    pot.a = stage_t_; pot.b = basis_dx_t_; pot.c = potential_;
+    pot.m = ny; pot.n = nx; pot.k = nx; pot.lda = nx; pot.ldb = nx; pot.ldc = nx; pot.c_step = 1;
+    launchGemm(&pot, 1, stream_);
+    launches_ += 5;
+    std::vector<float> p(bins);
+    std::vector<float2> f(bins);
+    checkCuda(cudaMemcpyAsync(p.data(), potential_, bins * sizeof(float), cudaMemcpyDeviceToHost, stream_), "field");
+    checkCuda(cudaMemcpyAsync(f.data(), field_, bins * sizeof(float2), cudaMemcpyDeviceToHost, stream_), "field");
+    checkCuda(cudaStreamSynchronize(stream_), "field solve");
+    for (std::size_t i = 0; i < bins; ++i) {
+        if (potential != nullptr) potential[i] = p[i];
+        if (field_x != nullptr) field_x[i] = f[i].x;
+        if (field_y != nullptr) field_y[i] = f[i].y;
+    }
+}
+
+void Engine::depositLayers(const double2* positions, int64_t* movable, int64_t* macro, int64_t* filler) {
+    // The metrics pass consumes (reads and clears) the layers, so the parity hook
+    // runs the scatter alone, copies the three layers out and clears them again.
+    ScatterArgs sa{};
+    sa.mode = kGiven;
+    sa.particle_count = static_cast<int>(particle_count_);
+    sa.positions = positions;
+    sa.size = size_;
+    sa.layer = layer_;
+    sa.llx = region_.llx;
+    sa.lly = region_.lly;
+    sa.urx = region_.urx;
+    sa.ury = region_.ury;
+    sa.bin_w = bin_w_;
+    sa.bin_h = bin_h_;
+    sa.bins_x = bins_x_;
+    sa.bins_y = bins_y_;
+    sa.layers = layers_;
+    sa.totals = totals_;
+    sa.partials = partials_sc_;
+    launchScatter(sa, particle_count_ > 0 ? scatter_blocks_ : 0, stream_);
+    launches_ += 1;
+    const std::size_t bins = static_cast<std::size_t>(bin_count_);
+    int64_t* out[3] = {movable, macro, filler};
+    for (int k = 0; k < 3; ++k) {
+        if (out[k] == nullptr) continue;
+        checkCuda(cudaMemcpyAsync(out[k], layers_ + k * bins, bins * sizeof(int64_t), cudaMemcpyDeviceToHost, stream_),
+                  "Download density layers");
+    }
+    checkCuda(cudaMemsetAsync(layers_, 0, 3 * bins * sizeof(unsigned long long), stream_), "clear layers");
+    checkCuda(cudaMemsetAsync(totals_, 0, 4 * sizeof(unsigned long long), stream_), "clear totals");
+    checkCuda(cudaStreamSynchronize(stream_), "density layers");
+}
+
+}  // namespace mpgp

@@ -1,0 +1,177 @@
+// The device engine: resident state of one placement problem and one evaluation
+// of the adaptive objective (wirelength, density, field, gradient) per call.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstdint>
+#include <vector>
+
+#include "kernels.cuh"
+#include "setup.hpp"
+
+namespace mpgp {
+
+// Explicit device allocations are counted against a budget before they are made
+// (DeviceMemoryBudget, CudaPlacementBackend.cu:60-79).
+class DeviceArena {
+public:
+    explicit DeviceArena(uint64_t limit) : limit_(limit) {}
+    ~DeviceArena();
+    DeviceArena(const DeviceArena&) = delete;
+    DeviceArena& operator=(const DeviceArena&) = delete;
+
+    void* allocate(std::size_t bytes, const char* what);
+    template <typename T>
+    T* array(std::size_t count, const char* what) {
+        return static_cast<T*>(allocate(count * sizeof(T), what));
+    }
+    [[nodiscard]] uint64_t reserved() const { return reserved_; }
+
+private:
+    uint64_t limit_;
+    uint64_t reserved_ = 0;
+    std::vector<void*> blocks_;
+};
+
+struct EvalRequest {
+    int mode = kGiven;
+    const double2* positions = nullptr;  // kGiven
+    const double2* base = nullptr;       // kPropose / kLookahead
+    const double2* direction = nullptr;
+    const double2* raw_direction = nullptr;
+    double2* out_positions = nullptr;
+    double step = 0.0;
+    double max_displacement = 0.0;
+    double smoothing = 1.0;
+    bool gradient = false;
+    // combined gradient outputs (controller)
+    double penalty = 0.0;
+    double precond_scale = 1.0;
+    double2* raw = nullptr;
+    double2* pre = nullptr;
+    // split outputs (drop-in backend)
+    double2* wire_out = nullptr;
+    double2* density_out = nullptr;
+    const double2* prev_positions = nullptr;
+    const double2* prev_gradient = nullptr;
+    const double2* velocity = nullptr;
+    bool want_potential = false;
+};
+
+struct EvalScalars {
+    double v[kScalarCount];
+};
+
+class Engine {
+public:
+    Engine(const Problem& problem, int device, uint64_t budget_bytes);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    // Launches one evaluation on the engine stream; the scalars are valid after sync().
+    void launch(const EvalRequest& request);
+    // Waits for the stream and returns the scalars of the last launched evaluation.
+    const EvalScalars& sync();
+    const EvalScalars& evaluate(const EvalRequest& request) {
+        launch(request);
+        return sync();
+    }
+    // Evaluation results in the reference's structures.
+    void densityMetrics(const EvalScalars& s, bool with_fillers, mpgp_density_metrics& out) const;
+    [[nodiscard]] double energy(const EvalScalars& s) const;
+
+    // Solves the field of an arbitrary FP64 deviation map (parity hook).
+    void fieldSolve(const double* deviation, double* potential, double* field_x, double* field_y);
+    // Runs the fixed-point scatter alone at `positions` and copies the three layers out (parity hook).
+    void depositLayers(const double2* positions, int64_t* movable, int64_t* macro, int64_t* filler);
+    [[nodiscard]] double2* scratchPositions() const { return scratch_positions_; }
+
+    [[nodiscard]] double2* newParticleArray(const char* what);
+    [[nodiscard]] cudaStream_t stream() const { return stream_; }
+    [[nodiscard]] int device() const { return device_; }
+    [[nodiscard]] uint64_t reservedBytes() const { return arena_.reserved(); }
+    [[nodiscard]] int64_t particleCount() const { return particle_count_; }
+    [[nodiscard]] int64_t movableCount() const { return movable_count_; }
+    [[nodiscard]] int64_t launches() const { return launches_; }
+    [[nodiscard]] const double* precondBase() const { return precond_; }
+    void countLaunches(int64_t n) { launches_ += n; }
+
+private:
+    void uploadStatic(const Problem& problem);
+    void buildNetLayout(const Problem& problem);
+    void buildBasis();
+
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    DeviceArena arena_;
+    int64_t launches_ = 0;
+
+    int64_t particle_count_ = 0;
+    int64_t movable_count_ = 0;
+    int bins_x_ = 0, bins_y_ = 0;
+    int bin_count_ = 0;
+    Rect2 region_;
+    double bin_w_ = 0.0, bin_h_ = 0.0, bin_area_ = 0.0;
+    double target_density_ = 0.0;
+    double static_fixed_sum_ = 0.0, static_dark_sum_ = 0.0, static_placeable_sum_ = 0.0;
+
+    // particles
+    double2* size_ = nullptr;
+    unsigned char* layer_ = nullptr;
+    double* charge_ = nullptr;
+    double* precond_ = nullptr;
+    double2* scratch_positions_ = nullptr;  // kGiven uploads for the drop-in path
+
+    // netlist
+    int* pin_particle_ = nullptr;
+    float2* pin_offset_ = nullptr;
+    double2* static_pins_ = nullptr;
+    int* net_start_ = nullptr;
+    float* net_weight_ = nullptr;
+    int4* block_work_ = nullptr;
+    int wl_blocks_ = 0;
+    float2* pin_gradient_ = nullptr;
+    int* particle_pin_start_ = nullptr;
+    int* particle_pins_ = nullptr;
+
+    // density
+    unsigned long long* layers_ = nullptr;
+    unsigned long long* totals_ = nullptr;
+    double* fixed_ = nullptr;
+    double* dark_ = nullptr;
+    float* source_ = nullptr;
+
+    // DCT
+    float* basis_cx_t_ = nullptr;  // nx x nx: 2 cos(pi k (2c+1) / 2nx), [c][k]
+    float* basis_cy_ = nullptr;    // ny x ny: [l][r]
+    float* basis_dy_ = nullptr;    // ny x ny: [r][l], l = 0 -> 1
+    float* basis_dx_t_ = nullptr;  // nx x nx: [k][c], k = 0 -> 1
+    float* basis_sx_w_ = nullptr;  // nx x nx: [k][c] = kx 2 sin(...)
+    float* basis_sy_w_ = nullptr;  // ny x ny: [r][l] = ky 2 sin(...)
+    float* spectral_scale_ = nullptr;  // ny x nx
+    float* weight_y_ = nullptr;
+    float* weight_x_ = nullptr;
+    float* stage_a_ = nullptr;
+    float* phi_hat_ = nullptr;
+    float* stage_t_ = nullptr;
+    float* stage_u_ = nullptr;
+    float2* field_ = nullptr;
+    float* potential_ = nullptr;
+
+    // partials and scalars
+    int scatter_blocks_ = 0, metrics_blocks_ = 0, gather_blocks_ = 0, energy_blocks_ = 0;
+    double* partials_wl_ = nullptr;
+    double* partials_sc_ = nullptr;
+    double* partials_m_ = nullptr;
+    double* partials_e_ = nullptr;
+    double* partials_g_ = nullptr;
+    double* scalars_ = nullptr;
+    EvalScalars* host_scalars_ = nullptr;
+    bool last_gradient_ = false;
+    bool last_propose_ = false;
+};
+
+}  // namespace mpgp

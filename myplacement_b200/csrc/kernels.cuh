@@ -1,0 +1,157 @@
+// Kernel argument blocks and launchers of the placement engine.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace mpgp {
+
+// ---- scalar slots of one evaluation (FP64, reduced on the device) ------------------------
+enum Scalar : int {
+    kSmooth = 0,      // sum of weighted LSE net lengths
+    kHpwl,            // sum of weighted net HPWL
+    kPredicted,       // proposal: sum raw_grad . (base - candidate)
+    kMaxDisplacement, // proposal: max |base - candidate|
+    kOverflowWith,    // density metrics with fillers / without fillers
+    kOverflowWithout,
+    kChargeWith,
+    kChargeWithout,
+    kNormalization,
+    kDensitySumWith,
+    kDensitySumWithout,
+    kDensityMaxWith,
+    kDensityMaxWithout,
+    kEnergy,          // sum phi_hat * rho_hat * w_l * w_k (times bin_area / 2 gives the energy)
+    kWireL1,
+    kDensityL1,
+    kRawNorm2,
+    kPreNorm2,
+    kDeltaPos2,       // sum |x - x_prev|^2
+    kDeltaGrad2,      // sum |g - g_prev|^2 (preconditioned)
+    kAlignment,       // sum velocity . g (preconditioned)
+    kScalarCount
+};
+
+// ---- wirelength (net-parallel LSE) ---------------------------------------------------
+struct WirelengthArgs {
+    const double2* positions;     // P particle centres
+    const int* pin_particle;      // I' pins in bucket order; < 0: static pin -(s+1)
+    const float2* pin_offset;     // I' transformed offsets (movable pins)
+    const double2* static_pins;   // S absolute static pin positions
+    const int* net_start;         // N'+1 (nets with >= 2 pins, bucket order)
+    const float* net_weight;      // N'
+    const int4* block_work;       // per block: {group size (0 = warp loop), first net, net count, 0}
+    float gamma;
+    float inv_gamma;
+    float2* pin_gradient;         // I' (written when gradient != 0, movable pins only)
+    int gradient;
+    double* partials;             // per block: smooth, hpwl
+};
+void launchWirelength(const WirelengthArgs& args, int blocks, cudaStream_t stream);
+
+// ---- density scatter (fixed point) ------------------------------------------------
+enum PositionMode : int { kGiven = 0, kPropose = 1, kLookahead = 2 };
+
+struct ScatterArgs {
+    int mode;
+    int particle_count;
+    const double2* positions;   // kGiven: positions to deposit
+    const double2* base;        // kPropose / kLookahead: base positions
+    const double2* direction;   // kPropose: preconditioned gradient; kLookahead: velocity
+    const double2* raw;         // kPropose: raw gradient (predicted reduction)
+    double step;                // kPropose: step size; kLookahead: momentum
+    double max_displacement;    // kPropose
+    double2* out_positions;     // kPropose / kLookahead: the clamped candidate
+    const double2* size;        // P (width, height)
+    const unsigned char* layer; // P
+    double llx, lly, urx, ury;  // region
+    double bin_w, bin_h;
+    int bins_x, bins_y;
+    unsigned long long* layers; // 3 * B fixed-point accumulators (movable, macro, filler)
+    unsigned long long* totals; // 3 exact layer totals
+    double* partials;           // per block: predicted, max displacement
+};
+void launchScatter(const ScatterArgs& args, int blocks, cudaStream_t stream);
+
+// ---- density metrics + DCT source --------------------------------------------------
+struct MetricsArgs {
+    unsigned long long* layers;        // 3 * B, read and reset to zero
+    const unsigned long long* totals;  // 3
+    const double* fixed;               // B
+    const double* dark;                // B
+    double static_fixed_sum;
+    double static_dark_sum;
+    double target_density;
+    double bin_area;
+    int bin_count;
+    float* source;                     // B: deviation - mean (FP32 DCT input)
+    double* partials;                  // per block: 9 metric partials
+};
+void launchMetrics(const MetricsArgs& args, int blocks, cudaStream_t stream);
+
+// ---- dense FP32 contractions for the DCT (SIMT path) ----------------------------------
+struct GemmTask {
+    const float* a;    // M x K row-major (lda)
+    const float* b;    // K x N row-major (ldb)
+    float* c;          // output
+    int m, n, k;
+    int lda, ldb;
+    int ldc;           // row stride of c (elements)
+    int c_step;        // column stride of c (1 plain, 2 interleaved)
+    const float* scale;   // spectral epilogue: c = acc * scale[r*n + c] (nullptr = plain)
+    const float* weight_r;  // energy weights per row / column (spectral epilogue)
+    const float* weight_c;
+    double* energy_partials;  // per block energy partial (spectral epilogue)
+};
+void launchGemm(const GemmTask* tasks, int task_count, cudaStream_t stream);
+int gemmBlocks(const GemmTask& task);
+
+// ---- field gather + gradient combine (the fused update pass) ----------------------------
+struct GatherArgs {
+    int particle_count;
+    int movable_count;
+    const double2* positions;
+    const int* particle_pin_start;  // M+1
+    const int* particle_pins;       // pin indices (bucket order)
+    const float2* pin_gradient;
+    const float2* field;            // B interleaved (Ex, Ey)
+    const double* charge;           // P
+    const double* precond_base;     // P (nullptr: split mode)
+    double llx, lly, urx, ury, bin_w, bin_h;
+    int bins_x, bins_y;
+    double penalty;
+    double precond_scale;           // 1 / density_strength
+    double2* raw;                   // combined mode outputs
+    double2* pre;
+    double2* wire_out;              // split mode outputs (drop-in backend)
+    double2* density_out;
+    const double2* prev_positions;  // optional (step estimate)
+    const double2* prev_gradient;
+    const double2* velocity;        // optional (momentum alignment)
+    double* partials;               // per block: 7 partials (kWireL1 .. kAlignment)
+};
+void launchGather(const GatherArgs& args, int blocks, cudaStream_t stream);
+
+// ---- small vector kernels ---------------------------------------------------------
+void launchVelocity(const double2* next, const double2* previous, double2* velocity, int count,
+                    cudaStream_t stream);
+
+// ---- deterministic reduction of all partials into the scalar block ----------------------
+struct ReduceSource {
+    const double* partials;
+    int rows;    // number of blocks that wrote partials
+    int stride;  // doubles per block
+    int column;  // which partial
+    int is_max;
+    int target;  // Scalar slot
+};
+struct ReduceArgs {
+    ReduceSource sources[kScalarCount];
+    int source_count;
+    double* scalars;             // kScalarCount
+    unsigned long long* totals;  // reset to zero after use (may be null)
+};
+void launchReduce(const ReduceArgs& args, cudaStream_t stream);
+
+}  // namespace mpgp

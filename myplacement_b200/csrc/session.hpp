@@ -1,0 +1,117 @@
+// Device-resident adaptive global placement (one design, one GPU).
+#pragma once
+
+#include <chrono>
+#include <memory>
+#include <vector>
+
+#include "engine.cuh"
+#include "setup.hpp"
+
+namespace mpgp {
+
+struct ObjectiveMetrics {
+    double hpwl = 0.0;
+    double smooth_wirelength = 0.0;
+    double density_energy = 0.0;
+    double objective = 0.0;
+    mpgp_density_metrics optimizer{};
+    mpgp_density_metrics design{};
+};
+
+// Host view of one evaluation; the vectors stay on the device.
+struct StateEval {
+    ObjectiveMetrics m;
+    double raw_norm = 0.0;
+    double pre_norm = 0.0;
+    double wire_l1 = 0.0;
+    double density_l1 = 0.0;
+    double delta_pos2 = 0.0;
+    double delta_grad2 = 0.0;
+    double alignment = 0.0;  // sum v . pre
+    double predicted = 0.0;
+    double max_displacement = 0.0;
+    double2* raw = nullptr;
+    double2* pre = nullptr;
+};
+
+struct CheckpointState {
+    double2* positions = nullptr;
+    int iteration = 0;
+    double hpwl = 0.0;
+    double overflow = 0.0;
+    double selection_score = 0.0;
+    bool found = false;
+};
+
+class Session {
+public:
+    Session(const mpgp_design& design, const mpgp_options& options);
+    // Runs up to `iterations` controller iterations; returns true once the run is done.
+    bool step(int iterations, int* completed);
+    void finish(double* module_x, double* module_y, mpgp_result* result, mpgp_history_row* history, int capacity);
+    [[nodiscard]] int64_t launches() const { return engine_ ? engine_->launches() : 0; }
+    [[nodiscard]] void* stream() const { return engine_ ? engine_->stream() : nullptr; }
+    [[nodiscard]] bool done() const { return done_; }
+    [[nodiscard]] const Problem& problem() const { return problem_; }
+    [[nodiscard]] const std::vector<Filler>& fillers() const { return fillers_; }
+    [[nodiscard]] const DerivedDesign& derived() const { return derived_; }
+    void currentPositions(double* xy) const;
+
+private:
+    StateEval evaluateGiven(double2* positions, bool gradient, double penalty, double2* raw, double2* pre,
+                            bool with_prev, bool with_velocity);
+    StateEval evaluateLookahead(double momentum, double penalty, double2* raw, double2* pre);
+    StateEval evaluateProposal(const double2* base, const StateEval& base_eval, double step, double max_disp,
+                               double penalty);
+    void fillMetrics(const EvalScalars& s, double penalty, StateEval& out) const;
+    void considerCheckpoint(double2* positions, const ObjectiveMetrics& metrics, int iteration, bool& is_new_best);
+    double smoothingFromOverflow(double overflow) const;
+    void iterate();
+
+    mpgp_options options_{};
+    std::vector<double> module_x_, module_y_;
+    std::vector<double> module_w_, module_h_;
+    DerivedDesign derived_;
+    std::vector<Filler> fillers_;
+    Problem problem_;
+    std::unique_ptr<Engine> engine_;
+    std::chrono::steady_clock::time_point started_;
+    bool empty_ = false;
+    bool done_ = false;
+
+    double min_bin_ = 0.0, max_bin_ = 0.0;
+    double density_strength_base_ = 1.0;
+
+    // device vectors
+    double2* cur_ = nullptr;
+    double2* look_ = nullptr;
+    double2* cand_ = nullptr;
+    double2* prev_pos_ = nullptr;
+    double2* velocity_ = nullptr;
+    double2* raw_cur_ = nullptr;
+    double2* pre_cur_ = nullptr;
+    double2* raw_look_ = nullptr;
+    double2* pre_look_ = nullptr;
+    double2* prev_grad_ = nullptr;
+    CheckpointState best_feasible_, best_fallback_;
+
+    // controller state (runAdaptiveGlobalPlacement locals, AdaptiveGlobalPlacer.cpp:656-733)
+    mpgp_result result_{};
+    std::vector<mpgp_history_row> history_;
+    double smoothing_ = 0.0;
+    double initial_overflow_ = 0.0;
+    double penalty_ = 1.0;
+    double reference_penalty_ = 1.0;
+    double last_optimizer_overflow_ = 0.0;
+    double last_step_size_ = 0.0;
+    bool has_previous_gradient_ = false;
+    int momentum_age_ = 0;
+    int objective_worse_streak_ = 0;
+    int feasible_refinement_iterations_ = 0;
+    int iteration_ = 0;
+    StateEval initial_;
+    bool velocity_zero_ = true;
+};
+
+}  // namespace mpgp
