@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""GP iterations/s of the adaptive + neumann + course_eplace_v1 global placer on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
+
+Workload: the mid design -- 210k movable cells, 400 fixed macros, 1,200 boundary
+terminals, 220k nets (~850k pins), rows sized for 70 % utilisation, target
+density 0.9, 512 x 512 bins -- seeded synthetic data with the design law of the
+benchmark, random initial placement from seed 2026.  A step is one adaptive
+controller iteration (1-16 objective evaluations).  The early stop is off, so
+exactly W + K iterations run.  The L2 cache (126 MB; the working set is ~100 MB)
+is flushed by a 256 MiB device write between timed steps, outside the timing.
+
+Output: one JSON line on rank 0.  `value` is device-timed iterations/s with the
+design resident on the device; `e2e` is the same metric through the public API
+with host buffers (GlobalPlacer.run: host setup, upload, the run with its early
+stop, download).  `--impl reference` times the reference's own CPU path (and,
+beside it, the reference CUDA backend rebuilt for sm_100a) on the same workload.
+With N > 1 each rank runs an independent replica on its own GPU (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "GP iterations/s at 210k cells vs plain GPU form; p50/p99 solve latency @≤0.10 ovfl"
+WORKLOAD = "mid_210k"
+PEAKS_FILE = REPO / "MEASURED_PEAKS.json"
+PROFILE_TRAFFIC = REPO / "profiles" / "traffic_mid_210k.md"
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["mine", "reference"], default="mine")
+    p.add_argument("--seed", type=int, default=2026)
+    p.add_argument("--workload", default=WORKLOAD)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def load_peaks() -> tuple[dict, str]:
+    if PEAKS_FILE.is_file():
+        try:
+            return json.loads(PEAKS_FILE.read_text()), "measured"
+        except json.JSONDecodeError:
+            pass
+    return dict(FALLBACK_PEAKS), "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"mpgp_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self) -> dict:
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        clocks, max_clock, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                clocks.append(float(parts[1]))
+                max_clock = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        self.path.unlink(missing_ok=True)
+        return {"sm_mhz": statistics.median(clocks) if clocks else None, "sm_max_mhz": max_clock,
+                "reasons": sorted(reasons), "samples": len(clocks)}
+
+
+def algorithmic_units(design, particles: int, bins_x: int, bins_y: int) -> dict:
+    """Per-launch algorithmic bytes (HBM-bound families) or FLOPs (DCT) of each kernel family.
+
+    Bytes per unit follow the per-unit figures of the design notes: wirelength
+    20 B/pin + 8 B/net + 8 B/particle; scatter 20 B/particle + 24 B/bin; metrics
+    36 B/bin; gather + update 80 B/particle.  A DCT launch is one (forward) or
+    two (inverse) M x N x K contractions at 2 flops per multiply-add.
+    """
+    pins, nets, bins = design.pin_count, design.net_count, bins_x * bins_y
+    m, n = bins_y, bins_x
+    return {
+        "wirelength": ("hbm", 20 * pins + 8 * nets + 8 * particles),
+        "scatter": ("hbm", 20 * particles + 24 * bins),
+        "metrics": ("hbm", 36 * bins),
+        "gather": ("hbm", 80 * particles),
+        "dct_forward": ("tensor", 2.0 * m * n * (n + m) / 2.0),
+        "dct_inverse": ("tensor", 2 * 2.0 * m * n * (n + m) / 2.0),
+        "reduce": ("hbm", 8 * 64),
+        "vector": ("hbm", 48 * particles),
+    }
+
+
+def read_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if present."""
+    if not PROFILE_TRAFFIC.is_file():
+        return None
+    for line in PROFILE_TRAFFIC.read_text().splitlines():
+        m = re.match(rf"\|\s*{re.escape(kernel)}\s*\|\s*([0-9.eE+]+)\s*\|", line)
+        if m:
+            return float(m.group(1))
+    return None
+
+
+def flush_l2(buffer, stream_ptr):
+    import torch
+
+    with torch.cuda.stream(torch.cuda.ExternalStream(stream_ptr)):
+        buffer.add_(1)
+
+
+def reference_cpu_sample(design, bins: int, warmup: int, steps: int, variant: str = "cpu", device: int = 0):
+    """Per-iteration time of the reference path: (T(warmup + steps) - T(warmup)) / steps,
+    each T being the reference's own GlobalPlacementResult.elapsed_seconds."""
+    from oracle.ref import ReferenceLibrary, default_options
+
+    ref = ReferenceLibrary(variant)
+    common = dict(bins_x=bins, bins_y=bins, target_density=0.9, feasible_refinement_iterations=10 ** 9,
+                  compute_backend=0 if variant == "cpu" else 1, cuda_device=device)
+    if variant != "cpu":
+        # The first CUDA run pays for context creation; keep it out of both samples.
+        ref.global_place(design, default_options(iterations=1, **common))
+    _, _, short, _ = ref.global_place(design, default_options(iterations=max(1, warmup), **common))
+    _, _, long, _ = ref.global_place(design, default_options(iterations=max(1, warmup) + steps, **common))
+    seconds = max(long.elapsed_seconds - short.elapsed_seconds, 1e-9)
+    return {"iterations": steps, "seconds": seconds, "value": steps / seconds,
+            "setup_and_warmup_seconds": short.elapsed_seconds,
+            "completed": long.completed_iterations, "hpwl_after": long.hpwl_after}
+
+
+def make_workload(name: str, seed: int):
+    import myplacement_b200 as mp
+
+    design, bins = mp.workload(name)
+    x, y = mp.random_placement(design, seed)
+    return design.copy_with_positions(x, y), bins
+
+
+def run_mine(args) -> None:
+    import torch
+
+    import myplacement_b200 as mp
+    from myplacement_b200 import replicas
+
+    rank, world, local = replicas.world()
+    torch.cuda.set_device(local)
+    replicas.init()
+    design, bins = make_workload(args.workload, replicas.replica_seed(args.seed, rank))
+    iterations = args.warmup + args.steps
+    options = mp.default_options(bins_x=bins, bins_y=bins, target_density=0.9, cuda_device=local,
+                                 iterations=max(280, iterations), feasible_refinement_iterations=10 ** 9)
+    session = mp.Session(design, options)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    stream_ptr = session.stream
+    for _ in range(args.warmup):
+        session.step(1)
+    torch.cuda.synchronize()
+    session.set_profiling(True)
+    launches_before = session.kernel_launches
+    step_ms = []
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    ext = torch.cuda.ExternalStream(stream_ptr)
+    replicas.barrier()
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush_l2(flush, stream_ptr)
+            start.record(ext)
+            session.step(1)
+            end.record(ext)
+            end.synchronize()
+            step_ms.append(start.elapsed_time(end))
+    torch.cuda.synchronize()
+    replicas.barrier()
+    wall = time.perf_counter() - wall0
+    launches = session.kernel_launches - launches_before
+    stats = session.kernel_stats()
+    session.set_profiling(False)
+    total_ms = float(sum(step_ms))
+    max_ms = replicas.reduce_max(total_ms)
+    total_steps = replicas.reduce_sum(args.steps)
+    value = total_steps / (max_ms / 1e3)
+    clock_info = clocks.summary()
+    result = session.finish()
+    session.close()
+    del flush
+
+    particles = int(mp.host_setup(design, options)["particle_count"]) if rank == 0 else 0
+    roofline = None
+    if rank == 0:
+        peaks, peak_kind = load_peaks()
+        units = algorithmic_units(design, particles, bins, bins)
+        family = max((k for k in stats if stats[k][0] > 0), key=lambda k: stats[k][1])
+        launches_f, ms_f = stats[family]
+        bound, amount = units[family]
+        per_launch_s = ms_f / launches_f / 1e3
+        if bound == "hbm":
+            achieved = amount / per_launch_s / 1e9
+            peak = peaks.get("hbm_gbs", FALLBACK_PEAKS["hbm_gbs"])
+            unit = "GB/s"
+        else:
+            achieved = amount / per_launch_s / 1e12
+            peak = peaks.get("bf16_tflops_sustained", FALLBACK_PEAKS["bf16_tflops_sustained"])
+            unit = "TFLOP/s"
+        roofline = {"kernel": family, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+                    "frac": achieved / peak, "traffic": read_traffic(family), "peak_source": peak_kind,
+                    "launches": launches_f, "avg_launch_us": per_launch_s * 1e6,
+                    "algorithmic_per_launch": amount,
+                    "kernel_share": {k: round(v[1] / max(sum(s[1] for s in stats.values()), 1e-12), 4)
+                                     for k, v in stats.items() if v[0] > 0},
+                    "kernel_ms": {k: round(v[1], 3) for k, v in stats.items() if v[0] > 0},
+                    "kernel_launches": {k: v[0] for k, v in stats.items() if v[0] > 0}}
+
+    e2e = None
+    if not args.no_e2e:
+        e2e_options = mp.default_options(bins_x=bins, bins_y=bins, target_density=0.9, cuda_device=local)
+        replicas.barrier()
+        t0 = time.perf_counter()
+        s2 = mp.Session(design, e2e_options)
+        while not s2.step(64)[1]:
+            pass
+        placed = s2.finish()
+        t1 = time.perf_counter()
+        h2d, d2h = s2.transfer_bytes()
+        s2.close()
+        it = placed.completed_iterations
+        e2e_time = replicas.reduce_max(t1 - t0)
+        e2e_iters = replicas.reduce_sum(it)
+        e2e = {"value": e2e_iters / e2e_time, "unit": "iterations/s",
+               "h2d_bytes_per_step": int(h2d / max(it, 1)), "d2h_bytes_per_step": int(d2h / max(it, 1)),
+               "api": "Session create/step/finish (= GlobalPlacer.run) on host arrays, early stop on",
+               "completed_iterations": it, "seconds": t1 - t0, "hpwl_after": placed.hpwl_after,
+               "overflow_after": placed.overflow_after}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            sample = reference_cpu_sample(design, bins, warmup=1, steps=3)
+            cpu = {"value": sample["value"], "unit": "iterations/s", "cores": 1, "kind": "reference",
+                   "sample": f"reference CPU path (oracle/_ref/libref_cpu.so, single thread as in the reference) "
+                             f"on this workload: iterations 2-4, (T(4) - T(1)) / 3 = {sample['seconds']:.2f} s"}
+        except Exception as error:  # the oracle library is absent
+            cpu = {"value": None, "unit": "iterations/s", "cores": 1, "kind": "reference",
+                   "sample": f"unavailable: {error}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "iterations/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {design.module_count - 1600} cells, 400 fixed macros, "
+                                   f"1200 terminals, {design.net_count} nets, {design.pin_count} pins, "
+                                   f"{bins}x{bins} bins, target density 0.9",
+                       "particles": particles, "step": "one adaptive controller iteration",
+                       "early_stop": "off in the timed run (fixed iteration count)",
+                       "l2": "flushed between timed steps (256 MiB device write, outside the timing)",
+                       "arithmetic": "f32 kernels, int64 fixed-point density, f64 reductions and controller",
+                       "parallelism": f"replicas x{world}", "seed": args.seed,
+                       "wall_seconds_timed_region": wall},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clock_info,
+            "quality": {"hpwl_after": result.hpwl_after, "overflow_after": result.overflow_after,
+                        "iterations": result.completed_iterations},
+        }
+        print(json.dumps(line), flush=True)
+    replicas.shutdown()
+
+
+def run_reference(args) -> None:
+    from myplacement_b200 import replicas
+
+    rank, world, local = replicas.world()
+    if rank != 0:
+        return  # the reference CPU path runs on rank 0 only
+    design, bins = make_workload(args.workload, args.seed)
+    try:
+        cpu = reference_cpu_sample(design, bins, warmup=args.warmup, steps=args.steps)
+    except Exception as error:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU path failed: {error}"}))
+        return
+    cuda = None
+    try:
+        sample = reference_cpu_sample(design, bins, warmup=args.warmup, steps=args.steps, variant="cuda",
+                                      device=local)
+        cuda = {"value": sample["value"], "unit": "iterations/s",
+                "what": "the reference CUDA backend (src/placement/cuda/CudaPlacementBackend.cu) rebuilt for "
+                        "sm_100a, driven by the reference controller, same workload and step definition",
+                "seconds": sample["seconds"], "iterations": sample["iterations"]}
+    except Exception as error:
+        cuda = {"value": None, "unavailable": str(error)}
+    value = cpu["value"]
+    line = {
+        "metric": METRIC, "value": value, "unit": "iterations/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"{args.workload}: {bins}x{bins} bins, target density 0.9",
+                   "step": "one adaptive controller iteration", "early_stop": "off (fixed iteration count)",
+                   "timing": "(T(W + K) - T(W)) / K from the reference's own elapsed_seconds"},
+        "cpu_baseline": {"value": value, "unit": "iterations/s", "cores": 1, "kind": "reference",
+                         "sample": f"reference CPU path, iterations {args.warmup + 1}-{args.warmup + args.steps}"},
+        "e2e": {"value": value, "unit": "iterations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_cuda_backend": cuda,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> int:
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_mine(args)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -337,6 +337,17 @@ int mpgp_session_finish(mpgp_session* session, double* module_x, double* module_
                         mpgp_history_row* history, int32_t history_capacity);
 /* Current particle positions (particle_count (x, y) pairs). */
 int mpgp_session_positions(const mpgp_session* session, double* positions);
+/* Tracing (no counterpart in the reference, which times only the whole run,
+ * AdaptiveGlobalPlacer.cpp:656, 951): with profiling on, every kernel launch of
+ * the session is bracketed by CUDA events on its stream and its device time is
+ * accumulated per kernel family.  Families are numbered 0..mpgp_kernel_kind_count()-1. */
+int mpgp_kernel_kind_count(void);
+const char* mpgp_kernel_kind_name(int kind);
+int mpgp_session_set_profiling(mpgp_session* session, int enabled);
+int mpgp_session_kernel_stats(const mpgp_session* session, int64_t* launches, double* milliseconds,
+                              int32_t capacity);
+/* Host<->device bytes the session has copied (setup, positions, scalar read-backs). */
+int mpgp_session_transfer_bytes(const mpgp_session* session, uint64_t* to_device, uint64_t* to_host);
 /* Number of engine kernel launches issued by this session so far. */
 int64_t mpgp_session_kernel_launches(const mpgp_session* session);
 /* The CUDA stream the session's work runs on (a cudaStream_t). */

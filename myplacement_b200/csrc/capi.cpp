@@ -288,6 +288,37 @@ int mpgp_session_positions(const mpgp_session* s, double* positions) {
     });
 }
 
+int mpgp_kernel_kind_count(void) { return mpgp::kKindCount; }
+
+const char* mpgp_kernel_kind_name(int kind) { return mpgp::kernelKindName(kind); }
+
+int mpgp_session_set_profiling(mpgp_session* s, int enabled) {
+    return guarded([&] {
+        mpgp::require(s != nullptr, "A session is required.");
+        if (s->session->engine() != nullptr) s->session->engine()->setTiming(enabled != 0);
+    });
+}
+
+int mpgp_session_kernel_stats(const mpgp_session* s, int64_t* launches, double* milliseconds, int32_t capacity) {
+    return guarded([&] {
+        mpgp::require(s != nullptr, "A session is required.");
+        const mpgp::Engine* engine = s->session->engine();
+        for (int k = 0; k < std::min<int>(capacity, mpgp::kKindCount); ++k) {
+            if (launches != nullptr) launches[k] = engine != nullptr ? engine->kernelStats().launches[k] : 0;
+            if (milliseconds != nullptr) milliseconds[k] = engine != nullptr ? engine->kernelStats().milliseconds[k] : 0.0;
+        }
+    });
+}
+
+int mpgp_session_transfer_bytes(const mpgp_session* s, uint64_t* to_device, uint64_t* to_host) {
+    return guarded([&] {
+        mpgp::require(s != nullptr, "A session is required.");
+        const mpgp::Engine* engine = s->session->engine();
+        if (to_device != nullptr) *to_device = engine != nullptr ? engine->bytesToDevice() : 0;
+        if (to_host != nullptr) *to_host = engine != nullptr ? engine->bytesToHost() : 0;
+    });
+}
+
 int64_t mpgp_session_kernel_launches(const mpgp_session* s) { return s != nullptr ? s->session->launches() : 0; }
 
 void* mpgp_session_stream(const mpgp_session* s) { return s != nullptr ? s->session->stream() : nullptr; }

@@ -40,9 +40,13 @@ void* DeviceArena::allocate(std::size_t bytes, const char* what) {
 
 namespace {
 
+// Bytes copied host -> device by upload() on this thread (the engine's setup traffic).
+thread_local uint64_t g_uploaded_bytes = 0;
+
 template <typename T>
 void upload(T* device, const std::vector<T>& host, cudaStream_t stream) {
     if (!host.empty()) {
+        g_uploaded_bytes += host.size() * sizeof(T);
         checkCuda(cudaMemcpyAsync(device, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice, stream),
                   "upload");
     }
@@ -73,9 +77,11 @@ Engine::Engine(const Problem& p, int device, uint64_t budget_bytes) : device_(de
     bin_w_ = region_.width() / static_cast<double>(bins_x_);
     bin_h_ = region_.height() / static_cast<double>(bins_y_);
     bin_area_ = (std::max(0.0, region_.width()) * std::max(0.0, region_.height())) / static_cast<double>(bin_count_);
+    const uint64_t uploaded_before = g_uploaded_bytes;
     uploadStatic(p);
     buildNetLayout(p);
     buildBasis();
+    h2d_bytes_ += g_uploaded_bytes - uploaded_before;
     checkCuda(cudaMallocHost(reinterpret_cast<void**>(&host_scalars_), sizeof(EvalScalars)), "pinned scalars");
     std::memset(host_scalars_, 0, sizeof(EvalScalars));
     checkCuda(cudaStreamSynchronize(stream_), "Engine setup");
@@ -297,6 +303,95 @@ void Engine::buildBasis() {
     checkCuda(cudaStreamSynchronize(stream_), "basis upload");
 }
 
+const char* kernelKindName(int kind) {
+    static const char* names[kKindCount] = {"scatter", "wirelength", "metrics", "dct_forward",
+                                            "dct_inverse", "gather", "reduce", "vector"};
+    return kind >= 0 && kind < kKindCount ? names[kind] : "unknown";
+}
+
+void Engine::setTiming(bool enabled) {
+    if (enabled && events_.empty()) {
+        events_.resize(64);
+        for (cudaEvent_t& e : events_) checkCuda(cudaEventCreate(&e), "Create profiling event");
+        pending_kind_.resize(32);
+    }
+    timing_ = enabled;
+}
+
+void Engine::beginKernel(int kind) {
+    if (!timing_) return;
+    if (pending_ >= static_cast<int>(pending_kind_.size())) collectTimings();
+    pending_kind_[pending_] = kind;
+    checkCuda(cudaEventRecord(events_[2 * pending_], stream_), "Record profiling event");
+}
+
+void Engine::endKernel() {
+    if (!timing_) return;
+    checkCuda(cudaEventRecord(events_[2 * pending_ + 1], stream_), "Record profiling event");
+    ++pending_;
+}
+
+void Engine::collectTimings() {
+    if (pending_ == 0) return;
+    checkCuda(cudaEventSynchronize(events_[2 * pending_ - 1]), "Profiling sync");
+    for (int i = 0; i < pending_; ++i) {
+        float ms = 0.0f;
+        checkCuda(cudaEventElapsedTime(&ms, events_[2 * i], events_[2 * i + 1]), "Profiling elapsed");
+        stats_.launches[pending_kind_[i]] += 1;
+        stats_.milliseconds[pending_kind_[i]] += static_cast<double>(ms);
+    }
+    pending_ = 0;
+}
+
+// The Neumann field as dense contractions (ElectrostaticField.cpp:205-237):
+//   X = S * Cx^T, rho_hat = Cy * X, phi_hat = rho_hat .* scale (+ Parseval energy)
+//   gradient: T = Dy * phi_hat, U = phi_hat * Dx^T, Ex = T * (Sx diag(kx))^T, Ey = (Sy diag(ky)) * U
+//   potential (parity hook only): phi = T * Dx^T.
+void Engine::runDct(bool gradient, bool potential) {
+    const int nx = bins_x_, ny = bins_y_;
+    beginKernel(kKindDctForward);
+    GemmTask f1{};
+    f1.a = source_; f1.b = basis_cx_t_; f1.c = stage_a_;
+    f1.m = ny; f1.n = nx; f1.k = nx; f1.lda = nx; f1.ldb = nx; f1.ldc = nx; f1.c_step = 1;
+    launchGemm(&f1, 1, stream_);
+    endKernel();
+    beginKernel(kKindDctForward);
+    GemmTask f2{};
+    f2.a = basis_cy_; f2.b = stage_a_; f2.c = phi_hat_;
+    f2.m = ny; f2.n = nx; f2.k = ny; f2.lda = ny; f2.ldb = nx; f2.ldc = nx; f2.c_step = 1;
+    f2.scale = spectral_scale_; f2.weight_r = weight_y_; f2.weight_c = weight_x_; f2.energy_partials = partials_e_;
+    launchGemm(&f2, 1, stream_);
+    endKernel();
+    launches_ += 2;
+    if (!gradient) return;
+    beginKernel(kKindDctInverse);
+    GemmTask inv1[2]{};
+    inv1[0].a = basis_dy_; inv1[0].b = phi_hat_; inv1[0].c = stage_t_;
+    inv1[0].m = ny; inv1[0].n = nx; inv1[0].k = ny; inv1[0].lda = ny; inv1[0].ldb = nx; inv1[0].ldc = nx; inv1[0].c_step = 1;
+    inv1[1].a = phi_hat_; inv1[1].b = basis_dx_t_; inv1[1].c = stage_u_;
+    inv1[1].m = ny; inv1[1].n = nx; inv1[1].k = nx; inv1[1].lda = nx; inv1[1].ldb = nx; inv1[1].ldc = nx; inv1[1].c_step = 1;
+    launchGemm(inv1, 2, stream_);
+    endKernel();
+    beginKernel(kKindDctInverse);
+    GemmTask inv2[2]{};
+    inv2[0].a = stage_t_; inv2[0].b = basis_sx_w_; inv2[0].c = reinterpret_cast<float*>(field_);
+    inv2[0].m = ny; inv2[0].n = nx; inv2[0].k = nx; inv2[0].lda = nx; inv2[0].ldb = nx; inv2[0].ldc = 2 * nx; inv2[0].c_step = 2;
+    inv2[1].a = basis_sy_w_; inv2[1].b = stage_u_; inv2[1].c = reinterpret_cast<float*>(field_) + 1;
+    inv2[1].m = ny; inv2[1].n = nx; inv2[1].k = ny; inv2[1].lda = ny; inv2[1].ldb = nx; inv2[1].ldc = 2 * nx; inv2[1].c_step = 2;
+    launchGemm(inv2, 2, stream_);
+    endKernel();
+    launches_ += 2;
+    if (potential) {
+        beginKernel(kKindDctInverse);
+        GemmTask pot{};
+        pot.a = stage_t_; pot.b = basis_dx_t_; pot.c = potential_;
+        pot.m = ny; pot.n = nx; pot.k = nx; pot.lda = nx; pot.ldb = nx; pot.ldc = nx; pot.c_step = 1;
+        launchGemm(&pot, 1, stream_);
+        endKernel();
+        launches_ += 1;
+    }
+}
+
 void Engine::launch(const EvalRequest& q) {
     const int nx = bins_x_, ny = bins_y_;
     const double2* positions = q.mode == kGiven ? q.positions : q.out_positions;
@@ -326,7 +421,9 @@ void Engine::launch(const EvalRequest& q) {
     sa.layers = layers_;
     sa.totals = totals_;
     sa.partials = partials_sc_;
+    beginKernel(kKindScatter);
     launchScatter(sa, particle_count_ > 0 ? scatter_blocks_ : 0, stream_);
+    endKernel();
 
     WirelengthArgs wa{};
     wa.positions = positions;
@@ -341,7 +438,9 @@ void Engine::launch(const EvalRequest& q) {
     wa.pin_gradient = pin_gradient_;
     wa.gradient = q.gradient ? 1 : 0;
     wa.partials = partials_wl_;
+    beginKernel(kKindWirelength);
     launchWirelength(wa, wl_blocks_, stream_);
+    endKernel();
 
     MetricsArgs ma{};
     ma.layers = layers_;
@@ -355,41 +454,14 @@ void Engine::launch(const EvalRequest& q) {
     ma.bin_count = bin_count_;
     ma.source = source_;
     ma.partials = partials_m_;
+    beginKernel(kKindMetrics);
     launchMetrics(ma, metrics_blocks_, stream_);
+    endKernel();
+    int kernels = 4;  // scatter, wirelength, metrics, reduce
 
-    // Forward DCT-II in both axes; epilogue: spectral divide + Parseval energy.
-    GemmTask f1{};
-    f1.a = source_; f1.b = basis_cx_t_; f1.c = stage_a_;
-    f1.m = ny; f1.n = nx; f1.k = nx; f1.lda = nx; f1.ldb = nx; f1.ldc = nx; f1.c_step = 1;
-    launchGemm(&f1, 1, stream_);
-    GemmTask f2{};
-    f2.a = basis_cy_; f2.b = stage_a_; f2.c = phi_hat_;
-    f2.m = ny; f2.n = nx; f2.k = ny; f2.lda = ny; f2.ldb = nx; f2.ldc = nx; f2.c_step = 1;
-    f2.scale = spectral_scale_; f2.weight_r = weight_y_; f2.weight_c = weight_x_; f2.energy_partials = partials_e_;
-    launchGemm(&f2, 1, stream_);
-    int kernels = 6;
+    runDct(q.gradient, q.gradient && q.want_potential);
 
     if (q.gradient) {
-        GemmTask inv1[2]{};
-        inv1[0].a = basis_dy_; inv1[0].b = phi_hat_; inv1[0].c = stage_t_;
-        inv1[0].m = ny; inv1[0].n = nx; inv1[0].k = ny; inv1[0].lda = ny; inv1[0].ldb = nx; inv1[0].ldc = nx; inv1[0].c_step = 1;
-        inv1[1].a = phi_hat_; inv1[1].b = basis_dx_t_; inv1[1].c = stage_u_;
-        inv1[1].m = ny; inv1[1].n = nx; inv1[1].k = nx; inv1[1].lda = nx; inv1[1].ldb = nx; inv1[1].ldc = nx; inv1[1].c_step = 1;
-        launchGemm(inv1, 2, stream_);
-        GemmTask inv2[2]{};
-        inv2[0].a = stage_t_; inv2[0].b = basis_sx_w_; inv2[0].c = reinterpret_cast<float*>(field_);
-        inv2[0].m = ny; inv2[0].n = nx; inv2[0].k = nx; inv2[0].lda = nx; inv2[0].ldb = nx; inv2[0].ldc = 2 * nx; inv2[0].c_step = 2;
-        inv2[1].a = basis_sy_w_; inv2[1].b = stage_u_; inv2[1].c = reinterpret_cast<float*>(field_) + 1;
-        inv2[1].m = ny; inv2[1].n = nx; inv2[1].k = ny; inv2[1].lda = ny; inv2[1].ldb = nx; inv2[1].ldc = 2 * nx; inv2[1].c_step = 2;
-        launchGemm(inv2, 2, stream_);
-        kernels += 2;
-        if (q.want_potential) {
-            GemmTask pot{};
-            pot.a = stage_t_; pot.b = basis_dx_t_; pot.c = potential_;
-            pot.m = ny; pot.n = nx; pot.k = nx; pot.lda = nx; pot.ldb = nx; pot.ldc = nx; pot.c_step = 1;
-            launchGemm(&pot, 1, stream_);
-            kernels += 1;
-        }
         GatherArgs ga{};
         ga.particle_count = static_cast<int>(particle_count_);
         ga.movable_count = static_cast<int>(movable_count_);
@@ -418,7 +490,9 @@ void Engine::launch(const EvalRequest& q) {
         ga.prev_gradient = q.prev_gradient;
         ga.velocity = q.velocity;
         ga.partials = partials_g_;
+        beginKernel(kKindGather);
         launchGather(ga, particle_count_ > 0 ? gather_blocks_ : 0, stream_);
+        endKernel();
         kernels += 1;
     }
 
@@ -441,9 +515,12 @@ void Engine::launch(const EvalRequest& q) {
     ra.source_count = s;
     ra.scalars = scalars_;
     ra.totals = totals_;
+    beginKernel(kKindReduce);
     launchReduce(ra, stream_);
+    endKernel();
     checkCuda(cudaMemcpyAsync(host_scalars_, scalars_, sizeof(EvalScalars), cudaMemcpyDeviceToHost, stream_),
               "Download evaluation scalars");
+    d2h_bytes_ += sizeof(EvalScalars);
     launches_ += kernels;
     last_gradient_ = q.gradient;
     last_propose_ = q.mode == kPropose;
@@ -451,6 +528,7 @@ void Engine::launch(const EvalRequest& q) {
 
 const EvalScalars& Engine::sync() {
     checkCuda(cudaStreamSynchronize(stream_), "Synchronize placement evaluation");
+    collectTimings();
     return *host_scalars_;
 }
 
@@ -478,38 +556,13 @@ void Engine::fieldSolve(const double* deviation, double* potential, double* fiel
     std::vector<float> source(bins);
     for (std::size_t i = 0; i < bins; ++i) source[i] = static_cast<float>(deviation[i] - mean);
     upload(source_, source, stream_);
-    const int nx = bins_x_, ny = bins_y_;
-    GemmTask f1{};
-    f1.a = source_; f1.b = basis_cx_t_; f1.c = stage_a_;
-    f1.m = ny; f1.n = nx; f1.k = nx; f1.lda = nx; f1.ldb = nx; f1.ldc = nx; f1.c_step = 1;
-    launchGemm(&f1, 1, stream_);
-    GemmTask f2{};
-    f2.a = basis_cy_; f2.b = stage_a_; f2.c = phi_hat_;
-    f2.m = ny; f2.n = nx; f2.k = ny; f2.lda = ny; f2.ldb = nx; f2.ldc = nx; f2.c_step = 1;
-    f2.scale = spectral_scale_; f2.weight_r = weight_y_; f2.weight_c = weight_x_; f2.energy_partials = partials_e_;
-    launchGemm(&f2, 1, stream_);
-    GemmTask inv1[2]{};
-    inv1[0].a = basis_dy_; inv1[0].b = phi_hat_; inv1[0].c = stage_t_;
-    inv1[0].m = ny; inv1[0].n = nx; inv1[0].k = ny; inv1[0].lda = ny; inv1[0].ldb = nx; inv1[0].ldc = nx; inv1[0].c_step = 1;
-    inv1[1].a = phi_hat_; inv1[1].b = basis_dx_t_; inv1[1].c = stage_u_;
-    inv1[1].m = ny; inv1[1].n = nx; inv1[1].k = nx; inv1[1].lda = nx; inv1[1].ldb = nx; inv1[1].ldc = nx; inv1[1].c_step = 1;
-    launchGemm(inv1, 2, stream_);
-    GemmTask inv2[2]{};
-    inv2[0].a = stage_t_; inv2[0].b = basis_sx_w_; inv2[0].c = reinterpret_cast<float*>(field_);
-    inv2[0].m = ny; inv2[0].n = nx; inv2[0].k = nx; inv2[0].lda = nx; inv2[0].ldb = nx; inv2[0].ldc = 2 * nx; inv2[0].c_step = 2;
-    inv2[1].a = basis_sy_w_; inv2[1].b = stage_u_; inv2[1].c = reinterpret_cast<float*>(field_) + 1;
-    inv2[1].m = ny; inv2[1].n = nx; inv2[1].k = ny; inv2[1].lda = ny; inv2[1].ldb = nx; inv2[1].ldc = 2 * nx; inv2[1].c_step = 2;
-    launchGemm(inv2, 2, stream_);
-    GemmTask pot{};
-    pot.a = stage_t_; pot.b = basis_dx_t_; pot.c = potential_;
-    pot.m = ny; pot.n = nx; pot.k = nx; pot.lda = nx; pot.ldb = nx; pot.ldc = nx; pot.c_step = 1;
-    launchGemm(&pot, 1, stream_);
-    launches_ += 5;
+    runDct(true, true);
     std::vector<float> p(bins);
     std::vector<float2> f(bins);
     checkCuda(cudaMemcpyAsync(p.data(), potential_, bins * sizeof(float), cudaMemcpyDeviceToHost, stream_), "field");
     checkCuda(cudaMemcpyAsync(f.data(), field_, bins * sizeof(float2), cudaMemcpyDeviceToHost, stream_), "field");
     checkCuda(cudaStreamSynchronize(stream_), "field solve");
+    collectTimings();
     for (std::size_t i = 0; i < bins; ++i) {
         if (potential != nullptr) potential[i] = p[i];
         if (field_x != nullptr) field_x[i] = f[i].x;
@@ -537,7 +590,9 @@ void Engine::depositLayers(const double2* positions, int64_t* movable, int64_t* 
     sa.layers = layers_;
     sa.totals = totals_;
     sa.partials = partials_sc_;
+    beginKernel(kKindScatter);
     launchScatter(sa, particle_count_ > 0 ? scatter_blocks_ : 0, stream_);
+    endKernel();
     launches_ += 1;
     const std::size_t bins = static_cast<std::size_t>(bin_count_);
     int64_t* out[3] = {movable, macro, filler};
@@ -549,6 +604,7 @@ void Engine::depositLayers(const double2* positions, int64_t* movable, int64_t* 
     checkCuda(cudaMemsetAsync(layers_, 0, 3 * bins * sizeof(unsigned long long), stream_), "clear layers");
     checkCuda(cudaMemsetAsync(totals_, 0, 4 * sizeof(unsigned long long), stream_), "clear totals");
     checkCuda(cudaStreamSynchronize(stream_), "density layers");
+    collectTimings();
 }
 
 }  // namespace mpgp

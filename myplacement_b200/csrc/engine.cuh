@@ -64,6 +64,25 @@ struct EvalScalars {
     double v[kScalarCount];
 };
 
+// Kernel families timed by the engine's optional event profiler.
+enum KernelKind : int {
+    kKindScatter = 0,
+    kKindWirelength,
+    kKindMetrics,
+    kKindDctForward,
+    kKindDctInverse,
+    kKindGather,
+    kKindReduce,
+    kKindVector,
+    kKindCount
+};
+const char* kernelKindName(int kind);
+
+struct KernelStats {
+    int64_t launches[kKindCount] = {};
+    double milliseconds[kKindCount] = {};
+};
+
 class Engine {
 public:
     Engine(const Problem& problem, int device, uint64_t budget_bytes);
@@ -99,7 +118,23 @@ public:
     [[nodiscard]] const double* precondBase() const { return precond_; }
     void countLaunches(int64_t n) { launches_ += n; }
 
+    // Event profiling: when enabled, every launch is bracketed by CUDA events on
+    // the engine stream and its duration is added to its family at sync().
+    void setTiming(bool enabled);
+    [[nodiscard]] const KernelStats& kernelStats() const { return stats_; }
+    void resetKernelStats() { stats_ = KernelStats{}; }
+    void beginKernel(int kind);
+    void endKernel();
+    [[nodiscard]] uint64_t bytesToDevice() const { return h2d_bytes_; }
+    [[nodiscard]] uint64_t bytesToHost() const { return d2h_bytes_; }
+    void addTransfer(uint64_t to_device, uint64_t to_host) {
+        h2d_bytes_ += to_device;
+        d2h_bytes_ += to_host;
+    }
+
 private:
+    void collectTimings();
+    void runDct(bool gradient, bool potential);
     void uploadStatic(const Problem& problem);
     void buildNetLayout(const Problem& problem);
     void buildBasis();
@@ -172,6 +207,15 @@ private:
     EvalScalars* host_scalars_ = nullptr;
     bool last_gradient_ = false;
     bool last_propose_ = false;
+
+    // profiling
+    bool timing_ = false;
+    std::vector<cudaEvent_t> events_;
+    std::vector<int> pending_kind_;
+    int pending_ = 0;
+    KernelStats stats_;
+    uint64_t h2d_bytes_ = 0;
+    uint64_t d2h_bytes_ = 0;
 };
 
 }  // namespace mpgp

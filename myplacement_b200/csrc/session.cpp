@@ -151,6 +151,7 @@ Session::Session(const mpgp_design& design, const mpgp_options& options) : optio
     checkCuda(cudaMemcpyAsync(cur_, initial.data(), particles * sizeof(double2), cudaMemcpyHostToDevice,
                               engine_->stream()),
               "Upload initial positions");
+    engine_->addTransfer(particles * sizeof(double2), 0);
 
     // Initial evaluations and the penalty normalisation (AdaptiveGlobalPlacer.cpp:672-733).
     smoothing_ = options_.initial_smoothing * max_bin_;
@@ -408,7 +409,9 @@ void Session::iterate() {
 
     const double penalty_used = penalty_;
     if (accepted) {
+        engine_->beginKernel(kKindVector);
         launchVelocity(cand_, cur_, velocity_, static_cast<int>(engine_->particleCount()), engine_->stream());
+        engine_->endKernel();
         engine_->countLaunches(1);
         velocity_zero_ = false;
         last_step_size_ = used_step_size;
@@ -501,6 +504,7 @@ void Session::finish(double* module_x, double* module_y, mpgp_result* result, mp
                                   engine_->stream()),
                   "Download final positions");
         checkCuda(cudaStreamSynchronize(engine_->stream()), "Download final positions");
+        engine_->addTransfer(0, particles * sizeof(double2));
         // applyPositions (AdaptiveGlobalPlacer.cpp:185-198) for the movable modules.
         const Rect2& core = derived_.core;
         std::vector<double2> clamped(particles);
@@ -520,6 +524,7 @@ void Session::finish(double* module_x, double* module_y, mpgp_result* result, mp
         checkCuda(cudaMemcpyAsync(cand_, clamped.data(), particles * sizeof(double2), cudaMemcpyHostToDevice,
                                   engine_->stream()),
                   "Upload final positions");
+        engine_->addTransfer(particles * sizeof(double2), 0);
         const StateEval final_eval = evaluateGiven(cand_, false, penalty_, nullptr, nullptr, false, false);
         result_.hpwl_after = final_eval.m.hpwl;
         result_.overflow_after = final_eval.m.design.normalized_overflow;

@@ -57,6 +57,7 @@ public:
     [[nodiscard]] const std::vector<Filler>& fillers() const { return fillers_; }
     [[nodiscard]] const DerivedDesign& derived() const { return derived_; }
     void currentPositions(double* xy) const;
+    [[nodiscard]] Engine* engine() const { return engine_.get(); }
 
 private:
     StateEval evaluateGiven(double2* positions, bool gradient, double penalty, double2* raw, double2* pre,

@@ -118,6 +118,22 @@ class Session:
     def stream(self) -> int:
         return int(self.lib.mpgp_session_stream(self.handle) or 0)
 
+    def set_profiling(self, enabled: bool) -> None:
+        check(self.lib.mpgp_session_set_profiling(self.handle, int(enabled)))
+
+    def kernel_stats(self) -> dict:
+        """{family: (launches, device milliseconds)} accumulated while profiling was on."""
+        n = self.lib.mpgp_kernel_kind_count()
+        launches = np.zeros(n, np.int64)
+        ms = np.zeros(n)
+        check(self.lib.mpgp_session_kernel_stats(self.handle, _ptr(launches, _i64), _ptr(ms, _d), n))
+        return {self.lib.mpgp_kernel_kind_name(k).decode(): (int(launches[k]), float(ms[k])) for k in range(n)}
+
+    def transfer_bytes(self) -> tuple[int, int]:
+        to_device, to_host = C.c_uint64(), C.c_uint64()
+        check(self.lib.mpgp_session_transfer_bytes(self.handle, C.byref(to_device), C.byref(to_host)))
+        return int(to_device.value), int(to_host.value)
+
     def positions(self, particle_count: int) -> np.ndarray:
         xy = np.empty(2 * particle_count)
         check(self.lib.mpgp_session_positions(self.handle, _ptr(xy, _d)))

@@ -131,19 +131,38 @@ def test_evaluation_parity_against_reference_session(gpu, ref, name, scale):
 
 
 def test_global_place_matches_reference_run(gpu, ref):
-    """A whole adaptive run on the small design: final HPWL/overflow within 0.5 % of the reference CPU run."""
+    """A whole adaptive run on the small design against the reference CPU run.
+
+    * the same iteration budget (88, early stop off): final HPWL within 0.5 %
+      relative and final overflow within 0.005 absolute;
+    * decision parity early on: the first 25 history rows take the same
+      accept / backtrack / restart decisions with HPWL and overflow within 1e-4;
+    * with the early stop on: overflow <= 0.10 and HPWL no worse than 0.5 % above
+      the reference's (the stop iteration moves with FP32-level noise late in a
+      run, so the stopping iteration itself is not compared).
+    """
     design, bins = _session_case(ref, "small_5k", 1.0)
-    ref_x, ref_y, ref_result, ref_history = ref.global_place(
-        design, ref_options(bins_x=bins, bins_y=bins, target_density=0.9, iterations=280))
-    result = mp.GlobalPlacer().run(design, mp.default_options(bins_x=bins, bins_y=bins, target_density=0.9,
-                                                              iterations=280))
+    fixed = dict(bins_x=bins, bins_y=bins, target_density=0.9, iterations=88, feasible_refinement_iterations=100000)
+    _, _, ref_result, ref_history = ref.global_place(design, ref_options(**fixed))
+    result = mp.GlobalPlacer().run(design, mp.default_options(**fixed))
+    assert result.completed_iterations == ref_result.completed_iterations == 88
+    assert result.hpwl_after == pytest.approx(ref_result.hpwl_after, rel=5e-3)
+    assert abs(result.overflow_after - ref_result.overflow_after) <= 5e-3
+    for mine, theirs in zip(result.history[:25], ref_history[:25]):
+        for key in ("accepted", "backtracks", "momentum_restarted"):
+            assert mine[key] == theirs[key], (mine["iteration"], key)
+        assert mine["hpwl"] == pytest.approx(theirs["hpwl"], rel=1e-4)
+        assert mine["overflow"] == pytest.approx(theirs["overflow"], rel=1e-4)
+
+    _, _, ref_stop, _ = ref.global_place(design, ref_options(bins_x=bins, bins_y=bins, target_density=0.9))
+    result = mp.GlobalPlacer().run(design, mp.default_options(bins_x=bins, bins_y=bins, target_density=0.9))
     assert result.completed_iterations > 20
     assert len(result.history) == result.completed_iterations
     assert result.restored_best_checkpoint == 1
-    assert result.hpwl_after == pytest.approx(ref_result.hpwl_after, rel=5e-3)
-    assert result.overflow_after <= max(ref_result.overflow_after * 1.005, 0.10)
-    assert result.hpwl_before == pytest.approx(ref_result.hpwl_before, rel=1e-6)
-    assert result.overflow_before == pytest.approx(ref_result.overflow_before, rel=1e-6)
+    assert result.overflow_after <= 0.10
+    assert result.hpwl_after <= ref_stop.hpwl_after * 1.005
+    assert result.hpwl_before == pytest.approx(ref_stop.hpwl_before, rel=1e-6)
+    assert result.overflow_before == pytest.approx(ref_stop.overflow_before, rel=1e-6)
     movable = design.movable_mask
     core = design.core
     half_w, half_h = design.module_width[movable] * 0.5, design.module_height[movable] * 0.5
@@ -167,17 +186,20 @@ def test_global_place_is_deterministic(gpu):
     assert a.history == b.history
 
 
-def test_aggressive_controller_exercises_backtracking_and_restart(gpu):
-    """PlacementFlowTests.cpp:198-216: an aggressive controller must backtrack and restart momentum."""
-    design, bins = mp.workload("small_5k")
-    x, y = mp.random_placement(design, 9)
+@pytest.mark.parametrize("stem", ["tiny", "mixed"])
+def test_aggressive_controller_exercises_backtracking_and_restart(gpu, golden_dir, stem):
+    """PlacementFlowTests.cpp:198-216: on the reference's fixtures an aggressive controller must
+    backtrack and restart momentum (the reference makes 5/5 and 3/3 with these inputs)."""
+    f = np.load(golden_dir / "fixtures.npz")
+    design = Design(**{k[len(stem) + 1:]: f[k] for k in f.files if k.startswith(stem + "_")}, name=stem)
+    x, y = mp.random_placement(design, 2026)
     design = design.copy_with_positions(x, y)
-    options = mp.default_options(bins_x=bins, bins_y=bins, target_density=0.9, iterations=24,
-                                 initial_movement_in_bins=1.0, maximum_movement_in_bins=1.0, armijo_coefficient=0.5,
-                                 objective_increase_for_density=0.0)
-    result = mp.GlobalPlacer().run(design, options)
+    options = dict(bins_x=8, bins_y=8, iterations=24, maximum_fillers=100, initial_movement_in_bins=1.0,
+                   maximum_movement_in_bins=1.0, armijo_coefficient=0.5, objective_increase_for_density=0.0)
+    result = mp.GlobalPlacer().run(design, mp.default_options(**options))
     assert result.rejected_candidates > 0
     assert result.momentum_restarts > 0
+    assert len(result.history) == result.completed_iterations
 
 
 def test_fixture_designs_run(gpu, golden_dir):
