@@ -297,6 +297,44 @@ int mpgp_backend_density_layers(mpgp_backend* backend, int64_t* movable, int64_t
 int mpgp_backend_field_solve(mpgp_backend* backend, const double* deviation, double* potential, double* field_x,
                              double* field_y);
 
+/*
+ * Allocation-free wirelength and wire gradient.  This entry point has no
+ * counterpart in the reference; it exists for callers that own every byte of
+ * device memory and cannot let a library call cudaMalloc -- a host framework
+ * whose caching allocator or fixed device-memory budget owns the GPU (as the
+ * reference's DeviceMemoryBudget does), or a latency-critical loop where the
+ * implicit device synchronisation of cudaMalloc/cudaFree is not acceptable.
+ *
+ * It computes the same log-sum-exp smooth wirelength, HPWL and per-particle
+ * wire gradient as one mpgp_backend_evaluate (evaluateSmoothWirelength,
+ * AdaptiveGlobalPlacer.cpp:29-82) from caller-owned DEVICE arrays:
+ *   positions          particle_count (x, y) doubles
+ *   net_pin_start      net_count + 1 int32 offsets into the pins
+ *   pin_particle       pin_count int32; < 0 marks a static pin
+ *   pin_xy             pin_count (x, y) doubles: the offset from the particle
+ *                      centre, or the absolute position of a static pin
+ *   net_weight         net_count doubles
+ *   particle_pin_start particle_count + 1 int32, particle_pins: the pins of
+ *                      each particle (indices into the pin arrays)
+ * and writes wire_gradient (particle_count (x, y) doubles) and totals[0] =
+ * smooth wirelength, totals[1] = HPWL.  Work is enqueued on `stream` (a
+ * cudaStream_t; NULL = the default stream) and is complete when the stream is.
+ *
+ * Its scratch is one fixed file-scope device array that every GPU loading the
+ * library holds until the process exits (8.03 MiB): pin_count may not exceed
+ * 1,048,576 (larger inputs return MPGP_ERR_INVALID_ARGUMENT and launch
+ * nothing).  The first call on each device looks up that array's device
+ * address with the device current; make that first call before any stream
+ * capture.  All calls share the one array: calls that overlap on the GPU
+ * (different streams, or threads) race and must be serialised by the caller.
+ * No device memory is allocated or freed.
+ */
+int mpgp_wirelength_noalloc(const double* positions, const int32_t* net_pin_start, const int32_t* pin_particle,
+                            const double* pin_xy, const double* net_weight, int32_t net_count, int32_t pin_count,
+                            const int32_t* particle_pin_start, const int32_t* particle_pins,
+                            int32_t particle_count, double smoothing, double* wire_gradient, double* totals,
+                            void* stream);
+
 /* ---- host setup restated from the reference ----------------------------------- */
 
 /* randomPlacement (src/placement/InitialPlacer.cpp:102-121): writes the module

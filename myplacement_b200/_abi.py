@@ -245,6 +245,8 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "mpgp_backend_density_layers": (C.c_int, [vp, _i64, _i64, _i64]),
         "mpgp_backend_field_solve": (C.c_int, [vp, _d, _d, _d, _d]),
         "mpgp_random_placement": (C.c_int, [C.POINTER(Design), C.c_uint64, _d, _d]),
+        "mpgp_wirelength_noalloc": (C.c_int, [vp, vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, C.c_int32,
+                                              C.c_double, vp, vp, vp]),
         "mpgp_global_place": (C.c_int, [C.POINTER(Design), C.POINTER(Options), _d, _d, C.POINTER(Result),
                                         C.POINTER(HistoryRow), C.c_int32]),
         "mpgp_session_create": (C.c_int, [C.POINTER(Design), C.POINTER(Options), C.POINTER(vp)]),

@@ -203,6 +203,20 @@ int mpgp_backend_field_solve(mpgp_backend* b, const double* deviation, double* p
     });
 }
 
+int mpgp_wirelength_noalloc(const double* positions, const int32_t* net_pin_start, const int32_t* pin_particle,
+                            const double* pin_xy, const double* net_weight, int32_t net_count, int32_t pin_count,
+                            const int32_t* particle_pin_start, const int32_t* particle_pins,
+                            int32_t particle_count, double smoothing, double* wire_gradient, double* totals,
+                            void* stream) {
+    return guarded([&] {
+        mpgp::NoAllocWirelengthArgs args{positions,          net_pin_start, pin_particle,   pin_xy,
+                                         net_weight,         net_count,     pin_count,      particle_pin_start,
+                                         particle_pins,      particle_count, smoothing,     wire_gradient,
+                                         totals,             stream};
+        mpgp::launchWirelengthNoAlloc(args);
+    });
+}
+
 int mpgp_random_placement(const mpgp_design* design, uint64_t seed, double* module_x, double* module_y) {
     return guarded([&] {
         mpgp::require(design != nullptr && module_x != nullptr && module_y != nullptr, "Arguments are required.");

@@ -50,6 +50,27 @@ struct WirelengthArgs {
 };
 void launchWirelength(const WirelengthArgs& args, int blocks, cudaStream_t stream);
 
+// The allocation-free wirelength entry (mpgp_wirelength_noalloc): caller-owned
+// device arrays in, scratch in a fixed file-scope device array.
+constexpr int kNoAllocMaxPins = 1 << 20;
+struct NoAllocWirelengthArgs {
+    const double* positions;
+    const int* net_pin_start;
+    const int* pin_particle;
+    const double* pin_xy;
+    const double* net_weight;
+    int net_count;
+    int pin_count;
+    const int* particle_pin_start;
+    const int* particle_pins;
+    int particle_count;
+    double smoothing;
+    double* wire_gradient;
+    double* totals;
+    void* stream;
+};
+void launchWirelengthNoAlloc(const NoAllocWirelengthArgs& args);
+
 // ---- density scatter (fixed point) ------------------------------------------------
 enum PositionMode : int { kGiven = 0, kPropose = 1, kLookahead = 2 };
 

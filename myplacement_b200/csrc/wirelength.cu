@@ -16,7 +16,11 @@
 // per-net totals are accumulated in FP64.  The per-pin gradient is written to
 // a pin-indexed buffer (no atomics); the particle gather sums it in a fixed
 // order, so the wire gradient is deterministic.
+#include <algorithm>
 #include <cfloat>
+#include <cmath>
+#include <mutex>
+#include <string>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -118,21 +122,19 @@ __device__ void netGroups(const WirelengthArgs& a, int first, int count, double&
     }
 }
 
-// One warp per net, any degree: three passes over the pins.
-__device__ void netWarps(const WirelengthArgs& a, int first, int count, double& smooth, double& hpwl) {
+// One net of any degree on one warp: three passes over its pins.  `load(pin)`
+// returns the pin's position and particle; gradients go to pin_gradient[pin].
+template <class Loader>
+__device__ void netOnWarp(const Loader& load, int begin, int end, float weight, float gamma, float inv_gamma,
+                          bool gradient, float2* pin_gradient, double& smooth, double& hpwl) {
     const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const int warps = blockDim.x >> 5;
-    for (int local = warp; local < count; local += warps) {
-        const int begin = a.net_start[first + local];
-        const int end = a.net_start[first + local + 1];
-        const float weight = a.net_weight[first + local];
-        const PinPoint first_pin = loadPin(a, begin);
+    {
+        const PinPoint first_pin = load(begin);
         const double rx = first_pin.x;
         const double ry = first_pin.y;
         float max_x = -FLT_MAX, min_x = FLT_MAX, max_y = -FLT_MAX, min_y = FLT_MAX;
         for (int pin = begin + lane; pin < end; pin += 32) {
-            const PinPoint p = loadPin(a, pin);
+            const PinPoint p = load(pin);
             const float dx = static_cast<float>(p.x - rx);
             const float dy = static_cast<float>(p.y - ry);
             max_x = fmaxf(max_x, dx);
@@ -146,13 +148,13 @@ __device__ void netWarps(const WirelengthArgs& a, int first, int count, double& 
         min_y = groupMin<32>(min_y);
         float spx = 0.0f, snx = 0.0f, spy = 0.0f, sny = 0.0f;
         for (int pin = begin + lane; pin < end; pin += 32) {
-            const PinPoint p = loadPin(a, pin);
+            const PinPoint p = load(pin);
             const float dx = static_cast<float>(p.x - rx);
             const float dy = static_cast<float>(p.y - ry);
-            spx += expf((dx - max_x) * a.inv_gamma);
-            snx += expf((min_x - dx) * a.inv_gamma);
-            spy += expf((dy - max_y) * a.inv_gamma);
-            sny += expf((min_y - dy) * a.inv_gamma);
+            spx += expf((dx - max_x) * inv_gamma);
+            snx += expf((min_x - dx) * inv_gamma);
+            spy += expf((dy - max_y) * inv_gamma);
+            sny += expf((min_y - dy) * inv_gamma);
         }
         spx = groupSum<32>(spx);
         snx = groupSum<32>(snx);
@@ -160,21 +162,37 @@ __device__ void netWarps(const WirelengthArgs& a, int first, int count, double& 
         sny = groupSum<32>(sny);
         if (lane == 0) {
             const float span = (max_x - min_x) + (max_y - min_y);
-            const float soft = a.gamma * (logf(spx) + logf(snx) + logf(spy) + logf(sny));
+            const float soft = gamma * (logf(spx) + logf(snx) + logf(spy) + logf(sny));
             smooth += static_cast<double>(weight) * (static_cast<double>(span) + static_cast<double>(soft));
             hpwl += static_cast<double>(weight) * static_cast<double>(span);
         }
-        if (a.gradient) {
+        if (gradient) {
             for (int pin = begin + lane; pin < end; pin += 32) {
-                const PinPoint p = loadPin(a, pin);
+                const PinPoint p = load(pin);
                 if (p.particle < 0) continue;
                 const float dx = static_cast<float>(p.x - rx);
                 const float dy = static_cast<float>(p.y - ry);
-                const float gx = weight * (expf((dx - max_x) * a.inv_gamma) / spx - expf((min_x - dx) * a.inv_gamma) / snx);
-                const float gy = weight * (expf((dy - max_y) * a.inv_gamma) / spy - expf((min_y - dy) * a.inv_gamma) / sny);
-                a.pin_gradient[pin] = make_float2(gx, gy);
+                const float gx = weight * (expf((dx - max_x) * inv_gamma) / spx - expf((min_x - dx) * inv_gamma) / snx);
+                const float gy = weight * (expf((dy - max_y) * inv_gamma) / spy - expf((min_y - dy) * inv_gamma) / sny);
+                pin_gradient[pin] = make_float2(gx, gy);
             }
         }
+    }
+}
+
+struct EnginePinLoader {
+    const WirelengthArgs* a;
+    __device__ PinPoint operator()(int pin) const { return loadPin(*a, pin); }
+};
+
+// Warp-per-net bucket (degree > 32) of the engine's wirelength pass.
+__device__ void netWarps(const WirelengthArgs& a, int first, int count, double& smooth, double& hpwl) {
+    const int warp = threadIdx.x >> 5;
+    const int warps = blockDim.x >> 5;
+    const EnginePinLoader load{&a};
+    for (int local = warp; local < count; local += warps) {
+        netOnWarp(load, a.net_start[first + local], a.net_start[first + local + 1], a.net_weight[first + local],
+                  a.gamma, a.inv_gamma, a.gradient != 0, a.pin_gradient, smooth, hpwl);
     }
 }
 
@@ -202,6 +220,161 @@ __global__ void __launch_bounds__(kThreads) wirelengthKernel(WirelengthArgs a) {
 void launchWirelength(const WirelengthArgs& args, int blocks, cudaStream_t stream) {
     if (blocks <= 0) return;
     wirelengthKernel<<<blocks, kThreads, 0, stream>>>(args);
+}
+
+// ---- allocation-free variant --------------------------------------------------------
+//
+// The same per-net LSE pass for callers that own all device memory and cannot
+// let the library allocate.  Its only scratch -- the per-pin gradient staging
+// buffer and the per-block partial sums -- lives in one file-scope device array
+// of fixed size, so the library never calls cudaMalloc for it.  Every GPU that
+// loads the library holds this array (8.03 MiB) until the process exits.
+namespace {
+
+constexpr int kNoAllocMaxBlocks = 2048;
+constexpr std::size_t kNoAllocPinBytes = sizeof(float2) * static_cast<std::size_t>(kNoAllocMaxPins);
+constexpr std::size_t kNoAllocScratchBytes = kNoAllocPinBytes + sizeof(double) * 2 * kNoAllocMaxBlocks;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_wirelength_scratch[kNoAllocScratchBytes];
+
+std::mutex g_scratch_mutex;
+void* g_scratch_address[kNoAllocMaxDevices] = {};
+
+// Pins as the caller lays them out: pin_xy is the offset from the particle
+// centre, or the absolute position of a pin whose particle is < 0.
+struct CallerPinLoader {
+    const double2* positions;
+    const int* pin_particle;
+    const double2* pin_xy;
+    int particle_count;
+    __device__ PinPoint operator()(int pin) const {
+        PinPoint p;
+        p.particle = pin_particle[pin];
+        const double2 v = pin_xy[pin];
+        if (p.particle >= 0 && p.particle < particle_count) {
+            const double2 c = positions[p.particle];
+            p.x = c.x + v.x;
+            p.y = c.y + v.y;
+        } else {
+            p.particle = -1;  // static (or an out-of-range index, treated as static)
+            p.x = v.x;
+            p.y = v.y;
+        }
+        return p;
+    }
+};
+
+__global__ void __launch_bounds__(kThreads) noAllocNetKernel(CallerPinLoader load, const int* net_pin_start,
+                                                            const double* net_weight, int net_count, int pin_count,
+                                                            float gamma, float inv_gamma, unsigned char* scratch) {
+    float2* pin_gradient = reinterpret_cast<float2*>(scratch);
+    double* partials = reinterpret_cast<double*>(scratch + kNoAllocPinBytes);
+    double values[2] = {0.0, 0.0};
+    const int lane = threadIdx.x & 31;
+    const int warps_total = static_cast<int>((gridDim.x * blockDim.x) >> 5);
+    for (int net = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5); net < net_count;
+         net += warps_total) {
+        const int begin = net_pin_start[net];
+        const int end = net_pin_start[net + 1];
+        if (begin < 0 || end > pin_count || end < begin) continue;  // malformed CSR: never write outside scratch
+        if (end - begin < 2) {
+            // Single-pin nets contribute nothing; their slots must read as zero in the gather.
+            for (int pin = begin + lane; pin < end; pin += 32) pin_gradient[pin] = make_float2(0.0f, 0.0f);
+            continue;
+        }
+        netOnWarp(load, begin, end, static_cast<float>(net_weight[net]), gamma, inv_gamma, true, pin_gradient,
+                  values[0], values[1]);
+    }
+    const bool is_max[2] = {false, false};
+    blockReduce<2>(values, is_max);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x + 0] = values[0];
+        partials[2 * blockIdx.x + 1] = values[1];
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) noAllocParticleKernel(const int* particle_pin_start,
+                                                                 const int* particle_pins, int particle_count,
+                                                                 int pin_count, const unsigned char* scratch,
+                                                                 int net_blocks, double2* wire_gradient,
+                                                                 double* totals) {
+    const float2* pin_gradient = reinterpret_cast<const float2*>(scratch);
+    const double* partials = reinterpret_cast<const double*>(scratch + kNoAllocPinBytes);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < particle_count) {
+        double gx = 0.0, gy = 0.0;
+        for (int j = particle_pin_start[i]; j < particle_pin_start[i + 1]; ++j) {
+            const int pin = particle_pins[j];
+            if (pin < 0 || pin >= pin_count) continue;
+            const float2 g = pin_gradient[pin];
+            gx += static_cast<double>(g.x);
+            gy += static_cast<double>(g.y);
+        }
+        wire_gradient[i] = make_double2(gx, gy);
+    }
+    if (blockIdx.x == 0) {  // fixed-order totals of the net pass (deterministic)
+        double values[2] = {0.0, 0.0};
+        for (int row = threadIdx.x; row < net_blocks; row += blockDim.x) {
+            values[0] += partials[2 * row + 0];
+            values[1] += partials[2 * row + 1];
+        }
+        const bool is_max[2] = {false, false};
+        blockReduce<2>(values, is_max);
+        if (threadIdx.x == 0) {
+            totals[0] = values[0];
+            totals[1] = values[1];
+        }
+    }
+}
+
+}  // namespace
+
+void launchWirelengthNoAlloc(const NoAllocWirelengthArgs& a) {
+    require(a.net_count >= 0 && a.pin_count >= 0 && a.particle_count >= 0, "Counts must be non-negative.");
+    if (a.pin_count > kNoAllocMaxPins) {
+        fail(MPGP_ERR_INVALID_ARGUMENT, "pin_count " + std::to_string(a.pin_count) +
+                                            " exceeds the allocation-free limit of " +
+                                            std::to_string(kNoAllocMaxPins) + " pins.");
+    }
+    require(std::isfinite(a.smoothing) && a.smoothing > 0.0, "Smoothing must be positive and finite.");
+    require(a.net_pin_start != nullptr && a.totals != nullptr, "net_pin_start and totals are required.");
+    require(a.pin_count == 0 || (a.pin_particle != nullptr && a.pin_xy != nullptr), "Pin arrays are required.");
+    require(a.net_count == 0 || a.net_weight != nullptr, "Net weights are required.");
+    require(a.particle_count == 0 || (a.positions != nullptr && a.particle_pin_start != nullptr &&
+                                      a.particle_pins != nullptr && a.wire_gradient != nullptr),
+            "Particle arrays are required.");
+    int device = 0;
+    checkCuda(cudaGetDevice(&device), "Query the current device");
+    require(device >= 0 && device < kNoAllocMaxDevices, "Device index out of range.");
+    void* scratch = nullptr;
+    {
+        // Set-up, once per device, with that device current: the host-side name of
+        // the array is not a device address, so ask the runtime for it.
+        std::lock_guard<std::mutex> lock(g_scratch_mutex);
+        if (g_scratch_address[device] == nullptr) {
+            void* address = nullptr;
+            checkCuda(cudaGetSymbolAddress(&address, g_wirelength_scratch), "Locate the wirelength scratch array");
+            g_scratch_address[device] = address;
+        }
+        scratch = g_scratch_address[device];
+    }
+    const cudaStream_t stream = static_cast<cudaStream_t>(a.stream);
+    const float gamma = static_cast<float>(std::max(a.smoothing, kEpsilon));
+    const float inv_gamma = static_cast<float>(1.0 / std::max(a.smoothing, kEpsilon));
+    const int net_blocks = std::min(kNoAllocMaxBlocks, std::max(1, ceilDiv(a.net_count, kThreads / 32)));
+    const CallerPinLoader load{reinterpret_cast<const double2*>(a.positions), a.pin_particle,
+                               reinterpret_cast<const double2*>(a.pin_xy), a.particle_count};
+    noAllocNetKernel<<<net_blocks, kThreads, 0, stream>>>(load, a.net_pin_start, a.net_weight, a.net_count,
+                                                          a.pin_count, gamma, inv_gamma,
+                                                          static_cast<unsigned char*>(scratch));
+    checkCuda(cudaGetLastError(), "Launch the allocation-free net pass");
+    const int particle_blocks = std::max(1, ceilDiv(a.particle_count, kThreads));
+    noAllocParticleKernel<<<particle_blocks, kThreads, 0, stream>>>(
+        a.particle_pin_start, a.particle_pins, a.particle_count, a.pin_count,
+        static_cast<const unsigned char*>(scratch), net_blocks, reinterpret_cast<double2*>(a.wire_gradient),
+        a.totals);
+    checkCuda(cudaGetLastError(), "Launch the allocation-free particle pass");
 }
 
 }  // namespace mpgp
