@@ -12,6 +12,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -93,6 +95,8 @@ Engine::~Engine() {
         cudaStreamDestroy(stream_);
     }
     if (host_scalars_ != nullptr) cudaFreeHost(host_scalars_);
+    if (host_error_ != nullptr) cudaFreeHost(host_error_);
+    for (cudaEvent_t e : events_) cudaEventDestroy(e);
 }
 
 double2* Engine::newParticleArray(const char* what) {
@@ -295,12 +299,141 @@ void Engine::buildBasis() {
     upload(spectral_scale_, scale, stream_);
     upload(weight_y_, wy, stream_);
     upload(weight_x_, wx, stream_);
-    GemmTask probe{};
-    probe.m = ny;
-    probe.n = nx;
-    energy_blocks_ = gemmBlocks(probe);
-    partials_e_ = arena_.array<double>(static_cast<std::size_t>(energy_blocks_), "energy partials");
+    const char* dct_mode = std::getenv("MPGP_DCT");
+    use_tc_ = !(dct_mode != nullptr && std::string(dct_mode) == "simt");
+    if (use_tc_) {
+        // K-major operands of C = A * B^T (engine.cu runDct), in FP64 before the bf16 split.
+        std::vector<double> cx(static_cast<std::size_t>(nx) * nx), dxc(cx.size()), sxwt(cx.size());
+        std::vector<double> cy2(static_cast<std::size_t>(ny) * ny), dy2(cy2.size()), syw(cy2.size());
+        for (int c = 0; c < nx; ++c) {
+            for (int k = 0; k < nx; ++k) {
+                const long long m = static_cast<long long>(k) * (2 * c + 1);
+                const double wave = kPi * static_cast<double>(k) / width;
+                cx[static_cast<std::size_t>(k) * nx + c] = 2.0 * cosQuarter(m, nx);
+                dxc[static_cast<std::size_t>(c) * nx + k] = k == 0 ? 1.0 : 2.0 * cosQuarter(m, nx);
+                sxwt[static_cast<std::size_t>(c) * nx + k] = k == 0 ? 0.0 : wave * 2.0 * sinQuarter(m, nx);
+            }
+        }
+        for (int r = 0; r < ny; ++r) {
+            for (int l = 0; l < ny; ++l) {
+                const long long m = static_cast<long long>(l) * (2 * r + 1);
+                const double wave = kPi * static_cast<double>(l) / height;
+                cy2[static_cast<std::size_t>(l) * ny + r] = 2.0 * cosQuarter(m, ny);
+                dy2[static_cast<std::size_t>(r) * ny + l] = l == 0 ? 1.0 : 2.0 * cosQuarter(m, ny);
+                syw[static_cast<std::size_t>(r) * ny + l] = l == 0 ? 0.0 : wave * 2.0 * sinQuarter(m, ny);
+            }
+        }
+        energy_blocks_ = tcTiles(ny, nx);
+        partials_e_ = arena_.array<double>(static_cast<std::size_t>(energy_blocks_), "energy partials");
+        buildTensorCoreBasis(cx, cy2, dy2, dxc, sxwt, syw);
+    } else {
+        GemmTask probe{};
+        probe.m = ny;
+        probe.n = nx;
+        energy_blocks_ = gemmBlocks(probe);
+        partials_e_ = arena_.array<double>(static_cast<std::size_t>(energy_blocks_), "energy partials");
+    }
     checkCuda(cudaStreamSynchronize(stream_), "basis upload");
+}
+
+SplitMatrix Engine::newSplit(int rows, int cols, const char* what) {
+    SplitMatrix m;
+    m.rows = rows;
+    m.cols = cols;
+    m.ld = paddedLd(cols);
+    m.data = arena_.array<__nv_bfloat16>(m.elements(), what);
+    checkCuda(cudaMemsetAsync(m.data, 0, m.elements() * sizeof(__nv_bfloat16), stream_), what);
+    return m;
+}
+
+void Engine::buildTensorCoreBasis(const std::vector<double>& cx, const std::vector<double>& cy,
+                                  const std::vector<double>& dy, const std::vector<double>& dxc,
+                                  const std::vector<double>& sxwt, const std::vector<double>& syw) {
+    const int nx = bins_x_, ny = bins_y_;
+    const auto splitUpload = [&](const std::vector<double>& values, int rows, int cols, const char* what) {
+        SplitMatrix m = newSplit(rows, cols, what);
+        std::vector<__nv_bfloat16> planes;
+        splitHost(values, rows, cols, m.ld, planes);
+        upload(m.data, planes, stream_);
+        return m;
+    };
+    tc_cx_ = splitUpload(cx, nx, nx, "DCT basis planes");
+    tc_cy_ = splitUpload(cy, ny, ny, "DCT basis planes");
+    tc_dy_ = splitUpload(dy, ny, ny, "DCT basis planes");
+    tc_dxc_ = splitUpload(dxc, nx, nx, "DCT basis planes");
+    tc_sxwt_ = splitUpload(sxwt, nx, nx, "DST basis planes");
+    tc_syw_ = splitUpload(syw, ny, ny, "DST basis planes");
+    tc_source_ = newSplit(ny, nx, "source planes");
+    tc_x1t_ = newSplit(nx, ny, "DCT stage planes");
+    tc_phi_ = newSplit(ny, nx, "potential coefficient planes");
+    tc_phit_ = newSplit(nx, ny, "potential coefficient planes");
+    tc_t_ = newSplit(ny, nx, "DCT stage planes");
+    tc_ut_ = newSplit(nx, ny, "DCT stage planes");
+    tc_error_ = arena_.array<int>(1, "contraction error flag");
+    checkCuda(cudaMemsetAsync(tc_error_, 0, sizeof(int), stream_), "clear error flag");
+    checkCuda(cudaMallocHost(reinterpret_cast<void**>(&host_error_), sizeof(int)), "pinned error flag");
+    *host_error_ = 0;
+
+    const auto task = [&](TcTask& t, const SplitMatrix& a, const SplitMatrix& b, int m, int n, int k, int mode) {
+        std::memset(static_cast<void*>(&t), 0, sizeof(TcTask));
+        makeOperandMap(&t.map_a, a, kTileM);
+        makeOperandMap(&t.map_b, b, kTileN);
+        t.m = m;
+        t.n = n;
+        t.k = k;
+        t.mode = mode;
+    };
+    // X = S * Cx^T, stored transposed (the K-major B operand of the next contraction).
+    task(tc_fwd1_.task[0], tc_source_, tc_cx_, ny, nx, nx, kTcSplitTransposed);
+    tc_fwd1_.task[0].out_t = tc_x1t_.data;
+    tc_fwd1_.task[0].out_t_ld = tc_x1t_.ld;
+    tc_fwd1_.task[0].out_t_plane = tc_x1t_.plane();
+    // rho_hat = Cy * X; epilogue: phi_hat = rho_hat .* scale, stored both ways, + Parseval energy.
+    task(tc_fwd2_.task[0], tc_cy_, tc_x1t_, ny, nx, ny, kTcSpectral);
+    tc_fwd2_.task[0].out = tc_phi_.data;
+    tc_fwd2_.task[0].out_ld = tc_phi_.ld;
+    tc_fwd2_.task[0].out_plane = tc_phi_.plane();
+    tc_fwd2_.task[0].out_t = tc_phit_.data;
+    tc_fwd2_.task[0].out_t_ld = tc_phit_.ld;
+    tc_fwd2_.task[0].out_t_plane = tc_phit_.plane();
+    tc_fwd2_.task[0].scale = spectral_scale_;
+    tc_fwd2_.task[0].weight_r = weight_y_;
+    tc_fwd2_.task[0].weight_c = weight_x_;
+    tc_fwd2_.task[0].energy_partials = partials_e_;
+    // T = Dy * phi_hat and U = phi_hat * Dx^T (stored transposed), one launch.
+    task(tc_inv1_.task[0], tc_dy_, tc_phit_, ny, nx, ny, kTcSplit);
+    tc_inv1_.task[0].out = tc_t_.data;
+    tc_inv1_.task[0].out_ld = tc_t_.ld;
+    tc_inv1_.task[0].out_plane = tc_t_.plane();
+    task(tc_inv1_.task[1], tc_phi_, tc_dxc_, ny, nx, nx, kTcSplitTransposed);
+    tc_inv1_.task[1].out_t = tc_ut_.data;
+    tc_inv1_.task[1].out_t_ld = tc_ut_.ld;
+    tc_inv1_.task[1].out_t_plane = tc_ut_.plane();
+    // Ex = T * (Sx diag(kx))^T and Ey = (Sy diag(ky)) * U into the interleaved field, one launch.
+    task(tc_inv2_.task[0], tc_t_, tc_sxwt_, ny, nx, nx, kTcField);
+    tc_inv2_.task[0].out_f = reinterpret_cast<float*>(field_);
+    tc_inv2_.task[0].out_f_ld = 2 * nx;
+    tc_inv2_.task[0].out_f_step = 2;
+    task(tc_inv2_.task[1], tc_syw_, tc_ut_, ny, nx, ny, kTcField);
+    tc_inv2_.task[1].out_f = reinterpret_cast<float*>(field_) + 1;
+    tc_inv2_.task[1].out_f_ld = 2 * nx;
+    tc_inv2_.task[1].out_f_step = 2;
+    // Potential (parity hook): phi = T * Dx^T.
+    task(tc_pot_.task[0], tc_t_, tc_dxc_, ny, nx, nx, kTcField);
+    tc_pot_.task[0].out_f = potential_;
+    tc_pot_.task[0].out_f_ld = nx;
+    tc_pot_.task[0].out_f_step = 1;
+    tc_fwd1_.error_flag = tc_fwd2_.error_flag = tc_inv1_.error_flag = tc_inv2_.error_flag = tc_pot_.error_flag =
+        tc_error_;
+    if (std::getenv("MPGP_TC_TRACE") != nullptr) {
+        unsigned long long* trace = arena_.array<unsigned long long>(5 * 64, "trace");
+        checkCuda(cudaMemsetAsync(trace, 0, 5 * 64 * 8, stream_), "trace");
+        tc_fwd1_.trace = trace;
+        tc_fwd2_.trace = trace + 64;
+        tc_inv1_.trace = trace + 128;
+        tc_inv2_.trace = trace + 192;
+        tc_pot_.trace = trace + 256;
+    }
 }
 
 const char* kernelKindName(int kind) {
@@ -349,6 +482,33 @@ void Engine::collectTimings() {
 //   potential (parity hook only): phi = T * Dx^T.
 void Engine::runDct(bool gradient, bool potential) {
     const int nx = bins_x_, ny = bins_y_;
+    if (use_tc_) {
+        beginKernel(kKindDctForward);
+        launchSplitSource(source_, tc_source_, nx, stream_);
+        endKernel();
+        beginKernel(kKindDctForward);
+        launchTcGemm(tc_fwd1_, 1, stream_);
+        endKernel();
+        beginKernel(kKindDctForward);
+        launchTcGemm(tc_fwd2_, 1, stream_);
+        endKernel();
+        launches_ += 3;
+        if (!gradient) return;
+        beginKernel(kKindDctInverse);
+        launchTcGemm(tc_inv1_, 2, stream_);
+        endKernel();
+        beginKernel(kKindDctInverse);
+        launchTcGemm(tc_inv2_, 2, stream_);
+        endKernel();
+        launches_ += 2;
+        if (potential) {
+            beginKernel(kKindDctInverse);
+            launchTcGemm(tc_pot_, 1, stream_);
+            endKernel();
+            launches_ += 1;
+        }
+        return;
+    }
     beginKernel(kKindDctForward);
     GemmTask f1{};
     f1.a = source_; f1.b = basis_cx_t_; f1.c = stage_a_;
@@ -521,6 +681,11 @@ void Engine::launch(const EvalRequest& q) {
     checkCuda(cudaMemcpyAsync(host_scalars_, scalars_, sizeof(EvalScalars), cudaMemcpyDeviceToHost, stream_),
               "Download evaluation scalars");
     d2h_bytes_ += sizeof(EvalScalars);
+    if (use_tc_) {
+        checkCuda(cudaMemcpyAsync(host_error_, tc_error_, sizeof(int), cudaMemcpyDeviceToHost, stream_),
+                  "Download contraction status");
+        d2h_bytes_ += sizeof(int);
+    }
     launches_ += kernels;
     last_gradient_ = q.gradient;
     last_propose_ = q.mode == kPropose;
@@ -529,6 +694,9 @@ void Engine::launch(const EvalRequest& q) {
 const EvalScalars& Engine::sync() {
     checkCuda(cudaStreamSynchronize(stream_), "Synchronize placement evaluation");
     collectTimings();
+    if (host_error_ != nullptr && *host_error_ != 0) {
+        fail(MPGP_ERR_TIMEOUT, "A tcgen05 field contraction timed out waiting on its pipeline.");
+    }
     return *host_scalars_;
 }
 
@@ -561,8 +729,28 @@ void Engine::fieldSolve(const double* deviation, double* potential, double* fiel
     std::vector<float2> f(bins);
     checkCuda(cudaMemcpyAsync(p.data(), potential_, bins * sizeof(float), cudaMemcpyDeviceToHost, stream_), "field");
     checkCuda(cudaMemcpyAsync(f.data(), field_, bins * sizeof(float2), cudaMemcpyDeviceToHost, stream_), "field");
+    if (use_tc_) {
+        checkCuda(cudaMemcpyAsync(host_error_, tc_error_, sizeof(int), cudaMemcpyDeviceToHost, stream_),
+                  "Download contraction status");
+    }
     checkCuda(cudaStreamSynchronize(stream_), "field solve");
     collectTimings();
+    if (tc_fwd1_.trace != nullptr) {
+        std::vector<unsigned long long> trace(5 * 64);
+        checkCuda(cudaMemcpy(trace.data(), tc_fwd1_.trace, trace.size() * 8, cudaMemcpyDeviceToHost), "trace");
+        for (int g = 0; g < 5; ++g) {
+            const unsigned long long base = trace[g * 64 + 51];
+            std::fprintf(stderr, "TRACE gemm %d:", g);
+            for (int i = 0; i < 52; ++i) {
+                const unsigned long long v = trace[g * 64 + i];
+                if (v != 0) std::fprintf(stderr, " %d:%lld", i, static_cast<long long>(v - base));
+            }
+            std::fprintf(stderr, "\n");
+        }
+    }
+    if (host_error_ != nullptr && *host_error_ != 0) {
+        fail(MPGP_ERR_TIMEOUT, "A tcgen05 field contraction timed out waiting on its pipeline.");
+    }
     for (std::size_t i = 0; i < bins; ++i) {
         if (potential != nullptr) potential[i] = p[i];
         if (field_x != nullptr) field_x[i] = f[i].x;

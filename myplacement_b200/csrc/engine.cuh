@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <vector>
 
+#include "dct_tc.cuh"
 #include "kernels.cuh"
 #include "setup.hpp"
 
@@ -195,6 +196,18 @@ private:
     float* stage_u_ = nullptr;
     float2* field_ = nullptr;
     float* potential_ = nullptr;
+
+    // tcgen05 split-precision form of the same contractions (dct_tc.cu)
+    bool use_tc_ = true;
+    SplitMatrix tc_source_, tc_cx_, tc_cy_, tc_dy_, tc_dxc_, tc_sxwt_, tc_syw_;
+    SplitMatrix tc_x1t_, tc_phi_, tc_phit_, tc_t_, tc_ut_;
+    TcBatch tc_fwd1_{}, tc_fwd2_{}, tc_inv1_{}, tc_inv2_{}, tc_pot_{};
+    int* tc_error_ = nullptr;
+    int* host_error_ = nullptr;
+    void buildTensorCoreBasis(const std::vector<double>& cx, const std::vector<double>& cy,
+                              const std::vector<double>& dy, const std::vector<double>& dxc,
+                              const std::vector<double>& sxwt, const std::vector<double>& syw);
+    SplitMatrix newSplit(int rows, int cols, const char* what);
 
     // partials and scalars
     int scatter_blocks_ = 0, metrics_blocks_ = 0, gather_blocks_ = 0, energy_blocks_ = 0;
