@@ -9,7 +9,10 @@
 
 namespace mpgp {
 
-constexpr int kSplit = 3;    // bf16 planes per operand (x = hi + mid + lo)
+#ifndef MPGP_SPLIT_PLANES
+#define MPGP_SPLIT_PLANES 3
+#endif
+constexpr int kSplit = MPGP_SPLIT_PLANES;  // bf16 planes per operand (x = hi + mid + lo)
 constexpr int kTileM = 128;  // UMMA M = TMEM lanes
 constexpr int kTileN = 64;   // UMMA N = accumulator columns per CTA
 constexpr int kBlockK = 64;  // bf16 elements per 128-byte swizzled row

@@ -69,6 +69,9 @@ double sinQuarter(long long m, int n) {
 Engine::Engine(const Problem& p, int device, uint64_t budget_bytes) : device_(device), arena_(budget_bytes) {
     checkCuda(cudaSetDevice(device_), "Select CUDA device");
     checkCuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "Create engine stream");
+    checkCuda(cudaStreamCreateWithFlags(&stream_wl_, cudaStreamNonBlocking), "Create wirelength stream");
+    checkCuda(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "Create fork event");
+    checkCuda(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "Create join event");
     particle_count_ = p.particle_count;
     movable_count_ = p.movable_count;
     bins_x_ = p.bins_x;
@@ -94,6 +97,12 @@ Engine::~Engine() {
         cudaStreamSynchronize(stream_);
         cudaStreamDestroy(stream_);
     }
+    if (stream_wl_ != nullptr) {
+        cudaStreamSynchronize(stream_wl_);
+        cudaStreamDestroy(stream_wl_);
+    }
+    if (fork_ != nullptr) cudaEventDestroy(fork_);
+    if (join_ != nullptr) cudaEventDestroy(join_);
     if (host_scalars_ != nullptr) cudaFreeHost(host_scalars_);
     if (host_error_ != nullptr) cudaFreeHost(host_error_);
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
@@ -451,24 +460,24 @@ void Engine::setTiming(bool enabled) {
     timing_ = enabled;
 }
 
-void Engine::beginKernel(int kind) {
+void Engine::beginKernel(int kind, cudaStream_t on) {
     if (!timing_) return;
     if (pending_ >= static_cast<int>(pending_kind_.size())) collectTimings();
     pending_kind_[pending_] = kind;
-    checkCuda(cudaEventRecord(events_[2 * pending_], stream_), "Record profiling event");
+    checkCuda(cudaEventRecord(events_[2 * pending_], on != nullptr ? on : stream_), "Record profiling event");
 }
 
-void Engine::endKernel() {
+void Engine::endKernel(cudaStream_t on) {
     if (!timing_) return;
-    checkCuda(cudaEventRecord(events_[2 * pending_ + 1], stream_), "Record profiling event");
+    checkCuda(cudaEventRecord(events_[2 * pending_ + 1], on != nullptr ? on : stream_), "Record profiling event");
     ++pending_;
 }
 
 void Engine::collectTimings() {
     if (pending_ == 0) return;
-    checkCuda(cudaEventSynchronize(events_[2 * pending_ - 1]), "Profiling sync");
     for (int i = 0; i < pending_; ++i) {
         float ms = 0.0f;
+        checkCuda(cudaEventSynchronize(events_[2 * i + 1]), "Profiling sync");
         checkCuda(cudaEventElapsedTime(&ms, events_[2 * i], events_[2 * i + 1]), "Profiling elapsed");
         stats_.launches[pending_kind_[i]] += 1;
         stats_.milliseconds[pending_kind_[i]] += static_cast<double>(ms);
@@ -480,9 +489,10 @@ void Engine::collectTimings() {
 //   X = S * Cx^T, rho_hat = Cy * X, phi_hat = rho_hat .* scale (+ Parseval energy)
 //   gradient: T = Dy * phi_hat, U = phi_hat * Dx^T, Ex = T * (Sx diag(kx))^T, Ey = (Sy diag(ky)) * U
 //   potential (parity hook only): phi = T * Dx^T.
-void Engine::runDct(bool gradient, bool potential) {
+void Engine::runDct(bool gradient, bool potential, bool forward) {
     const int nx = bins_x_, ny = bins_y_;
     if (use_tc_) {
+        if (forward) {
         beginKernel(kKindDctForward);
         launchSplitSource(source_, tc_source_, nx, stream_);
         endKernel();
@@ -493,6 +503,7 @@ void Engine::runDct(bool gradient, bool potential) {
         launchTcGemm(tc_fwd2_, 1, stream_);
         endKernel();
         launches_ += 3;
+        }
         if (!gradient) return;
         beginKernel(kKindDctInverse);
         launchTcGemm(tc_inv1_, 2, stream_);
@@ -581,9 +592,16 @@ void Engine::launch(const EvalRequest& q) {
     sa.layers = layers_;
     sa.totals = totals_;
     sa.partials = partials_sc_;
-    beginKernel(kKindScatter);
-    launchScatter(sa, particle_count_ > 0 ? scatter_blocks_ : 0, stream_);
-    endKernel();
+    if (q.mode == kGiven) checkCuda(cudaEventRecord(fork_, stream_), "fork");
+    if (!q.reuse_density) {
+        beginKernel(kKindScatter);
+        launchScatter(sa, particle_count_ > 0 ? scatter_blocks_ : 0, stream_);
+        endKernel();
+    }
+    // The wirelength pass needs the positions only: it runs beside the density
+    // chain on its own stream (after the scatter when the scatter forms them).
+    if (q.mode != kGiven) checkCuda(cudaEventRecord(fork_, stream_), "fork");
+    checkCuda(cudaStreamWaitEvent(stream_wl_, fork_, 0), "fork");
 
     WirelengthArgs wa{};
     wa.positions = positions;
@@ -598,9 +616,10 @@ void Engine::launch(const EvalRequest& q) {
     wa.pin_gradient = pin_gradient_;
     wa.gradient = q.gradient ? 1 : 0;
     wa.partials = partials_wl_;
-    beginKernel(kKindWirelength);
-    launchWirelength(wa, wl_blocks_, stream_);
-    endKernel();
+    beginKernel(kKindWirelength, stream_wl_);
+    launchWirelength(wa, wl_blocks_, stream_wl_);
+    endKernel(stream_wl_);
+    checkCuda(cudaEventRecord(join_, stream_wl_), "join");
 
     MetricsArgs ma{};
     ma.layers = layers_;
@@ -614,12 +633,16 @@ void Engine::launch(const EvalRequest& q) {
     ma.bin_count = bin_count_;
     ma.source = source_;
     ma.partials = partials_m_;
-    beginKernel(kKindMetrics);
-    launchMetrics(ma, metrics_blocks_, stream_);
-    endKernel();
-    int kernels = 4;  // scatter, wirelength, metrics, reduce
+    int kernels = 2;  // wirelength, reduce
+    if (!q.reuse_density) {
+        beginKernel(kKindMetrics);
+        launchMetrics(ma, metrics_blocks_, stream_);
+        endKernel();
+        kernels += 2;  // scatter, metrics
+    }
 
-    runDct(q.gradient, q.gradient && q.want_potential);
+    runDct(q.gradient, q.gradient && q.want_potential, !q.reuse_density);
+    checkCuda(cudaStreamWaitEvent(stream_, join_, 0), "join");
 
     if (q.gradient) {
         GatherArgs ga{};
@@ -664,10 +687,12 @@ void Engine::launch(const EvalRequest& q) {
     add(partials_wl_, wl_blocks_, 2, 0, false, kSmooth);
     add(partials_wl_, wl_blocks_, 2, 1, false, kHpwl);
     const int scatter_rows = particle_count_ > 0 ? scatter_blocks_ : 0;
-    add(partials_sc_, q.mode == kPropose ? scatter_rows : 0, 2, 0, false, kPredicted);
-    add(partials_sc_, q.mode == kPropose ? scatter_rows : 0, 2, 1, true, kMaxDisplacement);
-    for (int k = 0; k < 9; ++k) add(partials_m_, metrics_blocks_, 9, k, k >= 7, kOverflowWith + k);
-    add(partials_e_, energy_blocks_, 1, 0, false, kEnergy);
+    if (!q.reuse_density) {  // otherwise the density scalars of the previous evaluation stand
+        add(partials_sc_, q.mode == kPropose ? scatter_rows : 0, 2, 0, false, kPredicted);
+        add(partials_sc_, q.mode == kPropose ? scatter_rows : 0, 2, 1, true, kMaxDisplacement);
+        for (int k = 0; k < 9; ++k) add(partials_m_, metrics_blocks_, 9, k, k >= 7, kOverflowWith + k);
+        add(partials_e_, energy_blocks_, 1, 0, false, kEnergy);
+    }
     if (q.gradient) {
         const int rows = particle_count_ > 0 ? gather_blocks_ : 0;
         for (int k = 0; k < 7; ++k) add(partials_g_, rows, 7, k, false, kWireL1 + k);
@@ -724,7 +749,7 @@ void Engine::fieldSolve(const double* deviation, double* potential, double* fiel
     std::vector<float> source(bins);
     for (std::size_t i = 0; i < bins; ++i) source[i] = static_cast<float>(deviation[i] - mean);
     upload(source_, source, stream_);
-    runDct(true, true);
+    runDct(true, true, true);
     std::vector<float> p(bins);
     std::vector<float2> f(bins);
     checkCuda(cudaMemcpyAsync(p.data(), potential_, bins * sizeof(float), cudaMemcpyDeviceToHost, stream_), "field");

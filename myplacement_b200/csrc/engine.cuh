@@ -59,6 +59,10 @@ struct EvalRequest {
     const double2* prev_gradient = nullptr;
     const double2* velocity = nullptr;
     bool want_potential = false;
+    // The density map, forward field coefficients and energy of the previous
+    // evaluation are those of these positions (nothing moved since): keep them and
+    // run only the wirelength, the inverse field and the gather.
+    bool reuse_density = false;
 };
 
 struct EvalScalars {
@@ -124,8 +128,8 @@ public:
     void setTiming(bool enabled);
     [[nodiscard]] const KernelStats& kernelStats() const { return stats_; }
     void resetKernelStats() { stats_ = KernelStats{}; }
-    void beginKernel(int kind);
-    void endKernel();
+    void beginKernel(int kind, cudaStream_t on = nullptr);
+    void endKernel(cudaStream_t on = nullptr);
     [[nodiscard]] uint64_t bytesToDevice() const { return h2d_bytes_; }
     [[nodiscard]] uint64_t bytesToHost() const { return d2h_bytes_; }
     void addTransfer(uint64_t to_device, uint64_t to_host) {
@@ -135,13 +139,16 @@ public:
 
 private:
     void collectTimings();
-    void runDct(bool gradient, bool potential);
+    void runDct(bool gradient, bool potential, bool forward);
     void uploadStatic(const Problem& problem);
     void buildNetLayout(const Problem& problem);
     void buildBasis();
 
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
+    cudaStream_t stream_wl_ = nullptr;  // the wirelength pass overlaps the density chain
+    cudaEvent_t fork_ = nullptr;
+    cudaEvent_t join_ = nullptr;
     DeviceArena arena_;
     int64_t launches_ = 0;
 

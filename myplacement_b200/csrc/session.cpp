@@ -205,10 +205,12 @@ void Session::fillMetrics(const EvalScalars& s, double penalty, StateEval& out) 
 }
 
 StateEval Session::evaluateGiven(double2* positions, bool gradient, double penalty, double2* raw, double2* pre,
-                                 bool with_prev, bool with_velocity) {
+                                 bool with_prev, bool with_velocity, bool reuse_density) {
     EvalRequest q;
     q.mode = kGiven;
     q.positions = positions;
+    q.reuse_density = reuse_density;
+    density_cached_ = false;
     q.smoothing = smoothing_;
     q.gradient = gradient;
     q.penalty = penalty;
@@ -230,6 +232,7 @@ StateEval Session::evaluateGiven(double2* positions, bool gradient, double penal
 }
 
 StateEval Session::evaluateLookahead(double momentum, double penalty, double2* raw, double2* pre) {
+    density_cached_ = false;
     EvalRequest q;
     q.mode = kLookahead;
     q.base = cur_;
@@ -257,6 +260,7 @@ StateEval Session::evaluateLookahead(double momentum, double penalty, double2* r
 
 StateEval Session::evaluateProposal(const double2* base, const StateEval& base_eval, double step, double max_disp,
                                     double penalty) {
+    density_cached_ = false;
     EvalRequest q;
     q.mode = kPropose;
     q.base = base;
@@ -327,7 +331,8 @@ void Session::iterate() {
         current = initial_;
     } else {
         smoothing_ = smoothingFromOverflow(last_optimizer_overflow_);
-        current = evaluateGiven(cur_, true, penalty_, raw_cur_, pre_cur_, has_previous_gradient_, true);
+        current = evaluateGiven(cur_, true, penalty_, raw_cur_, pre_cur_, has_previous_gradient_, true,
+                                density_cached_);
     }
 
     bool restarted = objective_worse_streak_ >= 2;
@@ -439,6 +444,7 @@ void Session::iterate() {
             has_previous_gradient_ = true;
         }
         std::swap(cur_, cand_);  // current_positions = accepted positions
+        density_cached_ = true;  // the accepted candidate was the last evaluation
         last_optimizer_overflow_ = accepted_eval.m.optimizer.normalized_overflow;
         considerCheckpoint(cur_, accepted_eval.m, iteration + 1, new_best_checkpoint);
         ++result_.accepted_iterations;

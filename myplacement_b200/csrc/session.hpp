@@ -61,7 +61,7 @@ public:
 
 private:
     StateEval evaluateGiven(double2* positions, bool gradient, double penalty, double2* raw, double2* pre,
-                            bool with_prev, bool with_velocity);
+                            bool with_prev, bool with_velocity, bool reuse_density = false);
     StateEval evaluateLookahead(double momentum, double penalty, double2* raw, double2* pre);
     StateEval evaluateProposal(const double2* base, const StateEval& base_eval, double step, double max_disp,
                                double penalty);
@@ -113,6 +113,9 @@ private:
     int iteration_ = 0;
     StateEval initial_;
     bool velocity_zero_ = true;
+    // The last evaluation was the accepted candidate now held in cur_, so its
+    // density map, field coefficients and energy are still on the device.
+    bool density_cached_ = false;
 };
 
 }  // namespace mpgp

