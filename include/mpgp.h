@@ -376,14 +376,17 @@ int mpgp_session_finish(mpgp_session* session, double* module_x, double* module_
 /* Current particle positions (particle_count (x, y) pairs). */
 int mpgp_session_positions(const mpgp_session* session, double* positions);
 /* Tracing (no counterpart in the reference, which times only the whole run,
- * AdaptiveGlobalPlacer.cpp:656, 951): with profiling on, every kernel launch of
- * the session is bracketed by CUDA events on its stream and its device time is
- * accumulated per kernel family.  Families are numbered 0..mpgp_kernel_kind_count()-1. */
+ * AdaptiveGlobalPlacer.cpp:656, 951): every kernel launch of a family whose bit
+ * is set in `families` is bracketed by CUDA events on its stream and its device
+ * time is accumulated per family (families = 0 turns profiling off; each event
+ * pair costs host time, so time only the families of interest).  Families are
+ * numbered 0..mpgp_kernel_kind_count()-1. */
 int mpgp_kernel_kind_count(void);
 const char* mpgp_kernel_kind_name(int kind);
-int mpgp_session_set_profiling(mpgp_session* session, int enabled);
+int mpgp_session_set_profiling(mpgp_session* session, uint32_t families);
 int mpgp_session_kernel_stats(const mpgp_session* session, int64_t* launches, double* milliseconds,
                               int32_t capacity);
+int mpgp_session_reset_kernel_stats(mpgp_session* session);
 /* Host<->device bytes the session has copied (setup, positions, scalar read-backs). */
 int mpgp_session_transfer_bytes(const mpgp_session* session, uint64_t* to_device, uint64_t* to_host);
 /* Number of engine kernel launches issued by this session so far. */

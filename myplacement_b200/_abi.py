@@ -260,8 +260,9 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "mpgp_session_kernel_launches": (C.c_int64, [vp]),
         "mpgp_kernel_kind_count": (C.c_int, []),
         "mpgp_kernel_kind_name": (C.c_char_p, [C.c_int]),
-        "mpgp_session_set_profiling": (C.c_int, [vp, C.c_int]),
+        "mpgp_session_set_profiling": (C.c_int, [vp, C.c_uint32]),
         "mpgp_session_kernel_stats": (C.c_int, [vp, _i64, _d, C.c_int32]),
+        "mpgp_session_reset_kernel_stats": (C.c_int, [vp]),
         "mpgp_session_transfer_bytes": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "mpgp_session_stream": (vp, [vp]),
         "mpgp_session_destroy": (None, [vp]),

@@ -306,10 +306,17 @@ int mpgp_kernel_kind_count(void) { return mpgp::kKindCount; }
 
 const char* mpgp_kernel_kind_name(int kind) { return mpgp::kernelKindName(kind); }
 
-int mpgp_session_set_profiling(mpgp_session* s, int enabled) {
+int mpgp_session_set_profiling(mpgp_session* s, uint32_t families) {
     return guarded([&] {
         mpgp::require(s != nullptr, "A session is required.");
-        if (s->session->engine() != nullptr) s->session->engine()->setTiming(enabled != 0);
+        if (s->session->engine() != nullptr) s->session->engine()->setTiming(families);
+    });
+}
+
+int mpgp_session_reset_kernel_stats(mpgp_session* s) {
+    return guarded([&] {
+        mpgp::require(s != nullptr, "A session is required.");
+        if (s->session->engine() != nullptr) s->session->engine()->resetKernelStats();
     });
 }
 

@@ -1,32 +1,49 @@
 // Split-precision tcgen05 contractions for the Neumann DCT/DST field (sm_100a).
 //
 // The field solve of ElectrostaticField::solveNeumann (ElectrostaticField.cpp:
-// 205-237) is six dense contractions C = A * B^T (see engine.cu runDct).  Each
-// operand is stored as kSplit bf16 planes whose sum carries ~8 * kSplit bits of
-// the FP32 value (x = hi + mid + lo); a contraction accumulates the cross
-// products whose combined order is below kSplit (hh, hm, mh, hl, lh, mm for
-// three planes), smallest first.
+// 205-237) is six dense contractions C = A * B^T (engine.cu runDct).
 //
-// Per CTA: one 128 x kTileN output tile and six warps.
-//   warp 0 lane 0  TMA producer: K-blocks of 64 elements of every plane of A
+// Precision: each operand x is scaled by a power of two 2^-e (so that the
+// scaled magnitudes stay below 2^14) and stored as two fp16 planes,
+// hi = fp16(x 2^-e) and lo = fp16((x 2^-e - hi) 2^11), which carry ~22 bits;
+// lo is kept at the magnitude of x so that it does not fall into the fp16
+// subnormal range, which the tensor cores flush.  A contraction accumulates
+// hi*hi in one TMEM accumulator and hi*lo + lo*hi in a second one, combined as
+// main + 2^-11 corr (the error-corrected fp16 split of Ootomo and Yokota,
+// "Recovering single precision accuracy from Tensor Cores while surpassing the
+// FP32 theoretical peak performance", IJHPCA 2022); the dropped lo*lo term is
+// ~2^-22 relative.  Partials are restarted every K-block and summed in FP64
+// registers, which keeps the accumulation error of long K chains at FP64 level.  Plane
+// exponents follow the data: the source gets one exponent per row, every later
+// stage a bound from the measured maximum of its input (TcScales).
+//
+// A 128 x kTileN output tile is computed by a cluster of `ksplit` CTAs, each
+// owning a contiguous share of the K-blocks, so that a 512 x 512 contraction
+// (32 tiles) still occupies ~128 SMs.  Per CTA, six warps:
+//   warp 0 lane 0  TMA producer: K-blocks of 64 elements of both planes of A
 //                  and B into a kStages-deep shared-memory ring (3-D tensor
 //                  maps: K, rows, plane; 128-byte swizzle; zero fill past edges).
-//   warp 1 lane 0  tcgen05.mma issuer: the products of one K-block into one of
-//                  two TMEM accumulators (double-buffered), restarted every
-//                  K-block; tcgen05.commit releases the smem stage and
-//                  publishes the partial.
+//   warp 1 lane 0  tcgen05.mma issuer: the three products of one K-block into
+//                  one of two TMEM accumulator pairs (double-buffered),
+//                  restarted every K-block; tcgen05.commit releases the smem
+//                  stage and publishes the partial.
 //   warps 2-5      read each partial with tcgen05.ld (warp w owns TMEM lanes
-//                  32 * (w % 4) .. +31, i.e. tile rows) and sum the partials in
-//                  FP64 registers, which keeps the accumulation error of long K
-//                  chains at FP64 level; then the fused epilogue: re-split into
-//                  bf16 planes (plain or transposed), or the spectral divide with
-//                  the Parseval energy partials, or FP32 field stores.
-// Every mbarrier wait is bounded: on a timeout the CTA raises the error flag,
-// drains the copies it issued, frees its TMEM and returns.
+//                  32 * (w % 4) .. +31, i.e. tile rows), sum the partials in
+//                  FP64 registers and park the FP64 tile in shared memory.
+// CTA r of a cluster owns rows r * 128 / ksplit .. of the tile: every peer
+// sends it those parked rows with one bulk shared-to-shared copy (completion
+// on an mbarrier of the owner), and the owner sums the ksplit pieces in a
+// fixed order (the result does not depend on scheduling), then runs the fused
+// epilogue with all six warps and 16-byte stores: re-split into planes (plain
+// or transposed), the spectral divide with the Parseval energy partials, or
+// FP32 field stores.  Every mbarrier wait is bounded: on a timeout the CTA
+// raises the error flag, drains the copies it issued and frees its TMEM; a
+// failed CTA still sends its (flagged) rows, so its peers never wait on it.
 #include <cuda.h>
-#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -39,22 +56,43 @@ namespace {
 
 constexpr int kTcThreads = 192;
 constexpr int kStageBytes = kSplit * (kTileM + kTileN) * kBlockK * 2;
-constexpr int kSmemBytes = kStages * kStageBytes + 1024 /* alignment slack */ + 256 /* barriers */;
-constexpr uint32_t kTmemColumns = 2 * kTileN;  // two partial accumulators
-constexpr long kSpinLimit = 1L << 22;
+constexpr int kRingBytes = kStages * kStageBytes;
+constexpr int kParkPitch = kTileN + 2;  // doubles per parked row: 64 values, the failure flag, padding
+constexpr int kParkBytes = kTileM * kParkPitch * 8;
 constexpr int kTilePitch = kTileN + 1;  // floats per staged row (odd pitch: no bank conflicts)
-static_assert(kTileM * kTilePitch * 4 <= kStages * kStageBytes, "the staged tile must fit in the ring");
-
-__device__ __forceinline__ unsigned long long nowNs() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
-#define TC_TRACE(slot) \
-    do { if (batch.trace != nullptr && blockIdx.x == 0 && blockIdx.y == 0) batch.trace[(slot)] = nowNs(); } while (0)
+constexpr int kStagedOffset = kParkBytes;
+constexpr int kReceiveOffset = kRingBytes;
+constexpr int kBarrierOffset = kReceiveOffset + kParkBytes;
+constexpr int kSmemBytes = kBarrierOffset + 256 + 1024 /* alignment slack */;
+constexpr uint32_t kTmemColumns = 4 * kTileN;  // two buffers x (main, correction) accumulators
+constexpr long kSpinLimit = 1L << 22;
+static_assert(kStagedOffset + kTileM * kTilePitch * 4 <= kRingBytes, "the parked and staged tiles must fit in the ring");
+static_assert((kParkPitch * 8) % 16 == 0, "parked rows must keep 16-byte alignment for the bulk copies");
+static_assert(kTileM % (8 * kMaxSplit) == 0, "every split owns whole 8-row groups");
 
 __device__ __forceinline__ uint32_t smemAddress(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint32_t clusterRank() {
+    uint32_t rank;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    return rank;
+}
+
+// Address of the same shared-memory offset in cluster CTA `rank`.
+__device__ __forceinline__ uint32_t clusterAddress(uint32_t address, uint32_t rank) {
+    uint32_t out;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(address), "r"(rank));
+    return out;
+}
+
+__device__ __forceinline__ void clusterArrive() {
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void clusterWait() {
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
 __device__ __forceinline__ void mbarInit(uint32_t bar, uint32_t count) {
@@ -97,16 +135,24 @@ __device__ __forceinline__ void tmaLoad3d(uint32_t dst, const CUtensorMap* map, 
         : "memory");
 }
 
+// Bulk copy of `bytes` from this CTA's shared memory into a peer's (cluster
+// addresses for the destination and its mbarrier).
+__device__ __forceinline__ void bulkToPeer(uint32_t dst, uint32_t src, uint32_t bytes, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(dst), "r"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+
 // UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
 __device__ __forceinline__ uint64_t smemDescriptor(uint32_t address) {
     return static_cast<uint64_t>((address >> 4) & 0x3FFFu) | (1ull << 16) | (64ull << 32) | (1ull << 46) |
            (2ull << 61);
 }
 
-// Instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128, N = kTileN.
+// Instruction descriptor: F16 x F16 -> F32, both K-major, M = 128, N = kTileN.
 constexpr uint32_t kInstrDescriptor =
-    (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(kTileN >> 3) << 17) |
-    (static_cast<uint32_t>(kTileM >> 4) << 24);
+    (1u << 4) | (static_cast<uint32_t>(kTileN >> 3) << 17) | (static_cast<uint32_t>(kTileM >> 4) << 24);
 
 __device__ __forceinline__ void ummaF16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
     asm volatile(
@@ -121,75 +167,123 @@ __device__ __forceinline__ void ummaCommit(uint32_t bar) {
                  : "memory");
 }
 
-__device__ __forceinline__ void tmemLoad16(uint32_t address, float (&v)[16]) {
-    uint32_t r[16];
+// Issues a 16-column TMEM load into raw registers; they hold the values only
+// after tmemWait, which takes them as operands so that no use moves above it.
+__device__ __forceinline__ void tmemLoad16(uint32_t address, uint32_t (&r)[16]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
         "%14, %15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(address));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// x = sum of kSplit bf16 pieces, largest first.
-template <typename T>
-__device__ __forceinline__ void splitValue(T x, __nv_bfloat16 (&piece)[kSplit]) {
-    T rest = x;
-#pragma unroll
-    for (int p = 0; p < kSplit; ++p) {
-        piece[p] = __float2bfloat16_rn(static_cast<float>(rest));
-        rest = rest - static_cast<T>(__bfloat162float(piece[p]));
-    }
+__device__ __forceinline__ void tmemWait(uint32_t (&a)[16], uint32_t (&b)[16]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7]), "+r"(a[8]), "+r"(a[9]), "+r"(a[10]), "+r"(a[11]), "+r"(a[12]), "+r"(a[13]), "+r"(a[14]), "+r"(a[15]), "+r"(b[0]), "+r"(b[1]), "+r"(b[2]), "+r"(b[3]), "+r"(b[4]), "+r"(b[5]), "+r"(b[6]), "+r"(b[7]), "+r"(b[8]), "+r"(b[9]), "+r"(b[10]), "+r"(b[11]), "+r"(b[12]), "+r"(b[13]), "+r"(b[14]), "+r"(b[15])
+                 :
+                 : "memory");
 }
 
-// Cross products of planes kept by the split (a-plane, b-plane), smallest order first.
-__device__ __forceinline__ void planePair(int product, int& pa, int& pb) {
-    if (kSplit == 2) {
-        const int a[3] = {1, 0, 0};
-        const int b[3] = {0, 1, 0};
-        pa = a[product];
-        pb = b[product];
-    } else {
-        const int a[6] = {2, 0, 1, 1, 0, 0};
-        const int b[6] = {0, 2, 1, 0, 1, 0};
-        pa = a[product];
-        pb = b[product];
-    }
+// 2^e as a double (|e| < 1000), built from its exponent field.
+__device__ __forceinline__ double pow2(int e) {
+    return __longlong_as_double(static_cast<long long>(1023 + e) << 52);
 }
-constexpr int kProducts = kSplit == 2 ? 3 : 6;
+
+// Smallest e with v <= 2^e for a positive finite v (0 otherwise).
+__device__ __forceinline__ int exponentOf(float v) {
+    if (!(v > 0.0f) || !isfinite(v)) return 0;
+    int e = 0;
+    const float m = frexpf(v, &e);  // v = m * 2^e, m in [0.5, 1)
+    return m == 0.5f ? e - 1 : e;
+}
+
+// Plane exponent of an output bounded by ref_max * gain.
+__device__ __forceinline__ int planeExponent(const unsigned* ref_max, float gain) {
+    return min(120, max(-120, exponentOf(__uint_as_float(*ref_max) * gain) - kPlaneTop));
+}
+
+constexpr float kLoShift = 2048.0f;  // 2^11: the lo plane's extra scale
+
+// (hi, lo) planes of v * 2^-e.
+__device__ __forceinline__ void splitScaled(float v, float inv_scale, __half& hi, __half& lo) {
+    const float y = v * inv_scale;
+    hi = __float2half_rn(y);
+    lo = __float2half_rn((y - __half2float(hi)) * kLoShift);
+}
+
+__device__ __forceinline__ uint32_t packHalves(__half a, __half b) {
+    return static_cast<uint32_t>(__half_as_ushort(a)) | (static_cast<uint32_t>(__half_as_ushort(b)) << 16);
+}
+
+// Eight consecutive values as two 16-byte plane stores (dst 16-byte aligned).
+__device__ __forceinline__ void storeSplit8(const float (&v)[8], float inv_scale, __half* hi_dst, __half* lo_dst) {
+    __half hi[8], lo[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) splitScaled(v[i], inv_scale, hi[i], lo[i]);
+    *reinterpret_cast<uint4*>(hi_dst) = make_uint4(packHalves(hi[0], hi[1]), packHalves(hi[2], hi[3]),
+                                                   packHalves(hi[4], hi[5]), packHalves(hi[6], hi[7]));
+    *reinterpret_cast<uint4*>(lo_dst) = make_uint4(packHalves(lo[0], lo[1]), packHalves(lo[2], lo[3]),
+                                                   packHalves(lo[4], lo[5]), packHalves(lo[6], lo[7]));
+}
+
+__device__ __forceinline__ double2 loadShared2(uint32_t address) {
+    double2 v;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(address));
+    return v;
+}
+
+__device__ __forceinline__ void storeShared(uint32_t address, float v) {
+    asm volatile("st.shared.f32 [%0], %1;" ::"r"(address), "f"(v) : "memory");
+}
+
+__device__ __forceinline__ float loadShared(uint32_t address) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(address) : "memory");
+    return v;
+}
+
+// Parseval weight of a DCT-II index: 1/2 for the DC term, 1 otherwise.
+__device__ __forceinline__ double parsevalWeight(int index) { return index == 0 ? 0.5 : 1.0; }
 
 __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_constant__ TcBatch batch) {
     const TcTask& t = batch.task[blockIdx.y];
+    const int ksplit = batch.ksplit;
     const int tiles_n = (t.n + kTileN - 1) / kTileN;
     const int tiles_m = (t.m + kTileM - 1) / kTileM;
-    if (static_cast<int>(blockIdx.x) >= tiles_m * tiles_n) return;
-    const int m0 = (blockIdx.x / tiles_n) * kTileM;
-    const int n0 = (blockIdx.x % tiles_n) * kTileN;
+    const int tile_index = static_cast<int>(blockIdx.x) / ksplit;
+    // The whole cluster shares the tile, so the whole cluster leaves together.
+    if (tile_index >= tiles_m * tiles_n) return;
+    const int split = static_cast<int>(clusterRank());
+    const int m0 = (tile_index / tiles_n) * kTileM;
+    const int n0 = (tile_index % tiles_n) * kTileN;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) TC_TRACE(51);
+    const int k_blocks_total = (t.k + kBlockK - 1) / kBlockK;
+    const int per_split = (k_blocks_total + ksplit - 1) / ksplit;
+    const int kb_begin = min(k_blocks_total, split * per_split);
+    const int k_blocks = min(k_blocks_total, kb_begin + per_split) - kb_begin;
+    const int rows_per = kTileM / ksplit;
+    const int row_begin = split * rows_per;
+    const uint32_t slice_bytes = static_cast<uint32_t>(rows_per * kParkPitch * 8);
 
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-    uint64_t* barriers = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(barriers + 2 * kStages + 4);
-    volatile int* failed = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    uint64_t* barriers = reinterpret_cast<uint64_t*>(smem + kBarrierOffset);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(barriers + 2 * kStages + 5);
     const uint32_t full0 = smemAddress(barriers);
     const uint32_t empty0 = smemAddress(barriers + kStages);
     const uint32_t partial0 = smemAddress(barriers + 2 * kStages);
     const uint32_t consumed0 = smemAddress(barriers + 2 * kStages + 2);
+    const uint32_t received = smemAddress(barriers + 2 * kStages + 4);
+    // In the idle ring after the K-loop: the parked FP64 rows [kTileM][kParkPitch] and the
+    // staged FP32 tile [kTileM][kTilePitch]; past the ring: the rows the peers send,
+    // [ksplit][rows_per][kParkPitch].
+    const uint32_t parked_s = smemAddress(smem);
+    const uint32_t staged_s = smemAddress(smem + kStagedOffset);
+    const uint32_t incoming_s = smemAddress(smem + kReceiveOffset);
 
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddress(tmem_slot)),
-                     "r"(kTmemColumns));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
     if (threadIdx.x == 32) {
-        *failed = 0;
         for (int s = 0; s < kStages; ++s) {
             mbarInit(full0 + 8 * s, 1);
             mbarInit(empty0 + 8 * s, 1);
@@ -198,20 +292,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
             mbarInit(partial0 + 8 * b, 1);
             mbarInit(consumed0 + 8 * b, 4);  // one arrival per epilogue warp
         }
+        // The rows the peers send; its phase completes once they have all landed.
+        mbarInit(received, 1);
+        mbarExpectTx(received, static_cast<uint32_t>(ksplit - 1) * slice_bytes);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = *tmem_slot;
-    const int k_blocks = (t.k + kBlockK - 1) / kBlockK;
-    double energy = 0.0;
-    if (threadIdx.x == 0) TC_TRACE(0);
+    clusterArrive();  // this CTA's barriers are initialised; peers wait for it before sending
 
     if (warp == 0) {
         if (lane == 0) {
-            // TMA producer.
+            // TMA producer (starts while warp 1 allocates TMEM).
             bool ok = true;
             int issued = 0;
             for (int kb = 0; kb < k_blocks && ok; ++kb) {
@@ -219,13 +311,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
                 if (kb >= kStages) ok = mbarWait(empty0 + 8 * s, ((kb / kStages) - 1) & 1, batch.error_flag);
                 if (!ok) break;
                 unsigned char* stage = smem + s * kStageBytes;
-                if (kb < 16) TC_TRACE(1 + kb);
+                const int k0 = (kb_begin + kb) * kBlockK;
                 mbarExpectTx(full0 + 8 * s, kStageBytes);
                 for (int p = 0; p < kSplit; ++p) {
-                    tmaLoad3d(smemAddress(stage + p * kTileM * kBlockK * 2), &t.map_a, full0 + 8 * s, kb * kBlockK,
-                              m0, p);
+                    tmaLoad3d(smemAddress(stage + p * kTileM * kBlockK * 2), &t.map_a, full0 + 8 * s, k0, m0, p);
                     tmaLoad3d(smemAddress(stage + kSplit * kTileM * kBlockK * 2 + p * kTileN * kBlockK * 2),
-                              &t.map_b, full0 + 8 * s, kb * kBlockK, n0, p);
+                              &t.map_b, full0 + 8 * s, k0, n0, p);
                 }
                 issued = kb + 1;
             }
@@ -236,7 +327,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
                 }
             }
         }
+        __syncwarp();
+        clusterWait();
     } else if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddress(tmem_slot)),
+                     "r"(kTmemColumns));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        asm volatile("bar.sync 2, 160;" ::: "memory");  // TMEM address -> epilogue warps
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tmem_slot);
         if (lane == 0) {
             // tcgen05.mma issuer: K-block kb accumulates into buffer kb % 2 from zero.
             for (int kb = 0; kb < k_blocks; ++kb) {
@@ -244,31 +344,34 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
                 const int buffer = kb & 1;
                 if (kb >= 2 && !mbarWait(consumed0 + 8 * buffer, ((kb >> 1) - 1) & 1, batch.error_flag)) break;
                 if (!mbarWait(full0 + 8 * s, (kb / kStages) & 1, batch.error_flag)) break;
-                if (kb < 16) TC_TRACE(17 + kb);
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t stage = smemAddress(smem + s * kStageBytes);
                 const uint32_t a_base = stage;
                 const uint32_t b_base = stage + kSplit * kTileM * kBlockK * 2;
-                const uint32_t accumulator = tmem + static_cast<uint32_t>(buffer * kTileN);
+                const uint32_t main_acc = tmem + static_cast<uint32_t>(buffer * 2 * kTileN);
+                const uint32_t corr_acc = main_acc + kTileN;
 #pragma unroll
                 for (int kk = 0; kk < kBlockK / 16; ++kk) {
-#pragma unroll
-                    for (int product = 0; product < kProducts; ++product) {
-                        int pa, pb;
-                        planePair(product, pa, pb);
-                        const uint64_t da = smemDescriptor(a_base + pa * kTileM * kBlockK * 2 + kk * 32);
-                        const uint64_t db = smemDescriptor(b_base + pb * kTileN * kBlockK * 2 + kk * 32);
-                        ummaF16(accumulator, da, db, (kk > 0 || product > 0) ? 1u : 0u);
-                    }
+                    const uint64_t a_hi = smemDescriptor(a_base + kk * 32);
+                    const uint64_t a_lo = smemDescriptor(a_base + kTileM * kBlockK * 2 + kk * 32);
+                    const uint64_t b_hi = smemDescriptor(b_base + kk * 32);
+                    const uint64_t b_lo = smemDescriptor(b_base + kTileN * kBlockK * 2 + kk * 32);
+                    ummaF16(corr_acc, a_hi, b_lo, kk > 0 ? 1u : 0u);
+                    ummaF16(corr_acc, a_lo, b_hi, 1u);
+                    ummaF16(main_acc, a_hi, b_hi, kk > 0 ? 1u : 0u);
                 }
                 ummaCommit(empty0 + 8 * s);
                 ummaCommit(partial0 + 8 * buffer);
             }
         }
+        __syncwarp();
+        clusterWait();
     } else {
-        // Epilogue warps: FP64 sum of the K-block partials, then the fused output.
+        // Epilogue warps: FP64 sum of this split's K-block partials, parked in shared memory.
+        asm volatile("bar.sync 2, 160;" ::: "memory");
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tmem_slot);
         const int quarter = warp & 3;
-        const int row = m0 + quarter * 32 + lane;
         const uint32_t lane_base = tmem + (static_cast<uint32_t>(quarter * 32) << 16);
         double acc[kTileN];
 #pragma unroll
@@ -278,103 +381,196 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
             const int buffer = kb & 1;
             ok = __all_sync(0xffffffffu, mbarWait(partial0 + 8 * buffer, (kb >> 1) & 1, batch.error_flag) ? 1 : 0) != 0;
             if (!ok) break;
-            if (warp == 2 && lane == 0 && kb < 16) TC_TRACE(33 + kb);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
             for (int c0 = 0; c0 < kTileN; c0 += 16) {
-                float v[16];
-                tmemLoad16(lane_base + static_cast<uint32_t>(buffer * kTileN + c0), v);
+                uint32_t main_part[16], corr_part[16];
+                tmemLoad16(lane_base + static_cast<uint32_t>(buffer * 2 * kTileN + c0), main_part);
+                tmemLoad16(lane_base + static_cast<uint32_t>(buffer * 2 * kTileN + kTileN + c0), corr_part);
+                tmemWait(main_part, corr_part);
 #pragma unroll
-                for (int j = 0; j < 16; ++j) acc[c0 + j] += static_cast<double>(v[j]);
+                for (int j = 0; j < 16; ++j) {
+                    acc[c0 + j] += static_cast<double>(__uint_as_float(main_part[j])) +
+                                   static_cast<double>(__uint_as_float(corr_part[j])) *
+                                       (1.0 / static_cast<double>(kLoShift));
+                }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbarArrive(consumed0 + 8 * buffer);
         }
-        // Stage the tile in shared memory (the ring is idle once the last partial has
-        // been read).  FP32 keeps 24 bits, as many as the three bf16 output planes hold.
-        (void)row;
-        float* tile = reinterpret_cast<float*>(smem);
+        // The ring is idle once the last partial has been read (or was never used).
         const int local_row = quarter * 32 + lane;
-        if (ok) {
+        double* row = reinterpret_cast<double*>(smem) + local_row * kParkPitch;
 #pragma unroll
-            for (int j = 0; j < kTileN; ++j) tile[local_row * kTilePitch + j] = static_cast<float>(acc[j]);
-        } else {
-            *failed = 1;
+        for (int j = 0; j < kTileN; j += 2) *reinterpret_cast<double2*>(row + j) = make_double2(acc[j], acc[j + 1]);
+        row[kTileN] = ok ? 0.0 : 1.0;  // failure flag travels with the rows
+        row[kTileN + 1] = 0.0;
+        asm volatile("bar.sync 1, 128;" ::: "memory");  // the epilogue warps' rows are all parked
+        clusterWait();
+        if (threadIdx.x == 64 && ksplit > 1) {
+            // Send every peer the rows it owns; wait until the copies have read them.
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            for (int owner = 0; owner < ksplit; ++owner) {
+                if (owner == split) continue;
+                const uint32_t src = parked_s + static_cast<uint32_t>(owner * rows_per * kParkPitch * 8);
+                const uint32_t dst =
+                    clusterAddress(incoming_s + static_cast<uint32_t>(split * rows_per * kParkPitch * 8), owner);
+                bulkToPeer(dst, src, slice_bytes, clusterAddress(received, owner));
+            }
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+            asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
         }
     }
-    __syncwarp();
     __syncthreads();
-    float* tile = reinterpret_cast<float*>(smem);  // [kTileM][kTilePitch], staged by the epilogue warps
-    const bool tile_ok = *failed == 0 && k_blocks > 0;
-    // Output passes with all six warps, four independent elements per thread; a
-    // warp's lanes run along the contiguous dimension of the destination.
-    if (tile_ok && t.mode != kTcSplitTransposed) {
-        // Row-major pass: lane <-> column, four rows per thread.
-        for (int g = threadIdx.x; g < kTileM * kTileN / 4; g += kTcThreads) {
-            const int c = g % kTileN;
-            const int r0 = (g / kTileN) * 4;
-            const int gcol = n0 + c;
-            if (gcol >= t.n) continue;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int r = r0 + i;
-                const int grow = m0 + r;
-                if (grow >= t.m) continue;
-                float value = tile[r * kTilePitch + c];
-                if (t.mode == kTcSpectral) {
-                    const float phi = value * t.scale[static_cast<size_t>(grow) * t.n + gcol];
-                    energy += static_cast<double>(phi) * static_cast<double>(value) *
-                              static_cast<double>(t.weight_r[grow] * t.weight_c[gcol]);
-                    value = phi;
-                    tile[r * kTilePitch + c] = phi;
-                }
-                if (t.mode == kTcField) {
-                    t.out_f[static_cast<size_t>(grow) * t.out_f_ld + static_cast<size_t>(gcol) * t.out_f_step] = value;
-                    continue;
-                }
-                __nv_bfloat16 piece[kSplit];
-                splitValue(value, piece);
-                __nv_bfloat16* out = t.out + static_cast<size_t>(grow) * t.out_ld + gcol;
-#pragma unroll
-                for (int p = 0; p < kSplit; ++p) out[static_cast<size_t>(p) * t.out_plane] = piece[p];
-            }
-        }
+
+    bool tile_ok = mbarWait(received, 0, batch.error_flag);
+    tile_ok = __syncthreads_and(tile_ok ? 1 : 0) != 0;
+    for (int s = 0; s < ksplit && tile_ok; ++s) {
+        const uint32_t piece = s == split ? parked_s + static_cast<uint32_t>(row_begin * kParkPitch * 8)
+                                          : incoming_s + static_cast<uint32_t>(s * rows_per * kParkPitch * 8);
+        tile_ok = loadShared2(piece + kTileN * 8).x == 0.0;
     }
-    if (tile_ok && (t.mode == kTcSplitTransposed || t.mode == kTcSpectral)) {
-        if (t.mode == kTcSpectral) __syncthreads();  // the row-major pass rewrote the tile with phi
-        // Transposed pass: lane <-> row, four columns per thread.
-        for (int g = threadIdx.x; g < kTileM * kTileN / 4; g += kTcThreads) {
-            const int r = g % kTileM;
-            const int c0 = (g / kTileM) * 4;
+    if (!tile_ok && threadIdx.x == 0) atomicExch(batch.error_flag, 1);
+
+    // Fused sum and output, one (row, eight columns) unit per thread and pass: the
+    // fixed-order sum over the splits, the unscaling, then the row-major output
+    // (planes, field, or spectral divide + planes) and the staged copy for the
+    // transposed pass.  A warp's lanes run along the columns.
+    const int exp_b = *t.exp_b;
+    const int exp_a = t.exp_a != nullptr ? *t.exp_a : 0;
+    const bool split_out = t.mode != kTcField;
+    const int out_exp = split_out ? planeExponent(t.ref_max, t.gain) : 0;
+    const float inv_scale = static_cast<float>(pow2(-out_exp));
+    const bool staging = t.mode == kTcSplitTransposed || t.mode == kTcSpectral;
+    double energy = 0.0;
+    float magnitude = 0.0f;
+    if (tile_ok) {
+        for (int u = threadIdx.x; u < rows_per * (kTileN / 8); u += kTcThreads) {
+            const int r_local = u / (kTileN / 8);
+            const int c0 = (u % (kTileN / 8)) * 8;
+            const int r = row_begin + r_local;
             const int grow = m0 + r;
-            if (grow >= t.m) continue;
+            const int gcol0 = n0 + c0;
+            const bool row_in = grow < t.m;
+            const int valid = row_in ? max(0, min(8, t.n - gcol0)) : 0;
+            // Global inputs first, so their latency overlaps the shared-memory sum.
+            const int shift = exp_b + (t.row_exp_a != nullptr ? __ldg(t.row_exp_a + min(grow, t.m - 1)) : exp_a);
+            float sc[8];
+            if (t.mode == kTcSpectral) {
+                const float* scale = t.scale + static_cast<size_t>(min(grow, t.m - 1)) * t.n + gcol0;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int c = c0 + i;
-                const int gcol = n0 + c;
-                if (gcol >= t.n) continue;
-                __nv_bfloat16 piece[kSplit];
-                splitValue(tile[r * kTilePitch + c], piece);
-                __nv_bfloat16* out = t.out_t + static_cast<size_t>(gcol) * t.out_t_ld + grow;
+                for (int i = 0; i < 8; ++i) sc[i] = i < valid ? __ldg(scale + i) : 0.0f;
+            }
+            double sum[8];
 #pragma unroll
-                for (int p = 0; p < kSplit; ++p) out[static_cast<size_t>(p) * t.out_t_plane] = piece[p];
+            for (int i = 0; i < 8; ++i) sum[i] = 0.0;
+            for (int s = 0; s < ksplit; ++s) {
+                const uint32_t piece =
+                    (s == split ? parked_s + static_cast<uint32_t>((r * kParkPitch + c0) * 8)
+                                : incoming_s + static_cast<uint32_t>(((s * rows_per + r_local) * kParkPitch + c0) * 8));
+#pragma unroll
+                for (int i = 0; i < 8; i += 2) {
+                    const double2 p = loadShared2(piece + i * 8);
+                    sum[i] += p.x;
+                    sum[i + 1] += p.y;
+                }
+            }
+            const double unscale = pow2(shift);
+            float v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = static_cast<float>(sum[i] * unscale);
+            if (t.mode == kTcSpectral) {
+                const double wr = parsevalWeight(grow);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const float phi = v[i] * sc[i];
+                    if (i < valid) {
+                        energy += static_cast<double>(phi) * static_cast<double>(v[i]) * wr * parsevalWeight(gcol0 + i);
+                    }
+                    v[i] = phi;
+                }
+            }
+            if (staging) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) storeShared(staged_s + static_cast<uint32_t>((r * kTilePitch + c0 + i) * 4), v[i]);
+            }
+            if (valid == 0) continue;
+            if (t.mode == kTcField) {
+                float* dst = t.out_f + static_cast<size_t>(grow) * t.out_f_ld + static_cast<size_t>(gcol0) * t.out_f_step;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    if (i < valid) dst[static_cast<size_t>(i) * t.out_f_step] = v[i];
+                }
+                continue;
+            }
+            if (t.mode == kTcSplitTransposed) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    if (i < valid) magnitude = fmaxf(magnitude, fabsf(v[i]));
+                }
+                continue;
+            }
+            // kTcSplit and kTcSpectral: row-major planes.
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (i < valid) magnitude = fmaxf(magnitude, fabsf(v[i]));
+            }
+            __half* hi = t.out + static_cast<size_t>(grow) * t.out_ld + gcol0;
+            if (valid == 8) {
+                storeSplit8(v, inv_scale, hi, hi + t.out_plane);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    if (i < valid) splitScaled(v[i], inv_scale, hi[i], hi[i + t.out_plane]);
+                }
             }
         }
     }
-    if (threadIdx.x == 64) TC_TRACE(49);
-    if (t.mode == kTcSpectral && t.energy_partials != nullptr) {
-        double values[1] = {energy};
-        const bool is_max[1] = {false};
-        blockReduce<1>(values, is_max);
-        if (threadIdx.x == 0) t.energy_partials[blockIdx.x] = values[0];
+    if (staging) {
+        __syncthreads();
+        // Transposed pass: eight consecutive rows of one column per thread.
+        const int groups = rows_per / 8;
+        for (int g = threadIdx.x; g < groups * kTileN && tile_ok; g += kTcThreads) {
+            const int r0 = row_begin + (g % groups) * 8;
+            const int c = g / groups;
+            const int grow0 = m0 + r0;
+            const int gcol = n0 + c;
+            if (gcol >= t.n || grow0 >= t.m) continue;
+            const int valid = min(8, t.m - grow0);
+            float v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = loadShared(staged_s + static_cast<uint32_t>(((r0 + i) * kTilePitch + c) * 4));
+            __half* hi = t.out_t + static_cast<size_t>(gcol) * t.out_t_ld + grow0;
+            if (valid == 8) {
+                storeSplit8(v, inv_scale, hi, hi + t.out_t_plane);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    if (i < valid) splitScaled(v[i], inv_scale, hi[i], hi[i + t.out_t_plane]);
+                }
+            }
+        }
+    }
+    if (split_out) {
+        double values[2] = {energy, static_cast<double>(magnitude)};
+        const bool is_max[2] = {false, true};
+        blockReduce<2>(values, is_max);
+        if (threadIdx.x == 0) {
+            if (t.mode == kTcSpectral && t.energy_partials != nullptr) t.energy_partials[blockIdx.x] = values[0];
+            if (t.out_max != nullptr) atomicMax(t.out_max, __float_as_uint(static_cast<float>(values[1])));
+            if (blockIdx.x == 0) {
+                if (t.out_exp != nullptr) *t.out_exp = out_exp;
+                if (t.clear != nullptr) *t.clear = 0u;
+            }
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) {
+    if (warp == 1) {
+        const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tmem_slot);
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemColumns));
     }
-    if (threadIdx.x == 0) TC_TRACE(50);
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
@@ -396,22 +592,65 @@ EncodeTiled encoder() {
     return fn;
 }
 
-__global__ void splitSourceKernel(const float* source, int rows, int cols, __nv_bfloat16* out, int ld,
-                                  size_t plane) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= rows * cols) return;
-    const int r = i / cols;
-    const int c = i % cols;
-    __nv_bfloat16 piece[kSplit];
-    splitValue(source[i], piece);
-    __nv_bfloat16* dst = out + static_cast<size_t>(r) * ld + c;
+// One warp per source row: the row's exponent from its maximum, then its planes.
+__global__ void splitSourceKernel(const float* source, int rows, int cols, __half* out, int ld, size_t plane,
+                                  int* row_exp, TcScales* scales) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        scales->max_x = 0u;
+        scales->max_phi = 0u;
+    }
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= rows) return;
+    const float* src = source + static_cast<size_t>(row) * cols;
+    float top = 0.0f;
+    for (int c = lane; c < cols; c += 32) top = fmaxf(top, fabsf(src[c]));
 #pragma unroll
-    for (int p = 0; p < kSplit; ++p) dst[static_cast<size_t>(p) * plane] = piece[p];
+    for (int offset = 16; offset > 0; offset >>= 1) top = fmaxf(top, __shfl_xor_sync(0xffffffffu, top, offset));
+    const int e = exponentOf(top) - kPlaneTop;
+    if (lane == 0) {
+        row_exp[row] = e;
+        atomicMax(&scales->max_source, __float_as_uint(top));
+    }
+    const float inv_scale = static_cast<float>(pow2(-e));
+    __half* dst = out + static_cast<size_t>(row) * ld;
+    for (int c = lane; c < cols; c += 32) splitScaled(src[c], inv_scale, dst[c], dst[c + plane]);
+}
+
+void configureKernel() {
+    static std::once_flag once;
+    static cudaError_t attribute = cudaSuccess;
+    std::call_once(once, [] {
+        attribute = cudaFuncSetAttribute(tcGemmKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    });
+    checkCuda(attribute, "Configure the tcgen05 contraction kernel");
+}
+
+int batchTiles(const TcBatch& batch, int task_count) {
+    int tiles = 0;
+    for (int i = 0; i < task_count; ++i) {
+        const TcTask& t = batch.task[i];
+        tiles = std::max(tiles, ((t.m + kTileM - 1) / kTileM) * ((t.n + kTileN - 1) / kTileN));
+    }
+    return tiles;
+}
+
+cudaLaunchConfig_t launchConfig(dim3 grid, int ksplit, cudaStream_t stream, cudaLaunchAttribute* attribute) {
+    cudaLaunchConfig_t config{};
+    config.gridDim = grid;
+    config.blockDim = dim3(kTcThreads);
+    config.dynamicSmemBytes = kSmemBytes;
+    config.stream = stream;
+    attribute->id = cudaLaunchAttributeClusterDimension;
+    attribute->val.clusterDim.x = static_cast<unsigned>(ksplit);
+    attribute->val.clusterDim.y = 1;
+    attribute->val.clusterDim.z = 1;
+    config.attrs = attribute;
+    config.numAttrs = 1;
+    return config;
 }
 
 }  // namespace
-
-int tcSmemBytes() { return kSmemBytes; }
 
 void makeOperandMap(CUtensorMap* map, const SplitMatrix& m, int box_rows) {
     require(m.ld % kBlockK == 0 && m.rows > 0 && m.data != nullptr, "Split operand layout is invalid.");
@@ -422,7 +661,7 @@ void makeOperandMap(CUtensorMap* map, const SplitMatrix& m, int box_rows) {
     const cuuint32_t box[3] = {static_cast<cuuint32_t>(kBlockK), static_cast<cuuint32_t>(box_rows), 1};
     const cuuint32_t element_strides[3] = {1, 1, 1};
     const CUresult result =
-        encoder()(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, m.data, dims, strides, box, element_strides,
+        encoder()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, m.data, dims, strides, box, element_strides,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (result != CUDA_SUCCESS) {
@@ -430,40 +669,73 @@ void makeOperandMap(CUtensorMap* map, const SplitMatrix& m, int box_rows) {
     }
 }
 
-int tcTiles(int m, int n) { return ((m + kTileM - 1) / kTileM) * ((n + kTileN - 1) / kTileN); }
-
-void launchTcGemm(const TcBatch& batch, int task_count, cudaStream_t stream) {
-    static std::once_flag once;
-    static cudaError_t attribute = cudaSuccess;
-    std::call_once(once, [] {
-        attribute = cudaFuncSetAttribute(tcGemmKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-    });
-    checkCuda(attribute, "Configure the tcgen05 contraction kernel");
-    int blocks = 0;
-    for (int i = 0; i < task_count; ++i) blocks = std::max(blocks, tcTiles(batch.task[i].m, batch.task[i].n));
-    tcGemmKernel<<<dim3(blocks, task_count), kTcThreads, kSmemBytes, stream>>>(batch);
-}
-
-// Host split of FP64 values into kSplit bf16 planes (basis matrices).
-void splitHost(const std::vector<double>& values, int rows, int cols, int ld, std::vector<__nv_bfloat16>& planes) {
-    planes.assign(static_cast<size_t>(kSplit) * rows * ld, __float2bfloat16_rn(0.0f));
-    for (int r = 0; r < rows; ++r) {
-        for (int c = 0; c < cols; ++c) {
-            double rest = values[static_cast<size_t>(r) * cols + c];
-            for (int p = 0; p < kSplit; ++p) {
-                const __nv_bfloat16 piece = __float2bfloat16_rn(static_cast<float>(rest));
-                planes[static_cast<size_t>(p) * rows * ld + static_cast<size_t>(r) * ld + c] = piece;
-                rest -= static_cast<double>(__bfloat162float(piece));
-            }
+void tcPlan(TcBatch& batch, int task_count) {
+    configureKernel();
+    const int tiles = batchTiles(batch, task_count) * task_count;
+    int k_blocks = 0;
+    for (int i = 0; i < task_count; ++i) {
+        const int kb = (batch.task[i].k + kBlockK - 1) / kBlockK;
+        k_blocks = i == 0 ? kb : std::min(k_blocks, kb);
+    }
+    batch.ksplit = 1;
+    for (int ksplit = 2; ksplit <= kMaxSplit && ksplit <= k_blocks; ksplit *= 2) {
+        cudaLaunchAttribute attribute{};
+        cudaLaunchConfig_t config =
+            launchConfig(dim3(static_cast<unsigned>(tiles * ksplit)), ksplit, nullptr, &attribute);
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, tcGemmKernel, &config) != cudaSuccess) {
+            (void)cudaGetLastError();
+            break;
         }
+        if (tiles > clusters) break;  // the split would no longer run in one wave
+        batch.ksplit = ksplit;
     }
 }
 
-void launchSplitSource(const float* source, const SplitMatrix& out, int cols, cudaStream_t stream) {
-    const int count = out.rows * cols;
-    if (count <= 0) return;
-    splitSourceKernel<<<ceilDiv(count, kThreads), kThreads, 0, stream>>>(
-        source, out.rows, cols, out.data, out.ld, static_cast<size_t>(out.rows) * out.ld);
+int tcBlocks(const TcBatch& batch, int task_count) {
+    (void)task_count;
+    return batchTiles(batch, task_count) * batch.ksplit;
+}
+
+void launchTcGemm(const TcBatch& batch, int task_count, cudaStream_t stream) {
+    configureKernel();
+    require(batch.ksplit >= 1 && batch.ksplit <= kMaxSplit && (batch.ksplit & (batch.ksplit - 1)) == 0,
+            "Contraction K split must be a power of two up to 8.");
+    cudaLaunchAttribute attribute{};
+    const cudaLaunchConfig_t config =
+        launchConfig(dim3(static_cast<unsigned>(tcBlocks(batch, task_count)), static_cast<unsigned>(task_count)),
+                     batch.ksplit, stream, &attribute);
+    checkCuda(cudaLaunchKernelEx(&config, tcGemmKernel, batch), "Launch the tcgen05 contraction kernel");
+}
+
+int splitHost(const std::vector<double>& values, int rows, int cols, int ld, std::vector<__half>& planes) {
+    double top = 0.0;
+    for (double v : values) top = std::max(top, std::fabs(v));
+    int e = 0;
+    if (top > 0.0) {
+        const double m = std::frexp(top, &e);
+        if (m == 0.5) e -= 1;
+    }
+    e -= kPlaneTop;
+    planes.assign(static_cast<size_t>(kSplit) * rows * ld, __float2half_rn(0.0f));
+    for (int r = 0; r < rows; ++r) {
+        for (int c = 0; c < cols; ++c) {
+            const double y = std::ldexp(values[static_cast<size_t>(r) * cols + c], -e);
+            const __half hi = __double2half(y);
+            const __half lo = __double2half((y - static_cast<double>(__half2float(hi))) * 2048.0);
+            planes[static_cast<size_t>(r) * ld + c] = hi;
+            planes[static_cast<size_t>(rows) * ld + static_cast<size_t>(r) * ld + c] = lo;
+        }
+    }
+    return e;
+}
+
+void launchSplitSource(const float* source, const SplitMatrix& out, int cols, int* row_exp, TcScales* scales,
+                       cudaStream_t stream) {
+    if (out.rows <= 0) return;
+    const int rows_per_block = kThreads / 32;
+    splitSourceKernel<<<ceilDiv(out.rows, rows_per_block), kThreads, 0, stream>>>(
+        source, out.rows, cols, out.data, out.ld, out.plane(), row_exp, scales);
 }
 
 }  // namespace mpgp

@@ -2,26 +2,28 @@
 #pragma once
 
 #include <cuda.h>
-#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <vector>
 
 namespace mpgp {
 
-#ifndef MPGP_SPLIT_PLANES
-#define MPGP_SPLIT_PLANES 3
-#endif
-constexpr int kSplit = MPGP_SPLIT_PLANES;  // bf16 planes per operand (x = hi + mid + lo)
-constexpr int kTileM = 128;  // UMMA M = TMEM lanes
-constexpr int kTileN = 64;   // UMMA N = accumulator columns per CTA
-constexpr int kBlockK = 64;  // bf16 elements per 128-byte swizzled row
+// Operands are stored as two fp16 planes of a power-of-two scaled value:
+// x * 2^-e = hi + 2^-11 lo, |x * 2^-e| <= 2^kPlaneTop, hi = fp16(x * 2^-e),
+// lo = fp16((x * 2^-e - hi) * 2^11).
+constexpr int kSplit = 2;
+constexpr int kPlaneTop = 14;  // log2 of the largest scaled magnitude (fp16 max is 65504)
+constexpr int kTileM = 128;    // UMMA M = TMEM lanes
+constexpr int kTileN = 64;     // UMMA N = accumulator columns per CTA
+constexpr int kBlockK = 64;    // fp16 elements per 128-byte swizzled row
 constexpr int kStages = 3;
+constexpr int kMaxSplit = 8;   // largest K split (cluster size)
 
-// A row-major matrix stored as kSplit bf16 planes; ld is a multiple of kBlockK
+// A row-major matrix stored as kSplit fp16 planes; ld is a multiple of kBlockK
 // and the padding columns are zero.
 struct SplitMatrix {
-    __nv_bfloat16* data = nullptr;
+    __half* data = nullptr;
     int rows = 0;
     int cols = 0;
     int ld = 0;
@@ -38,16 +40,40 @@ enum TcMode : int {
     kTcField = 3,            // C -> FP32 (strided)
 };
 
+// Device-resident scale bookkeeping of one field solve.  Magnitudes are the bit
+// patterns of non-negative floats (ordered like the floats, so atomicMax works).
+struct TcScales {
+    unsigned max_source;  // max |S|            (split kernel; cleared by the spectral contraction)
+    unsigned max_x;       // max |S Cx^T|       (first contraction; cleared by the split kernel)
+    unsigned max_phi;     // max |phi_hat|      (spectral contraction; cleared by the split kernel)
+    int exp_x;            // plane exponents written by the producing contraction
+    int exp_phi;
+    int exp_t;
+    int exp_u;
+    int exp_basis[8];     // fixed exponents of the basis operands
+};
+
 // C (m x n) = A (m x k) * B (n x k)^T with A and B K-major split operands.
+// A value of C is sum * 2^(exp_a + exp_b [+ row_exp_a[row]]).
 struct alignas(64) TcTask {
     CUtensorMap map_a;
     CUtensorMap map_b;
     int m, n, k;
     int mode;
-    __nv_bfloat16* out;
+    const int* exp_a;      // exponent of A, or null when row_exp_a is given
+    const int* row_exp_a;  // per-row exponents of A
+    const int* exp_b;
+    // Output planes: exponent = exponent_of(ref_max * gain) - kPlaneTop, published
+    // in out_exp by block 0; the actual max |C| is folded into out_max.
+    const unsigned* ref_max;
+    float gain;
+    int* out_exp;
+    unsigned* out_max;
+    unsigned* clear;  // block 0 zeroes this magnitude (chain bookkeeping), or null
+    __half* out;
     int out_ld;
     size_t out_plane;
-    __nv_bfloat16* out_t;
+    __half* out_t;
     int out_t_ld;
     size_t out_t_plane;
     float* out_f;
@@ -56,20 +82,29 @@ struct alignas(64) TcTask {
     const float* scale;
     const float* weight_r;
     const float* weight_c;
-    double* energy_partials;
+    double* energy_partials;  // one per CTA of the launch (tcBlocks)
 };
 
+// One launch: up to two independent tasks (grid.y), each output tile computed by
+// a cluster of `ksplit` CTAs that split its K range (tcPlan chooses ksplit).
 struct alignas(64) TcBatch {
     TcTask task[2];
     int* error_flag;
-    unsigned long long* trace;  // development timeline of CTA (0, 0), or null
+    int ksplit;
 };
 
 void makeOperandMap(CUtensorMap* map, const SplitMatrix& m, int box_rows);
+// Chooses the K split of a batch: the largest cluster size whose clusters all fit
+// on the GPU at once.  Call after the tasks are filled in.
+void tcPlan(TcBatch& batch, int task_count);
+// CTAs of one task row of the launch (the count of energy partials a spectral task writes).
+int tcBlocks(const TcBatch& batch, int task_count);
 void launchTcGemm(const TcBatch& batch, int task_count, cudaStream_t stream);
-int tcTiles(int m, int n);
-int tcSmemBytes();
-void splitHost(const std::vector<double>& values, int rows, int cols, int ld, std::vector<__nv_bfloat16>& planes);
-void launchSplitSource(const float* source, const SplitMatrix& out, int cols, cudaStream_t stream);
+// Host split of FP64 values into the planes of x * 2^-exponent; returns the exponent.
+int splitHost(const std::vector<double>& values, int rows, int cols, int ld, std::vector<__half>& planes);
+// Splits the FP32 source S with one exponent per row (row_exp), folds max |S| into
+// scales->max_source and clears the magnitudes the forward contractions fold into.
+void launchSplitSource(const float* source, const SplitMatrix& out, int cols, int* row_exp, TcScales* scales,
+                       cudaStream_t stream);
 
 }  // namespace mpgp

@@ -138,45 +138,75 @@ __global__ void __launch_bounds__(kThreads) scatterKernel(ScatterArgs a) {
     }
 }
 
-__global__ void __launch_bounds__(kThreads) metricsKernel(MetricsArgs a) {
-    const double t = a.target_density;
-    const double unit = a.bin_area * kFixedUnit;
-    const double capacity = t * a.bin_area;
-    // Mean of the density deviation from the exact layer totals.
-    const double movable_sum = static_cast<double>(static_cast<long long>(a.totals[0])) * unit;
-    const double macro_sum = static_cast<double>(static_cast<long long>(a.totals[1])) * unit;
-    const double filler_sum = static_cast<double>(static_cast<long long>(a.totals[2])) * unit;
-    const double charge_total = movable_sum + t * (a.static_fixed_sum + macro_sum + a.static_dark_sum + filler_sum);
-    const double mean = charge_total / (a.bin_area * static_cast<double>(a.bin_count)) - t;
-
-    double v[9] = {0, 0, 0, 0, 0, 0, 0, -1.0e308, -1.0e308};
-    const size_t bins = static_cast<size_t>(a.bin_count);
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < a.bin_count; b += gridDim.x * blockDim.x) {
-        const long long qm = static_cast<long long>(a.layers[b]);
-        const long long qc = static_cast<long long>(a.layers[bins + b]);
-        const long long qf = static_cast<long long>(a.layers[2 * bins + b]);
-        a.layers[b] = 0ULL;
-        a.layers[bins + b] = 0ULL;
-        a.layers[2 * bins + b] = 0ULL;
-        const double movable = static_cast<double>(qm) * unit;
-        const double macro = static_cast<double>(qc) * unit;
-        const double filler = static_cast<double>(qf) * unit;
-        const double fixed = a.fixed[b];
-        const double dark = a.dark[b];
-        const double without = movable + t * (fixed + macro + dark + 0.0);  // DensityBin::chargeArea(t, false)
-        const double with = movable + t * (fixed + macro + dark + filler);  // DensityBin::chargeArea(t, true)
-        const double density_with = with / a.bin_area;
-        const double density_without = without / a.bin_area;
+// One bin's metric terms (DensityBin::chargeArea / normalizationArea, Metrics.hpp:25-35).
+struct BinTerms {
+    double t, unit, capacity, inv_area, mean;
+    __device__ void add(unsigned long long qm, unsigned long long qc, unsigned long long qf, double static_charge,
+                        double (&v)[9], float& source) const {
+        const double movable = static_cast<double>(static_cast<long long>(qm)) * unit;
+        const double macro = static_cast<double>(static_cast<long long>(qc)) * unit;
+        const double filler = static_cast<double>(static_cast<long long>(qf)) * unit;
+        const double without = movable + t * macro + static_charge;  // chargeArea(t, false)
+        const double with = without + t * filler;                    // chargeArea(t, true)
+        const double density_with = with * inv_area;
+        const double density_without = without * inv_area;
         v[0] += fmax(0.0, with - capacity);
         v[1] += fmax(0.0, without - capacity);
         v[2] += with;
         v[3] += without;
-        v[4] += movable + t * macro;  // DensityBin::normalizationArea
+        v[4] += movable + t * macro;  // normalizationArea
         v[5] += density_with;
         v[6] += density_without;
         v[7] = fmax(v[7], density_with);
         v[8] = fmax(v[8], density_without);
-        a.source[b] = static_cast<float>((density_with - t) - mean);
+        source = static_cast<float>((density_with - t) - mean);
+    }
+};
+
+__global__ void __launch_bounds__(kThreads) metricsKernel(MetricsArgs a) {
+    BinTerms terms;
+    terms.t = a.target_density;
+    terms.unit = a.bin_area * kFixedUnit;
+    terms.capacity = terms.t * a.bin_area;
+    terms.inv_area = 1.0 / a.bin_area;
+    // Mean of the density deviation from the exact layer totals.
+    const double movable_sum = static_cast<double>(static_cast<long long>(a.totals[0])) * terms.unit;
+    const double macro_sum = static_cast<double>(static_cast<long long>(a.totals[1])) * terms.unit;
+    const double filler_sum = static_cast<double>(static_cast<long long>(a.totals[2])) * terms.unit;
+    const double charge_total =
+        movable_sum + terms.t * (a.static_fixed_sum + macro_sum + a.static_dark_sum + filler_sum);
+    terms.mean = charge_total / (a.bin_area * static_cast<double>(a.bin_count)) - terms.t;
+
+    double v[9] = {0, 0, 0, 0, 0, 0, 0, -1.0e308, -1.0e308};
+    const int bins = a.bin_count;
+    unsigned long long* qm = a.layers;
+    unsigned long long* qc = a.layers + bins;
+    unsigned long long* qf = a.layers + 2 * static_cast<size_t>(bins);
+    const int stride = gridDim.x * blockDim.x;
+    if ((bins & 1) == 0) {
+        // Two bins per step: 16-byte loads of every layer, stores of zeros and the source pair.
+        for (int pair = blockIdx.x * blockDim.x + threadIdx.x; pair < bins / 2; pair += stride) {
+            const ulonglong2 m = reinterpret_cast<const ulonglong2*>(qm)[pair];
+            const ulonglong2 c = reinterpret_cast<const ulonglong2*>(qc)[pair];
+            const ulonglong2 f = reinterpret_cast<const ulonglong2*>(qf)[pair];
+            const double2 st = reinterpret_cast<const double2*>(a.static_charge)[pair];
+            const ulonglong2 zero = make_ulonglong2(0ULL, 0ULL);
+            reinterpret_cast<ulonglong2*>(qm)[pair] = zero;
+            reinterpret_cast<ulonglong2*>(qc)[pair] = zero;
+            reinterpret_cast<ulonglong2*>(qf)[pair] = zero;
+            float2 out;
+            terms.add(m.x, c.x, f.x, st.x, v, out.x);
+            terms.add(m.y, c.y, f.y, st.y, v, out.y);
+            reinterpret_cast<float2*>(a.source)[pair] = out;
+        }
+    } else {
+        for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < bins; b += stride) {
+            const unsigned long long m = qm[b], c = qc[b], f = qf[b];
+            qm[b] = 0ULL;
+            qc[b] = 0ULL;
+            qf[b] = 0ULL;
+            terms.add(m, c, f, a.static_charge[b], v, a.source[b]);
+        }
     }
     const bool is_max[9] = {false, false, false, false, false, false, false, true, true};
     blockReduce<9>(v, is_max);

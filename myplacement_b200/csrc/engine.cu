@@ -135,13 +135,17 @@ void Engine::uploadStatic(const Problem& p) {
     const std::size_t bins = static_cast<std::size_t>(bin_count_);
     layers_ = arena_.array<unsigned long long>(3 * bins, "fixed-point density layers");
     totals_ = arena_.array<unsigned long long>(4, "density layer totals");
-    fixed_ = arena_.array<double>(bins, "fixed density layer");
-    dark_ = arena_.array<double>(bins, "dark density layer");
+    static_charge_ = arena_.array<double>(bins, "static charge");
     source_ = arena_.array<float>(bins, "density source");
     checkCuda(cudaMemsetAsync(layers_, 0, 3 * bins * sizeof(unsigned long long), stream_), "clear layers");
     checkCuda(cudaMemsetAsync(totals_, 0, 4 * sizeof(unsigned long long), stream_), "clear totals");
-    upload(fixed_, p.static_fixed, stream_);
-    upload(dark_, p.static_dark, stream_);
+    {
+        // t * (fixed + dark): the part of every bin's charge area that never moves.
+        std::vector<double> static_charge(bins);
+        for (std::size_t b = 0; b < bins; ++b) static_charge[b] = target_density_ * (p.static_fixed[b] + p.static_dark[b]);
+        upload(static_charge_, static_charge, stream_);
+        checkCuda(cudaStreamSynchronize(stream_), "static charge upload");  // the host vector leaves scope
+    }
     // Static sums in bin order: DensityMap::metrics (Metrics.cpp:101-119) uses each
     // bin's own rectangle area for the placeable area.
     for (int row = 0; row < bins_y_; ++row) {
@@ -157,7 +161,7 @@ void Engine::uploadStatic(const Problem& p) {
     }
     scatter_blocks_ = ceilDiv(std::max<int64_t>(1, particle_count_), kThreads);
     gather_blocks_ = scatter_blocks_;
-    metrics_blocks_ = std::min(ceilDiv(bin_count_, kThreads), 148 * 8);
+    metrics_blocks_ = std::min(ceilDiv(bin_count_, 2 * kThreads), 148 * 2);
     partials_sc_ = arena_.array<double>(2 * static_cast<std::size_t>(scatter_blocks_), "scatter partials");
     partials_m_ = arena_.array<double>(9 * static_cast<std::size_t>(metrics_blocks_), "metric partials");
     partials_g_ = arena_.array<double>(7 * static_cast<std::size_t>(gather_blocks_), "gather partials");
@@ -167,8 +171,9 @@ void Engine::uploadStatic(const Problem& p) {
 
 void Engine::buildNetLayout(const Problem& p) {
     const int net_count = static_cast<int>(p.net_weight.size());
-    // Degree buckets: G lanes per net for degree <= G, a warp loop above 32.
-    const int kGroups[6] = {2, 4, 8, 16, 32, 0};
+    // Degree buckets: one thread per two-pin net, G lanes per net for degree <= G,
+    // a warp loop above 32.
+    const int kGroups[6] = {1, 4, 8, 16, 32, 0};
     std::vector<std::vector<int>> bucket(6);
     for (int n = 0; n < net_count; ++n) {
         const int64_t degree = p.net_pin_start[n + 1] - p.net_pin_start[n];
@@ -182,9 +187,13 @@ void Engine::buildNetLayout(const Problem& p) {
     std::vector<int> net_start{0};
     std::vector<float> net_weight;
     std::vector<int4> work;
+    // Pins and nets are laid out bucket by bucket; the blocks run heaviest bucket
+    // first (one round of the block's lanes each), so the long warp-loop nets do
+    // not form the kernel's tail.
+    std::vector<int4> bucket_work[6];
     for (int b = 0; b < 6; ++b) {
         const int group = kGroups[b];
-        const int nets_per_block = group == 0 ? 32 : (kThreads / group) * 4;
+        const int nets_per_block = group == 0 ? kThreads / 32 : group == 1 ? kThreads : kThreads / group;
         const int first_net = static_cast<int>(net_weight.size());
         for (const int n : bucket[b]) {
             for (int64_t pin = p.net_pin_start[n]; pin < p.net_pin_start[n + 1]; ++pin) {
@@ -203,9 +212,10 @@ void Engine::buildNetLayout(const Problem& p) {
         }
         const int count = static_cast<int>(bucket[b].size());
         for (int off = 0; off < count; off += nets_per_block) {
-            work.push_back(make_int4(group, first_net + off, std::min(nets_per_block, count - off), 0));
+            bucket_work[b].push_back(make_int4(group, first_net + off, std::min(nets_per_block, count - off), 0));
         }
     }
+    for (int b = 5; b >= 0; --b) work.insert(work.end(), bucket_work[b].begin(), bucket_work[b].end());
     wl_blocks_ = static_cast<int>(work.size());
     const std::size_t pins = std::max<std::size_t>(1, pin_particle.size());
     pin_particle_ = arena_.array<int>(pins, "pin particles");
@@ -224,48 +234,56 @@ void Engine::buildNetLayout(const Problem& p) {
     upload(block_work_, work, stream_);
     checkCuda(cudaMemsetAsync(pin_gradient_, 0, pins * sizeof(float2), stream_), "clear pin gradients");
 
-    // Per-particle pin lists (bucketed pin indices, ascending) for the deterministic gather.
+    // Particle-ordered gradient slots: particle i's pins (ascending bucketed pin
+    // index) own slots count[i] .. count[i + 1] - 1, so the gather reads one
+    // contiguous range per particle in a fixed order.
     const std::size_t movable = static_cast<std::size_t>(movable_count_);
     std::vector<int> count(movable + 1, 0);
     for (std::size_t i = 0; i < pin_particle.size(); ++i) {
         const int particle = pin_particle[i];
-        if (particle >= 0 && static_cast<std::size_t>(particle) < movable) ++count[particle + 1];
+        require(particle < 0 || static_cast<std::size_t>(particle) < movable, "A pin refers to a non-movable particle.");
+        if (particle >= 0) ++count[particle + 1];
     }
     for (std::size_t i = 0; i < movable; ++i) count[i + 1] += count[i];
-    std::vector<int> list(static_cast<std::size_t>(count[movable]));
+    std::vector<int> slot(pin_particle.size(), -1);
     std::vector<int> fill(count.begin(), count.end() - 1);
     for (std::size_t i = 0; i < pin_particle.size(); ++i) {
         const int particle = pin_particle[i];
-        if (particle >= 0 && static_cast<std::size_t>(particle) < movable) list[fill[particle]++] = static_cast<int>(i);
+        if (particle >= 0) slot[i] = fill[particle]++;
     }
     particle_pin_start_ = arena_.array<int>(count.size(), "particle pin offsets");
-    particle_pins_ = arena_.array<int>(std::max<std::size_t>(1, list.size()), "particle pins");
+    pin_slot_ = arena_.array<int>(std::max<std::size_t>(1, slot.size()), "pin gradient slots");
     upload(particle_pin_start_, count, stream_);
-    upload(particle_pins_, list, stream_);
+    upload(pin_slot_, slot, stream_);
     checkCuda(cudaStreamSynchronize(stream_), "net layout upload");
 }
 
 void Engine::buildBasis() {
     const int nx = bins_x_, ny = bins_y_;
     const double width = region_.width(), height = region_.height();
-    std::vector<float> cx_t(static_cast<std::size_t>(nx) * nx), dx_t(cx_t.size()), sx_w(cx_t.size());
-    std::vector<float> cy(static_cast<std::size_t>(ny) * ny), dy(cy.size()), sy_w(cy.size());
+    // K-major operands of C = A * B^T (runDct), in FP64 before the bf16 split:
+    //   cx[k][c] = 2 cos(pi k (2c+1) / 2nx)          (DCT-II, REDFT10)
+    //   dxc[c][k] = 2 cos(...), k = 0 -> 1            (DCT-III, REDFT01)
+    //   sxwt[c][k] = kx 2 sin(pi k (2c+1) / 2nx)      (DST-III, RODFT01, times the wave number)
+    // and the same along y.
+    std::vector<double> cx(static_cast<std::size_t>(nx) * nx), dxc(cx.size()), sxwt(cx.size());
+    std::vector<double> cy(static_cast<std::size_t>(ny) * ny), dy(cy.size()), syw(cy.size());
     for (int c = 0; c < nx; ++c) {
         for (int k = 0; k < nx; ++k) {
             const long long m = static_cast<long long>(k) * (2 * c + 1);
             const double wave = kPi * static_cast<double>(k) / width;
-            cx_t[static_cast<std::size_t>(c) * nx + k] = static_cast<float>(2.0 * cosQuarter(m, nx));
-            dx_t[static_cast<std::size_t>(k) * nx + c] = static_cast<float>(k == 0 ? 1.0 : 2.0 * cosQuarter(m, nx));
-            sx_w[static_cast<std::size_t>(k) * nx + c] = static_cast<float>(k == 0 ? 0.0 : wave * 2.0 * sinQuarter(m, nx));
+            cx[static_cast<std::size_t>(k) * nx + c] = 2.0 * cosQuarter(m, nx);
+            dxc[static_cast<std::size_t>(c) * nx + k] = k == 0 ? 1.0 : 2.0 * cosQuarter(m, nx);
+            sxwt[static_cast<std::size_t>(c) * nx + k] = k == 0 ? 0.0 : wave * 2.0 * sinQuarter(m, nx);
         }
     }
     for (int r = 0; r < ny; ++r) {
         for (int l = 0; l < ny; ++l) {
             const long long m = static_cast<long long>(l) * (2 * r + 1);
             const double wave = kPi * static_cast<double>(l) / height;
-            cy[static_cast<std::size_t>(l) * ny + r] = static_cast<float>(2.0 * cosQuarter(m, ny));
-            dy[static_cast<std::size_t>(r) * ny + l] = static_cast<float>(l == 0 ? 1.0 : 2.0 * cosQuarter(m, ny));
-            sy_w[static_cast<std::size_t>(r) * ny + l] = static_cast<float>(l == 0 ? 0.0 : wave * 2.0 * sinQuarter(m, ny));
+            cy[static_cast<std::size_t>(l) * ny + r] = 2.0 * cosQuarter(m, ny);
+            dy[static_cast<std::size_t>(r) * ny + l] = l == 0 ? 1.0 : 2.0 * cosQuarter(m, ny);
+            syw[static_cast<std::size_t>(r) * ny + l] = l == 0 ? 0.0 : wave * 2.0 * sinQuarter(m, ny);
         }
     }
     // Spectral divide (ElectrostaticField.cpp:212-221): 1/(4 Nx Ny) / (kx^2 + ky^2), DC removed.
@@ -284,64 +302,17 @@ void Engine::buildBasis() {
     wy[0] = 0.5f;
     wx[0] = 0.5f;
     const std::size_t bins = static_cast<std::size_t>(bin_count_);
-    basis_cx_t_ = arena_.array<float>(cx_t.size(), "DCT basis");
-    basis_dx_t_ = arena_.array<float>(dx_t.size(), "DCT basis");
-    basis_sx_w_ = arena_.array<float>(sx_w.size(), "DST basis");
-    basis_cy_ = arena_.array<float>(cy.size(), "DCT basis");
-    basis_dy_ = arena_.array<float>(dy.size(), "DCT basis");
-    basis_sy_w_ = arena_.array<float>(sy_w.size(), "DST basis");
     spectral_scale_ = arena_.array<float>(bins, "spectral scale");
     weight_y_ = arena_.array<float>(wy.size(), "Parseval weights");
     weight_x_ = arena_.array<float>(wx.size(), "Parseval weights");
-    stage_a_ = arena_.array<float>(bins, "DCT stage");
-    phi_hat_ = arena_.array<float>(bins, "potential coefficients");
-    stage_t_ = arena_.array<float>(bins, "DCT stage");
-    stage_u_ = arena_.array<float>(bins, "DCT stage");
     field_ = arena_.array<float2>(bins, "electric field");
     potential_ = arena_.array<float>(bins, "potential");
-    upload(basis_cx_t_, cx_t, stream_);
-    upload(basis_dx_t_, dx_t, stream_);
-    upload(basis_sx_w_, sx_w, stream_);
-    upload(basis_cy_, cy, stream_);
-    upload(basis_dy_, dy, stream_);
-    upload(basis_sy_w_, sy_w, stream_);
     upload(spectral_scale_, scale, stream_);
     upload(weight_y_, wy, stream_);
     upload(weight_x_, wx, stream_);
-    const char* dct_mode = std::getenv("MPGP_DCT");
-    use_tc_ = !(dct_mode != nullptr && std::string(dct_mode) == "simt");
-    if (use_tc_) {
-        // K-major operands of C = A * B^T (engine.cu runDct), in FP64 before the bf16 split.
-        std::vector<double> cx(static_cast<std::size_t>(nx) * nx), dxc(cx.size()), sxwt(cx.size());
-        std::vector<double> cy2(static_cast<std::size_t>(ny) * ny), dy2(cy2.size()), syw(cy2.size());
-        for (int c = 0; c < nx; ++c) {
-            for (int k = 0; k < nx; ++k) {
-                const long long m = static_cast<long long>(k) * (2 * c + 1);
-                const double wave = kPi * static_cast<double>(k) / width;
-                cx[static_cast<std::size_t>(k) * nx + c] = 2.0 * cosQuarter(m, nx);
-                dxc[static_cast<std::size_t>(c) * nx + k] = k == 0 ? 1.0 : 2.0 * cosQuarter(m, nx);
-                sxwt[static_cast<std::size_t>(c) * nx + k] = k == 0 ? 0.0 : wave * 2.0 * sinQuarter(m, nx);
-            }
-        }
-        for (int r = 0; r < ny; ++r) {
-            for (int l = 0; l < ny; ++l) {
-                const long long m = static_cast<long long>(l) * (2 * r + 1);
-                const double wave = kPi * static_cast<double>(l) / height;
-                cy2[static_cast<std::size_t>(l) * ny + r] = 2.0 * cosQuarter(m, ny);
-                dy2[static_cast<std::size_t>(r) * ny + l] = l == 0 ? 1.0 : 2.0 * cosQuarter(m, ny);
-                syw[static_cast<std::size_t>(r) * ny + l] = l == 0 ? 0.0 : wave * 2.0 * sinQuarter(m, ny);
-            }
-        }
-        energy_blocks_ = tcTiles(ny, nx);
-        partials_e_ = arena_.array<double>(static_cast<std::size_t>(energy_blocks_), "energy partials");
-        buildTensorCoreBasis(cx, cy2, dy2, dxc, sxwt, syw);
-    } else {
-        GemmTask probe{};
-        probe.m = ny;
-        probe.n = nx;
-        energy_blocks_ = gemmBlocks(probe);
-        partials_e_ = arena_.array<double>(static_cast<std::size_t>(energy_blocks_), "energy partials");
-    }
+    double max_scale = 0.0;
+    for (float v : scale) max_scale = std::max(max_scale, static_cast<double>(v));
+    buildTensorCoreBasis(cx, cy, dy, dxc, sxwt, syw, max_scale);
     checkCuda(cudaStreamSynchronize(stream_), "basis upload");
 }
 
@@ -350,39 +321,65 @@ SplitMatrix Engine::newSplit(int rows, int cols, const char* what) {
     m.rows = rows;
     m.cols = cols;
     m.ld = paddedLd(cols);
-    m.data = arena_.array<__nv_bfloat16>(m.elements(), what);
-    checkCuda(cudaMemsetAsync(m.data, 0, m.elements() * sizeof(__nv_bfloat16), stream_), what);
+    m.data = arena_.array<__half>(m.elements(), what);
+    checkCuda(cudaMemsetAsync(m.data, 0, m.elements() * sizeof(__half), stream_), what);
     return m;
 }
 
+namespace {
+
+// Largest row sum of |values| (rows x cols, row-major): |A x| <= this * max |x|.
+double maxRowL1(const std::vector<double>& values, int rows, int cols) {
+    double top = 0.0;
+    for (int r = 0; r < rows; ++r) {
+        double sum = 0.0;
+        for (int c = 0; c < cols; ++c) sum += std::fabs(values[static_cast<std::size_t>(r) * cols + c]);
+        top = std::max(top, sum);
+    }
+    return top;
+}
+
+}  // namespace
+
 void Engine::buildTensorCoreBasis(const std::vector<double>& cx, const std::vector<double>& cy,
                                   const std::vector<double>& dy, const std::vector<double>& dxc,
-                                  const std::vector<double>& sxwt, const std::vector<double>& syw) {
+                                  const std::vector<double>& sxwt, const std::vector<double>& syw,
+                                  double max_scale) {
     const int nx = bins_x_, ny = bins_y_;
-    const auto splitUpload = [&](const std::vector<double>& values, int rows, int cols, const char* what) {
+    TcScales host_scales{};
+    const auto splitUpload = [&](const std::vector<double>& values, int rows, int cols, int slot, const char* what) {
         SplitMatrix m = newSplit(rows, cols, what);
-        std::vector<__nv_bfloat16> planes;
-        splitHost(values, rows, cols, m.ld, planes);
+        std::vector<__half> planes;
+        host_scales.exp_basis[slot] = splitHost(values, rows, cols, m.ld, planes);
         upload(m.data, planes, stream_);
         return m;
     };
-    tc_cx_ = splitUpload(cx, nx, nx, "DCT basis planes");
-    tc_cy_ = splitUpload(cy, ny, ny, "DCT basis planes");
-    tc_dy_ = splitUpload(dy, ny, ny, "DCT basis planes");
-    tc_dxc_ = splitUpload(dxc, nx, nx, "DCT basis planes");
-    tc_sxwt_ = splitUpload(sxwt, nx, nx, "DST basis planes");
-    tc_syw_ = splitUpload(syw, ny, ny, "DST basis planes");
+    enum { kCx = 0, kCy, kDy, kDxc, kSxwt, kSyw };
+    tc_cx_ = splitUpload(cx, nx, nx, kCx, "DCT basis planes");
+    tc_cy_ = splitUpload(cy, ny, ny, kCy, "DCT basis planes");
+    tc_dy_ = splitUpload(dy, ny, ny, kDy, "DCT basis planes");
+    tc_dxc_ = splitUpload(dxc, nx, nx, kDxc, "DCT basis planes");
+    tc_sxwt_ = splitUpload(sxwt, nx, nx, kSxwt, "DST basis planes");
+    tc_syw_ = splitUpload(syw, ny, ny, kSyw, "DST basis planes");
     tc_source_ = newSplit(ny, nx, "source planes");
     tc_x1t_ = newSplit(nx, ny, "DCT stage planes");
     tc_phi_ = newSplit(ny, nx, "potential coefficient planes");
     tc_phit_ = newSplit(nx, ny, "potential coefficient planes");
     tc_t_ = newSplit(ny, nx, "DCT stage planes");
     tc_ut_ = newSplit(nx, ny, "DCT stage planes");
+    tc_row_exp_ = arena_.array<int>(static_cast<std::size_t>(ny), "source plane exponents");
+    tc_scales_ = arena_.array<TcScales>(1, "field scales");
+    checkCuda(cudaMemcpyAsync(tc_scales_, &host_scales, sizeof(TcScales), cudaMemcpyHostToDevice, stream_),
+              "upload field scales");
+    checkCuda(cudaStreamSynchronize(stream_), "upload field scales");  // host_scales leaves scope
     tc_error_ = arena_.array<int>(1, "contraction error flag");
     checkCuda(cudaMemsetAsync(tc_error_, 0, sizeof(int), stream_), "clear error flag");
     checkCuda(cudaMallocHost(reinterpret_cast<void**>(&host_error_), sizeof(int)), "pinned error flag");
     *host_error_ = 0;
 
+    // Output bounds |C| <= gain * max |data operand|, with a margin for FP32 rounding.
+    constexpr double kMargin = 1.02;
+    TcScales* sc = tc_scales_;
     const auto task = [&](TcTask& t, const SplitMatrix& a, const SplitMatrix& b, int m, int n, int k, int mode) {
         std::memset(static_cast<void*>(&t), 0, sizeof(TcTask));
         makeOperandMap(&t.map_a, a, kTileM);
@@ -394,11 +391,24 @@ void Engine::buildTensorCoreBasis(const std::vector<double>& cx, const std::vect
     };
     // X = S * Cx^T, stored transposed (the K-major B operand of the next contraction).
     task(tc_fwd1_.task[0], tc_source_, tc_cx_, ny, nx, nx, kTcSplitTransposed);
+    tc_fwd1_.task[0].row_exp_a = tc_row_exp_;
+    tc_fwd1_.task[0].exp_b = &sc->exp_basis[kCx];
+    tc_fwd1_.task[0].ref_max = &sc->max_source;
+    tc_fwd1_.task[0].gain = static_cast<float>(maxRowL1(cx, nx, nx) * kMargin);
+    tc_fwd1_.task[0].out_exp = &sc->exp_x;
+    tc_fwd1_.task[0].out_max = &sc->max_x;
     tc_fwd1_.task[0].out_t = tc_x1t_.data;
     tc_fwd1_.task[0].out_t_ld = tc_x1t_.ld;
     tc_fwd1_.task[0].out_t_plane = tc_x1t_.plane();
     // rho_hat = Cy * X; epilogue: phi_hat = rho_hat .* scale, stored both ways, + Parseval energy.
     task(tc_fwd2_.task[0], tc_cy_, tc_x1t_, ny, nx, ny, kTcSpectral);
+    tc_fwd2_.task[0].exp_a = &sc->exp_basis[kCy];
+    tc_fwd2_.task[0].exp_b = &sc->exp_x;
+    tc_fwd2_.task[0].ref_max = &sc->max_x;
+    tc_fwd2_.task[0].gain = static_cast<float>(maxRowL1(cy, ny, ny) * max_scale * kMargin);
+    tc_fwd2_.task[0].out_exp = &sc->exp_phi;
+    tc_fwd2_.task[0].out_max = &sc->max_phi;
+    tc_fwd2_.task[0].clear = &sc->max_source;
     tc_fwd2_.task[0].out = tc_phi_.data;
     tc_fwd2_.task[0].out_ld = tc_phi_.ld;
     tc_fwd2_.task[0].out_plane = tc_phi_.plane();
@@ -408,67 +418,83 @@ void Engine::buildTensorCoreBasis(const std::vector<double>& cx, const std::vect
     tc_fwd2_.task[0].scale = spectral_scale_;
     tc_fwd2_.task[0].weight_r = weight_y_;
     tc_fwd2_.task[0].weight_c = weight_x_;
-    tc_fwd2_.task[0].energy_partials = partials_e_;
     // T = Dy * phi_hat and U = phi_hat * Dx^T (stored transposed), one launch.
     task(tc_inv1_.task[0], tc_dy_, tc_phit_, ny, nx, ny, kTcSplit);
+    tc_inv1_.task[0].exp_a = &sc->exp_basis[kDy];
+    tc_inv1_.task[0].exp_b = &sc->exp_phi;
+    tc_inv1_.task[0].ref_max = &sc->max_phi;
+    tc_inv1_.task[0].gain = static_cast<float>(maxRowL1(dy, ny, ny) * kMargin);
+    tc_inv1_.task[0].out_exp = &sc->exp_t;
     tc_inv1_.task[0].out = tc_t_.data;
     tc_inv1_.task[0].out_ld = tc_t_.ld;
     tc_inv1_.task[0].out_plane = tc_t_.plane();
     task(tc_inv1_.task[1], tc_phi_, tc_dxc_, ny, nx, nx, kTcSplitTransposed);
+    tc_inv1_.task[1].exp_a = &sc->exp_phi;
+    tc_inv1_.task[1].exp_b = &sc->exp_basis[kDxc];
+    tc_inv1_.task[1].ref_max = &sc->max_phi;
+    tc_inv1_.task[1].gain = static_cast<float>(maxRowL1(dxc, nx, nx) * kMargin);
+    tc_inv1_.task[1].out_exp = &sc->exp_u;
     tc_inv1_.task[1].out_t = tc_ut_.data;
     tc_inv1_.task[1].out_t_ld = tc_ut_.ld;
     tc_inv1_.task[1].out_t_plane = tc_ut_.plane();
     // Ex = T * (Sx diag(kx))^T and Ey = (Sy diag(ky)) * U into the interleaved field, one launch.
     task(tc_inv2_.task[0], tc_t_, tc_sxwt_, ny, nx, nx, kTcField);
+    tc_inv2_.task[0].exp_a = &sc->exp_t;
+    tc_inv2_.task[0].exp_b = &sc->exp_basis[kSxwt];
     tc_inv2_.task[0].out_f = reinterpret_cast<float*>(field_);
     tc_inv2_.task[0].out_f_ld = 2 * nx;
     tc_inv2_.task[0].out_f_step = 2;
     task(tc_inv2_.task[1], tc_syw_, tc_ut_, ny, nx, ny, kTcField);
+    tc_inv2_.task[1].exp_a = &sc->exp_basis[kSyw];
+    tc_inv2_.task[1].exp_b = &sc->exp_u;
     tc_inv2_.task[1].out_f = reinterpret_cast<float*>(field_) + 1;
     tc_inv2_.task[1].out_f_ld = 2 * nx;
     tc_inv2_.task[1].out_f_step = 2;
     // Potential (parity hook): phi = T * Dx^T.
     task(tc_pot_.task[0], tc_t_, tc_dxc_, ny, nx, nx, kTcField);
+    tc_pot_.task[0].exp_a = &sc->exp_t;
+    tc_pot_.task[0].exp_b = &sc->exp_basis[kDxc];
     tc_pot_.task[0].out_f = potential_;
     tc_pot_.task[0].out_f_ld = nx;
     tc_pot_.task[0].out_f_step = 1;
     tc_fwd1_.error_flag = tc_fwd2_.error_flag = tc_inv1_.error_flag = tc_inv2_.error_flag = tc_pot_.error_flag =
         tc_error_;
-    if (std::getenv("MPGP_TC_TRACE") != nullptr) {
-        unsigned long long* trace = arena_.array<unsigned long long>(5 * 64, "trace");
-        checkCuda(cudaMemsetAsync(trace, 0, 5 * 64 * 8, stream_), "trace");
-        tc_fwd1_.trace = trace;
-        tc_fwd2_.trace = trace + 64;
-        tc_inv1_.trace = trace + 128;
-        tc_inv2_.trace = trace + 192;
-        tc_pot_.trace = trace + 256;
-    }
+    tcPlan(tc_fwd1_, 1);
+    tcPlan(tc_fwd2_, 1);
+    tcPlan(tc_inv1_, 2);
+    tcPlan(tc_inv2_, 2);
+    tcPlan(tc_pot_, 1);
+    energy_blocks_ = tcBlocks(tc_fwd2_, 1);
+    partials_e_ = arena_.array<double>(static_cast<std::size_t>(energy_blocks_), "energy partials");
+    tc_fwd2_.task[0].energy_partials = partials_e_;
 }
 
 const char* kernelKindName(int kind) {
     static const char* names[kKindCount] = {"scatter", "wirelength", "metrics", "dct_forward",
-                                            "dct_inverse", "gather", "reduce", "vector"};
+                                            "dct_inverse", "gather", "reduce", "vector", "dct_split"};
     return kind >= 0 && kind < kKindCount ? names[kind] : "unknown";
 }
 
-void Engine::setTiming(bool enabled) {
-    if (enabled && events_.empty()) {
+void Engine::setTiming(uint32_t families) {
+    if (families != 0 && events_.empty()) {
         events_.resize(64);
         for (cudaEvent_t& e : events_) checkCuda(cudaEventCreate(&e), "Create profiling event");
         pending_kind_.resize(32);
     }
-    timing_ = enabled;
+    timing_mask_ = families;
 }
 
 void Engine::beginKernel(int kind, cudaStream_t on) {
-    if (!timing_) return;
+    open_ = ((timing_mask_ >> kind) & 1u) != 0;
+    if (!open_) return;
     if (pending_ >= static_cast<int>(pending_kind_.size())) collectTimings();
     pending_kind_[pending_] = kind;
     checkCuda(cudaEventRecord(events_[2 * pending_], on != nullptr ? on : stream_), "Record profiling event");
 }
 
 void Engine::endKernel(cudaStream_t on) {
-    if (!timing_) return;
+    if (!open_) return;
+    open_ = false;
     checkCuda(cudaEventRecord(events_[2 * pending_ + 1], on != nullptr ? on : stream_), "Record profiling event");
     ++pending_;
 }
@@ -490,11 +516,10 @@ void Engine::collectTimings() {
 //   gradient: T = Dy * phi_hat, U = phi_hat * Dx^T, Ex = T * (Sx diag(kx))^T, Ey = (Sy diag(ky)) * U
 //   potential (parity hook only): phi = T * Dx^T.
 void Engine::runDct(bool gradient, bool potential, bool forward) {
-    const int nx = bins_x_, ny = bins_y_;
-    if (use_tc_) {
-        if (forward) {
-        beginKernel(kKindDctForward);
-        launchSplitSource(source_, tc_source_, nx, stream_);
+    const int nx = bins_x_;
+    if (forward) {
+        beginKernel(kKindDctSplit);
+        launchSplitSource(source_, tc_source_, nx, tc_row_exp_, tc_scales_, stream_);
         endKernel();
         beginKernel(kKindDctForward);
         launchTcGemm(tc_fwd1_, 1, stream_);
@@ -503,61 +528,18 @@ void Engine::runDct(bool gradient, bool potential, bool forward) {
         launchTcGemm(tc_fwd2_, 1, stream_);
         endKernel();
         launches_ += 3;
-        }
-        if (!gradient) return;
-        beginKernel(kKindDctInverse);
-        launchTcGemm(tc_inv1_, 2, stream_);
-        endKernel();
-        beginKernel(kKindDctInverse);
-        launchTcGemm(tc_inv2_, 2, stream_);
-        endKernel();
-        launches_ += 2;
-        if (potential) {
-            beginKernel(kKindDctInverse);
-            launchTcGemm(tc_pot_, 1, stream_);
-            endKernel();
-            launches_ += 1;
-        }
-        return;
     }
-    beginKernel(kKindDctForward);
-    GemmTask f1{};
-    f1.a = source_; f1.b = basis_cx_t_; f1.c = stage_a_;
-    f1.m = ny; f1.n = nx; f1.k = nx; f1.lda = nx; f1.ldb = nx; f1.ldc = nx; f1.c_step = 1;
-    launchGemm(&f1, 1, stream_);
-    endKernel();
-    beginKernel(kKindDctForward);
-    GemmTask f2{};
-    f2.a = basis_cy_; f2.b = stage_a_; f2.c = phi_hat_;
-    f2.m = ny; f2.n = nx; f2.k = ny; f2.lda = ny; f2.ldb = nx; f2.ldc = nx; f2.c_step = 1;
-    f2.scale = spectral_scale_; f2.weight_r = weight_y_; f2.weight_c = weight_x_; f2.energy_partials = partials_e_;
-    launchGemm(&f2, 1, stream_);
-    endKernel();
-    launches_ += 2;
     if (!gradient) return;
     beginKernel(kKindDctInverse);
-    GemmTask inv1[2]{};
-    inv1[0].a = basis_dy_; inv1[0].b = phi_hat_; inv1[0].c = stage_t_;
-    inv1[0].m = ny; inv1[0].n = nx; inv1[0].k = ny; inv1[0].lda = ny; inv1[0].ldb = nx; inv1[0].ldc = nx; inv1[0].c_step = 1;
-    inv1[1].a = phi_hat_; inv1[1].b = basis_dx_t_; inv1[1].c = stage_u_;
-    inv1[1].m = ny; inv1[1].n = nx; inv1[1].k = nx; inv1[1].lda = nx; inv1[1].ldb = nx; inv1[1].ldc = nx; inv1[1].c_step = 1;
-    launchGemm(inv1, 2, stream_);
+    launchTcGemm(tc_inv1_, 2, stream_);
     endKernel();
     beginKernel(kKindDctInverse);
-    GemmTask inv2[2]{};
-    inv2[0].a = stage_t_; inv2[0].b = basis_sx_w_; inv2[0].c = reinterpret_cast<float*>(field_);
-    inv2[0].m = ny; inv2[0].n = nx; inv2[0].k = nx; inv2[0].lda = nx; inv2[0].ldb = nx; inv2[0].ldc = 2 * nx; inv2[0].c_step = 2;
-    inv2[1].a = basis_sy_w_; inv2[1].b = stage_u_; inv2[1].c = reinterpret_cast<float*>(field_) + 1;
-    inv2[1].m = ny; inv2[1].n = nx; inv2[1].k = ny; inv2[1].lda = ny; inv2[1].ldb = nx; inv2[1].ldc = 2 * nx; inv2[1].c_step = 2;
-    launchGemm(inv2, 2, stream_);
+    launchTcGemm(tc_inv2_, 2, stream_);
     endKernel();
     launches_ += 2;
     if (potential) {
         beginKernel(kKindDctInverse);
-        GemmTask pot{};
-        pot.a = stage_t_; pot.b = basis_dx_t_; pot.c = potential_;
-        pot.m = ny; pot.n = nx; pot.k = nx; pot.lda = nx; pot.ldb = nx; pot.ldc = nx; pot.c_step = 1;
-        launchGemm(&pot, 1, stream_);
+        launchTcGemm(tc_pot_, 1, stream_);
         endKernel();
         launches_ += 1;
     }
@@ -613,6 +595,7 @@ void Engine::launch(const EvalRequest& q) {
     wa.block_work = block_work_;
     wa.gamma = static_cast<float>(std::max(q.smoothing, kEpsilon));
     wa.inv_gamma = static_cast<float>(1.0 / std::max(q.smoothing, kEpsilon));
+    wa.pin_slot = pin_slot_;
     wa.pin_gradient = pin_gradient_;
     wa.gradient = q.gradient ? 1 : 0;
     wa.partials = partials_wl_;
@@ -624,8 +607,7 @@ void Engine::launch(const EvalRequest& q) {
     MetricsArgs ma{};
     ma.layers = layers_;
     ma.totals = totals_;
-    ma.fixed = fixed_;
-    ma.dark = dark_;
+    ma.static_charge = static_charge_;
     ma.static_fixed_sum = static_fixed_sum_;
     ma.static_dark_sum = static_dark_sum_;
     ma.target_density = target_density_;
@@ -650,7 +632,6 @@ void Engine::launch(const EvalRequest& q) {
         ga.movable_count = static_cast<int>(movable_count_);
         ga.positions = positions;
         ga.particle_pin_start = particle_pin_start_;
-        ga.particle_pins = particle_pins_;
         ga.pin_gradient = pin_gradient_;
         ga.field = field_;
         ga.charge = charge_;
@@ -659,8 +640,8 @@ void Engine::launch(const EvalRequest& q) {
         ga.lly = region_.lly;
         ga.urx = region_.urx;
         ga.ury = region_.ury;
-        ga.bin_w = bin_w_;
-        ga.bin_h = bin_h_;
+        ga.inv_bin_w = 1.0 / bin_w_;
+        ga.inv_bin_h = 1.0 / bin_h_;
         ga.bins_x = nx;
         ga.bins_y = ny;
         ga.penalty = q.penalty;
@@ -706,11 +687,9 @@ void Engine::launch(const EvalRequest& q) {
     checkCuda(cudaMemcpyAsync(host_scalars_, scalars_, sizeof(EvalScalars), cudaMemcpyDeviceToHost, stream_),
               "Download evaluation scalars");
     d2h_bytes_ += sizeof(EvalScalars);
-    if (use_tc_) {
-        checkCuda(cudaMemcpyAsync(host_error_, tc_error_, sizeof(int), cudaMemcpyDeviceToHost, stream_),
-                  "Download contraction status");
-        d2h_bytes_ += sizeof(int);
-    }
+    checkCuda(cudaMemcpyAsync(host_error_, tc_error_, sizeof(int), cudaMemcpyDeviceToHost, stream_),
+              "Download contraction status");
+    d2h_bytes_ += sizeof(int);
     launches_ += kernels;
     last_gradient_ = q.gradient;
     last_propose_ = q.mode == kPropose;
@@ -754,25 +733,10 @@ void Engine::fieldSolve(const double* deviation, double* potential, double* fiel
     std::vector<float2> f(bins);
     checkCuda(cudaMemcpyAsync(p.data(), potential_, bins * sizeof(float), cudaMemcpyDeviceToHost, stream_), "field");
     checkCuda(cudaMemcpyAsync(f.data(), field_, bins * sizeof(float2), cudaMemcpyDeviceToHost, stream_), "field");
-    if (use_tc_) {
-        checkCuda(cudaMemcpyAsync(host_error_, tc_error_, sizeof(int), cudaMemcpyDeviceToHost, stream_),
-                  "Download contraction status");
-    }
+    checkCuda(cudaMemcpyAsync(host_error_, tc_error_, sizeof(int), cudaMemcpyDeviceToHost, stream_),
+              "Download contraction status");
     checkCuda(cudaStreamSynchronize(stream_), "field solve");
     collectTimings();
-    if (tc_fwd1_.trace != nullptr) {
-        std::vector<unsigned long long> trace(5 * 64);
-        checkCuda(cudaMemcpy(trace.data(), tc_fwd1_.trace, trace.size() * 8, cudaMemcpyDeviceToHost), "trace");
-        for (int g = 0; g < 5; ++g) {
-            const unsigned long long base = trace[g * 64 + 51];
-            std::fprintf(stderr, "TRACE gemm %d:", g);
-            for (int i = 0; i < 52; ++i) {
-                const unsigned long long v = trace[g * 64 + i];
-                if (v != 0) std::fprintf(stderr, " %d:%lld", i, static_cast<long long>(v - base));
-            }
-            std::fprintf(stderr, "\n");
-        }
-    }
     if (host_error_ != nullptr && *host_error_ != 0) {
         fail(MPGP_ERR_TIMEOUT, "A tcgen05 field contraction timed out waiting on its pipeline.");
     }

@@ -79,6 +79,7 @@ enum KernelKind : int {
     kKindGather,
     kKindReduce,
     kKindVector,
+    kKindDctSplit,
     kKindCount
 };
 const char* kernelKindName(int kind);
@@ -123,9 +124,10 @@ public:
     [[nodiscard]] const double* precondBase() const { return precond_; }
     void countLaunches(int64_t n) { launches_ += n; }
 
-    // Event profiling: when enabled, every launch is bracketed by CUDA events on
-    // the engine stream and its duration is added to its family at sync().
-    void setTiming(bool enabled);
+    // Event profiling: every launch of a family whose bit is set in `families` is
+    // bracketed by CUDA events on its stream and its duration is added to the
+    // family at sync() (0 turns profiling off).
+    void setTiming(uint32_t families);
     [[nodiscard]] const KernelStats& kernelStats() const { return stats_; }
     void resetKernelStats() { stats_ = KernelStats{}; }
     void beginKernel(int kind, cudaStream_t on = nullptr);
@@ -178,42 +180,32 @@ private:
     int wl_blocks_ = 0;
     float2* pin_gradient_ = nullptr;
     int* particle_pin_start_ = nullptr;
-    int* particle_pins_ = nullptr;
+    int* pin_slot_ = nullptr;
 
     // density
     unsigned long long* layers_ = nullptr;
     unsigned long long* totals_ = nullptr;
-    double* fixed_ = nullptr;
-    double* dark_ = nullptr;
+    double* static_charge_ = nullptr;
     float* source_ = nullptr;
 
-    // DCT
-    float* basis_cx_t_ = nullptr;  // nx x nx: 2 cos(pi k (2c+1) / 2nx), [c][k]
-    float* basis_cy_ = nullptr;    // ny x ny: [l][r]
-    float* basis_dy_ = nullptr;    // ny x ny: [r][l], l = 0 -> 1
-    float* basis_dx_t_ = nullptr;  // nx x nx: [k][c], k = 0 -> 1
-    float* basis_sx_w_ = nullptr;  // nx x nx: [k][c] = kx 2 sin(...)
-    float* basis_sy_w_ = nullptr;  // ny x ny: [r][l] = ky 2 sin(...)
+    // field solve: spectral divide, Parseval weights, outputs
     float* spectral_scale_ = nullptr;  // ny x nx
     float* weight_y_ = nullptr;
     float* weight_x_ = nullptr;
-    float* stage_a_ = nullptr;
-    float* phi_hat_ = nullptr;
-    float* stage_t_ = nullptr;
-    float* stage_u_ = nullptr;
     float2* field_ = nullptr;
     float* potential_ = nullptr;
 
-    // tcgen05 split-precision form of the same contractions (dct_tc.cu)
-    bool use_tc_ = true;
+    // tcgen05 split-precision contractions (dct_tc.cu)
     SplitMatrix tc_source_, tc_cx_, tc_cy_, tc_dy_, tc_dxc_, tc_sxwt_, tc_syw_;
     SplitMatrix tc_x1t_, tc_phi_, tc_phit_, tc_t_, tc_ut_;
     TcBatch tc_fwd1_{}, tc_fwd2_{}, tc_inv1_{}, tc_inv2_{}, tc_pot_{};
+    int* tc_row_exp_ = nullptr;
+    TcScales* tc_scales_ = nullptr;
     int* tc_error_ = nullptr;
     int* host_error_ = nullptr;
     void buildTensorCoreBasis(const std::vector<double>& cx, const std::vector<double>& cy,
                               const std::vector<double>& dy, const std::vector<double>& dxc,
-                              const std::vector<double>& sxwt, const std::vector<double>& syw);
+                              const std::vector<double>& sxwt, const std::vector<double>& syw, double max_scale);
     SplitMatrix newSplit(int rows, int cols, const char* what);
 
     // partials and scalars
@@ -229,7 +221,8 @@ private:
     bool last_propose_ = false;
 
     // profiling
-    bool timing_ = false;
+    uint32_t timing_mask_ = 0;
+    bool open_ = false;
     std::vector<cudaEvent_t> events_;
     std::vector<int> pending_kind_;
     int pending_ = 0;

@@ -1,7 +1,8 @@
 // The fused per-particle pass of a gradient evaluation, and the scalar reduction.
 //
 // gather: for each particle, in one pass,
-//   wire     = sum of its pins' LSE gradients (fixed pin order: deterministic)
+//   wire     = sum of its pins' LSE gradients, which the wirelength pass wrote
+//              into consecutive slots (fixed pin order: deterministic)
 //   density  = -charge * E(position)  -- bilinear sample of the DCT field with
 //              the Neumann mirror parity (sampleWithParity / reflectIndex,
 //              ElectrostaticField.cpp:289-320; CudaPlacementBackend.cu:158-192, 575-591)
@@ -28,8 +29,8 @@ namespace {
 __device__ __forceinline__ double2 sampleField(const GatherArgs& a, double x, double y) {
     x = fmax(a.llx, fmin(x, a.urx));
     y = fmax(a.lly, fmin(y, a.ury));
-    const double gx = (x - a.llx) / a.bin_w - 0.5;
-    const double gy = (y - a.lly) / a.bin_h - 0.5;
+    const double gx = (x - a.llx) * a.inv_bin_w - 0.5;
+    const double gy = (y - a.lly) * a.inv_bin_h - 0.5;
     const double fx = floor(gx);
     const double fy = floor(gy);
     const int left = static_cast<int>(fx);
@@ -70,7 +71,7 @@ __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
             const int begin = a.particle_pin_start[i];
             const int end = a.particle_pin_start[i + 1];
             for (int j = begin; j < end; ++j) {
-                const float2 g = a.pin_gradient[a.particle_pins[j]];
+                const float2 g = a.pin_gradient[j];
                 wx += static_cast<double>(g.x);
                 wy += static_cast<double>(g.y);
             }

@@ -41,10 +41,11 @@ struct WirelengthArgs {
     const double2* static_pins;   // S absolute static pin positions
     const int* net_start;         // N'+1 (nets with >= 2 pins, bucket order)
     const float* net_weight;      // N'
-    const int4* block_work;       // per block: {group size (0 = warp loop), first net, net count, 0}
+    const int4* block_work;       // per block: {lanes per net (1: two-pin nets, 0: warp loop), first net, net count, 0}
     float gamma;
     float inv_gamma;
-    float2* pin_gradient;         // I' (written when gradient != 0, movable pins only)
+    const int* pin_slot;          // I': the pin's slot in the particle-ordered gradient array (-1: static)
+    float2* pin_gradient;         // particle-ordered slots (written when gradient != 0, movable pins only)
     int gradient;
     double* partials;             // per block: smooth, hpwl
 };
@@ -99,8 +100,7 @@ void launchScatter(const ScatterArgs& args, int blocks, cudaStream_t stream);
 struct MetricsArgs {
     unsigned long long* layers;        // 3 * B, read and reset to zero
     const unsigned long long* totals;  // 3
-    const double* fixed;               // B
-    const double* dark;                // B
+    const double* static_charge;       // B: t * (fixed + dark), the static part of the charge
     double static_fixed_sum;
     double static_dark_sum;
     double target_density;
@@ -111,35 +111,17 @@ struct MetricsArgs {
 };
 void launchMetrics(const MetricsArgs& args, int blocks, cudaStream_t stream);
 
-// ---- dense FP32 contractions for the DCT (SIMT path) ----------------------------------
-struct GemmTask {
-    const float* a;    // M x K row-major (lda)
-    const float* b;    // K x N row-major (ldb)
-    float* c;          // output
-    int m, n, k;
-    int lda, ldb;
-    int ldc;           // row stride of c (elements)
-    int c_step;        // column stride of c (1 plain, 2 interleaved)
-    const float* scale;   // spectral epilogue: c = acc * scale[r*n + c] (nullptr = plain)
-    const float* weight_r;  // energy weights per row / column (spectral epilogue)
-    const float* weight_c;
-    double* energy_partials;  // per block energy partial (spectral epilogue)
-};
-void launchGemm(const GemmTask* tasks, int task_count, cudaStream_t stream);
-int gemmBlocks(const GemmTask& task);
-
 // ---- field gather + gradient combine (the fused update pass) ----------------------------
 struct GatherArgs {
     int particle_count;
     int movable_count;
     const double2* positions;
-    const int* particle_pin_start;  // M+1
-    const int* particle_pins;       // pin indices (bucket order)
-    const float2* pin_gradient;
+    const int* particle_pin_start;  // M+1: particle i's pin gradients are slots [start[i], start[i+1])
+    const float2* pin_gradient;     // particle-ordered slots
     const float2* field;            // B interleaved (Ex, Ey)
     const double* charge;           // P
     const double* precond_base;     // P (nullptr: split mode)
-    double llx, lly, urx, ury, bin_w, bin_h;
+    double llx, lly, urx, ury, inv_bin_w, inv_bin_h;
     int bins_x, bins_y;
     double penalty;
     double precond_scale;           // 1 / density_strength

@@ -8,11 +8,15 @@
 //               + the same in y ),           HPWL_e = w_e * (max x - min x + max y - min y)
 //   dW_e/dx_i = w_e * ( exp((x_i - max)/g) / S+ - exp((min - x_i)/g) / S- )
 //
-// Nets are grouped by degree into buckets of G = 2, 4, 8, 16, 32 lanes per net
-// (a warp loop for degree > 32); the G lanes of a net hold one pin each, so the
-// max/min and the four exponential sums are G-wide shuffle reductions and the
-// pin loads of a warp are contiguous.  Coordinates are taken relative to the
-// net's first pin in FP64 and then carried in FP32 (max-shifted exponentials),
+// Nets are grouped by degree into buckets.  Two-pin nets (most of a netlist)
+// take one thread each and a closed form of the same expressions: with
+// d = x_a - x_b and t = exp(-|d|/g), W = |d| + 2 g ln(1 + t) and
+// dW/dx_a = -dW/dx_b = w tanh(d / 2g) = w sign(d) (1 - t) / (1 + t).  Larger
+// nets take G = 4, 8, 16, 32 lanes (a warp loop above 32); the G lanes of a
+// net hold one pin each, so the max/min and the four exponential sums are
+// G-wide shuffle reductions and the pin loads of a warp are contiguous.
+// Coordinates are taken relative to the net's first pin in FP64 and then
+// carried in FP32 (max-shifted exponentials, hardware exp2/log2/reciprocal),
 // per-net totals are accumulated in FP64.  The per-pin gradient is written to
 // a pin-indexed buffer (no atomics); the particle gather sums it in a fixed
 // order, so the wire gradient is deterministic.
@@ -70,6 +74,36 @@ __device__ __forceinline__ float groupSum(float v) {
     return v;
 }
 
+// exp(v) for v <= 0 and ln(v) for v >= 1 on the special-function unit.
+__device__ __forceinline__ float fastExp(float v) { return __expf(v); }
+__device__ __forceinline__ float fastLog(float v) { return __logf(v); }
+
+// Two-pin nets, one thread per net; the bucket's pins are consecutive pairs.
+__device__ void netPairs(const WirelengthArgs& a, int first, int count, double& smooth, double& hpwl) {
+    const int local = static_cast<int>(threadIdx.x);
+    if (local >= count) return;  // the caller's block reduction follows; every thread still reaches it
+    const int net = first + local;
+    const int begin = a.net_start[net];
+    const PinPoint p = loadPin(a, begin);
+    const PinPoint q = loadPin(a, begin + 1);
+    const float weight = a.net_weight[net];
+    const float dx = static_cast<float>(p.x - q.x);
+    const float dy = static_cast<float>(p.y - q.y);
+    const float ax = fabsf(dx), ay = fabsf(dy);
+    const float tx = fastExp(-ax * a.inv_gamma);
+    const float ty = fastExp(-ay * a.inv_gamma);
+    const float span = ax + ay;
+    const float soft = 2.0f * a.gamma * (fastLog(1.0f + tx) + fastLog(1.0f + ty));
+    smooth += static_cast<double>(weight) * (static_cast<double>(span) + static_cast<double>(soft));
+    hpwl += static_cast<double>(weight) * static_cast<double>(span);
+    if (a.gradient) {
+        const float gx = copysignf(weight * __fdividef(1.0f - tx, 1.0f + tx), dx);
+        const float gy = copysignf(weight * __fdividef(1.0f - ty, 1.0f + ty), dy);
+        if (p.particle >= 0) a.pin_gradient[a.pin_slot[begin]] = make_float2(gx, gy);
+        if (q.particle >= 0) a.pin_gradient[a.pin_slot[begin + 1]] = make_float2(-gx, -gy);
+    }
+}
+
 // G lanes per net, degree <= G.
 template <int G>
 __device__ void netGroups(const WirelengthArgs& a, int first, int count, double& smooth, double& hpwl) {
@@ -100,33 +134,34 @@ __device__ void netGroups(const WirelengthArgs& a, int first, int count, double&
         const float min_x = groupMin<G>(pin_ok ? dx : FLT_MAX);
         const float max_y = groupMax<G>(pin_ok ? dy : -FLT_MAX);
         const float min_y = groupMin<G>(pin_ok ? dy : FLT_MAX);
-        const float epx = pin_ok ? expf((dx - max_x) * a.inv_gamma) : 0.0f;
-        const float enx = pin_ok ? expf((min_x - dx) * a.inv_gamma) : 0.0f;
-        const float epy = pin_ok ? expf((dy - max_y) * a.inv_gamma) : 0.0f;
-        const float eny = pin_ok ? expf((min_y - dy) * a.inv_gamma) : 0.0f;
+        const float epx = pin_ok ? fastExp((dx - max_x) * a.inv_gamma) : 0.0f;
+        const float enx = pin_ok ? fastExp((min_x - dx) * a.inv_gamma) : 0.0f;
+        const float epy = pin_ok ? fastExp((dy - max_y) * a.inv_gamma) : 0.0f;
+        const float eny = pin_ok ? fastExp((min_y - dy) * a.inv_gamma) : 0.0f;
         const float spx = groupSum<G>(epx);
         const float snx = groupSum<G>(enx);
         const float spy = groupSum<G>(epy);
         const float sny = groupSum<G>(eny);
         if (net_ok && sub == 0) {
             const float span = (max_x - min_x) + (max_y - min_y);
-            const float soft = a.gamma * (logf(spx) + logf(snx) + logf(spy) + logf(sny));
+            const float soft = a.gamma * (fastLog(spx) + fastLog(snx) + fastLog(spy) + fastLog(sny));
             smooth += static_cast<double>(weight) * (static_cast<double>(span) + static_cast<double>(soft));
             hpwl += static_cast<double>(weight) * static_cast<double>(span);
         }
         if (a.gradient && pin_ok && p.particle >= 0) {
-            const float gx = weight * (epx / spx - enx / snx);
-            const float gy = weight * (epy / spy - eny / sny);
-            a.pin_gradient[begin + sub] = make_float2(gx, gy);
+            const float gx = weight * (__fdividef(epx, spx) - __fdividef(enx, snx));
+            const float gy = weight * (__fdividef(epy, spy) - __fdividef(eny, sny));
+            a.pin_gradient[a.pin_slot[begin + sub]] = make_float2(gx, gy);
         }
     }
 }
 
 // One net of any degree on one warp: three passes over its pins.  `load(pin)`
-// returns the pin's position and particle; gradients go to pin_gradient[pin].
-template <class Loader>
+// returns the pin's position and particle; store(pin, gradient) keeps a
+// movable pin's gradient.
+template <class Loader, class Store>
 __device__ void netOnWarp(const Loader& load, int begin, int end, float weight, float gamma, float inv_gamma,
-                          bool gradient, float2* pin_gradient, double& smooth, double& hpwl) {
+                          bool gradient, const Store& store, double& smooth, double& hpwl) {
     const int lane = threadIdx.x & 31;
     {
         const PinPoint first_pin = load(begin);
@@ -174,7 +209,7 @@ __device__ void netOnWarp(const Loader& load, int begin, int end, float weight, 
                 const float dy = static_cast<float>(p.y - ry);
                 const float gx = weight * (expf((dx - max_x) * inv_gamma) / spx - expf((min_x - dx) * inv_gamma) / snx);
                 const float gy = weight * (expf((dy - max_y) * inv_gamma) / spy - expf((min_y - dy) * inv_gamma) / sny);
-                pin_gradient[pin] = make_float2(gx, gy);
+                store(pin, make_float2(gx, gy));
             }
         }
     }
@@ -185,6 +220,16 @@ struct EnginePinLoader {
     __device__ PinPoint operator()(int pin) const { return loadPin(*a, pin); }
 };
 
+struct SlotStore {
+    const WirelengthArgs* a;
+    __device__ void operator()(int pin, float2 g) const { a->pin_gradient[a->pin_slot[pin]] = g; }
+};
+
+struct PinStore {
+    float2* pin_gradient;
+    __device__ void operator()(int pin, float2 g) const { pin_gradient[pin] = g; }
+};
+
 // Warp-per-net bucket (degree > 32) of the engine's wirelength pass.
 __device__ void netWarps(const WirelengthArgs& a, int first, int count, double& smooth, double& hpwl) {
     const int warp = threadIdx.x >> 5;
@@ -192,7 +237,7 @@ __device__ void netWarps(const WirelengthArgs& a, int first, int count, double& 
     const EnginePinLoader load{&a};
     for (int local = warp; local < count; local += warps) {
         netOnWarp(load, a.net_start[first + local], a.net_start[first + local + 1], a.net_weight[first + local],
-                  a.gamma, a.inv_gamma, a.gradient != 0, a.pin_gradient, smooth, hpwl);
+                  a.gamma, a.inv_gamma, a.gradient != 0, SlotStore{&a}, smooth, hpwl);
     }
 }
 
@@ -200,7 +245,7 @@ __global__ void __launch_bounds__(kThreads) wirelengthKernel(WirelengthArgs a) {
     const int4 work = a.block_work[blockIdx.x];
     double values[2] = {0.0, 0.0};
     switch (work.x) {
-        case 2: netGroups<2>(a, work.y, work.z, values[0], values[1]); break;
+        case 1: netPairs(a, work.y, work.z, values[0], values[1]); break;
         case 4: netGroups<4>(a, work.y, work.z, values[0], values[1]); break;
         case 8: netGroups<8>(a, work.y, work.z, values[0], values[1]); break;
         case 16: netGroups<16>(a, work.y, work.z, values[0], values[1]); break;
@@ -283,8 +328,8 @@ __global__ void __launch_bounds__(kThreads) noAllocNetKernel(CallerPinLoader loa
             for (int pin = begin + lane; pin < end; pin += 32) pin_gradient[pin] = make_float2(0.0f, 0.0f);
             continue;
         }
-        netOnWarp(load, begin, end, static_cast<float>(net_weight[net]), gamma, inv_gamma, true, pin_gradient,
-                  values[0], values[1]);
+        netOnWarp(load, begin, end, static_cast<float>(net_weight[net]), gamma, inv_gamma, true,
+                  PinStore{pin_gradient}, values[0], values[1]);
     }
     const bool is_max[2] = {false, false};
     blockReduce<2>(values, is_max);

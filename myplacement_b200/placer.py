@@ -118,8 +118,21 @@ class Session:
     def stream(self) -> int:
         return int(self.lib.mpgp_session_stream(self.handle) or 0)
 
-    def set_profiling(self, enabled: bool) -> None:
-        check(self.lib.mpgp_session_set_profiling(self.handle, int(enabled)))
+    def set_profiling(self, families=True) -> None:
+        """Times every launch of the given kernel families (names, or True for all, False for none)."""
+        if families is True:
+            mask = (1 << self.lib.mpgp_kernel_kind_count()) - 1
+        elif families is False or families is None:
+            mask = 0
+        else:
+            names = [self.lib.mpgp_kernel_kind_name(k).decode() for k in range(self.lib.mpgp_kernel_kind_count())]
+            mask = 0
+            for name in families:
+                mask |= 1 << names.index(name)
+        check(self.lib.mpgp_session_set_profiling(self.handle, mask))
+
+    def reset_kernel_stats(self) -> None:
+        check(self.lib.mpgp_session_reset_kernel_stats(self.handle))
 
     def kernel_stats(self) -> dict:
         """{family: (launches, device milliseconds)} accumulated while profiling was on."""
