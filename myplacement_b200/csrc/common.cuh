@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 #include "mpgp.h"
 
@@ -47,6 +48,15 @@ inline int ceilDiv(long long value, long long divisor) {
 // ---- device helpers -------------------------------------------------------------------
 
 #ifdef __CUDACC__
+
+// Programmatic dependent launch.  A kernel started with launchChained may begin
+// while its predecessor on the stream is still running: it releases its own
+// successor with releaseNext() at entry, does work that reads nothing the
+// predecessor writes, and calls waitForPrior() before the first access to the
+// predecessor's results (griddepcontrol.wait returns once the predecessor grid
+// has completed and its memory is visible).
+__device__ __forceinline__ void waitForPrior() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void releaseNext() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 __device__ __forceinline__ double warpSum(double value) {
 #pragma unroll
@@ -91,5 +101,22 @@ __device__ __forceinline__ long long warpSumI64(long long value) {
 }
 
 #endif
+
+// Launch with programmatic stream serialisation (see waitForPrior / releaseNext).
+template <typename... Params, typename... Args>
+inline void launchChained(const char* what, void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem,
+                          cudaStream_t stream, Args&&... args) {
+    cudaLaunchConfig_t config{};
+    config.gridDim = grid;
+    config.blockDim = block;
+    config.dynamicSmemBytes = smem;
+    config.stream = stream;
+    cudaLaunchAttribute attribute[1];
+    attribute[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attribute[0].val.programmaticStreamSerializationAllowed = 1;
+    config.attrs = attribute;
+    config.numAttrs = 1;
+    checkCuda(cudaLaunchKernelEx(&config, kernel, std::forward<Args>(args)...), what);
+}
 
 }  // namespace mpgp

@@ -251,6 +251,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
     const int tiles_n = (t.n + kTileN - 1) / kTileN;
     const int tiles_m = (t.m + kTileM - 1) / kTileM;
     const int tile_index = static_cast<int>(blockIdx.x) / ksplit;
+    releaseNext();
     // The whole cluster shares the tile, so the whole cluster leaves together.
     if (tile_index >= tiles_m * tiles_n) return;
     const int split = static_cast<int>(clusterRank());
@@ -300,6 +301,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
     }
     __syncthreads();
     clusterArrive();  // this CTA's barriers are initialised; peers wait for it before sending
+    waitForPrior();   // the operands and scale bookkeeping come from the previous kernels
 
     if (warp == 0) {
         if (lane == 0) {
@@ -595,6 +597,8 @@ EncodeTiled encoder() {
 // One warp per source row: the row's exponent from its maximum, then its planes.
 __global__ void splitSourceKernel(const float* source, int rows, int cols, __half* out, int ld, size_t plane,
                                   int* row_exp, TcScales* scales) {
+    releaseNext();
+    waitForPrior();
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         scales->max_x = 0u;
         scales->max_phi = 0u;
@@ -641,12 +645,14 @@ cudaLaunchConfig_t launchConfig(dim3 grid, int ksplit, cudaStream_t stream, cuda
     config.blockDim = dim3(kTcThreads);
     config.dynamicSmemBytes = kSmemBytes;
     config.stream = stream;
-    attribute->id = cudaLaunchAttributeClusterDimension;
-    attribute->val.clusterDim.x = static_cast<unsigned>(ksplit);
-    attribute->val.clusterDim.y = 1;
-    attribute->val.clusterDim.z = 1;
+    attribute[0].id = cudaLaunchAttributeClusterDimension;
+    attribute[0].val.clusterDim.x = static_cast<unsigned>(ksplit);
+    attribute[0].val.clusterDim.y = 1;
+    attribute[0].val.clusterDim.z = 1;
+    attribute[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attribute[1].val.programmaticStreamSerializationAllowed = 1;
     config.attrs = attribute;
-    config.numAttrs = 1;
+    config.numAttrs = 2;
     return config;
 }
 
@@ -679,9 +685,9 @@ void tcPlan(TcBatch& batch, int task_count) {
     }
     batch.ksplit = 1;
     for (int ksplit = 2; ksplit <= kMaxSplit && ksplit <= k_blocks; ksplit *= 2) {
-        cudaLaunchAttribute attribute{};
+        cudaLaunchAttribute attribute[2] = {};
         cudaLaunchConfig_t config =
-            launchConfig(dim3(static_cast<unsigned>(tiles * ksplit)), ksplit, nullptr, &attribute);
+            launchConfig(dim3(static_cast<unsigned>(tiles * ksplit)), ksplit, nullptr, attribute);
         int clusters = 0;
         if (cudaOccupancyMaxActiveClusters(&clusters, tcGemmKernel, &config) != cudaSuccess) {
             (void)cudaGetLastError();
@@ -701,10 +707,10 @@ void launchTcGemm(const TcBatch& batch, int task_count, cudaStream_t stream) {
     configureKernel();
     require(batch.ksplit >= 1 && batch.ksplit <= kMaxSplit && (batch.ksplit & (batch.ksplit - 1)) == 0,
             "Contraction K split must be a power of two up to 8.");
-    cudaLaunchAttribute attribute{};
+    cudaLaunchAttribute attribute[2] = {};
     const cudaLaunchConfig_t config =
         launchConfig(dim3(static_cast<unsigned>(tcBlocks(batch, task_count)), static_cast<unsigned>(task_count)),
-                     batch.ksplit, stream, &attribute);
+                     batch.ksplit, stream, attribute);
     checkCuda(cudaLaunchKernelEx(&config, tcGemmKernel, batch), "Launch the tcgen05 contraction kernel");
 }
 
@@ -734,8 +740,8 @@ void launchSplitSource(const float* source, const SplitMatrix& out, int cols, in
                        cudaStream_t stream) {
     if (out.rows <= 0) return;
     const int rows_per_block = kThreads / 32;
-    splitSourceKernel<<<ceilDiv(out.rows, rows_per_block), kThreads, 0, stream>>>(
-        source, out.rows, cols, out.data, out.ld, out.plane(), row_exp, scales);
+    launchChained("Launch the source split", splitSourceKernel, dim3(ceilDiv(out.rows, rows_per_block)),
+                  dim3(kThreads), 0, stream, source, out.rows, cols, out.data, out.ld, out.plane(), row_exp, scales);
 }
 
 }  // namespace mpgp

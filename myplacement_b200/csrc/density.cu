@@ -35,6 +35,8 @@ __device__ __forceinline__ double clampCenter(double value, double size, double 
 }
 
 __global__ void __launch_bounds__(kThreads) scatterKernel(ScatterArgs a) {
+    releaseNext();
+    waitForPrior();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double predicted = 0.0;
     double displacement = 0.0;
@@ -164,6 +166,8 @@ struct BinTerms {
 };
 
 __global__ void __launch_bounds__(kThreads) metricsKernel(MetricsArgs a) {
+    releaseNext();
+    waitForPrior();
     BinTerms terms;
     terms.t = a.target_density;
     terms.unit = a.bin_area * kFixedUnit;
@@ -217,6 +221,8 @@ __global__ void __launch_bounds__(kThreads) metricsKernel(MetricsArgs a) {
 }
 
 __global__ void velocityKernel(const double2* next, const double2* previous, double2* velocity, int count) {
+    releaseNext();
+    waitForPrior();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const double2 n = next[i];
@@ -228,16 +234,17 @@ __global__ void velocityKernel(const double2* next, const double2* previous, dou
 
 void launchScatter(const ScatterArgs& args, int blocks, cudaStream_t stream) {
     if (blocks <= 0) return;
-    scatterKernel<<<blocks, kThreads, 0, stream>>>(args);
+    launchChained("Launch the density scatter", scatterKernel, dim3(blocks), dim3(kThreads), 0, stream, args);
 }
 
 void launchMetrics(const MetricsArgs& args, int blocks, cudaStream_t stream) {
-    metricsKernel<<<blocks, kThreads, 0, stream>>>(args);
+    launchChained("Launch the density metrics", metricsKernel, dim3(blocks), dim3(kThreads), 0, stream, args);
 }
 
 void launchVelocity(const double2* next, const double2* previous, double2* velocity, int count, cudaStream_t stream) {
     if (count <= 0) return;
-    velocityKernel<<<ceilDiv(count, kThreads), kThreads, 0, stream>>>(next, previous, velocity, count);
+    launchChained("Launch the velocity update", velocityKernel, dim3(ceilDiv(count, kThreads)), dim3(kThreads), 0,
+                  stream, next, previous, velocity, count);
 }
 
 }  // namespace mpgp

@@ -63,6 +63,8 @@ __device__ __forceinline__ double2 sampleField(const GatherArgs& a, double x, do
 }
 
 __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
+    releaseNext();
+    waitForPrior();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v[7] = {0, 0, 0, 0, 0, 0, 0};
     if (i < a.particle_count) {
@@ -119,6 +121,8 @@ __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
 }
 
 __global__ void __launch_bounds__(kThreads) reduceKernel(ReduceArgs a) {
+    releaseNext();
+    waitForPrior();
     const int s = blockIdx.x;
     if (s >= a.source_count) {
         return;
@@ -146,12 +150,13 @@ __global__ void __launch_bounds__(kThreads) reduceKernel(ReduceArgs a) {
 
 void launchGather(const GatherArgs& args, int blocks, cudaStream_t stream) {
     if (blocks <= 0) return;
-    gatherKernel<<<blocks, kThreads, 0, stream>>>(args);
+    launchChained("Launch the field gather", gatherKernel, dim3(blocks), dim3(kThreads), 0, stream, args);
 }
 
 void launchReduce(const ReduceArgs& args, cudaStream_t stream) {
     if (args.source_count <= 0) return;
-    reduceKernel<<<args.source_count, kThreads, 0, stream>>>(args);
+    launchChained("Launch the scalar reduction", reduceKernel, dim3(args.source_count), dim3(kThreads), 0, stream,
+                  args);
 }
 
 }  // namespace mpgp

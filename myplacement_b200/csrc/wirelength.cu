@@ -242,6 +242,8 @@ __device__ void netWarps(const WirelengthArgs& a, int first, int count, double& 
 }
 
 __global__ void __launch_bounds__(kThreads) wirelengthKernel(WirelengthArgs a) {
+    releaseNext();
+    waitForPrior();
     const int4 work = a.block_work[blockIdx.x];
     double values[2] = {0.0, 0.0};
     switch (work.x) {
@@ -264,7 +266,7 @@ __global__ void __launch_bounds__(kThreads) wirelengthKernel(WirelengthArgs a) {
 
 void launchWirelength(const WirelengthArgs& args, int blocks, cudaStream_t stream) {
     if (blocks <= 0) return;
-    wirelengthKernel<<<blocks, kThreads, 0, stream>>>(args);
+    launchChained("Launch the wirelength pass", wirelengthKernel, dim3(blocks), dim3(kThreads), 0, stream, args);
 }
 
 // ---- allocation-free variant --------------------------------------------------------
