@@ -395,6 +395,64 @@ int64_t mpgp_session_kernel_launches(const mpgp_session* session);
 void* mpgp_session_stream(const mpgp_session* session);
 void mpgp_session_destroy(mpgp_session* session);
 
+/* ---- batched and served forms ------------------------------------------------
+ *
+ * No counterpart in the reference, which places one design per process
+ * (main.cpp:413, GlobalPlacer::run).  A server runs many independent
+ * placements (each exactly mpgp_global_place) at once on one GPU: a FIFO of
+ * jobs, `workers` host threads each driving one device-resident session on its
+ * own streams, and admission by estimated device footprint against
+ * `memory_budget_bytes` (0 = 90 % of the device's free memory).  A job that
+ * arrives while others run starts as soon as a worker and the memory are free;
+ * its result is the same as when it runs alone. */
+typedef struct mpgp_server mpgp_server;
+
+typedef struct mpgp_job_stats {
+    double queued_seconds;          /* submit -> start */
+    double run_seconds;             /* start -> finish */
+    double latency_seconds;         /* submit -> finish */
+    uint64_t estimated_bytes;       /* the footprint the admission reserved */
+    uint64_t reserved_bytes;        /* device bytes the job's session actually reserved */
+    int32_t completed_iterations;
+    int32_t status;                 /* MPGP_OK, or the job's failure */
+} mpgp_job_stats;
+
+typedef struct mpgp_server_stats {
+    int64_t submitted;
+    int64_t completed;
+    int64_t failed;
+    int64_t iterations;             /* controller iterations of completed jobs */
+    int32_t workers;
+    int32_t peak_running;           /* most jobs on the device at once */
+    uint64_t memory_budget;
+    uint64_t peak_reserved;         /* largest sum of admitted footprints */
+    double seconds;                 /* since the server was created */
+} mpgp_server_stats;
+
+/* Upper bound of the device bytes one placement of `design` reserves. */
+int mpgp_estimate_bytes(const mpgp_design* design, const mpgp_options* options, uint64_t* bytes);
+int mpgp_server_create(int device, uint64_t memory_budget_bytes, int32_t workers, mpgp_server** out);
+/* Copies the design and options (options->cuda_device is replaced by the
+ * server's device).  A job whose footprint exceeds the budget is refused with
+ * MPGP_ERR_BUDGET. */
+int mpgp_server_submit(mpgp_server* server, const mpgp_design* design, const mpgp_options* options, int64_t* job);
+/* Waits up to timeout_seconds (< 0: without limit); *done = 1 once the job has finished. */
+int mpgp_server_wait(mpgp_server* server, int64_t job, double timeout_seconds, int32_t* done);
+/* Copies a finished job's outputs (as mpgp_global_place) and releases it; a
+ * failed job returns its failure status here. */
+int mpgp_server_take(mpgp_server* server, int64_t job, double* module_x, double* module_y, mpgp_result* result,
+                     mpgp_history_row* history, int32_t history_capacity, mpgp_job_stats* stats);
+int mpgp_server_stats_get(const mpgp_server* server, mpgp_server_stats* stats);
+/* Finishes the running jobs, abandons the queued ones, joins the workers. */
+void mpgp_server_destroy(mpgp_server* server);
+
+/* The batched form: `count` placements through a server (submit all, take all).
+ * module_x[i] / module_y[i] receive design i's positions; history is not kept. */
+int mpgp_batch_place(int32_t count, const mpgp_design* designs, const mpgp_options* options, int device,
+                     int32_t workers, uint64_t memory_budget_bytes, double* const* module_x,
+                     double* const* module_y, mpgp_result* results, mpgp_job_stats* job_stats,
+                     mpgp_server_stats* server_stats);
+
 #ifdef __cplusplus
 }
 #endif

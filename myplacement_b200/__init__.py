@@ -7,11 +7,12 @@ synthetic designs the engine is measured on.
 """
 from ._abi import EngineError, load_library
 from .design import Design, synthetic_design, workload
-from .placer import (BackendLayout, CudaPlacementBackend, GlobalPlacer, PlacementResult, Session, build_layout,
-                     default_options, host_setup, random_placement, try_create_backend)
+from .placer import (BackendLayout, CudaPlacementBackend, GlobalPlacer, PlacementResult, PlacementServer, Session,
+                     batch_place, build_layout, default_options, estimate_bytes, host_setup, random_placement,
+                     try_create_backend)
 
 __all__ = [
-    "BackendLayout", "CudaPlacementBackend", "Design", "EngineError", "GlobalPlacer", "PlacementResult", "Session",
-    "build_layout", "default_options", "host_setup", "load_library", "random_placement", "synthetic_design", "try_create_backend",
+    "BackendLayout", "CudaPlacementBackend", "Design", "EngineError", "GlobalPlacer", "PlacementResult",
+    "PlacementServer", "Session", "batch_place", "build_layout", "estimate_bytes", "default_options", "host_setup", "load_library", "random_placement", "synthetic_design", "try_create_backend",
     "workload",
 ]

@@ -229,6 +229,38 @@ class Layout(C.Structure):
     ]
 
 
+class JobStats(C.Structure):
+    _fields_ = [
+        ("queued_seconds", C.c_double),
+        ("run_seconds", C.c_double),
+        ("latency_seconds", C.c_double),
+        ("estimated_bytes", C.c_uint64),
+        ("reserved_bytes", C.c_uint64),
+        ("completed_iterations", C.c_int32),
+        ("status", C.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64),
+        ("completed", C.c_int64),
+        ("failed", C.c_int64),
+        ("iterations", C.c_int64),
+        ("workers", C.c_int32),
+        ("peak_running", C.c_int32),
+        ("memory_budget", C.c_uint64),
+        ("peak_reserved", C.c_uint64),
+        ("seconds", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 def _declare(lib: C.CDLL) -> C.CDLL:
     vp = C.c_void_p
     sig = {
@@ -266,6 +298,17 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "mpgp_session_transfer_bytes": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "mpgp_session_stream": (vp, [vp]),
         "mpgp_session_destroy": (None, [vp]),
+        "mpgp_estimate_bytes": (C.c_int, [C.POINTER(Design), C.POINTER(Options), C.POINTER(C.c_uint64)]),
+        "mpgp_server_create": (C.c_int, [C.c_int, C.c_uint64, C.c_int32, C.POINTER(vp)]),
+        "mpgp_server_submit": (C.c_int, [vp, C.POINTER(Design), C.POINTER(Options), C.POINTER(C.c_int64)]),
+        "mpgp_server_wait": (C.c_int, [vp, C.c_int64, C.c_double, _i32]),
+        "mpgp_server_take": (C.c_int, [vp, C.c_int64, _d, _d, C.POINTER(Result), C.POINTER(HistoryRow), C.c_int32,
+                                       C.POINTER(JobStats)]),
+        "mpgp_server_stats_get": (C.c_int, [vp, C.POINTER(ServerStats)]),
+        "mpgp_server_destroy": (None, [vp]),
+        "mpgp_batch_place": (C.c_int, [C.c_int32, C.POINTER(Design), C.POINTER(Options), C.c_int, C.c_int32,
+                                       C.c_uint64, C.POINTER(_d), C.POINTER(_d), C.POINTER(Result),
+                                       C.POINTER(JobStats), C.POINTER(ServerStats)]),
     }
     for name, (restype, argtypes) in sig.items():
         fn = getattr(lib, name)

@@ -15,6 +15,7 @@
 #include "engine.cuh"
 #include "mpgp.h"
 #include "session.hpp"
+#include "server.hpp"
 #include "setup.hpp"
 
 namespace {
@@ -55,6 +56,10 @@ struct mpgp_backend {
 
 struct mpgp_session {
     std::unique_ptr<mpgp::Session> session;
+};
+
+struct mpgp_server {
+    std::unique_ptr<mpgp::Server> server;
 };
 
 struct mpgp_setup {
@@ -355,6 +360,86 @@ int mpgp_global_place(const mpgp_design* design, const mpgp_options* options, do
         while (!session.step(64, nullptr)) {
         }
         session.finish(module_x, module_y, result, history, history_capacity);
+    });
+}
+
+
+int mpgp_estimate_bytes(const mpgp_design* design, const mpgp_options* options, uint64_t* bytes) {
+    return guarded([&] {
+        mpgp::require(design != nullptr && options != nullptr && bytes != nullptr, "Arguments are required.");
+        *bytes = mpgp::estimateSessionBytes(*design, *options);
+    });
+}
+
+int mpgp_server_create(int device, uint64_t memory_budget_bytes, int32_t workers, mpgp_server** out) {
+    return guarded([&] {
+        mpgp::require(out != nullptr, "An output handle is required.");
+        *out = nullptr;
+        auto handle = std::make_unique<mpgp_server>();
+        handle->server = std::make_unique<mpgp::Server>(device, memory_budget_bytes, workers);
+        *out = handle.release();
+    });
+}
+
+int mpgp_server_submit(mpgp_server* s, const mpgp_design* design, const mpgp_options* options, int64_t* job) {
+    return guarded([&] {
+        mpgp::require(s != nullptr && design != nullptr && options != nullptr && job != nullptr,
+                      "Arguments are required.");
+        *job = s->server->submit(*design, *options);
+    });
+}
+
+int mpgp_server_wait(mpgp_server* s, int64_t job, double timeout_seconds, int32_t* done) {
+    return guarded([&] {
+        mpgp::require(s != nullptr, "A server is required.");
+        const bool finished = s->server->wait(job, timeout_seconds);
+        if (done != nullptr) *done = finished ? 1 : 0;
+    });
+}
+
+int mpgp_server_take(mpgp_server* s, int64_t job, double* module_x, double* module_y, mpgp_result* result,
+                     mpgp_history_row* history, int32_t history_capacity, mpgp_job_stats* stats) {
+    return guarded([&] {
+        mpgp::require(s != nullptr, "A server is required.");
+        s->server->take(job, module_x, module_y, result, history, history_capacity, stats);
+    });
+}
+
+int mpgp_server_stats_get(const mpgp_server* s, mpgp_server_stats* stats) {
+    return guarded([&] {
+        mpgp::require(s != nullptr && stats != nullptr, "Arguments are required.");
+        *stats = s->server->stats();
+    });
+}
+
+void mpgp_server_destroy(mpgp_server* s) { delete s; }
+
+int mpgp_batch_place(int32_t count, const mpgp_design* designs, const mpgp_options* options, int device,
+                     int32_t workers, uint64_t memory_budget_bytes, double* const* module_x, double* const* module_y,
+                     mpgp_result* results, mpgp_job_stats* job_stats, mpgp_server_stats* server_stats) {
+    return guarded([&] {
+        mpgp::require(count >= 0 && (count == 0 || (designs != nullptr && options != nullptr)),
+                      "Designs and options are required.");
+        mpgp::Server server(device, memory_budget_bytes, workers);
+        std::vector<int64_t> ids(static_cast<std::size_t>(count));
+        for (int32_t i = 0; i < count; ++i) ids[i] = server.submit(designs[i], options[i]);
+        int first_failure = MPGP_OK;
+        std::string message;
+        for (int32_t i = 0; i < count; ++i) {
+            server.wait(ids[i], -1.0);
+            try {
+                server.take(ids[i], module_x != nullptr ? module_x[i] : nullptr,
+                            module_y != nullptr ? module_y[i] : nullptr, results != nullptr ? &results[i] : nullptr,
+                            nullptr, 0, job_stats != nullptr ? &job_stats[i] : nullptr);
+            } catch (const mpgp::Error& e) {
+                if (first_failure == MPGP_OK) {
+                    first_failure = e.status();
+                    message = "job " + std::to_string(i) + ": " + e.what();
+                }
+            }
+        }
+        if (server_stats != nullptr) *server_stats = server.stats();
+        if (first_failure != MPGP_OK) mpgp::fail(first_failure, message);
     });
 }
 

@@ -621,13 +621,18 @@ __global__ void splitSourceKernel(const float* source, int rows, int cols, __hal
     for (int c = lane; c < cols; c += 32) splitScaled(src[c], inv_scale, dst[c], dst[c + plane]);
 }
 
+// The shared-memory attribute is per device: set it once on each device that launches.
 void configureKernel() {
-    static std::once_flag once;
-    static cudaError_t attribute = cudaSuccess;
-    std::call_once(once, [] {
-        attribute = cudaFuncSetAttribute(tcGemmKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    constexpr int kMaxDevices = 64;
+    static std::once_flag once[kMaxDevices];
+    static cudaError_t attribute[kMaxDevices] = {};
+    int device = 0;
+    checkCuda(cudaGetDevice(&device), "Query the current device");
+    require(device >= 0 && device < kMaxDevices, "Device index out of range.");
+    std::call_once(once[device], [device] {
+        attribute[device] = cudaFuncSetAttribute(tcGemmKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
     });
-    checkCuda(attribute, "Configure the tcgen05 contraction kernel");
+    checkCuda(attribute[device], "Configure the tcgen05 contraction kernel");
 }
 
 int batchTiles(const TcBatch& batch, int task_count) {

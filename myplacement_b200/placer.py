@@ -322,3 +322,97 @@ def try_create_backend(layout: BackendLayout, device: int = 0, maximum_bytes: in
         return None, reason.value.decode(errors="replace")
     check(status)
     return CudaPlacementBackend(handle, int(s.particle_count)), ""
+
+
+# ---- batched and served forms ------------------------------------------------------
+
+
+def estimate_bytes(design: Design, options: _abi.Options) -> int:
+    """Upper bound of the device bytes one placement of `design` reserves (the server's admission unit)."""
+    lib = load_library()
+    out = C.c_uint64()
+    s = design.as_c()
+    check(lib.mpgp_estimate_bytes(C.byref(s), C.byref(options), C.byref(out)))
+    return int(out.value)
+
+
+class PlacementServer:
+    """Many placements at once on one GPU (mpgp_server_*): submit jobs as they arrive, take results.
+
+    Each job is a full adaptive global placement (GlobalPlacer.run).  `workers`
+    host threads each drive one device-resident session; a job starts when a
+    worker is free and its estimated footprint fits in `memory_budget` (bytes;
+    0 = 90 % of the device's free memory).  Results do not depend on the mix.
+    """
+
+    def __init__(self, device: int = 0, memory_budget: int = 0, workers: int = 8):
+        self.lib = load_library()
+        self.handle = C.c_void_p()
+        check(self.lib.mpgp_server_create(device, memory_budget, workers, C.byref(self.handle)))
+        self._modules: dict[int, int] = {}
+        self._capacity: dict[int, int] = {}
+
+    def submit(self, design: Design, options: _abi.Options) -> int:
+        job = C.c_int64()
+        s = design.as_c()
+        check(self.lib.mpgp_server_submit(self.handle, C.byref(s), C.byref(options), C.byref(job)))
+        self._modules[job.value] = design.module_count
+        self._capacity[job.value] = max(1, options.iterations)
+        return int(job.value)
+
+    def wait(self, job: int, timeout: float = -1.0) -> bool:
+        done = C.c_int32()
+        check(self.lib.mpgp_server_wait(self.handle, job, timeout, C.byref(done)))
+        return bool(done.value)
+
+    def take(self, job: int, history: bool = True) -> tuple[PlacementResult, dict]:
+        """The finished job's PlacementResult and its timing (queued, run, latency seconds; footprint)."""
+        n = self._modules.pop(job)
+        capacity = self._capacity.pop(job) if history else 0
+        x, y = np.empty(n), np.empty(n)
+        result = _abi.Result()
+        stats = _abi.JobStats()
+        rows = (_abi.HistoryRow * max(1, capacity))()
+        check(self.lib.mpgp_server_take(self.handle, job, _ptr(x, _d), _ptr(y, _d), C.byref(result), rows, capacity,
+                                        C.byref(stats)))
+        rows_kept = [rows[i].as_dict() for i in range(min(result.history_count, capacity))]
+        return PlacementResult(x, y, result.as_dict(), rows_kept), stats.as_dict()
+
+    def stats(self) -> dict:
+        out = _abi.ServerStats()
+        check(self.lib.mpgp_server_stats_get(self.handle, C.byref(out)))
+        return out.as_dict()
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.mpgp_server_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        self.close()
+
+
+def batch_place(designs: list[Design], options: list[_abi.Options], device: int = 0, workers: int = 16,
+                memory_budget: int = 0) -> tuple[list[PlacementResult], list[dict], dict]:
+    """The batched form (mpgp_batch_place): every design placed, many at once; (results, job stats, server stats)."""
+    lib = load_library()
+    count = len(designs)
+    structs = (_abi.Design * count)(*[d.as_c() for d in designs])
+    opts = (_abi.Options * count)(*options)
+    xs = [np.empty(d.module_count) for d in designs]
+    ys = [np.empty(d.module_count) for d in designs]
+    px = (_d * count)(*[_ptr(a, _d) for a in xs])
+    py = (_d * count)(*[_ptr(a, _d) for a in ys])
+    results = (_abi.Result * count)()
+    job_stats = (_abi.JobStats * count)()
+    server_stats = _abi.ServerStats()
+    check(lib.mpgp_batch_place(count, structs, opts, device, workers, memory_budget, px, py, results, job_stats,
+                               C.byref(server_stats)))
+    placed = [PlacementResult(xs[i], ys[i], results[i].as_dict()) for i in range(count)]
+    return placed, [job_stats[i].as_dict() for i in range(count)], server_stats.as_dict()
