@@ -51,6 +51,12 @@ def parse_args():
     p.add_argument("--workload", default=WORKLOAD)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--form", choices=["plain", "batched", "serving"], default="plain",
+                   help="plain: the one-design metric; batched: many small instances at once; "
+                        "serving: an open-loop stream of jobs")
+    p.add_argument("--instances", type=int, default=256, help="batched form: instance count")
+    p.add_argument("--jobs", type=int, default=240, help="serving form: job count")
+    p.add_argument("--workers", type=int, default=32, help="batched / serving forms: worker threads")
     return p.parse_args()
 
 
@@ -366,10 +372,143 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def batched_instances(count: int, seed: int):
+    """Instances of the batched form: cells log-normal (median 4k) clipped to 1k-20k, the small
+    design's structure, bins the power of two nearest sqrt(cells) (32..256), early stop on."""
+    import numpy as np
+
+    import myplacement_b200 as mp
+    from myplacement_b200.design import small_instance
+
+    rng = np.random.default_rng(seed)
+    sigma = math.log(20_000 / 4_000) / 2.5
+    cells = np.clip(np.round(np.exp(rng.normal(math.log(4_000), sigma, count))), 1_000, 20_000).astype(int)
+    jobs = []
+    for k, c in enumerate(cells):
+        design, bins = small_instance(int(c), seed + k)
+        bins = max(32, min(256, bins))
+        x, y = mp.random_placement(design, seed + k)
+        jobs.append((design.copy_with_positions(x, y),
+                     mp.default_options(bins_x=bins, bins_y=bins, target_density=0.9)))
+    return jobs
+
+
+def run_batched(args) -> None:
+    """Aggregate iterations/s of many independent instances: one at a time vs all through the server."""
+    import myplacement_b200 as mp
+
+    jobs = batched_instances(args.instances, args.seed)
+    placer = mp.GlobalPlacer()
+    placer.run(*jobs[0])  # context and module load outside the timing
+    t0 = time.perf_counter()
+    plain = [placer.run(d, o) for d, o in jobs]
+    plain_seconds = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    placed, job_stats, server_stats = mp.batch_place([d for d, _ in jobs], [o for _, o in jobs],
+                                                     workers=args.workers)
+    batched_seconds = time.perf_counter() - t0
+    iterations = sum(r.completed_iterations for r in placed)
+    same = all(a.hpwl_after == b.hpwl_after and a.completed_iterations == b.completed_iterations
+               for a, b in zip(placed, plain))
+    line = {
+        "form": "batched", "metric": "aggregate GP iterations/s, independent instances on one GPU",
+        "value": iterations / batched_seconds, "unit": "iterations/s", "n_gpus": 1, "higher_is_better": True,
+        "plain_one_at_a_time": sum(r.completed_iterations for r in plain) / plain_seconds,
+        "speedup_vs_plain": (iterations / batched_seconds) / (sum(r.completed_iterations for r in plain) / plain_seconds),
+        "instances": len(jobs), "workers": args.workers, "iterations": iterations,
+        "seconds": batched_seconds, "plain_seconds": plain_seconds,
+        "results_identical_to_plain": same,
+        "overflow_le_0.10": sum(r.overflow_after <= 0.10 for r in placed),
+        "peak_running": server_stats["peak_running"],
+        "data": "synthetic: cells log-normal median 4k in 1k-20k, small-design net law, bins 32^2-256^2, "
+                "early stop on (280-iteration budget)",
+    }
+    print(json.dumps(line))
+
+
+def run_serving(args) -> None:
+    """Jobs of 2k-210k cells (log-uniform, mid-design structure scaled), each run to overflow <= 0.10
+    (1000-iteration budget, early stop on): the plain capacity (one job at a time), the served
+    capacity (all at once) and an open-loop Poisson stream at 70 % of the served capacity."""
+    import numpy as np
+
+    import myplacement_b200 as mp
+
+    rng = np.random.default_rng(args.seed)
+    pool = []
+    for k, cells in enumerate(np.exp(rng.uniform(math.log(2_000), math.log(210_000), 24))):
+        design, bins = mp.workload("mid_210k", seed=args.seed + k, scale=float(cells) / 210_000)
+        pool.append((design, max(32, bins)))
+
+    def job(i: int):
+        design, bins = pool[i % len(pool)]
+        x, y = mp.random_placement(design, args.seed + 1000 + i)
+        return design.copy_with_positions(x, y), mp.default_options(bins_x=bins, bins_y=bins, target_density=0.9,
+                                                                    iterations=1000)
+
+    # Plain: the first three rounds of the pool, one job at a time.
+    placer = mp.GlobalPlacer()
+    placer.run(*job(0))
+    first = [job(i) for i in range(3 * len(pool))]
+    t0 = time.perf_counter()
+    plain = [placer.run(d, o) for d, o in first]
+    plain_capacity = len(first) / (time.perf_counter() - t0)
+    plain_iterations = sum(r.completed_iterations for r in plain)
+
+    jobs = [job(i) for i in range(args.jobs)]
+    with mp.PlacementServer(device=0, workers=args.workers) as server:
+        # Served capacity: the same jobs, all submitted at once.
+        t0 = time.perf_counter()
+        ids = [server.submit(d, o) for d, o in first]
+        served = []
+        for i in ids:
+            server.wait(i)
+            served.append(server.take(i, history=False)[0])
+        capacity = len(first) / (time.perf_counter() - t0)
+        same = all(a.hpwl_after == b.hpwl_after for a, b in zip(served, plain))
+        rate = 0.7 * capacity
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, len(jobs)))
+        t0 = time.perf_counter()
+        submitted = []
+        for (design, options), at in zip(jobs, arrivals):
+            delay = at - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            submitted.append(server.submit(design, options))
+        latencies, overflow_ok, iterations = [], 0, 0
+        for i in submitted:
+            server.wait(i)
+            placed, stats = server.take(i, history=False)
+            latencies.append(stats["latency_seconds"])
+            overflow_ok += placed.overflow_after <= 0.10
+            iterations += placed.completed_iterations
+        seconds = time.perf_counter() - t0
+        server_stats = server.stats()
+    line = {
+        "form": "serving", "metric": "jobs/s and p50/p99 latency, open-loop Poisson arrivals at 70% capacity",
+        "value": len(jobs) / seconds, "unit": "jobs/s", "n_gpus": 1, "higher_is_better": True,
+        "p50_latency_s": float(np.percentile(latencies, 50)), "p99_latency_s": float(np.percentile(latencies, 99)),
+        "served_capacity_jobs_per_s": capacity, "plain_capacity_jobs_per_s": plain_capacity,
+        "capacity_speedup_vs_plain": capacity / plain_capacity,
+        "plain_iterations_per_s": plain_iterations * plain_capacity / len(first),
+        "served_results_identical_to_plain": same,
+        "arrival_rate_jobs_per_s": rate, "jobs": len(jobs), "workers": args.workers,
+        "aggregate_iterations_per_s": iterations / seconds,
+        "overflow_le_0.10": overflow_ok, "peak_running": server_stats["peak_running"],
+        "data": "synthetic: 24 mid-design-structured designs, cells log-uniform 2k-210k, each job its own "
+                "random initial placement; 1000-iteration budget, early stop on",
+    }
+    print(json.dumps(line))
+
+
 def main() -> int:
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.form == "batched":
+        run_batched(args)
+    elif args.form == "serving":
+        run_serving(args)
     else:
         run_mine(args)
     return 0
