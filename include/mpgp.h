@@ -204,6 +204,17 @@ typedef struct mpgp_result {
     int32_t history_count;
     int32_t evaluations; /* gradient + candidate evaluations performed */
     double rudy_energy_after;
+    /* RudyMetrics at the final placement (GlobalPlacementResult::rudy_metrics and
+     * rudy_validation_metrics, GlobalPlacer.hpp:107-129); zero when RUDY never activated. */
+    double rudy_horizontal_capacity;
+    double rudy_vertical_capacity;
+    double rudy_proxy_overflow_after;
+    double rudy_maximum_utilization_after;
+    double rudy_p95_utilization_after;
+    double rudy_validation_energy_after;
+    double rudy_validation_proxy_overflow_after;
+    double rudy_validation_maximum_utilization_after;
+    double rudy_validation_p95_utilization_after;
 } mpgp_result;
 
 /*
@@ -296,6 +307,21 @@ int mpgp_backend_density_layers(mpgp_backend* backend, int64_t* movable, int64_t
  * (ElectrostaticField.cpp:119-133, 205-237).  Any output may be NULL. */
 int mpgp_backend_field_solve(mpgp_backend* backend, const double* deviation, double* potential, double* field_x,
                              double* field_y);
+
+/* Parity hook: the RUDY routing-demand proxy of one placement on the backend's
+ * nets, as evaluateRudy (Rudy.cpp:227-340) computes it with a fixed capacity.
+ * `options` gives rudy_columns, rudy_rows, rudy_minimum_span_in_bins,
+ * rudy_penalty_model and rudy_softplus_temperature; the first call fixes the
+ * grid and later calls must give the same one.  A zero capacity evaluates the
+ * demand alone.  metrics (10 doubles): horizontal and vertical total demand,
+ * horizontal and vertical mean demand, horizontal and vertical capacity, proxy
+ * overflow, maximum and 95th-percentile utilisation, energy.  With
+ * calculate_gradient (positive capacities required) `gradient` receives the
+ * subgradient per particle (x, y), zero for fillers, and `energy` the energy of
+ * the evaluation that produced it. */
+int mpgp_backend_rudy(mpgp_backend* backend, const mpgp_options* options, const double* positions,
+                      double horizontal_capacity, double vertical_capacity, int calculate_gradient, double* metrics,
+                      double* energy, double* gradient);
 
 /*
  * Allocation-free wirelength and wire gradient.  This entry point has no

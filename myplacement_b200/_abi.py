@@ -195,6 +195,15 @@ class Result(C.Structure):
         ("history_count", C.c_int32),
         ("evaluations", C.c_int32),
         ("rudy_energy_after", C.c_double),
+        ("rudy_horizontal_capacity", C.c_double),
+        ("rudy_vertical_capacity", C.c_double),
+        ("rudy_proxy_overflow_after", C.c_double),
+        ("rudy_maximum_utilization_after", C.c_double),
+        ("rudy_p95_utilization_after", C.c_double),
+        ("rudy_validation_energy_after", C.c_double),
+        ("rudy_validation_proxy_overflow_after", C.c_double),
+        ("rudy_validation_maximum_utilization_after", C.c_double),
+        ("rudy_validation_p95_utilization_after", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -276,6 +285,7 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "mpgp_backend_destroy": (None, [vp]),
         "mpgp_backend_density_layers": (C.c_int, [vp, _i64, _i64, _i64]),
         "mpgp_backend_field_solve": (C.c_int, [vp, _d, _d, _d, _d]),
+        "mpgp_backend_rudy": (C.c_int, [vp, C.POINTER(Options), _d, C.c_double, C.c_double, C.c_int, _d, _d, _d]),
         "mpgp_random_placement": (C.c_int, [C.POINTER(Design), C.c_uint64, _d, _d]),
         "mpgp_wirelength_noalloc": (C.c_int, [vp, vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, C.c_int32,
                                               C.c_double, vp, vp, vp]),

@@ -50,6 +50,8 @@ struct mpgp_backend {
     std::unique_ptr<mpgp::Engine> engine;
     double2* wire = nullptr;
     double2* density = nullptr;
+    double2* rudy = nullptr;
+    int rudy_columns = 0, rudy_rows = 0;
     int64_t particles = 0;
     std::vector<double2> host;
 };
@@ -205,6 +207,72 @@ int mpgp_backend_field_solve(mpgp_backend* b, const double* deviation, double* p
         mpgp::require(b != nullptr && deviation != nullptr, "A backend and a deviation map are required.");
         mpgp::checkCuda(cudaSetDevice(b->engine->device()), "Select CUDA device");
         b->engine->fieldSolve(deviation, potential, field_x, field_y);
+    });
+}
+
+int mpgp_backend_rudy(mpgp_backend* b, const mpgp_options* options, const double* positions,
+                      double horizontal_capacity, double vertical_capacity, int calculate_gradient, double* metrics,
+                      double* energy, double* gradient) {
+    return guarded([&] {
+        mpgp::require(b != nullptr && options != nullptr && metrics != nullptr,
+                      "A backend, RUDY options and a metrics output are required.");
+        mpgp::require(options->rudy_columns > 0 && options->rudy_rows > 0 &&
+                          std::isfinite(options->rudy_minimum_span_in_bins) && options->rudy_minimum_span_in_bins > 0.0 &&
+                          std::isfinite(options->rudy_softplus_temperature) && options->rudy_softplus_temperature > 0.0,
+                      "RUDY evaluation requires a positive finite grid configuration and penalty model.");
+        mpgp::require(static_cast<uint64_t>(options->rudy_columns) * static_cast<uint64_t>(options->rudy_rows) <=
+                          1000000ULL,
+                      "RUDY grid exceeds the safe one-million-bin workspace limit.");
+        mpgp::require(options->rudy_penalty_model >= MPGP_RUDY_DISABLED && options->rudy_penalty_model <= MPGP_RUDY_HINGE_L4,
+                      "Unknown RUDY penalty model.");
+        mpgp::require(b->particles == 0 || positions != nullptr, "CUDA placement positions are missing.");
+        mpgp::require(!calculate_gradient || (horizontal_capacity > 0.0 && vertical_capacity > 0.0 &&
+                                              energy != nullptr && (b->particles == 0 || gradient != nullptr)),
+                      "A RUDY gradient needs positive capacities and its outputs.");
+        mpgp::Engine& e = *b->engine;
+        mpgp::checkCuda(cudaSetDevice(e.device()), "Select CUDA device");
+        if (b->rudy_columns == 0) {
+            mpgp_options grid = *options;
+            grid.rudy_validation_bins = 0;
+            e.enableRudy(grid);
+            b->rudy = e.newParticleArray("RUDY gradients");
+            b->rudy_columns = options->rudy_columns;
+            b->rudy_rows = options->rudy_rows;
+        }
+        mpgp::require(b->rudy_columns == options->rudy_columns && b->rudy_rows == options->rudy_rows &&
+                          e.rudyMinimumSpan() == options->rudy_minimum_span_in_bins,
+                      "The backend's RUDY grid is fixed by its first use.");
+        e.setRudyModel(options->rudy_penalty_model, options->rudy_softplus_temperature);
+        const std::size_t bytes = sizeof(double2) * static_cast<std::size_t>(b->particles);
+        if (b->particles > 0) {
+            mpgp::checkCuda(cudaMemcpyAsync(e.scratchPositions(), positions, bytes, cudaMemcpyHostToDevice, e.stream()),
+                            "Upload CUDA particle positions");
+        }
+        e.setRudyCapacity(false, horizontal_capacity, vertical_capacity);
+        const mpgp::RudyReport r = e.rudyEvaluate(e.scratchPositions(), false);
+        const double values[10] = {r.horizontal_total, r.vertical_total, r.horizontal_mean, r.vertical_mean,
+                                   r.horizontal_capacity, r.vertical_capacity, r.proxy_overflow,
+                                   r.maximum_utilization, r.p95_utilization, r.energy};
+        std::copy(values, values + 10, metrics);
+        if (calculate_gradient) {
+            mpgp::EvalRequest q;
+            q.mode = mpgp::kGiven;
+            q.positions = e.scratchPositions();
+            q.smoothing = 1.0;
+            q.gradient = true;
+            q.wire_out = b->wire;
+            q.density_out = b->density;
+            q.rudy_out = b->rudy;
+            q.rudy = true;
+            q.rudy_weight = 1.0;
+            const mpgp::EvalScalars& s = e.evaluate(q);
+            *energy = s.v[mpgp::kRudyEnergy];
+            if (b->particles > 0) {
+                mpgp::checkCuda(cudaMemcpyAsync(gradient, b->rudy, bytes, cudaMemcpyDeviceToHost, e.stream()),
+                                "Download RUDY gradients");
+                mpgp::checkCuda(cudaStreamSynchronize(e.stream()), "Synchronize RUDY evaluation");
+            }
+        }
     });
 }
 

@@ -104,6 +104,7 @@ Engine::~Engine() {
     if (fork_ != nullptr) cudaEventDestroy(fork_);
     if (join_ != nullptr) cudaEventDestroy(join_);
     if (host_scalars_ != nullptr) cudaFreeHost(host_scalars_);
+    if (host_rudy_ != nullptr) cudaFreeHost(host_rudy_);
     if (host_error_ != nullptr) cudaFreeHost(host_error_);
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
 }
@@ -164,7 +165,7 @@ void Engine::uploadStatic(const Problem& p) {
     metrics_blocks_ = std::min(ceilDiv(bin_count_, 2 * kThreads), 148 * 2);
     partials_sc_ = arena_.array<double>(2 * static_cast<std::size_t>(scatter_blocks_), "scatter partials");
     partials_m_ = arena_.array<double>(9 * static_cast<std::size_t>(metrics_blocks_), "metric partials");
-    partials_g_ = arena_.array<double>(7 * static_cast<std::size_t>(gather_blocks_), "gather partials");
+    partials_g_ = arena_.array<double>(8 * static_cast<std::size_t>(gather_blocks_), "gather partials");
     scalars_ = arena_.array<double>(kScalarCount, "evaluation scalars");
     checkCuda(cudaMemsetAsync(scalars_, 0, kScalarCount * sizeof(double), stream_), "clear scalars");
 }
@@ -209,6 +210,7 @@ void Engine::buildNetLayout(const Problem& p) {
             }
             net_start.push_back(static_cast<int>(pin_particle.size()));
             net_weight.push_back(static_cast<float>(p.net_weight[n]));
+            bucket_net_weight_.push_back(p.net_weight[n]);
         }
         const int count = static_cast<int>(bucket[b].size());
         for (int off = 0; off < count; off += nets_per_block) {
@@ -217,6 +219,8 @@ void Engine::buildNetLayout(const Problem& p) {
     }
     for (int b = 5; b >= 0; --b) work.insert(work.end(), bucket_work[b].begin(), bucket_work[b].end());
     wl_blocks_ = static_cast<int>(work.size());
+    wl_net_count_ = static_cast<int>(net_weight.size());
+    wl_pin_count_ = static_cast<int>(pin_particle.size());
     const std::size_t pins = std::max<std::size_t>(1, pin_particle.size());
     pin_particle_ = arena_.array<int>(pins, "pin particles");
     pin_offset_ = arena_.array<float2>(pins, "pin offsets");
@@ -471,7 +475,7 @@ void Engine::buildTensorCoreBasis(const std::vector<double>& cx, const std::vect
 
 const char* kernelKindName(int kind) {
     static const char* names[kKindCount] = {"scatter", "wirelength", "metrics", "dct_forward",
-                                            "dct_inverse", "gather", "reduce", "vector", "dct_split"};
+                                            "dct_inverse", "gather", "reduce", "vector", "dct_split", "rudy"};
     return kind >= 0 && kind < kKindCount ? names[kind] : "unknown";
 }
 
@@ -602,6 +606,16 @@ void Engine::launch(const EvalRequest& q) {
     beginKernel(kKindWirelength, stream_wl_);
     launchWirelength(wa, wl_blocks_, stream_wl_);
     endKernel(stream_wl_);
+    if (q.rudy) {
+        // The routability term runs beside the density chain, after the wirelength pass.
+        require(rudy_main_.columns > 0, "RUDY was not enabled for this engine.");
+        const RudyArgs ra = rudyArgs(rudy_main_, positions, true);
+        beginKernel(kKindRudy, stream_wl_);
+        launchRudyDeposit(ra, stream_wl_);
+        launchRudyMetrics(ra, rudy_main_.blocks, stream_wl_);
+        if (q.gradient) launchRudyGradient(ra, stream_wl_);
+        endKernel(stream_wl_);
+    }
     checkCuda(cudaEventRecord(join_, stream_wl_), "join");
 
     MetricsArgs ma{};
@@ -650,9 +664,12 @@ void Engine::launch(const EvalRequest& q) {
         ga.pre = q.pre;
         ga.wire_out = q.wire_out;
         ga.density_out = q.density_out;
+        ga.rudy_out = q.rudy_out;
         ga.prev_positions = q.prev_positions;
         ga.prev_gradient = q.prev_gradient;
         ga.velocity = q.velocity;
+        ga.rudy_gradient = q.rudy ? rudy_pin_gradient_ : nullptr;
+        ga.rudy_weight = q.rudy ? q.rudy_weight : 0.0;
         ga.partials = partials_g_;
         beginKernel(kKindGather);
         launchGather(ga, particle_count_ > 0 ? gather_blocks_ : 0, stream_);
@@ -674,9 +691,12 @@ void Engine::launch(const EvalRequest& q) {
         for (int k = 0; k < 9; ++k) add(partials_m_, metrics_blocks_, 9, k, k >= 7, kOverflowWith + k);
         add(partials_e_, energy_blocks_, 1, 0, false, kEnergy);
     }
+    for (int k = 0; k < 5; ++k) {
+        add(rudy_main_.partials, q.rudy ? rudy_main_.blocks : 0, 5, k, k == 4, kRudyEnergy + k);
+    }
     if (q.gradient) {
         const int rows = particle_count_ > 0 ? gather_blocks_ : 0;
-        for (int k = 0; k < 7; ++k) add(partials_g_, rows, 7, k, false, kWireL1 + k);
+        for (int k = 0; k < 8; ++k) add(partials_g_, rows, 8, k, false, kWireL1 + k);
     }
     ra.source_count = s;
     ra.scalars = scalars_;
@@ -690,6 +710,7 @@ void Engine::launch(const EvalRequest& q) {
     checkCuda(cudaMemcpyAsync(host_error_, tc_error_, sizeof(int), cudaMemcpyDeviceToHost, stream_),
               "Download contraction status");
     d2h_bytes_ += sizeof(int);
+    if (q.rudy) kernels += q.gradient ? 3 : 2;
     launches_ += kernels;
     last_gradient_ = q.gradient;
     last_propose_ = q.mode == kPropose;
@@ -745,6 +766,141 @@ void Engine::fieldSolve(const double* deviation, double* potential, double* fiel
         if (field_x != nullptr) field_x[i] = f[i].x;
         if (field_y != nullptr) field_y[i] = f[i].y;
     }
+}
+
+// ---- RUDY (rudy.cu) -------------------------------------------------------------------
+
+void Engine::allocateRudyGrid(RudyGrid& g, int columns, int rows, const char* what) {
+    g.columns = columns;
+    g.rows = rows;
+    g.bin_w = region_.width() / static_cast<double>(columns);
+    g.bin_h = region_.height() / static_cast<double>(rows);
+    g.min_x_span = rudy_minimum_span_ * g.bin_w;
+    g.min_y_span = rudy_minimum_span_ * g.bin_h;
+    const std::size_t bins = static_cast<std::size_t>(columns) * static_cast<std::size_t>(rows);
+    g.horizontal = arena_.array<unsigned long long>(bins, what);
+    g.vertical = arena_.array<unsigned long long>(bins, what);
+    g.adjoint_h = arena_.array<double>(bins, what);
+    g.adjoint_v = arena_.array<double>(bins, what);
+    g.utilization = arena_.array<double>(bins, what);
+    g.blocks = std::max(1, std::min(ceilDiv(static_cast<long long>(bins), kThreads), 148 * 2));
+    g.partials = arena_.array<double>(5 * static_cast<std::size_t>(g.blocks), what);
+    checkCuda(cudaMemsetAsync(g.horizontal, 0, bins * sizeof(unsigned long long), stream_), what);
+    checkCuda(cudaMemsetAsync(g.vertical, 0, bins * sizeof(unsigned long long), stream_), what);
+    checkCuda(cudaMemsetAsync(g.adjoint_h, 0, bins * sizeof(double), stream_), what);
+    checkCuda(cudaMemsetAsync(g.adjoint_v, 0, bins * sizeof(double), stream_), what);
+}
+
+void Engine::setRudyModel(int model, double temperature) {
+    rudy_model_ = model;
+    rudy_temperature_ = temperature;
+}
+
+void Engine::enableRudy(const mpgp_options& o) {
+    if (rudy_main_.columns > 0) return;
+    rudy_model_ = o.rudy_penalty_model;
+    rudy_temperature_ = o.rudy_softplus_temperature;
+    rudy_minimum_span_ = o.rudy_minimum_span_in_bins;
+    allocateRudyGrid(rudy_main_, o.rudy_columns, o.rudy_rows, "RUDY maps");
+    if (o.rudy_validation_bins > 0) {
+        allocateRudyGrid(rudy_validation_, o.rudy_validation_bins, o.rudy_validation_bins, "RUDY validation maps");
+    }
+    rudy_net_weight_ = arena_.array<double>(std::max<std::size_t>(1, bucket_net_weight_.size()), "RUDY net weights");
+    upload(rudy_net_weight_, bucket_net_weight_, stream_);
+    rudy_pin_gradient_ =
+        arena_.array<double2>(std::max<std::size_t>(1, static_cast<std::size_t>(wl_pin_count_)), "RUDY pin gradients");
+    rudy_scalars_ = arena_.array<double>(5, "RUDY scalars");
+    checkCuda(cudaMallocHost(reinterpret_cast<void**>(&host_rudy_), 5 * sizeof(double)), "pinned RUDY scalars");
+    checkCuda(cudaStreamSynchronize(stream_), "RUDY set-up");
+}
+
+RudyArgs Engine::rudyArgs(const RudyGrid& g, const double2* positions, bool with_capacity) const {
+    RudyArgs a{};
+    a.positions = positions;
+    a.pin_particle = pin_particle_;
+    a.pin_offset = pin_offset_;
+    a.static_pins = static_pins_;
+    a.net_start = net_start_;
+    a.net_weight = rudy_net_weight_;
+    a.net_count = wl_net_count_;
+    a.pin_slot = pin_slot_;
+    a.pin_gradient = rudy_pin_gradient_;
+    a.llx = region_.llx;
+    a.lly = region_.lly;
+    a.urx = region_.urx;
+    a.ury = region_.ury;
+    a.bin_w = g.bin_w;
+    a.bin_h = g.bin_h;
+    a.columns = g.columns;
+    a.rows = g.rows;
+    a.minimum_x_span = g.min_x_span;
+    a.minimum_y_span = g.min_y_span;
+    a.inv_unit_h = 4294967296.0 / g.bin_w;
+    a.inv_unit_v = 4294967296.0 / g.bin_h;
+    a.horizontal = g.horizontal;
+    a.vertical = g.vertical;
+    a.capacity_h = with_capacity ? g.capacity_h : 0.0;
+    a.capacity_v = with_capacity ? g.capacity_v : 0.0;
+    a.model = rudy_model_;
+    a.temperature = rudy_temperature_;
+    a.adjoint_h = g.adjoint_h;
+    a.adjoint_v = g.adjoint_v;
+    a.utilization = g.utilization;
+    a.partials = g.partials;
+    return a;
+}
+
+void Engine::setRudyCapacity(bool validation, double horizontal, double vertical) {
+    RudyGrid& g = validation ? rudy_validation_ : rudy_main_;
+    require(g.columns > 0, "RUDY grid is not enabled.");
+    g.capacity_h = horizontal;
+    g.capacity_v = vertical;
+}
+
+RudyReport Engine::rudyEvaluate(const double2* positions, bool validation) {
+    const RudyGrid& g = validation ? rudy_validation_ : rudy_main_;
+    require(g.columns > 0, "RUDY grid is not enabled.");
+    const bool with_capacity = g.capacity_h > 0.0 && g.capacity_v > 0.0;
+    const RudyArgs ra = rudyArgs(g, positions, with_capacity);
+    launchRudyDeposit(ra, stream_);
+    launchRudyMetrics(ra, g.blocks, stream_);
+    ReduceArgs rr{};
+    for (int k = 0; k < 5; ++k) rr.sources[k] = ReduceSource{g.partials, g.blocks, 5, k, k == 4 ? 1 : 0, k};
+    rr.source_count = 5;
+    rr.scalars = rudy_scalars_;
+    rr.totals = nullptr;
+    launchReduce(rr, stream_);
+    launches_ += 3;
+    checkCuda(cudaMemcpyAsync(host_rudy_, rudy_scalars_, 5 * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+              "Download RUDY scalars");
+    const std::size_t bins = static_cast<std::size_t>(g.columns) * static_cast<std::size_t>(g.rows);
+    std::vector<double> utilization;
+    if (with_capacity) {
+        utilization.resize(bins);
+        checkCuda(cudaMemcpyAsync(utilization.data(), g.utilization, bins * sizeof(double), cudaMemcpyDeviceToHost,
+                                  stream_),
+                  "Download RUDY utilisation");
+    }
+    checkCuda(cudaStreamSynchronize(stream_), "RUDY evaluation");
+    RudyReport r;
+    r.horizontal_total = host_rudy_[1];
+    r.vertical_total = host_rudy_[2];
+    r.horizontal_mean = r.horizontal_total / static_cast<double>(bins);
+    r.vertical_mean = r.vertical_total / static_cast<double>(bins);
+    r.horizontal_capacity = with_capacity ? g.capacity_h : 0.0;
+    r.vertical_capacity = with_capacity ? g.capacity_v : 0.0;
+    if (with_capacity) {
+        r.energy = host_rudy_[0];
+        r.proxy_overflow = host_rudy_[3] / static_cast<double>(bins);
+        r.maximum_utilization = std::max(0.0, host_rudy_[4]);
+        // The 95th percentile of the sorted per-bin utilisation (Rudy.cpp:310-314).
+        const std::size_t index = static_cast<std::size_t>(
+            std::floor(0.95 * static_cast<double>(std::max<std::size_t>(1U, bins - 1U))));
+        std::nth_element(utilization.begin(), utilization.begin() + static_cast<std::ptrdiff_t>(index),
+                         utilization.end());
+        r.p95_utilization = utilization[index];
+    }
+    return r;
 }
 
 void Engine::depositLayers(const double2* positions, int64_t* movable, int64_t* macro, int64_t* filler) {

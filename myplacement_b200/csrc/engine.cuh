@@ -55,6 +55,7 @@ struct EvalRequest {
     // split outputs (drop-in backend)
     double2* wire_out = nullptr;
     double2* density_out = nullptr;
+    double2* rudy_out = nullptr;
     const double2* prev_positions = nullptr;
     const double2* prev_gradient = nullptr;
     const double2* velocity = nullptr;
@@ -63,6 +64,18 @@ struct EvalRequest {
     // evaluation are those of these positions (nothing moved since): keep them and
     // run only the wirelength, the inverse field and the gather.
     bool reuse_density = false;
+    // The routability term: RUDY map, energy and (with gradient) its weighted
+    // subgradient in the combined gradient.
+    bool rudy = false;
+    double rudy_weight = 0.0;
+};
+
+// RUDY metrics of one evaluation of a grid (RudyMetrics, Rudy.hpp:51-64, and the energy).
+struct RudyReport {
+    double horizontal_total = 0.0, vertical_total = 0.0;
+    double horizontal_mean = 0.0, vertical_mean = 0.0;
+    double horizontal_capacity = 0.0, vertical_capacity = 0.0;
+    double energy = 0.0, proxy_overflow = 0.0, maximum_utilization = 0.0, p95_utilization = 0.0;
 };
 
 struct EvalScalars {
@@ -80,6 +93,7 @@ enum KernelKind : int {
     kKindReduce,
     kKindVector,
     kKindDctSplit,
+    kKindRudy,
     kKindCount
 };
 const char* kernelKindName(int kind);
@@ -107,6 +121,17 @@ public:
     // Evaluation results in the reference's structures.
     void densityMetrics(const EvalScalars& s, bool with_fillers, mpgp_density_metrics& out) const;
     [[nodiscard]] double energy(const EvalScalars& s) const;
+
+    // The routability term (rudy.cu): allocate the RUDY grid(s), freeze capacities,
+    // and evaluate a grid's metrics at given positions (calibration, validation, final).
+    void enableRudy(const mpgp_options& options);
+    [[nodiscard]] bool rudyEnabled() const { return rudy_main_.columns > 0; }
+    [[nodiscard]] bool rudyValidationEnabled() const { return rudy_validation_.columns > 0; }
+    void setRudyCapacity(bool validation, double horizontal, double vertical);
+    void setRudyModel(int model, double temperature);
+    [[nodiscard]] double rudyMinimumSpan() const { return rudy_minimum_span_; }
+    RudyReport rudyEvaluate(const double2* positions, bool validation);
+    [[nodiscard]] int rudyBins() const { return rudy_main_.columns * rudy_main_.rows; }
 
     // Solves the field of an arbitrary FP64 deviation map (parity hook).
     void fieldSolve(const double* deviation, double* potential, double* field_x, double* field_y);
@@ -140,6 +165,32 @@ public:
     }
 
 private:
+    struct RudyGrid {
+        int columns = 0, rows = 0;
+        double bin_w = 0.0, bin_h = 0.0, min_x_span = 0.0, min_y_span = 0.0;
+        double capacity_h = 0.0, capacity_v = 0.0;
+        unsigned long long* horizontal = nullptr;
+        unsigned long long* vertical = nullptr;
+        double* adjoint_h = nullptr;
+        double* adjoint_v = nullptr;
+        double* utilization = nullptr;
+        double* partials = nullptr;
+        int blocks = 0;
+    };
+    void allocateRudyGrid(RudyGrid& grid, int columns, int rows, const char* what);
+    [[nodiscard]] RudyArgs rudyArgs(const RudyGrid& grid, const double2* positions, bool with_capacity) const;
+    RudyGrid rudy_main_, rudy_validation_;
+    int rudy_model_ = 0;
+    double rudy_temperature_ = 0.1;
+    double rudy_minimum_span_ = 0.25;
+    double* rudy_net_weight_ = nullptr;
+    double2* rudy_pin_gradient_ = nullptr;
+    double* rudy_scalars_ = nullptr;
+    double* host_rudy_ = nullptr;
+    std::vector<double> bucket_net_weight_;
+    int wl_net_count_ = 0;
+    int wl_pin_count_ = 0;
+
     void collectTimings();
     void runDct(bool gradient, bool potential, bool forward);
     void uploadStatic(const Problem& problem);

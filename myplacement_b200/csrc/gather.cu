@@ -6,7 +6,7 @@
 //   density  = -charge * E(position)  -- bilinear sample of the DCT field with
 //              the Neumann mirror parity (sampleWithParity / reflectIndex,
 //              ElectrostaticField.cpp:289-320; CudaPlacementBackend.cu:158-192, 575-591)
-//   raw      = wire + penalty * density
+//   raw      = wire + penalty * density [+ rudy_weight * RUDY, summed over the pins' slots]
 //   pre      = raw * precond_base / density_strength
 // and the FP64 block partials the controller needs: |wire|_1, |density|_1,
 // |raw|^2, |pre|^2 (GlobalPlacementSession::evaluateCuda, AdaptiveGlobalPlacer.cpp:
@@ -66,9 +66,9 @@ __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
     releaseNext();
     waitForPrior();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (i < a.particle_count) {
-        double wx = 0.0, wy = 0.0;
+        double wx = 0.0, wy = 0.0, rx_rudy = 0.0, ry_rudy = 0.0;
         if (i < a.movable_count) {
             const int begin = a.particle_pin_start[i];
             const int end = a.particle_pin_start[i + 1];
@@ -76,6 +76,14 @@ __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
                 const float2 g = a.pin_gradient[j];
                 wx += static_cast<double>(g.x);
                 wy += static_cast<double>(g.y);
+            }
+            if (a.rudy_gradient != nullptr) {
+                for (int j = begin; j < end; ++j) {
+                    const double2 g = a.rudy_gradient[j];
+                    rx_rudy += g.x;
+                    ry_rudy += g.y;
+                }
+                v[7] = fabs(rx_rudy) + fabs(ry_rudy);
             }
         }
         const double2 p = a.positions[i];
@@ -88,9 +96,10 @@ __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
         if (a.precond_base == nullptr) {
             a.wire_out[i] = make_double2(wx, wy);
             a.density_out[i] = make_double2(dx, dy);
+            if (a.rudy_out != nullptr) a.rudy_out[i] = make_double2(rx_rudy, ry_rudy);
         } else {
-            const double rx = wx + dx * a.penalty;
-            const double ry = wy + dy * a.penalty;
+            const double rx = wx + dx * a.penalty + rx_rudy * a.rudy_weight;
+            const double ry = wy + dy * a.penalty + ry_rudy * a.rudy_weight;
             const double s = a.precond_base[i] * a.precond_scale;
             const double px = rx * s;
             const double py = ry * s;
@@ -112,11 +121,11 @@ __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
             }
         }
     }
-    const bool is_max[7] = {false, false, false, false, false, false, false};
-    blockReduce<7>(v, is_max);
+    const bool is_max[8] = {false, false, false, false, false, false, false, false};
+    blockReduce<8>(v, is_max);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < 7; ++k) a.partials[7 * blockIdx.x + k] = v[k];
+        for (int k = 0; k < 8; ++k) a.partials[8 * blockIdx.x + k] = v[k];
     }
 }
 

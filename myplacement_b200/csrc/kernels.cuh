@@ -30,6 +30,12 @@ enum Scalar : int {
     kDeltaPos2,       // sum |x - x_prev|^2
     kDeltaGrad2,      // sum |g - g_prev|^2 (preconditioned)
     kAlignment,       // sum velocity . g (preconditioned)
+    kRudyL1,          // sum |RUDY gradient| over particles (unweighted)
+    kRudyEnergy,      // RUDY hotspot energy (with capacity)
+    kRudyHorizontal,  // total horizontal / vertical demand
+    kRudyVertical,
+    kRudyProxy,       // sum of utilisation overflow (divide by bins for the proxy overflow)
+    kRudyMaxUtil,     // maximum utilisation
     kScalarCount
 };
 
@@ -111,6 +117,37 @@ struct MetricsArgs {
 };
 void launchMetrics(const MetricsArgs& args, int blocks, cudaStream_t stream);
 
+// ---- RUDY routing-demand map (rudy.cu) -------------------------------------------------
+struct RudyArgs {
+    const double2* positions;
+    const int* pin_particle;      // the wirelength pass's bucketed pins and nets
+    const float2* pin_offset;
+    const double2* static_pins;
+    const int* net_start;
+    const double* net_weight;     // FP64 weights in bucket order
+    int net_count;
+    const int* pin_slot;
+    double2* pin_gradient;        // particle-ordered pin slots (gradient pass)
+    double llx, lly, urx, ury;    // core region
+    double bin_w, bin_h;
+    int columns, rows;
+    double minimum_x_span, minimum_y_span;
+    double inv_unit_h, inv_unit_v;  // fixed point: 2^32 / bin_w, 2^32 / bin_h
+    unsigned long long* horizontal; // columns * rows, read and cleared by the metrics pass
+    unsigned long long* vertical;
+    double capacity_h, capacity_v;  // 0: maps and totals only
+    int model;                      // MPGP_RUDY_*
+    double temperature;
+    double* adjoint_h;
+    double* adjoint_v;
+    double* utilization;            // per bin max(uh, uv), or null
+    double* partials;               // per block: energy, H total, V total, proxy, max utilisation
+};
+int rudyBlocks(int count);
+void launchRudyDeposit(const RudyArgs& args, cudaStream_t stream);
+void launchRudyMetrics(const RudyArgs& args, int blocks, cudaStream_t stream);
+void launchRudyGradient(const RudyArgs& args, cudaStream_t stream);
+
 // ---- field gather + gradient combine (the fused update pass) ----------------------------
 struct GatherArgs {
     int particle_count;
@@ -129,10 +166,13 @@ struct GatherArgs {
     double2* pre;
     double2* wire_out;              // split mode outputs (drop-in backend)
     double2* density_out;
+    double2* rudy_out;              // split mode, optional: the RUDY subgradient per particle
     const double2* prev_positions;  // optional (step estimate)
     const double2* prev_gradient;
     const double2* velocity;        // optional (momentum alignment)
-    double* partials;               // per block: 7 partials (kWireL1 .. kAlignment)
+    const double2* rudy_gradient;   // optional: RUDY pin slots (particle order), added with rudy_weight
+    double rudy_weight;
+    double* partials;               // per block: 8 partials (kWireL1 .. kRudyL1)
 };
 void launchGather(const GatherArgs& args, int blocks, cudaStream_t stream);
 

@@ -63,7 +63,8 @@ double updateDensityPenalty(double penalty, double reference_penalty, const Obje
 
 mpgp_history_row makeHistoryRow(int iteration, const ObjectiveMetrics& m, double penalty, double smoothing,
                                 double step_size, double maximum_displacement, double gradient_norm, double curvature,
-                                int backtracks, bool restarted, bool accepted, bool best_checkpoint) {
+                                int backtracks, bool restarted, bool accepted, bool best_checkpoint, double rudy_weight,
+                                bool rudy_active) {
     mpgp_history_row row{};
     row.iteration = iteration;
     row.hpwl = m.hpwl;
@@ -78,6 +79,11 @@ mpgp_history_row makeHistoryRow(int iteration, const ObjectiveMetrics& m, double
     row.maximum_displacement = maximum_displacement;
     row.gradient_norm = gradient_norm;
     row.curvature = curvature;
+    row.rudy_energy = m.rudy_energy;
+    row.rudy_proxy_overflow = m.rudy_proxy_overflow;
+    row.rudy_maximum_utilization = m.rudy_maximum_utilization;
+    row.rudy_weight = rudy_weight;
+    row.rudy_active = rudy_active ? 1 : 0;
     row.backtracks = backtracks;
     row.momentum_restarted = restarted ? 1 : 0;
     row.accepted = accepted ? 1 : 0;
@@ -94,8 +100,7 @@ Session::Session(const mpgp_design& design, const mpgp_options& options) : optio
         // validatePublicGlobalOptions + validateAdaptiveOptions.
         validateOptions(options_);
     }
-    require(options_.rudy_penalty_model == MPGP_RUDY_DISABLED,
-            "The B200 engine does not run the RUDY routability term in the controller.");
+    rudy_requested_ = options_.rudy_penalty_model != MPGP_RUDY_DISABLED;
     derived_ = deriveDesign(design);
     module_x_.assign(design.module_x, design.module_x + design.module_count);
     module_y_.assign(design.module_y, design.module_y + design.module_count);
@@ -118,6 +123,7 @@ Session::Session(const mpgp_design& design, const mpgp_options& options) : optio
     require(options_.cuda_device >= 0 && options_.cuda_device < device_count,
             "Requested CUDA device does not exist on this host.");
     engine_ = std::make_unique<Engine>(problem, options_.cuda_device, options_.maximum_cuda_memory_bytes);
+    if (rudy_requested_) engine_->enableRudy(options_);
     result_.cuda_device_used = options_.cuda_device;
 
     const double bin_w = derived_.core.width() / static_cast<double>(options_.bins_x);
@@ -164,6 +170,9 @@ Session::Session(const mpgp_design& design, const mpgp_options& options) : optio
     penalty_ = clampValue(raw_penalty, options_.minimum_density_penalty, options_.maximum_density_penalty);
     reference_penalty_ = penalty_;
     initial_ = evaluateGiven(cur_, true, penalty_, raw_cur_, pre_cur_, false, false);
+    if (rudy_requested_ && initial_.m.design.normalized_overflow <= options_.routability_start_overflow) {
+        activateRudy(initial_, false, false);
+    }
     last_optimizer_overflow_ = initial_.m.optimizer.normalized_overflow;
     {
         const double count = static_cast<double>(std::max<std::size_t>(1U, particles));
@@ -183,13 +192,20 @@ double Session::smoothingFromOverflow(double overflow) const {
     return (options_.final_smoothing + (options_.initial_smoothing - options_.final_smoothing) * annealing) * max_bin_;
 }
 
-void Session::fillMetrics(const EvalScalars& s, double penalty, StateEval& out) const {
+void Session::fillMetrics(const EvalScalars& s, double penalty, double rudy_weight, StateEval& out) const {
     out.m.hpwl = s.v[kHpwl];
     out.m.smooth_wirelength = s.v[kSmooth];
     out.m.density_energy = engine_->energy(s);
     engine_->densityMetrics(s, true, out.m.optimizer);
     engine_->densityMetrics(s, false, out.m.design);
-    out.m.objective = out.m.smooth_wirelength + penalty * out.m.density_energy;
+    out.m.rudy_energy = s.v[kRudyEnergy];
+    if (engine_->rudyEnabled()) {
+        out.m.rudy_proxy_overflow = s.v[kRudyProxy] / static_cast<double>(engine_->rudyBins());
+        out.m.rudy_maximum_utilization = std::max(0.0, s.v[kRudyMaxUtil]);
+    }
+    out.rudy_l1 = s.v[kRudyL1];
+    // GlobalPlacementSession::evaluate objective (AdaptiveGlobalPlacer.cpp:221-222, 294-295).
+    out.m.objective = out.m.smooth_wirelength + penalty * out.m.density_energy + rudy_weight * out.m.rudy_energy;
     if (!std::isfinite(out.m.objective) || !std::isfinite(out.m.hpwl)) {
         fail(MPGP_ERR_NON_FINITE, "CUDA adaptive placement objective produced a non-finite value.");
     }
@@ -205,9 +221,11 @@ void Session::fillMetrics(const EvalScalars& s, double penalty, StateEval& out) 
 }
 
 StateEval Session::evaluateGiven(double2* positions, bool gradient, double penalty, double2* raw, double2* pre,
-                                 bool with_prev, bool with_velocity, bool reuse_density) {
+                                 bool with_prev, bool with_velocity, bool reuse_density, double rudy_weight_override) {
     EvalRequest q;
     q.mode = kGiven;
+    q.rudy = rudy_active_;
+    q.rudy_weight = rudy_weight_override >= 0.0 ? rudy_weight_override : rudy_weight_;
     q.positions = positions;
     q.reuse_density = reuse_density;
     density_cached_ = false;
@@ -225,7 +243,7 @@ StateEval Session::evaluateGiven(double2* positions, bool gradient, double penal
     const EvalScalars& s = engine_->evaluate(q);
     ++result_.evaluations;
     StateEval out;
-    fillMetrics(s, penalty, out);
+    fillMetrics(s, penalty, q.rudy ? q.rudy_weight : 0.0, out);
     out.raw = raw;
     out.pre = pre;
     return out;
@@ -235,6 +253,8 @@ StateEval Session::evaluateLookahead(double momentum, double penalty, double2* r
     density_cached_ = false;
     EvalRequest q;
     q.mode = kLookahead;
+    q.rudy = rudy_active_;
+    q.rudy_weight = rudy_weight_;
     q.base = cur_;
     q.direction = velocity_;
     q.step = momentum;
@@ -252,7 +272,7 @@ StateEval Session::evaluateLookahead(double momentum, double penalty, double2* r
     const EvalScalars& s = engine_->evaluate(q);
     ++result_.evaluations;
     StateEval out;
-    fillMetrics(s, penalty, out);
+    fillMetrics(s, penalty, q.rudy ? q.rudy_weight : 0.0, out);
     out.raw = raw;
     out.pre = pre;
     return out;
@@ -263,6 +283,8 @@ StateEval Session::evaluateProposal(const double2* base, const StateEval& base_e
     density_cached_ = false;
     EvalRequest q;
     q.mode = kPropose;
+    q.rudy = rudy_active_;
+    q.rudy_weight = rudy_weight_;
     q.base = base;
     q.direction = base_eval.pre;
     q.raw_direction = base_eval.raw;
@@ -274,16 +296,67 @@ StateEval Session::evaluateProposal(const double2* base, const StateEval& base_e
     const EvalScalars& s = engine_->evaluate(q);
     ++result_.evaluations;
     StateEval out;
-    fillMetrics(s, penalty, out);
+    fillMetrics(s, penalty, q.rudy ? q.rudy_weight : 0.0, out);
     return out;
 }
 
-// considerCheckpoint (AdaptiveGlobalPlacer.cpp:563-596); the routability weight is 0.
+// refreshRudyWeight (AdaptiveGlobalPlacer.cpp:689-698): the weight ramps to its
+// target over routability_ramp_iterations accepted iterations.
+bool Session::refreshRudyWeight() {
+    if (!rudy_active_) return false;
+    const double progress =
+        std::min(1.0, static_cast<double>(rudy_accepted_age_ + 1) /
+                          static_cast<double>(std::max(1, options_.routability_ramp_iterations)));
+    const double updated = rudy_target_weight_ * progress;
+    const bool changed =
+        std::abs(updated - rudy_weight_) > 1e-12 * std::max({1.0, std::abs(updated), std::abs(rudy_weight_)});
+    rudy_weight_ = updated;
+    return changed;
+}
+
+// activateRudy (AdaptiveGlobalPlacer.cpp:699-713 with GlobalPlacementSession::activateRudy
+// :149-162 and calibrateRudyCapacity, Rudy.cpp:215-225): capacities frozen from the
+// current map, the target weight matched to the wire-plus-density force, and the
+// evaluation replaced by one with the routability term.
+void Session::activateRudy(StateEval& evaluation, bool with_prev, bool with_velocity) {
+    const auto calibrate = [&](bool validation, double factor) {
+        const RudyReport raw = engine_->rudyEvaluate(cur_, validation);
+        if (!std::isfinite(raw.horizontal_mean) || !std::isfinite(raw.vertical_mean) || raw.horizontal_mean < 0.0 ||
+            raw.vertical_mean < 0.0) {
+            fail(MPGP_ERR_INVALID_ARGUMENT, "RUDY mean demand must be finite and non-negative.");
+        }
+        engine_->setRudyCapacity(validation, std::max(kEpsilon, factor * raw.horizontal_mean),
+                                 std::max(kEpsilon, factor * raw.vertical_mean));
+    };
+    calibrate(false, options_.rudy_capacity_factor);
+    if (engine_->rudyValidationEnabled()) calibrate(true, options_.rudy_validation_capacity_factor);
+    rudy_active_ = true;
+    const StateEval probe = evaluateGiven(cur_, true, penalty_, raw_cur_, pre_cur_, with_prev, with_velocity, false, 0.0);
+    const double base_l1 = probe.wire_l1 + penalty_ * probe.density_l1;
+    rudy_target_weight_ =
+        probe.rudy_l1 > kEpsilon ? options_.routability_weight_scale * base_l1 / probe.rudy_l1 : 0.0;
+    rudy_accepted_age_ = 0;
+    rudy_weight_ = 0.0;
+    refreshRudyWeight();
+    evaluation = evaluateGiven(cur_, true, penalty_, raw_cur_, pre_cur_, with_prev, with_velocity, false);
+}
+
+// refreshCheckpointRudyScore (AdaptiveGlobalPlacer.cpp:598-608).
+void Session::refreshCheckpointRudyScore(CheckpointState& checkpoint) {
+    if (!checkpoint.found) return;
+    const StateEval e = evaluateGiven(checkpoint.positions, false, penalty_, nullptr, nullptr, false, false, false,
+                                      rudy_target_weight_);
+    checkpoint.rudy_energy = e.m.rudy_energy;
+    checkpoint.selection_score = e.m.hpwl + rudy_target_weight_ * e.m.rudy_energy;
+}
+
+// considerCheckpoint (AdaptiveGlobalPlacer.cpp:559-596); the score adds the routability
+// target weight times the RUDY energy.
 void Session::considerCheckpoint(double2* positions, const ObjectiveMetrics& m, int iteration, bool& is_new_best) {
     is_new_best = false;
     const double overflow = m.design.normalized_overflow;
     const bool feasible = overflow <= options_.maximum_bin_overflow;
-    const double score = m.hpwl;
+    const double score = m.hpwl + rudy_target_weight_ * m.rudy_energy;
     const std::size_t bytes = sizeof(double2) * static_cast<std::size_t>(engine_->particleCount());
     if (feasible && (!best_feasible_.found || score < best_feasible_.selection_score - 1e-10 ||
                      (std::abs(score - best_feasible_.selection_score) <= 1e-10 && m.hpwl < best_feasible_.hpwl))) {
@@ -294,6 +367,7 @@ void Session::considerCheckpoint(double2* positions, const ObjectiveMetrics& m, 
         best_feasible_.hpwl = m.hpwl;
         best_feasible_.overflow = overflow;
         best_feasible_.selection_score = score;
+        best_feasible_.rudy_energy = m.rudy_energy;
         best_feasible_.found = true;
         is_new_best = true;
     }
@@ -307,6 +381,7 @@ void Session::considerCheckpoint(double2* positions, const ObjectiveMetrics& m, 
         best_fallback_.hpwl = m.hpwl;
         best_fallback_.overflow = overflow;
         best_fallback_.selection_score = score;
+        best_fallback_.rudy_energy = m.rudy_energy;
         best_fallback_.found = true;
         is_new_best = true;
     }
@@ -331,11 +406,24 @@ void Session::iterate() {
         current = initial_;
     } else {
         smoothing_ = smoothingFromOverflow(last_optimizer_overflow_);
+        if (rudy_active_ && refreshRudyWeight()) has_previous_gradient_ = false;
         current = evaluateGiven(cur_, true, penalty_, raw_cur_, pre_cur_, has_previous_gradient_, true,
                                 density_cached_);
     }
+    bool rudy_just_activated = false;
+    if (rudy_requested_ && !rudy_active_ &&
+        current.m.design.normalized_overflow <= o.routability_start_overflow) {
+        activateRudy(current, has_previous_gradient_, true);
+        refreshCheckpointRudyScore(best_feasible_);
+        has_previous_gradient_ = false;
+        checkCuda(cudaMemsetAsync(velocity_, 0, sizeof(double2) * static_cast<std::size_t>(engine_->particleCount()),
+                                  engine_->stream()),
+                  "Clear velocity");
+        velocity_zero_ = true;
+        rudy_just_activated = true;
+    }
 
-    bool restarted = objective_worse_streak_ >= 2;
+    bool restarted = objective_worse_streak_ >= 2 || rudy_just_activated;
     bool momentum_used = false;
     double2* base_positions = cur_;
     const StateEval* base = &current;
@@ -448,6 +536,7 @@ void Session::iterate() {
         last_optimizer_overflow_ = accepted_eval.m.optimizer.normalized_overflow;
         considerCheckpoint(cur_, accepted_eval.m, iteration + 1, new_best_checkpoint);
         ++result_.accepted_iterations;
+        if (rudy_active_) ++rudy_accepted_age_;
         if (accepted_eval.m.design.normalized_overflow <= o.maximum_bin_overflow) {
             ++feasible_refinement_iterations_;
         } else {
@@ -455,7 +544,7 @@ void Session::iterate() {
         }
         history_.push_back(makeHistoryRow(iteration + 1, accepted_eval.m, penalty_used, smoothing_, used_step_size,
                                           used_maximum_displacement, base_pre_norm, used_curvature, backtracks,
-                                          restarted, true, new_best_checkpoint));
+                                          restarted, true, new_best_checkpoint, rudy_weight_, rudy_active_));
     } else {
         checkCuda(cudaMemsetAsync(velocity_, 0, sizeof(double2) * static_cast<std::size_t>(engine_->particleCount()),
                                   engine_->stream()),
@@ -475,7 +564,8 @@ void Session::iterate() {
             feasible_refinement_iterations_ = 0;
         }
         history_.push_back(makeHistoryRow(iteration + 1, current.m, penalty_used, smoothing_, 0.0, 0.0,
-                                          current.pre_norm, 0.0, backtracks, restarted, false, false));
+                                          current.pre_norm, 0.0, backtracks, restarted, false, false, rudy_weight_,
+                                          rudy_active_));
     }
     result_.completed_iterations = iteration + 1;
     ++iteration_;
@@ -534,6 +624,23 @@ void Session::finish(double* module_x, double* module_y, mpgp_result* result, mp
         const StateEval final_eval = evaluateGiven(cand_, false, penalty_, nullptr, nullptr, false, false);
         result_.hpwl_after = final_eval.m.hpwl;
         result_.overflow_after = final_eval.m.design.normalized_overflow;
+        if (rudy_active_) {
+            // The RUDY metrics of the final placement (AdaptiveGlobalPlacer.cpp:941-950).
+            const RudyReport r = engine_->rudyEvaluate(cand_, false);
+            result_.rudy_energy_after = r.energy;
+            result_.rudy_horizontal_capacity = r.horizontal_capacity;
+            result_.rudy_vertical_capacity = r.vertical_capacity;
+            result_.rudy_proxy_overflow_after = r.proxy_overflow;
+            result_.rudy_maximum_utilization_after = r.maximum_utilization;
+            result_.rudy_p95_utilization_after = r.p95_utilization;
+            if (engine_->rudyValidationEnabled()) {
+                const RudyReport v = engine_->rudyEvaluate(cand_, true);
+                result_.rudy_validation_energy_after = v.energy;
+                result_.rudy_validation_proxy_overflow_after = v.proxy_overflow;
+                result_.rudy_validation_maximum_utilization_after = v.maximum_utilization;
+                result_.rudy_validation_p95_utilization_after = v.p95_utilization;
+            }
+        }
         result_.cuda_reserved_memory_bytes = engine_->reservedBytes();
     }
     result_.elapsed_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - started_).count();

@@ -15,6 +15,9 @@ struct ObjectiveMetrics {
     double smooth_wirelength = 0.0;
     double density_energy = 0.0;
     double objective = 0.0;
+    double rudy_energy = 0.0;
+    double rudy_proxy_overflow = 0.0;
+    double rudy_maximum_utilization = 0.0;
     mpgp_density_metrics optimizer{};
     mpgp_density_metrics design{};
 };
@@ -29,6 +32,7 @@ struct StateEval {
     double delta_pos2 = 0.0;
     double delta_grad2 = 0.0;
     double alignment = 0.0;  // sum v . pre
+    double rudy_l1 = 0.0;    // |RUDY gradient|_1 over particles (unweighted)
     double predicted = 0.0;
     double max_displacement = 0.0;
     double2* raw = nullptr;
@@ -41,6 +45,7 @@ struct CheckpointState {
     double hpwl = 0.0;
     double overflow = 0.0;
     double selection_score = 0.0;
+    double rudy_energy = 0.0;
     bool found = false;
 };
 
@@ -61,11 +66,16 @@ public:
 
 private:
     StateEval evaluateGiven(double2* positions, bool gradient, double penalty, double2* raw, double2* pre,
-                            bool with_prev, bool with_velocity, bool reuse_density = false);
+                            bool with_prev, bool with_velocity, bool reuse_density = false,
+                            double rudy_weight_override = -1.0);
     StateEval evaluateLookahead(double momentum, double penalty, double2* raw, double2* pre);
     StateEval evaluateProposal(const double2* base, const StateEval& base_eval, double step, double max_disp,
                                double penalty);
-    void fillMetrics(const EvalScalars& s, double penalty, StateEval& out) const;
+    void fillMetrics(const EvalScalars& s, double penalty, double rudy_weight, StateEval& out) const;
+    // The routability schedule (AdaptiveGlobalPlacer.cpp:685-719).
+    bool refreshRudyWeight();
+    void activateRudy(StateEval& evaluation, bool with_prev, bool with_velocity);
+    void refreshCheckpointRudyScore(CheckpointState& checkpoint);
     void considerCheckpoint(double2* positions, const ObjectiveMetrics& metrics, int iteration, bool& is_new_best);
     double smoothingFromOverflow(double overflow) const;
     void iterate();
@@ -116,6 +126,12 @@ private:
     // The last evaluation was the accepted candidate now held in cur_, so its
     // density map, field coefficients and energy are still on the device.
     bool density_cached_ = false;
+    // RUDY routability term.
+    bool rudy_requested_ = false;
+    bool rudy_active_ = false;
+    int rudy_accepted_age_ = 0;
+    double rudy_target_weight_ = 0.0;
+    double rudy_weight_ = 0.0;
 };
 
 }  // namespace mpgp

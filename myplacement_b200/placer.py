@@ -253,6 +253,10 @@ def build_layout(design: Design, particle_width, particle_height, particle_layer
                          design.core, target_density, static_fixed, static_dark)
 
 
+RUDY_METRIC_NAMES = ("horizontal_total", "vertical_total", "horizontal_mean", "vertical_mean", "horizontal_capacity",
+                     "vertical_capacity", "proxy_overflow", "maximum_utilization", "p95_utilization", "energy")
+
+
 class CudaPlacementBackend:
     """CudaPlacementBackend::evaluate over mpgp_backend_* (host positions in, host gradients out)."""
 
@@ -292,6 +296,27 @@ class CudaPlacementBackend:
         check(self.lib.mpgp_backend_field_solve(self.handle, _ptr(deviation.reshape(-1), _d),
                                                 *(_ptr(a, _d) for a in out)))
         return [a.reshape(deviation.shape) for a in out]
+
+    def rudy(self, positions: np.ndarray, options, capacity=(0.0, 0.0), gradient: bool = False) -> dict:
+        """The RUDY metrics (and subgradient) of one placement on the backend's nets.
+
+        `options` supplies the grid, minimum span, penalty model and softplus
+        temperature; the first call fixes the grid.  The ten metrics are named
+        by RUDY_METRIC_NAMES; with `gradient` the result also holds the
+        per-particle subgradient and the energy of the evaluation that made it.
+        """
+        positions = np.ascontiguousarray(positions, np.float64).reshape(-1)
+        metrics = np.empty(10)
+        energy = C.c_double(0.0)
+        grad = np.zeros(positions.size)
+        check(self.lib.mpgp_backend_rudy(self.handle, C.byref(options), _ptr(positions, _d), float(capacity[0]),
+                                         float(capacity[1]), int(gradient), _ptr(metrics, _d), C.byref(energy),
+                                         _ptr(grad, _d)))
+        out = dict(zip(RUDY_METRIC_NAMES, metrics.tolist()))
+        if gradient:
+            out["gradient"] = grad.reshape(-1, 2)
+            out["evaluation_energy"] = energy.value
+        return out
 
     def device(self) -> int:
         return int(self.lib.mpgp_backend_device(self.handle))

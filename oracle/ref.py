@@ -54,6 +54,8 @@ class ReferenceLibrary:
                                                C.POINTER(_abi.DensityMetrics), C.POINTER(_abi.DensityMetrics),
                                                _d, _d]),
             "ref_session_components": (C.c_int, [_vp, _d, C.c_double, _d, _d, _d, _d, _d, _d, _d, _d, _d, _d]),
+            "ref_session_rudy": (C.c_int, [_vp, _d, C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_double,
+                                           C.c_double, C.c_double, C.c_int, _d, _d]),
             "ref_field_solve": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
                                           _d, _d, _d, _d]),
             "ref_field_sample": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
@@ -211,6 +213,23 @@ class ReferenceSession:
             "potential": fields[0].reshape(shape), "field_x": fields[1].reshape(shape),
             "field_y": fields[2].reshape(shape),
         }
+
+    def rudy(self, positions: np.ndarray, columns: int, rows: int, model: int, capacity=(0.0, 0.0),
+             minimum_span: float = 0.25, temperature: float = 0.10, gradient: bool = False) -> dict:
+        """evaluateRudy at `positions`: the ten metrics of RUDY_METRIC_NAMES and the per-particle subgradient."""
+        positions = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1)
+        metrics = np.empty(10)
+        grad = np.zeros(positions.size)
+        self.ref._check(self.ref.lib.ref_session_rudy(
+            self.handle, _ptr(positions, _d), columns, rows, minimum_span, model, temperature, float(capacity[0]),
+            float(capacity[1]), int(gradient), _ptr(metrics, _d), _ptr(grad, _d)))
+        out = dict(zip(RUDY_METRIC_NAMES, metrics.tolist()))
+        out["gradient"] = grad.reshape(-1, 2)
+        return out
+
+
+RUDY_METRIC_NAMES = ("horizontal_total", "vertical_total", "horizontal_mean", "vertical_mean", "horizontal_capacity",
+                     "vertical_capacity", "proxy_overflow", "maximum_utilization", "p95_utilization", "energy")
 
 
 # ---- the project's fixed-point restatement (oracle/density_fixed.c) ----------------------

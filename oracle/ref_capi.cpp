@@ -208,6 +208,15 @@ int ref_global_place(const mpgp_design* design, const mpgp_options* flat_options
         result->cuda_reserved_memory_bytes = run.cuda_reserved_memory_bytes;
         result->history_count = static_cast<int32_t>(run.history.size());
         result->rudy_energy_after = run.rudy_energy_after;
+        result->rudy_horizontal_capacity = run.rudy_metrics.horizontal_capacity;
+        result->rudy_vertical_capacity = run.rudy_metrics.vertical_capacity;
+        result->rudy_proxy_overflow_after = run.rudy_metrics.proxy_overflow;
+        result->rudy_maximum_utilization_after = run.rudy_metrics.maximum_utilization;
+        result->rudy_p95_utilization_after = run.rudy_metrics.p95_utilization;
+        result->rudy_validation_energy_after = run.rudy_validation_energy_after;
+        result->rudy_validation_proxy_overflow_after = run.rudy_validation_metrics.proxy_overflow;
+        result->rudy_validation_maximum_utilization_after = run.rudy_validation_metrics.maximum_utilization;
+        result->rudy_validation_p95_utilization_after = run.rudy_validation_metrics.p95_utilization;
         const std::size_t rows = std::min<std::size_t>(run.history.size(), static_cast<std::size_t>(
                                                                                std::max(0, history_capacity)));
         for (std::size_t index = 0; index < rows; ++index) {
@@ -416,6 +425,49 @@ int ref_session_components(void* handle, const double* positions, double smoothi
             const Vec2 value = field.sampleField(clamped[index]) * (-charge);
             density_gradient[2 * index] = value.x;
             density_gradient[2 * index + 1] = value.y;
+        }
+        return MPGP_OK;
+    } catch (const std::exception& error) {
+        return fail(error);
+    }
+}
+
+// evaluateRudy (Rudy.cpp:227-456) of the session's design at `positions` (applied
+// with the session's clamping), with the given grid, model and capacities.
+// metrics (10): horizontal/vertical total, horizontal/vertical mean, horizontal/
+// vertical capacity, proxy overflow, maximum and p95 utilisation, energy.  The
+// gradient is returned in particle order (zero for fillers).
+int ref_session_rudy(void* handle, const double* positions, int32_t columns, int32_t rows, double minimum_span,
+                     int32_t model, double temperature, double capacity_h, double capacity_v,
+                     int calculate_gradient, double* metrics, double* gradient) {
+    try {
+        auto* state = static_cast<RefSession*>(handle);
+        const std::size_t count = state->session->particleCount();
+        std::vector<Vec2> applied(count);
+        for (std::size_t index = 0; index < count; ++index) applied[index] = {positions[2 * index], positions[2 * index + 1]};
+        state->session->applyPositions(applied);
+        RudyOptions options = state->options.rudy_options;
+        options.columns = columns;
+        options.rows = rows;
+        options.minimum_span_in_bins = minimum_span;
+        options.penalty_model = static_cast<RudyPenaltyModel>(model);
+        options.softplus_temperature = temperature;
+        const RudyEvaluation r =
+            evaluateRudy(state->database, options, RudyCapacity{capacity_h, capacity_v}, calculate_gradient != 0);
+        const double values[10] = {r.metrics.horizontal_total_demand, r.metrics.vertical_total_demand,
+                                   r.metrics.horizontal_mean_demand,  r.metrics.vertical_mean_demand,
+                                   r.metrics.horizontal_capacity,     r.metrics.vertical_capacity,
+                                   r.metrics.proxy_overflow,          r.metrics.maximum_utilization,
+                                   r.metrics.p95_utilization,         r.energy};
+        std::copy(values, values + 10, metrics);
+        if (calculate_gradient != 0 && gradient != nullptr) {
+            const auto& movable_ids = state->database.movableModules();
+            for (std::size_t index = 0; index < count; ++index) {
+                const Vec2 value = index < movable_ids.size() && !r.gradient.empty() ? r.gradient[movable_ids[index]]
+                                                                                    : Vec2{};
+                gradient[2 * index] = value.x;
+                gradient[2 * index + 1] = value.y;
+            }
         }
         return MPGP_OK;
     } catch (const std::exception& error) {

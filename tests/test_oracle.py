@@ -165,3 +165,76 @@ def _fixture(golden_dir, stem: str) -> Design:
 
 def _golden_design(g) -> Design:
     return Design(**{k[len("dsg_"):]: g[k] for k in g.files if k.startswith("dsg_")}, name="eval_small")
+
+
+# ---- RUDY (RudyTests.cpp) --------------------------------------------------------------------
+
+RUDY_GRID = dict(columns=5, rows=5, minimum_span=0.01)  # RudyTests.cpp:44-48
+
+
+def _rudy_session(ref, first=(1.3, 1.7), second=(6.4, 4.6)):
+    from conftest import two_pin_design
+    from oracle.ref import default_options
+
+    return ref.session(two_pin_design(first, second), default_options(bins_x=4, bins_y=4, target_density=0.9))
+
+
+def _finite_difference(session, positions, particle, axis, capacity, model, delta=1e-5):
+    plus, minus = positions.copy(), positions.copy()
+    plus[particle, axis] += delta
+    minus[particle, axis] -= delta
+    e_plus = session.rudy(plus, model=model, capacity=capacity, **RUDY_GRID)["energy"]
+    e_minus = session.rudy(minus, model=model, capacity=capacity, **RUDY_GRID)["energy"]
+    return (e_plus - e_minus) / (2.0 * delta)
+
+
+def test_rudy_reference_known_answers(ref):
+    """RudyTests.cpp:50-110: demand integrates to the net spans (5.1, 2.9), a 0.45 x mean
+    capacity exposes a hotspot, and the analytical gradient of every penalty model agrees
+    with a central difference to 3e-6."""
+    session = _rudy_session(ref)
+    pos = session.positions
+    raw = session.rudy(pos, model=1, **RUDY_GRID)
+    assert raw["horizontal_total"] == pytest.approx(5.1, abs=1e-12)
+    assert raw["vertical_total"] == pytest.approx(2.9, abs=1e-12)
+    capacity = (0.45 * raw["horizontal_mean"], 0.45 * raw["vertical_mean"])
+    for model in (1, 2, 3):
+        ev = session.rudy(pos, model=model, capacity=capacity, gradient=True, **RUDY_GRID)
+        assert np.isfinite(ev["energy"]) and ev["energy"] > 0.0
+        assert ev["maximum_utilization"] > 1.0
+        for axis in (0, 1):
+            fd = _finite_difference(session, pos, 0, axis, capacity, model)
+            assert ev["gradient"][0, axis] == pytest.approx(fd, abs=3e-6), (model, axis)
+    assert abs(session.rudy(pos, model=3, capacity=capacity, gradient=True, **RUDY_GRID)["gradient"][0, 0]) > 1e-10
+
+
+def test_rudy_reference_boundary_and_degenerate_nets(ref):
+    """RudyTests.cpp:112-148: a net whose box edges lie on grid lines keeps a non-zero
+    Clarke subgradient; a zero-span net keeps its translation gradient."""
+    session = _rudy_session(ref, first=(2.0, 1.7), second=(6.0, 4.6))
+    pos = session.positions
+    raw = session.rudy(pos, model=2, **RUDY_GRID)
+    capacity = (0.45 * raw["horizontal_mean"], 0.45 * raw["vertical_mean"])
+    ev = session.rudy(pos, model=2, capacity=capacity, gradient=True, **RUDY_GRID)
+    assert abs(ev["gradient"][0, 0]) + abs(ev["gradient"][1, 0]) > 1e-10
+
+    session = _rudy_session(ref)
+    pos = session.positions
+    raw = session.rudy(pos, model=2, **RUDY_GRID)
+    capacity = (0.45 * raw["horizontal_mean"], 0.45 * raw["vertical_mean"])
+    pos[1] = pos[0]
+    ev = session.rudy(pos, model=2, capacity=capacity, gradient=True, **RUDY_GRID)
+    assert np.isfinite(ev["energy"])
+    plus, minus = pos.copy(), pos.copy()
+    plus[:2, 0] += 1e-5
+    minus[:2, 0] -= 1e-5
+    fd = (session.rudy(plus, model=2, capacity=capacity, **RUDY_GRID)["energy"] -
+          session.rudy(minus, model=2, capacity=capacity, **RUDY_GRID)["energy"]) / 2e-5
+    assert ev["gradient"][0, 0] + ev["gradient"][1, 0] == pytest.approx(fd, abs=3e-6)
+
+
+def test_rudy_reference_rejects_partial_capacity(ref):
+    """RudyTests.cpp:150-166: a capacity with one zero component is refused."""
+    session = _rudy_session(ref)
+    with pytest.raises(RuntimeError):
+        session.rudy(session.positions, model=1, capacity=(1.0, 0.0), **RUDY_GRID)
