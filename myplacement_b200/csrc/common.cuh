@@ -94,6 +94,56 @@ __device__ __forceinline__ void blockReduce(double (&values)[K], const bool (&is
     __syncthreads();
 }
 
+// atomicAdd with acquire-release semantics at GPU scope: the caller's earlier
+// writes are visible to whoever observes the new count, and a caller that sees
+// the final count sees every earlier writer's data.
+__device__ __forceinline__ unsigned int atomicAddAcqRel(unsigned int* address, unsigned int value) {
+    unsigned int old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(address), "r"(value) : "memory");
+    return old;
+}
+
+// Second level of a deterministic grid reduction, called by every block after
+// thread 0 wrote the block's K partials at partials[K * blockIdx.x + k]: the
+// last block of each group of 32 consecutive blocks reduces the group's rows (in
+// block order) into group_partials[K * group + k].  counters holds 1 + groups
+// zeros and is left zeroed.  Returns 0 in most blocks, 1 in a block that
+// finished a group, 2 in the block that finished the last group (after which
+// every group row is visible to it).  Thread 0 does every global write and
+// counter update, so its release / acquire atomics order all of them.
+template <int K>
+__device__ int reduceGroups(const double* partials, double* group_partials, unsigned int* counters,
+                            const bool (&is_max)[K]) {
+    __shared__ int state;
+    __shared__ double folded[K];
+    const unsigned int group = blockIdx.x / 32U;
+    const unsigned int groups = (gridDim.x + 31U) / 32U;
+    const unsigned int first = group * 32U;
+    const unsigned int size = min(32U, gridDim.x - first);
+    if (threadIdx.x == 0) state = atomicAddAcqRel(counters + 1 + group, 1U) == size - 1U ? 1 : 0;
+    __syncthreads();
+    if (state == 0) return 0;
+    const unsigned int lane = threadIdx.x & 31U;
+    const int warp = static_cast<int>(threadIdx.x >> 5);
+    const int warps = static_cast<int>(blockDim.x >> 5);
+    for (int k = warp; k < K; k += warps) {
+        double x = is_max[k] ? -1.0e308 : 0.0;
+        if (lane < size) x = __ldcg(partials + static_cast<size_t>(first + lane) * K + k);
+        x = is_max[k] ? warpMax(x) : warpSum(x);
+        if (lane == 0) folded[k] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) group_partials[static_cast<size_t>(group) * K + k] = folded[k];
+        counters[1 + group] = 0U;
+        state = atomicAddAcqRel(counters, 1U) == groups - 1U ? 2 : 1;
+        if (state == 2) counters[0] = 0U;
+    }
+    __syncthreads();
+    return state;
+}
+
 __device__ __forceinline__ long long warpSumI64(long long value) {
 #pragma unroll
     for (int offset = 16; offset > 0; offset >>= 1) value += __shfl_xor_sync(0xffffffffu, value, offset);

@@ -49,6 +49,7 @@
 #include <string>
 
 #include "common.cuh"
+#include "split.cuh"
 #include "dct_tc.cuh"
 
 namespace mpgp {
@@ -184,35 +185,9 @@ __device__ __forceinline__ void tmemWait(uint32_t (&a)[16], uint32_t (&b)[16]) {
                  : "memory");
 }
 
-// 2^e as a double (|e| < 1000), built from its exponent field.
-__device__ __forceinline__ double pow2(int e) {
-    return __longlong_as_double(static_cast<long long>(1023 + e) << 52);
-}
-
-// Smallest e with v <= 2^e for a positive finite v (0 otherwise).
-__device__ __forceinline__ int exponentOf(float v) {
-    if (!(v > 0.0f) || !isfinite(v)) return 0;
-    int e = 0;
-    const float m = frexpf(v, &e);  // v = m * 2^e, m in [0.5, 1)
-    return m == 0.5f ? e - 1 : e;
-}
-
 // Plane exponent of an output bounded by ref_max * gain.
 __device__ __forceinline__ int planeExponent(const unsigned* ref_max, float gain) {
     return min(120, max(-120, exponentOf(__uint_as_float(*ref_max) * gain) - kPlaneTop));
-}
-
-constexpr float kLoShift = 2048.0f;  // 2^11: the lo plane's extra scale
-
-// (hi, lo) planes of v * 2^-e.
-__device__ __forceinline__ void splitScaled(float v, float inv_scale, __half& hi, __half& lo) {
-    const float y = v * inv_scale;
-    hi = __float2half_rn(y);
-    lo = __float2half_rn((y - __half2float(hi)) * kLoShift);
-}
-
-__device__ __forceinline__ uint32_t packHalves(__half a, __half b) {
-    return static_cast<uint32_t>(__half_as_ushort(a)) | (static_cast<uint32_t>(__half_as_ushort(b)) << 16);
 }
 
 // Eight consecutive values as two 16-byte plane stores (dst 16-byte aligned).
@@ -301,6 +276,24 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
     }
     __syncthreads();
     clusterArrive();  // this CTA's barriers are initialised; peers wait for it before sending
+    // The first stages' basis tiles do not depend on the previous kernels: issue them
+    // now, so that only the data operand's latency follows the dependency wait.
+    const int prefetched = t.constant_operand != 0 ? min(k_blocks, kStages) : 0;
+    if (warp == 0 && lane == 0) {
+        for (int kb = 0; kb < prefetched; ++kb) {
+            unsigned char* stage = smem + kb * kStageBytes;
+            const int k0 = (kb_begin + kb) * kBlockK;
+            mbarExpectTx(full0 + 8 * kb, kStageBytes);
+            for (int p = 0; p < kSplit; ++p) {
+                if (t.constant_operand == 1) {
+                    tmaLoad3d(smemAddress(stage + p * kTileM * kBlockK * 2), &t.map_a, full0 + 8 * kb, k0, m0, p);
+                } else {
+                    tmaLoad3d(smemAddress(stage + kSplit * kTileM * kBlockK * 2 + p * kTileN * kBlockK * 2),
+                              &t.map_b, full0 + 8 * kb, k0, n0, p);
+                }
+            }
+        }
+    }
     waitForPrior();   // the operands and scale bookkeeping come from the previous kernels
 
     if (warp == 0) {
@@ -314,11 +307,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
                 if (!ok) break;
                 unsigned char* stage = smem + s * kStageBytes;
                 const int k0 = (kb_begin + kb) * kBlockK;
-                mbarExpectTx(full0 + 8 * s, kStageBytes);
+                const bool early = kb < prefetched;  // its basis tile is already on the way
+                if (!early) mbarExpectTx(full0 + 8 * s, kStageBytes);
                 for (int p = 0; p < kSplit; ++p) {
-                    tmaLoad3d(smemAddress(stage + p * kTileM * kBlockK * 2), &t.map_a, full0 + 8 * s, k0, m0, p);
-                    tmaLoad3d(smemAddress(stage + kSplit * kTileM * kBlockK * 2 + p * kTileN * kBlockK * 2),
-                              &t.map_b, full0 + 8 * s, k0, n0, p);
+                    if (!early || t.constant_operand != 1) {
+                        tmaLoad3d(smemAddress(stage + p * kTileM * kBlockK * 2), &t.map_a, full0 + 8 * s, k0, m0, p);
+                    }
+                    if (!early || t.constant_operand != 2) {
+                        tmaLoad3d(smemAddress(stage + kSplit * kTileM * kBlockK * 2 + p * kTileN * kBlockK * 2),
+                                  &t.map_b, full0 + 8 * s, k0, n0, p);
+                    }
                 }
                 issued = kb + 1;
             }

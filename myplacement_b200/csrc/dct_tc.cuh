@@ -18,7 +18,7 @@ constexpr int kTileM = 128;    // UMMA M = TMEM lanes
 constexpr int kTileN = 64;     // UMMA N = accumulator columns per CTA
 constexpr int kBlockK = 64;    // fp16 elements per 128-byte swizzled row
 constexpr int kStages = 3;
-constexpr int kMaxSplit = 8;   // largest K split (cluster size)
+constexpr int kMaxSplit = 2;   // largest K split (cluster size)
 
 // A row-major matrix stored as kSplit fp16 planes; ld is a multiple of kBlockK
 // and the padding columns are zero.
@@ -60,6 +60,7 @@ struct alignas(64) TcTask {
     CUtensorMap map_b;
     int m, n, k;
     int mode;
+    int constant_operand;  // 1: A, 2: B is a fixed basis matrix (loaded before the dependency wait); 0: none
     const int* exp_a;      // exponent of A, or null when row_exp_a is given
     const int* row_exp_a;  // per-row exponents of A
     const int* exp_b;

@@ -19,7 +19,9 @@
 // mean-free FP32 source of the Poisson solve (ElectrostaticField.cpp:119-133);
 // the mean comes from the exact integer layer totals of the scatter.
 #include "common.cuh"
+#include "dct_tc.cuh"
 #include "kernels.cuh"
+#include "split.cuh"
 
 namespace mpgp {
 namespace {
@@ -138,6 +140,9 @@ __global__ void __launch_bounds__(kThreads) scatterKernel(ScatterArgs a) {
             a.partials[2 * blockIdx.x + 1] = values[1];
         }
     }
+    if (a.mode == kPropose && a.partials != nullptr) {
+        reduceGroups<2>(a.partials, a.group_partials, a.group_counters, is_max);
+    }
 }
 
 // One bin's metric terms (DensityBin::chargeArea / normalizationArea, Metrics.hpp:25-35).
@@ -220,6 +225,122 @@ __global__ void __launch_bounds__(kThreads) metricsKernel(MetricsArgs a) {
     }
 }
 
+// The metrics pass fused with the source split of the field solve: one block
+// per bin row forms the row's sources in registers (they are never stored),
+// takes the row maximum for the row's plane exponent (splitSourceKernel's rule)
+// and writes the fp16 hi / lo planes of the first contraction's operand.  The
+// per-row partials are folded per 32 rows (reduceGroups).
+__global__ void __launch_bounds__(kThreads) metricsSplitKernel(MetricsArgs a) {
+    releaseNext();
+    waitForPrior();
+    BinTerms terms;
+    terms.t = a.target_density;
+    terms.unit = a.bin_area * kFixedUnit;
+    terms.capacity = terms.t * a.bin_area;
+    terms.inv_area = 1.0 / a.bin_area;
+    const double movable_sum = static_cast<double>(static_cast<long long>(a.totals[0])) * terms.unit;
+    const double macro_sum = static_cast<double>(static_cast<long long>(a.totals[1])) * terms.unit;
+    const double filler_sum = static_cast<double>(static_cast<long long>(a.totals[2])) * terms.unit;
+    const double charge_total =
+        movable_sum + terms.t * (a.static_fixed_sum + macro_sum + a.static_dark_sum + filler_sum);
+    terms.mean = charge_total / (a.bin_area * static_cast<double>(a.bin_count)) - terms.t;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.scales->max_x = 0u;
+        a.scales->max_phi = 0u;
+    }
+
+    const int row = blockIdx.x;
+    const int cols = a.columns;
+    const size_t base = static_cast<size_t>(row) * cols;
+    const int bins = a.bin_count;
+    unsigned long long* qm = a.layers + base;
+    unsigned long long* qc = a.layers + bins + base;
+    unsigned long long* qf = a.layers + 2 * static_cast<size_t>(bins) + base;
+    const double* st = a.static_charge + base;
+    double v[9] = {0, 0, 0, 0, 0, 0, 0, -1.0e308, -1.0e308};
+    float out[kMetricsSplitPerThread];
+    float top = 0.0f;
+    const bool pairs = (cols & 1) == 0;
+    if (pairs) {
+#pragma unroll
+        for (int j = 0; j < kMetricsSplitPerThread / 2; ++j) {
+            const int pair = static_cast<int>(threadIdx.x) + j * kThreads;
+            out[2 * j] = 0.0f;
+            out[2 * j + 1] = 0.0f;
+            if (pair < cols / 2) {
+                const ulonglong2 m = reinterpret_cast<const ulonglong2*>(qm)[pair];
+                const ulonglong2 c = reinterpret_cast<const ulonglong2*>(qc)[pair];
+                const ulonglong2 f = reinterpret_cast<const ulonglong2*>(qf)[pair];
+                const double2 s = reinterpret_cast<const double2*>(st)[pair];
+                const ulonglong2 zero = make_ulonglong2(0ULL, 0ULL);
+                reinterpret_cast<ulonglong2*>(qm)[pair] = zero;
+                reinterpret_cast<ulonglong2*>(qc)[pair] = zero;
+                reinterpret_cast<ulonglong2*>(qf)[pair] = zero;
+                terms.add(m.x, c.x, f.x, s.x, v, out[2 * j]);
+                terms.add(m.y, c.y, f.y, s.y, v, out[2 * j + 1]);
+                top = fmaxf(top, fmaxf(fabsf(out[2 * j]), fabsf(out[2 * j + 1])));
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < kMetricsSplitPerThread; ++j) {
+            const int c = static_cast<int>(threadIdx.x) + j * kThreads;
+            out[j] = 0.0f;
+            if (c < cols) {
+                const unsigned long long m = qm[c], cm = qc[c], f = qf[c];
+                qm[c] = 0ULL;
+                qc[c] = 0ULL;
+                qf[c] = 0ULL;
+                terms.add(m, cm, f, st[c], v, out[j]);
+                top = fmaxf(top, fabsf(out[j]));
+            }
+        }
+    }
+    __shared__ float warp_top[kThreads / 32];
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int offset = 16; offset > 0; offset >>= 1) top = fmaxf(top, __shfl_xor_sync(0xffffffffu, top, offset));
+    if (lane == 0) warp_top[threadIdx.x >> 5] = top;
+    __syncthreads();
+    top = 0.0f;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) top = fmaxf(top, warp_top[w]);
+    const int e = exponentOf(top) - kPlaneTop;
+    if (threadIdx.x == 0) {
+        a.row_exp[row] = e;
+        atomicMax(&a.scales->max_source, __float_as_uint(top));
+    }
+    const float inv_scale = static_cast<float>(pow2(-e));
+    __half* hi = a.split_out + static_cast<size_t>(row) * a.split_ld;
+    __half* lo = hi + a.split_plane;
+    if (pairs) {
+#pragma unroll
+        for (int j = 0; j < kMetricsSplitPerThread / 2; ++j) {
+            const int pair = static_cast<int>(threadIdx.x) + j * kThreads;
+            if (pair < cols / 2) {
+                __half h0, l0, h1, l1;
+                splitScaled(out[2 * j], inv_scale, h0, l0);
+                splitScaled(out[2 * j + 1], inv_scale, h1, l1);
+                reinterpret_cast<uint32_t*>(hi)[pair] = packHalves(h0, h1);
+                reinterpret_cast<uint32_t*>(lo)[pair] = packHalves(l0, l1);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < kMetricsSplitPerThread; ++j) {
+            const int c = static_cast<int>(threadIdx.x) + j * kThreads;
+            if (c < cols) splitScaled(out[j], inv_scale, hi[c], lo[c]);
+        }
+    }
+    const bool is_max[9] = {false, false, false, false, false, false, false, true, true};
+    blockReduce<9>(v, is_max);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) a.partials[9 * blockIdx.x + k] = v[k];
+    }
+    reduceGroups<9>(a.partials, a.group_partials, a.group_counters, is_max);
+}
+
 __global__ void velocityKernel(const double2* next, const double2* previous, double2* velocity, int count) {
     releaseNext();
     waitForPrior();
@@ -239,6 +360,12 @@ void launchScatter(const ScatterArgs& args, int blocks, cudaStream_t stream) {
 
 void launchMetrics(const MetricsArgs& args, int blocks, cudaStream_t stream) {
     launchChained("Launch the density metrics", metricsKernel, dim3(blocks), dim3(kThreads), 0, stream, args);
+}
+
+void launchMetricsSplit(const MetricsArgs& args, cudaStream_t stream) {
+    if (args.rows <= 0) return;
+    launchChained("Launch the density metrics and source split", metricsSplitKernel, dim3(args.rows),
+                  dim3(kThreads), 0, stream, args);
 }
 
 void launchVelocity(const double2* next, const double2* previous, double2* velocity, int count, cudaStream_t stream) {

@@ -16,6 +16,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <atomic>
+#include <thread>
 
 #include "common.cuh"
 
@@ -86,9 +88,17 @@ Engine::Engine(const Problem& p, int device, uint64_t budget_bytes) : device_(de
     uploadStatic(p);
     buildNetLayout(p);
     buildBasis();
+    allocateGroups();
     h2d_bytes_ += g_uploaded_bytes - uploaded_before;
+    // The reduction publishes the scalars and the error flag into mapped pinned
+    // memory; the host polls it, with no copy or stream synchronisation on the
+    // evaluation's critical path.
     checkCuda(cudaMallocHost(reinterpret_cast<void**>(&host_scalars_), sizeof(EvalScalars)), "pinned scalars");
     std::memset(host_scalars_, 0, sizeof(EvalScalars));
+    const std::size_t slot_bytes = 2 * (static_cast<std::size_t>(kScalarCount) + 1) * sizeof(unsigned long long);
+    checkCuda(cudaHostAlloc(reinterpret_cast<void**>(&host_slots_), slot_bytes, cudaHostAllocMapped),
+              "pinned evaluation record");
+    std::memset(host_slots_, 0, slot_bytes);
     checkCuda(cudaStreamSynchronize(stream_), "Engine setup");
 }
 
@@ -106,6 +116,7 @@ Engine::~Engine() {
     if (host_scalars_ != nullptr) cudaFreeHost(host_scalars_);
     if (host_rudy_ != nullptr) cudaFreeHost(host_rudy_);
     if (host_error_ != nullptr) cudaFreeHost(host_error_);
+    if (host_slots_ != nullptr) cudaFreeHost(host_slots_);
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
 }
 
@@ -161,8 +172,9 @@ void Engine::uploadStatic(const Problem& p) {
         }
     }
     scatter_blocks_ = ceilDiv(std::max<int64_t>(1, particle_count_), kThreads);
-    gather_blocks_ = scatter_blocks_;
-    metrics_blocks_ = std::min(ceilDiv(bin_count_, 2 * kThreads), 148 * 2);
+    gather_blocks_ = gatherBlocks(static_cast<int>(std::min<int64_t>(particle_count_, 1 << 30)));
+    metrics_fused_ = metricsSplitFits(bins_x_);
+    metrics_blocks_ = metrics_fused_ ? bins_y_ : std::min(ceilDiv(bin_count_, 2 * kThreads), 148 * 2);
     partials_sc_ = arena_.array<double>(2 * static_cast<std::size_t>(scatter_blocks_), "scatter partials");
     partials_m_ = arena_.array<double>(9 * static_cast<std::size_t>(metrics_blocks_), "metric partials");
     partials_g_ = arena_.array<double>(8 * static_cast<std::size_t>(gather_blocks_), "gather partials");
@@ -463,6 +475,12 @@ void Engine::buildTensorCoreBasis(const std::vector<double>& cx, const std::vect
     tc_pot_.task[0].out_f_step = 1;
     tc_fwd1_.error_flag = tc_fwd2_.error_flag = tc_inv1_.error_flag = tc_inv2_.error_flag = tc_pot_.error_flag =
         tc_error_;
+    // The basis operands never change, so their tiles may be fetched before the
+    // contraction waits for its predecessor.
+    const auto basis = [&](const int* e) { return e != nullptr && e >= sc->exp_basis && e < sc->exp_basis + 8; };
+    for (TcBatch* b : {&tc_fwd1_, &tc_fwd2_, &tc_inv1_, &tc_inv2_, &tc_pot_}) {
+        for (TcTask& t : b->task) t.constant_operand = basis(t.exp_a) ? 1 : (basis(t.exp_b) ? 2 : 0);
+    }
     tcPlan(tc_fwd1_, 1);
     tcPlan(tc_fwd2_, 1);
     tcPlan(tc_inv1_, 2);
@@ -519,19 +537,43 @@ void Engine::collectTimings() {
 //   X = S * Cx^T, rho_hat = Cy * X, phi_hat = rho_hat .* scale (+ Parseval energy)
 //   gradient: T = Dy * phi_hat, U = phi_hat * Dx^T, Ex = T * (Sx diag(kx))^T, Ey = (Sy diag(ky)) * U
 //   potential (parity hook only): phi = T * Dx^T.
-void Engine::runDct(bool gradient, bool potential, bool forward) {
+void Engine::allocateGroups() {
+    const auto groups = [](int blocks) { return std::max(1, ceilDiv(std::max(1, blocks), 32)); };
+    const auto counters = [this](int count, const char* what) {
+        unsigned int* c = arena_.array<unsigned int>(static_cast<std::size_t>(count) + 1, what);
+        checkCuda(cudaMemsetAsync(c, 0, (static_cast<std::size_t>(count) + 1) * sizeof(unsigned int), stream_), what);
+        return c;
+    };
+    wl_groups_ = groups(wl_blocks_);
+    sc_groups_ = groups(scatter_blocks_);
+    g_groups_ = groups(gather_blocks_);
+    wl_group_ = arena_.array<double>(2 * static_cast<std::size_t>(wl_groups_), "wirelength group partials");
+    sc_group_ = arena_.array<double>(2 * static_cast<std::size_t>(sc_groups_), "scatter group partials");
+    g_group_ = arena_.array<double>(8 * static_cast<std::size_t>(g_groups_), "gather group partials");
+    m_groups_ = groups(metrics_blocks_);
+    m_group_ = arena_.array<double>(9 * static_cast<std::size_t>(m_groups_), "metric group partials");
+    m_counters_ = counters(m_groups_, "metric group counters");
+    wl_counters_ = counters(wl_groups_, "wirelength group counters");
+    sc_counters_ = counters(sc_groups_, "scatter group counters");
+    g_counters_ = counters(g_groups_, "gather group counters");
+}
+
+void Engine::runDct(bool gradient, bool potential, bool forward, bool split_source) {
     const int nx = bins_x_;
     if (forward) {
-        beginKernel(kKindDctSplit);
-        launchSplitSource(source_, tc_source_, nx, tc_row_exp_, tc_scales_, stream_);
-        endKernel();
+        if (split_source) {
+            beginKernel(kKindDctSplit);
+            launchSplitSource(source_, tc_source_, nx, tc_row_exp_, tc_scales_, stream_);
+            endKernel();
+            launches_ += 1;
+        }
         beginKernel(kKindDctForward);
         launchTcGemm(tc_fwd1_, 1, stream_);
         endKernel();
         beginKernel(kKindDctForward);
         launchTcGemm(tc_fwd2_, 1, stream_);
         endKernel();
-        launches_ += 3;
+        launches_ += 2;
     }
     if (!gradient) return;
     beginKernel(kKindDctInverse);
@@ -578,6 +620,8 @@ void Engine::launch(const EvalRequest& q) {
     sa.layers = layers_;
     sa.totals = totals_;
     sa.partials = partials_sc_;
+    sa.group_partials = sc_group_;
+    sa.group_counters = sc_counters_;
     if (q.mode == kGiven) checkCuda(cudaEventRecord(fork_, stream_), "fork");
     if (!q.reuse_density) {
         beginKernel(kKindScatter);
@@ -603,6 +647,8 @@ void Engine::launch(const EvalRequest& q) {
     wa.pin_gradient = pin_gradient_;
     wa.gradient = q.gradient ? 1 : 0;
     wa.partials = partials_wl_;
+    wa.group_partials = wl_group_;
+    wa.group_counters = wl_counters_;
     beginKernel(kKindWirelength, stream_wl_);
     launchWirelength(wa, wl_blocks_, stream_wl_);
     endKernel(stream_wl_);
@@ -629,18 +675,68 @@ void Engine::launch(const EvalRequest& q) {
     ma.bin_count = bin_count_;
     ma.source = source_;
     ma.partials = partials_m_;
-    int kernels = 2;  // wirelength, reduce
+    int kernels = 1;  // wirelength
     if (!q.reuse_density) {
         beginKernel(kKindMetrics);
-        launchMetrics(ma, metrics_blocks_, stream_);
+        if (metrics_fused_) {
+            ma.columns = nx;
+            ma.rows = ny;
+            ma.split_out = tc_source_.data;
+            ma.split_ld = tc_source_.ld;
+            ma.split_plane = tc_source_.plane();
+            ma.row_exp = tc_row_exp_;
+            ma.scales = tc_scales_;
+            ma.group_partials = m_group_;
+            ma.group_counters = m_counters_;
+            launchMetricsSplit(ma, stream_);
+        } else {
+            launchMetrics(ma, metrics_blocks_, stream_);
+        }
         endKernel();
         kernels += 2;  // scatter, metrics
     }
 
-    runDct(q.gradient, q.gradient && q.want_potential, !q.reuse_density);
+    runDct(q.gradient, q.gradient && q.want_potential, !q.reuse_density, !metrics_fused_);
     checkCuda(cudaStreamWaitEvent(stream_, join_, 0), "join");
 
+    ReduceArgs ra{};
+    int s = 0;
+    const auto add = [&](const double* partials, int rows, int stride, int column, bool is_max, int target) {
+        ra.sources[s++] = ReduceSource{partials, rows, stride, column, is_max ? 1 : 0, target};
+    };
+    add(wl_group_, wl_blocks_ > 0 ? wl_groups_ : 0, 2, 0, false, kSmooth);
+    add(wl_group_, wl_blocks_ > 0 ? wl_groups_ : 0, 2, 1, false, kHpwl);
+    const int scatter_rows = particle_count_ > 0 && q.mode == kPropose ? sc_groups_ : 0;
+    if (!q.reuse_density) {  // otherwise the density scalars of the previous evaluation stand
+        add(sc_group_, scatter_rows, 2, 0, false, kPredicted);
+        add(sc_group_, scatter_rows, 2, 1, true, kMaxDisplacement);
+        for (int k = 0; k < 9; ++k) {
+            if (metrics_fused_) {
+                add(m_group_, m_groups_, 9, k, k >= 7, kOverflowWith + k);
+            } else {
+                add(partials_m_, metrics_blocks_, 9, k, k >= 7, kOverflowWith + k);
+            }
+        }
+        add(partials_e_, energy_blocks_, 1, 0, false, kEnergy);
+    }
+    for (int k = 0; k < 5; ++k) {
+        add(rudy_main_.partials, q.rudy ? rudy_main_.blocks : 0, 5, k, k == 4, kRudyEnergy + k);
+    }
+    const bool gather = q.gradient && particle_count_ > 0;
     if (q.gradient) {
+        for (int k = 0; k < 8; ++k) add(g_group_, gather ? g_groups_ : 0, 8, k, false, kWireL1 + k);
+    }
+    ra.source_count = s;
+    ra.scalars = scalars_;
+    ra.totals = totals_;
+    ra.host_slots = host_slots_;
+    ra.device_error = tc_error_;
+    ra.sequence = static_cast<unsigned int>(++sequence_);
+    if (ra.sequence == 0) ra.sequence = static_cast<unsigned int>(++sequence_);  // 0 marks an empty record
+    expected_mask_ = 0;
+    for (int k = 0; k < s; ++k) expected_mask_ |= 1U << ra.sources[k].target;
+    if (gather) {
+        // The gather's last group finisher also reduces every scalar (no reduce launch).
         GatherArgs ga{};
         ga.particle_count = static_cast<int>(particle_count_);
         ga.movable_count = static_cast<int>(movable_count_);
@@ -671,45 +767,22 @@ void Engine::launch(const EvalRequest& q) {
         ga.rudy_gradient = q.rudy ? rudy_pin_gradient_ : nullptr;
         ga.rudy_weight = q.rudy ? q.rudy_weight : 0.0;
         ga.partials = partials_g_;
+        ga.group_partials = g_group_;
+        ga.group_counters = g_counters_;
+        ga.reduce = ra;
         beginKernel(kKindGather);
-        launchGather(ga, particle_count_ > 0 ? gather_blocks_ : 0, stream_);
+        launchGather(ga, gather_blocks_, stream_);
+        endKernel();
+        kernels += 1;
+    } else {
+        beginKernel(kKindReduce);
+        launchReduce(ra, stream_);
         endKernel();
         kernels += 1;
     }
 
-    ReduceArgs ra{};
-    int s = 0;
-    const auto add = [&](const double* partials, int rows, int stride, int column, bool is_max, int target) {
-        ra.sources[s++] = ReduceSource{partials, rows, stride, column, is_max ? 1 : 0, target};
-    };
-    add(partials_wl_, wl_blocks_, 2, 0, false, kSmooth);
-    add(partials_wl_, wl_blocks_, 2, 1, false, kHpwl);
-    const int scatter_rows = particle_count_ > 0 ? scatter_blocks_ : 0;
-    if (!q.reuse_density) {  // otherwise the density scalars of the previous evaluation stand
-        add(partials_sc_, q.mode == kPropose ? scatter_rows : 0, 2, 0, false, kPredicted);
-        add(partials_sc_, q.mode == kPropose ? scatter_rows : 0, 2, 1, true, kMaxDisplacement);
-        for (int k = 0; k < 9; ++k) add(partials_m_, metrics_blocks_, 9, k, k >= 7, kOverflowWith + k);
-        add(partials_e_, energy_blocks_, 1, 0, false, kEnergy);
-    }
-    for (int k = 0; k < 5; ++k) {
-        add(rudy_main_.partials, q.rudy ? rudy_main_.blocks : 0, 5, k, k == 4, kRudyEnergy + k);
-    }
-    if (q.gradient) {
-        const int rows = particle_count_ > 0 ? gather_blocks_ : 0;
-        for (int k = 0; k < 8; ++k) add(partials_g_, rows, 8, k, false, kWireL1 + k);
-    }
-    ra.source_count = s;
-    ra.scalars = scalars_;
-    ra.totals = totals_;
-    beginKernel(kKindReduce);
-    launchReduce(ra, stream_);
-    endKernel();
-    checkCuda(cudaMemcpyAsync(host_scalars_, scalars_, sizeof(EvalScalars), cudaMemcpyDeviceToHost, stream_),
-              "Download evaluation scalars");
-    d2h_bytes_ += sizeof(EvalScalars);
-    checkCuda(cudaMemcpyAsync(host_error_, tc_error_, sizeof(int), cudaMemcpyDeviceToHost, stream_),
-              "Download contraction status");
-    d2h_bytes_ += sizeof(int);
+
+    d2h_bytes_ += static_cast<uint64_t>(s) * sizeof(double) + sizeof(int) + sizeof(unsigned long long);
     if (q.rudy) kernels += q.gradient ? 3 : 2;
     launches_ += kernels;
     last_gradient_ = q.gradient;
@@ -717,9 +790,40 @@ void Engine::launch(const EvalRequest& q) {
 }
 
 const EvalScalars& Engine::sync() {
-    checkCuda(cudaStreamSynchronize(stream_), "Synchronize placement evaluation");
+    // Poll the record until every scalar of this evaluation and the error flag carry
+    // its sequence; now and then ask the stream for a fault, so an evaluation that
+    // can no longer publish surfaces as an error instead of a hang.
+    const unsigned long long tag = static_cast<unsigned long long>(static_cast<unsigned int>(sequence_)) << 32;
+    const volatile unsigned long long* slots = host_slots_;
+    const auto current = [&](int index) { return (slots[index] & 0xffffffff00000000ULL) == tag; };
+    const auto complete = [&]() {
+        if (!current(2 * kScalarCount)) return false;
+        for (uint32_t m = expected_mask_; m != 0; m &= m - 1) {
+            const int k = __builtin_ctz(m);
+            if (!current(2 * k) || !current(2 * k + 1)) return false;
+        }
+        return true;
+    };
+    for (uint64_t polls = 1; !complete(); ++polls) {
+        if ((polls & 255U) == 0) {
+            const cudaError_t status = cudaStreamQuery(stream_);
+            if (status == cudaSuccess) {
+                std::atomic_thread_fence(std::memory_order_seq_cst);
+                if (!complete()) fail(MPGP_ERR_CUDA, "An evaluation ended without publishing its scalars.");
+                break;
+            }
+            if (status != cudaErrorNotReady) checkCuda(status, "Evaluation on the device");
+        }
+        if (polls > 4096) std::this_thread::yield();
+    }
+    std::atomic_thread_fence(std::memory_order_acquire);
+    for (uint32_t m = expected_mask_; m != 0; m &= m - 1) {
+        const int k = __builtin_ctz(m);
+        const unsigned long long bits = (slots[2 * k] & 0xffffffffULL) | ((slots[2 * k + 1] & 0xffffffffULL) << 32);
+        std::memcpy(&host_scalars_->v[k], &bits, sizeof(double));
+    }
     collectTimings();
-    if (host_error_ != nullptr && *host_error_ != 0) {
+    if ((slots[2 * kScalarCount] & 0xffffffffULL) != 0) {
         fail(MPGP_ERR_TIMEOUT, "A tcgen05 field contraction timed out waiting on its pipeline.");
     }
     return *host_scalars_;

@@ -192,7 +192,7 @@ private:
     int wl_pin_count_ = 0;
 
     void collectTimings();
-    void runDct(bool gradient, bool potential, bool forward);
+    void runDct(bool gradient, bool potential, bool forward, bool split_source = true);
     void uploadStatic(const Problem& problem);
     void buildNetLayout(const Problem& problem);
     void buildBasis();
@@ -254,6 +254,12 @@ private:
     TcScales* tc_scales_ = nullptr;
     int* tc_error_ = nullptr;
     int* host_error_ = nullptr;
+    // Evaluation results published by the reduction into mapped pinned memory
+    // (ReduceArgs::host_slots), the scalars the current evaluation writes, and
+    // the cache of the latest value of every scalar.
+    unsigned long long* host_slots_ = nullptr;
+    uint32_t expected_mask_ = 0;
+    unsigned long long sequence_ = 0;
     void buildTensorCoreBasis(const std::vector<double>& cx, const std::vector<double>& cy,
                               const std::vector<double>& dy, const std::vector<double>& dxc,
                               const std::vector<double>& sxwt, const std::vector<double>& syw, double max_scale);
@@ -261,6 +267,12 @@ private:
 
     // partials and scalars
     int scatter_blocks_ = 0, metrics_blocks_ = 0, gather_blocks_ = 0, energy_blocks_ = 0;
+    bool metrics_fused_ = false;  // metrics pass writes the first contraction's operand planes
+    // Second-level (per 32 blocks) partials and their counters (reduceGroups).
+    double *wl_group_ = nullptr, *sc_group_ = nullptr, *g_group_ = nullptr, *m_group_ = nullptr;
+    unsigned int *wl_counters_ = nullptr, *sc_counters_ = nullptr, *g_counters_ = nullptr, *m_counters_ = nullptr;
+    int wl_groups_ = 0, sc_groups_ = 0, g_groups_ = 0, m_groups_ = 0;
+    void allocateGroups();
     double* partials_wl_ = nullptr;
     double* partials_sc_ = nullptr;
     double* partials_m_ = nullptr;

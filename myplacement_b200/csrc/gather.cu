@@ -18,6 +18,8 @@
 // reduce: folds every kernel's per-block partials into the evaluation's
 // scalar block in a fixed order (deterministic) and clears the integer layer
 // totals for the next scatter.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -62,12 +64,78 @@ __device__ __forceinline__ double2 sampleField(const GatherArgs& a, double x, do
     return make_double2(lower_x * (1.0 - ty) + upper_x * ty, lower_y * (1.0 - ty) + upper_y * ty);
 }
 
+// One scalar into the host record: low and high 32 bits, each beside the sequence.
+__device__ __forceinline__ void publishScalar(unsigned long long* slots, int target, double value,
+                                              unsigned int sequence) {
+    const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(value));
+    const unsigned long long tag = static_cast<unsigned long long>(sequence) << 32;
+    volatile unsigned long long* slot = reinterpret_cast<volatile unsigned long long*>(slots) + 2 * target;
+    slot[0] = tag | (bits & 0xffffffffULL);
+    slot[1] = tag | (bits >> 32);
+}
+
+// Every source of `a` reduced by the calling block: warp w takes sources w,
+// w + warps, ... (four at a time, their first rows loaded together); lane l
+// sums rows l, l + 32, ... in order, then a fixed shuffle tree, so the scalars
+// do not depend on timing.  With a completion record, the scalars and the
+// error flag are also published to host memory.
+__device__ void reduceAllSources(const ReduceArgs& a) {
+    constexpr int kSourcesPerWarp = 4;  // sources a warp handles per pass, loads issued together
+    constexpr int kRowsPerLane = 4;     // rows lane + 32 j prefetched per source
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int warps = blockDim.x >> 5;
+    for (int first = warp; first < a.source_count; first += warps * kSourcesPerWarp) {
+        double x[kSourcesPerWarp][kRowsPerLane];
+#pragma unroll
+        for (int i = 0; i < kSourcesPerWarp; ++i) {
+            const int s = first + i * warps;
+            const ReduceSource src = s < a.source_count ? a.sources[s] : ReduceSource{nullptr, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int j = 0; j < kRowsPerLane; ++j) {
+                const int row = lane + 32 * j;
+                x[i][j] = row < src.rows ? __ldcg(src.partials + static_cast<size_t>(row) * src.stride + src.column)
+                                         : (src.is_max ? -1.0e308 : 0.0);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kSourcesPerWarp; ++i) {
+            const int s = first + i * warps;
+            if (s >= a.source_count) break;
+            const ReduceSource src = a.sources[s];
+            double value = src.is_max ? -1.0e308 : 0.0;
+#pragma unroll
+            for (int j = 0; j < kRowsPerLane; ++j) value = src.is_max ? fmax(value, x[i][j]) : value + x[i][j];
+            for (int row = lane + 32 * kRowsPerLane; row < src.rows; row += 32) {
+                const double y = __ldcg(src.partials + static_cast<size_t>(row) * src.stride + src.column);
+                value = src.is_max ? fmax(value, y) : value + y;
+            }
+            value = src.is_max ? warpMax(value) : warpSum(value);
+            if (lane == 0) {
+                const double result = src.rows > 0 ? value : 0.0;
+                a.scalars[src.target] = result;
+                if (a.host_slots != nullptr) publishScalar(a.host_slots, src.target, result, a.sequence);
+            }
+        }
+    }
+    if (threadIdx.x == 0 && a.totals != nullptr) {
+        a.totals[0] = 0ULL;
+        a.totals[1] = 0ULL;
+        a.totals[2] = 0ULL;
+    }
+    if (a.host_slots != nullptr && threadIdx.x == 0) {
+        const unsigned int error = static_cast<unsigned int>(*reinterpret_cast<const volatile int*>(a.device_error));
+        const unsigned long long tag = static_cast<unsigned long long>(a.sequence) << 32;
+        reinterpret_cast<volatile unsigned long long*>(a.host_slots)[2 * kScalarCount] = tag | error;
+    }
+}
+
 __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
     releaseNext();
     waitForPrior();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (i < a.particle_count) {
+    // Grid-stride over the particles (one resident wave), each thread in ascending order.
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.particle_count; i += gridDim.x * blockDim.x) {
         double wx = 0.0, wy = 0.0, rx_rudy = 0.0, ry_rudy = 0.0;
         if (i < a.movable_count) {
             const int begin = a.particle_pin_start[i];
@@ -83,7 +151,7 @@ __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
                     rx_rudy += g.x;
                     ry_rudy += g.y;
                 }
-                v[7] = fabs(rx_rudy) + fabs(ry_rudy);
+                v[7] += fabs(rx_rudy) + fabs(ry_rudy);
             }
         }
         const double2 p = a.positions[i];
@@ -91,8 +159,8 @@ __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
         const double q = a.charge[i];
         const double dx = -q * e.x;
         const double dy = -q * e.y;
-        v[0] = fabs(wx) + fabs(wy);
-        v[1] = fabs(dx) + fabs(dy);
+        v[0] += fabs(wx) + fabs(wy);
+        v[1] += fabs(dx) + fabs(dy);
         if (a.precond_base == nullptr) {
             a.wire_out[i] = make_double2(wx, wy);
             a.density_out[i] = make_double2(dx, dy);
@@ -105,19 +173,19 @@ __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
             const double py = ry * s;
             a.raw[i] = make_double2(rx, ry);
             a.pre[i] = make_double2(px, py);
-            v[2] = rx * rx + ry * ry;
-            v[3] = px * px + py * py;
+            v[2] += rx * rx + ry * ry;
+            v[3] += px * px + py * py;
             if (a.prev_positions != nullptr) {
                 const double2 pp = a.prev_positions[i];
                 const double2 pg = a.prev_gradient[i];
                 const double ax = p.x - pp.x, ay = p.y - pp.y;
                 const double gx = px - pg.x, gy = py - pg.y;
-                v[4] = ax * ax + ay * ay;
-                v[5] = gx * gx + gy * gy;
+                v[4] += ax * ax + ay * ay;
+                v[5] += gx * gx + gy * gy;
             }
             if (a.velocity != nullptr) {
                 const double2 vel = a.velocity[i];
-                v[6] = vel.x * px + vel.y * py;
+                v[6] += vel.x * px + vel.y * py;
             }
         }
     }
@@ -127,35 +195,29 @@ __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
 #pragma unroll
         for (int k = 0; k < 8; ++k) a.partials[8 * blockIdx.x + k] = v[k];
     }
+    if (a.group_counters != nullptr) {
+        // The block that finishes the last group reduces every partial of the
+        // evaluation (the other passes completed before this grid started).
+        const bool sums[8] = {false, false, false, false, false, false, false, false};
+        if (reduceGroups<8>(a.partials, a.group_partials, a.group_counters, sums) == 2) reduceAllSources(a.reduce);
+    }
 }
 
 __global__ void __launch_bounds__(kThreads) reduceKernel(ReduceArgs a) {
     releaseNext();
     waitForPrior();
-    const int s = blockIdx.x;
-    if (s >= a.source_count) {
-        return;
-    }
-    const ReduceSource src = a.sources[s];
-    double value = src.is_max ? -1.0e308 : 0.0;
-    for (int row = threadIdx.x; row < src.rows; row += blockDim.x) {
-        const double x = src.partials[static_cast<size_t>(row) * src.stride + src.column];
-        value = src.is_max ? fmax(value, x) : value + x;
-    }
-    double values[1] = {value};
-    const bool is_max[1] = {src.is_max != 0};
-    blockReduce<1>(values, is_max);
-    if (threadIdx.x == 0) {
-        a.scalars[src.target] = src.rows > 0 ? values[0] : 0.0;
-        if (s == 0 && a.totals != nullptr) {
-            a.totals[0] = 0ULL;
-            a.totals[1] = 0ULL;
-            a.totals[2] = 0ULL;
-        }
-    }
+    reduceAllSources(a);
 }
 
 }  // namespace
+
+int gatherBlocks(int particle_count) {
+    int per_sm = 0, sms = 0, device = 0;
+    checkCuda(cudaGetDevice(&device), "Query the current device");
+    checkCuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "Query the SM count");
+    checkCuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gatherKernel, kThreads, 0), "Gather occupancy");
+    return std::max(1, std::min(ceilDiv(std::max(1, particle_count), kThreads), std::max(1, per_sm) * sms));
+}
 
 void launchGather(const GatherArgs& args, int blocks, cudaStream_t stream) {
     if (blocks <= 0) return;
@@ -164,8 +226,7 @@ void launchGather(const GatherArgs& args, int blocks, cudaStream_t stream) {
 
 void launchReduce(const ReduceArgs& args, cudaStream_t stream) {
     if (args.source_count <= 0) return;
-    launchChained("Launch the scalar reduction", reduceKernel, dim3(args.source_count), dim3(kThreads), 0, stream,
-                  args);
+    launchChained("Launch the scalar reduction", reduceKernel, dim3(1), dim3(kThreads), 0, stream, args);
 }
 
 }  // namespace mpgp

@@ -1,11 +1,14 @@
 // Kernel argument blocks and launchers of the placement engine.
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
 namespace mpgp {
+
+struct TcScales;
 
 // ---- scalar slots of one evaluation (FP64, reduced on the device) ------------------------
 enum Scalar : int {
@@ -54,6 +57,8 @@ struct WirelengthArgs {
     float2* pin_gradient;         // particle-ordered slots (written when gradient != 0, movable pins only)
     int gradient;
     double* partials;             // per block: smooth, hpwl
+    double* group_partials;       // per 32 blocks: smooth, hpwl (reduceGroups)
+    unsigned int* group_counters;
 };
 void launchWirelength(const WirelengthArgs& args, int blocks, cudaStream_t stream);
 
@@ -99,6 +104,8 @@ struct ScatterArgs {
     unsigned long long* layers; // 3 * B fixed-point accumulators (movable, macro, filler)
     unsigned long long* totals; // 3 exact layer totals
     double* partials;           // per block: predicted, max displacement
+    double* group_partials;     // proposal mode: per 32 blocks (reduceGroups)
+    unsigned int* group_counters;
 };
 void launchScatter(const ScatterArgs& args, int blocks, cudaStream_t stream);
 
@@ -114,8 +121,23 @@ struct MetricsArgs {
     int bin_count;
     float* source;                     // B: deviation - mean (FP32 DCT input)
     double* partials;                  // per block: 9 metric partials
+    // Fused form: the source is not stored; each row's fp16 planes go straight
+    // into the first contraction's operand, with the row exponent from its maximum.
+    int columns, rows;
+    __half* split_out;
+    int split_ld;
+    size_t split_plane;
+    int* row_exp;
+    TcScales* scales;
+    double* group_partials;            // fused form: per 32 rows (reduceGroups)
+    unsigned int* group_counters;
 };
 void launchMetrics(const MetricsArgs& args, int blocks, cudaStream_t stream);
+// The fused metrics-and-split pass takes one block per bin row and keeps a
+// row's sources in registers: up to kMetricsSplitPerThread bins per thread.
+constexpr int kMetricsSplitPerThread = 8;
+inline bool metricsSplitFits(int columns) { return columns > 0 && columns <= kMetricsSplitPerThread * 256; }
+void launchMetricsSplit(const MetricsArgs& args, cudaStream_t stream);
 
 // ---- RUDY routing-demand map (rudy.cu) -------------------------------------------------
 struct RudyArgs {
@@ -148,6 +170,33 @@ void launchRudyDeposit(const RudyArgs& args, cudaStream_t stream);
 void launchRudyMetrics(const RudyArgs& args, int blocks, cudaStream_t stream);
 void launchRudyGradient(const RudyArgs& args, cudaStream_t stream);
 
+// ---- deterministic reduction of all partials into the scalar block ----------------------
+struct ReduceSource {
+    const double* partials;
+    int rows;    // number of blocks that wrote partials
+    int stride;  // doubles per block
+    int column;  // which partial
+    int is_max;
+    int target;  // Scalar slot
+};
+struct ReduceArgs {
+    ReduceSource sources[kScalarCount];
+    int source_count;
+    double* scalars;             // kScalarCount
+    unsigned long long* totals;  // reset to zero after use (may be null)
+    // Optional completion record in mapped pinned host memory, written without
+    // fences: every scalar travels as two 8-byte words (32 bits of the value and
+    // the 32-bit evaluation sequence each), slot kScalarCount carries the sticky
+    // device error flag the same way.  An aligned 8-byte store arrives whole, so
+    // the host takes a value once both of its words show the current sequence.
+    unsigned long long* host_slots;  // 2 * (kScalarCount + 1) words
+    const int* device_error;
+    unsigned int sequence;
+};
+static_assert(kScalarCount < 32, "the expected-scalar mask is 32 bits wide");
+// One block reduces every source (one warp per source, rows in a fixed order).
+void launchReduce(const ReduceArgs& args, cudaStream_t stream);
+
 // ---- field gather + gradient combine (the fused update pass) ----------------------------
 struct GatherArgs {
     int particle_count;
@@ -173,28 +222,19 @@ struct GatherArgs {
     const double2* rudy_gradient;   // optional: RUDY pin slots (particle order), added with rudy_weight
     double rudy_weight;
     double* partials;               // per block: 8 partials (kWireL1 .. kRudyL1)
+    // Optional fused reduction: the last block to finish reduces `reduce`
+    // (counted on reduce_counter, which is zero between launches).
+    double* group_partials;         // per 32 blocks: the 8 partials (reduceGroups)
+    unsigned int* group_counters;
+    ReduceArgs reduce;              // reduced by the block that finishes the last group
 };
 void launchGather(const GatherArgs& args, int blocks, cudaStream_t stream);
+// The gather's grid: one resident wave of blocks (grid-stride over the particles).
+int gatherBlocks(int particle_count);
 
 // ---- small vector kernels ---------------------------------------------------------
 void launchVelocity(const double2* next, const double2* previous, double2* velocity, int count,
                     cudaStream_t stream);
 
-// ---- deterministic reduction of all partials into the scalar block ----------------------
-struct ReduceSource {
-    const double* partials;
-    int rows;    // number of blocks that wrote partials
-    int stride;  // doubles per block
-    int column;  // which partial
-    int is_max;
-    int target;  // Scalar slot
-};
-struct ReduceArgs {
-    ReduceSource sources[kScalarCount];
-    int source_count;
-    double* scalars;             // kScalarCount
-    unsigned long long* totals;  // reset to zero after use (may be null)
-};
-void launchReduce(const ReduceArgs& args, cudaStream_t stream);
 
 }  // namespace mpgp

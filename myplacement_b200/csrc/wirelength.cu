@@ -260,6 +260,7 @@ __global__ void __launch_bounds__(kThreads) wirelengthKernel(WirelengthArgs a) {
         a.partials[2 * blockIdx.x + 0] = values[0];
         a.partials[2 * blockIdx.x + 1] = values[1];
     }
+    reduceGroups<2>(a.partials, a.group_partials, a.group_counters, is_max);
 }
 
 }  // namespace
