@@ -35,6 +35,11 @@ inline void require(bool condition, const std::string& message) {
     if (!condition) fail(MPGP_ERR_INVALID_ARGUMENT, message);
 }
 
+// The literal form builds no string unless the check fails (validation loops run per pin).
+inline void require(bool condition, const char* message) {
+    if (!condition) fail(MPGP_ERR_INVALID_ARGUMENT, message);
+}
+
 constexpr double kEpsilon = 1e-9;  // Geometry.hpp:8
 constexpr double kPi = 3.141592653589793238462643383279502884;
 constexpr int kThreads = 256;
@@ -104,9 +109,9 @@ __device__ __forceinline__ unsigned int atomicAddAcqRel(unsigned int* address, u
 }
 
 // Second level of a deterministic grid reduction, called by every block after
-// thread 0 wrote the block's K partials at partials[K * blockIdx.x + k]: the
-// last block of each group of 32 consecutive blocks reduces the group's rows (in
-// block order) into group_partials[K * group + k].  counters holds 1 + groups
+// thread 0 wrote the block's K partials at partials[k * gridDim.x + blockIdx.x]
+// (column-major): the last block of each group of 32 consecutive blocks reduces
+// the group's rows (in block order) into group_partials[k * groups + group].  counters holds 1 + groups
 // zeros and is left zeroed.  Returns 0 in most blocks, 1 in a block that
 // finished a group, 2 in the block that finished the last group (after which
 // every group row is visible to it).  Thread 0 does every global write and
@@ -128,14 +133,14 @@ __device__ int reduceGroups(const double* partials, double* group_partials, unsi
     const int warps = static_cast<int>(blockDim.x >> 5);
     for (int k = warp; k < K; k += warps) {
         double x = is_max[k] ? -1.0e308 : 0.0;
-        if (lane < size) x = __ldcg(partials + static_cast<size_t>(first + lane) * K + k);
+        if (lane < size) x = __ldcg(partials + static_cast<size_t>(k) * gridDim.x + first + lane);
         x = is_max[k] ? warpMax(x) : warpSum(x);
         if (lane == 0) folded[k] = x;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < K; ++k) group_partials[static_cast<size_t>(group) * K + k] = folded[k];
+        for (int k = 0; k < K; ++k) group_partials[static_cast<size_t>(k) * groups + group] = folded[k];
         counters[1 + group] = 0U;
         state = atomicAddAcqRel(counters, 1U) == groups - 1U ? 2 : 1;
         if (state == 2) counters[0] = 0U;

@@ -739,6 +739,103 @@ int splitHost(const std::vector<double>& values, int rows, int cols, int ld, std
     return e;
 }
 
+// Basis value t at (row i, column j); n is the transform length of matrix t.
+__device__ double basisValue(int t, int i, int j, int nx, int ny, double width, double height) {
+    const bool along_x = t == 0 || t == 3 || t == 4;
+    const int n = along_x ? nx : ny;
+    const int freq = t <= 1 ? i : j;
+    const int pos = t <= 1 ? j : i;
+    const double turn = static_cast<double>((static_cast<long long>(freq) * (2 * pos + 1)) % (4LL * n)) /
+                        (2.0 * static_cast<double>(n));  // the angle over pi
+    if (t <= 1) return 2.0 * cospi(turn);
+    if (t <= 3) return freq == 0 ? 1.0 : 2.0 * cospi(turn);
+    if (freq == 0) return 0.0;
+    const double wave = 3.141592653589793 * static_cast<double>(freq) / (along_x ? width : height);
+    return wave * 2.0 * sinpi(turn);
+}
+
+struct BasisShape {
+    int nx, ny;
+    double width, height;
+};
+
+// Pass 1: per matrix, the largest |value| and the largest row sum of |values|
+// (non-negative doubles compare like their bit patterns, so atomicMax is exact).
+__global__ void __launch_bounds__(kThreads) basisRangeKernel(BasisShape b, unsigned long long* scratch) {
+    const int t = blockIdx.y;
+    const int n = (t == 0 || t == 3 || t == 4) ? b.nx : b.ny;
+    const int i = blockIdx.x;
+    if (i >= n) return;
+    double values[2] = {0.0, 0.0};  // row sum, row max
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const double v = fabs(basisValue(t, i, j, b.nx, b.ny, b.width, b.height));
+        values[0] += v;
+        values[1] = fmax(values[1], v);
+    }
+    const bool is_max[2] = {false, true};
+    blockReduce<2>(values, is_max);
+    if (threadIdx.x == 0) {
+        atomicMax(scratch + t, static_cast<unsigned long long>(__double_as_longlong(values[1])));
+        atomicMax(scratch + kBasisCount + t, static_cast<unsigned long long>(__double_as_longlong(values[0])));
+    }
+}
+
+struct BasisPlanes {
+    __half* data[kBasisCount];
+    int ld[kBasisCount];
+    size_t plane[kBasisCount];
+    int exponent[kBasisCount];
+};
+
+// Pass 2: the planes, as splitHost forms them.
+__global__ void __launch_bounds__(kThreads) basisPlanesKernel(BasisShape b, BasisPlanes p) {
+    const int t = blockIdx.y;
+    const int n = (t == 0 || t == 3 || t == 4) ? b.nx : b.ny;
+    const int i = blockIdx.x;
+    if (i >= n) return;
+    const double inv_scale = pow2(-p.exponent[t]);
+    __half* hi = p.data[t] + static_cast<size_t>(i) * p.ld[t];
+    __half* lo = hi + p.plane[t];
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const double y = basisValue(t, i, j, b.nx, b.ny, b.width, b.height) * inv_scale;
+        const __half h = __double2half(y);
+        hi[j] = h;
+        lo[j] = __double2half((y - static_cast<double>(__half2float(h))) * 2048.0);
+    }
+}
+
+void buildBasisPlanes(int nx, int ny, double width, double height, const SplitMatrix (&out)[kBasisCount],
+                      unsigned long long* scratch, int (&exponents)[kBasisCount],
+                      double (&max_row_l1)[kBasisCount], cudaStream_t stream) {
+    const BasisShape shape{nx, ny, width, height};
+    const dim3 grid(static_cast<unsigned>(std::max(nx, ny)), kBasisCount);
+    checkCuda(cudaMemsetAsync(scratch, 0, 2 * kBasisCount * sizeof(unsigned long long), stream), "basis ranges");
+    basisRangeKernel<<<grid, kThreads, 0, stream>>>(shape, scratch);
+    checkCuda(cudaGetLastError(), "Launch the basis range pass");
+    unsigned long long ranges[2 * kBasisCount] = {};
+    checkCuda(cudaMemcpyAsync(ranges, scratch, sizeof(ranges), cudaMemcpyDeviceToHost, stream), "basis ranges");
+    checkCuda(cudaStreamSynchronize(stream), "basis ranges");
+    BasisPlanes planes{};
+    for (int t = 0; t < kBasisCount; ++t) {
+        double top = 0.0, row = 0.0;
+        std::memcpy(&top, &ranges[t], sizeof(double));
+        std::memcpy(&row, &ranges[kBasisCount + t], sizeof(double));
+        int e = 0;
+        if (top > 0.0) {
+            const double m = std::frexp(top, &e);
+            if (m == 0.5) e -= 1;
+        }
+        exponents[t] = e - kPlaneTop;
+        max_row_l1[t] = row;
+        planes.data[t] = out[t].data;
+        planes.ld[t] = out[t].ld;
+        planes.plane[t] = out[t].plane();
+        planes.exponent[t] = exponents[t];
+    }
+    basisPlanesKernel<<<grid, kThreads, 0, stream>>>(shape, planes);
+    checkCuda(cudaGetLastError(), "Launch the basis plane pass");
+}
+
 void launchSplitSource(const float* source, const SplitMatrix& out, int cols, int* row_exp, TcScales* scales,
                        cudaStream_t stream) {
     if (out.rows <= 0) return;

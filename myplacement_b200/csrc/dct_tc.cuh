@@ -103,6 +103,21 @@ int tcBlocks(const TcBatch& batch, int task_count);
 void launchTcGemm(const TcBatch& batch, int task_count, cudaStream_t stream);
 // Host split of FP64 values into the planes of x * 2^-exponent; returns the exponent.
 int splitHost(const std::vector<double>& values, int rows, int cols, int ld, std::vector<__half>& planes);
+
+// The six basis operands of the field solve, built on the device (FP64 values,
+// split into planes with one exponent per matrix):
+//   0 cx[k][c]   = 2 cos(pi k (2c+1) / 2nx)                 DCT-II along x
+//   1 cy[l][r]   = 2 cos(pi l (2r+1) / 2ny)                 DCT-II along y
+//   2 dy[r][l]   = 2 cos(pi l (2r+1) / 2ny), 1 for l = 0    DCT-III along y
+//   3 dxc[c][k]  = 2 cos(pi k (2c+1) / 2nx), 1 for k = 0    DCT-III along x
+//   4 sxwt[c][k] = (pi k / width) 2 sin(pi k (2c+1) / 2nx)  DST-III along x times the wave number
+//   5 syw[r][l]  = (pi l / height) 2 sin(pi l (2r+1) / 2ny) DST-III along y times the wave number
+// The planes go to out[t]; exponents[t] and max_row_l1[t] (the largest row sum
+// of |values|, which bounds |A x| / max |x|) come back to the host.
+constexpr int kBasisCount = 6;
+void buildBasisPlanes(int nx, int ny, double width, double height, const SplitMatrix (&out)[kBasisCount],
+                      unsigned long long* scratch, int (&exponents)[kBasisCount],
+                      double (&max_row_l1)[kBasisCount], cudaStream_t stream);
 // Splits the FP32 source S with one exponent per row (row_exp), folds max |S| into
 // scales->max_source and clears the magnitudes the forward contractions fold into.
 void launchSplitSource(const float* source, const SplitMatrix& out, int cols, int* row_exp, TcScales* scales,

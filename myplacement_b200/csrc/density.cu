@@ -136,13 +136,11 @@ __global__ void __launch_bounds__(kThreads) scatterKernel(ScatterArgs a) {
             if (block_totals[k] != 0) atomicAdd(a.totals + k, static_cast<unsigned long long>(block_totals[k]));
         }
         if (a.partials != nullptr) {
-            a.partials[2 * blockIdx.x + 0] = values[0];
-            a.partials[2 * blockIdx.x + 1] = values[1];
+            a.partials[blockIdx.x] = values[0];
+            a.partials[gridDim.x + blockIdx.x] = values[1];
         }
     }
-    if (a.mode == kPropose && a.partials != nullptr) {
-        reduceGroups<2>(a.partials, a.group_partials, a.group_counters, is_max);
-    }
+
 }
 
 // One bin's metric terms (DensityBin::chargeArea / normalizationArea, Metrics.hpp:25-35).
@@ -221,15 +219,14 @@ __global__ void __launch_bounds__(kThreads) metricsKernel(MetricsArgs a) {
     blockReduce<9>(v, is_max);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k) a.partials[9 * blockIdx.x + k] = v[k];
+        for (int k = 0; k < 9; ++k) a.partials[k * gridDim.x + blockIdx.x] = v[k];
     }
 }
 
 // The metrics pass fused with the source split of the field solve: one block
 // per bin row forms the row's sources in registers (they are never stored),
 // takes the row maximum for the row's plane exponent (splitSourceKernel's rule)
-// and writes the fp16 hi / lo planes of the first contraction's operand.  The
-// per-row partials are folded per 32 rows (reduceGroups).
+// and writes the fp16 hi / lo planes of the first contraction's operand.
 __global__ void __launch_bounds__(kThreads) metricsSplitKernel(MetricsArgs a) {
     releaseNext();
     waitForPrior();
@@ -336,9 +333,8 @@ __global__ void __launch_bounds__(kThreads) metricsSplitKernel(MetricsArgs a) {
     blockReduce<9>(v, is_max);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k) a.partials[9 * blockIdx.x + k] = v[k];
+        for (int k = 0; k < 9; ++k) a.partials[k * gridDim.x + blockIdx.x] = v[k];
     }
-    reduceGroups<9>(a.partials, a.group_partials, a.group_counters, is_max);
 }
 
 __global__ void velocityKernel(const double2* next, const double2* previous, double2* velocity, int count) {

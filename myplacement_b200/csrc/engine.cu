@@ -56,16 +56,6 @@ void upload(T* device, const std::vector<T>& host, cudaStream_t stream) {
     }
 }
 
-// cos(pi * m / (2n)) for an integer m, reduced exactly modulo 4n.
-double cosQuarter(long long m, int n) {
-    m %= 4LL * n;
-    return std::cos(kPi * static_cast<double>(m) / (2.0 * n));
-}
-double sinQuarter(long long m, int n) {
-    m %= 4LL * n;
-    return std::sin(kPi * static_cast<double>(m) / (2.0 * n));
-}
-
 }  // namespace
 
 Engine::Engine(const Problem& p, int device, uint64_t budget_bytes) : device_(device), arena_(budget_bytes) {
@@ -185,51 +175,72 @@ void Engine::uploadStatic(const Problem& p) {
 void Engine::buildNetLayout(const Problem& p) {
     const int net_count = static_cast<int>(p.net_weight.size());
     // Degree buckets: one thread per two-pin net, G lanes per net for degree <= G,
-    // a warp loop above 32.
+    // a warp loop above 32.  Nets are ordered bucket by bucket (a stable counting
+    // sort), and every output array is sized before it is filled.
     const int kGroups[6] = {1, 4, 8, 16, 32, 0};
-    std::vector<std::vector<int>> bucket(6);
+    std::vector<int8_t> bucket_of(static_cast<std::size_t>(net_count), -1);
+    int bucket_nets[7] = {0, 0, 0, 0, 0, 0, 0};
+    std::size_t kept_pins = 0, kept_static = 0;
     for (int n = 0; n < net_count; ++n) {
         const int64_t degree = p.net_pin_start[n + 1] - p.net_pin_start[n];
         if (degree < 2) continue;  // nets with fewer than two pins contribute nothing
         const int b = degree <= 2 ? 0 : degree <= 4 ? 1 : degree <= 8 ? 2 : degree <= 16 ? 3 : degree <= 32 ? 4 : 5;
-        bucket[b].push_back(n);
+        bucket_of[static_cast<std::size_t>(n)] = static_cast<int8_t>(b);
+        ++bucket_nets[b + 1];
+        kept_pins += static_cast<std::size_t>(degree);
+        for (int64_t pin = p.net_pin_start[n]; pin < p.net_pin_start[n + 1]; ++pin) {
+            if (p.pin_particle[pin] < 0) ++kept_static;
+        }
     }
-    std::vector<int> pin_particle;
-    std::vector<float2> pin_offset;
-    std::vector<double2> static_pins;
-    std::vector<int> net_start{0};
-    std::vector<float> net_weight;
-    std::vector<int4> work;
+    for (int b = 0; b < 6; ++b) bucket_nets[b + 1] += bucket_nets[b];
+    const int kept_nets = bucket_nets[6];
+    std::vector<int> order(static_cast<std::size_t>(kept_nets));
+    {
+        int next[6];
+        for (int b = 0; b < 6; ++b) next[b] = bucket_nets[b];
+        for (int n = 0; n < net_count; ++n) {
+            const int b = bucket_of[static_cast<std::size_t>(n)];
+            if (b >= 0) order[static_cast<std::size_t>(next[b]++)] = n;
+        }
+    }
+    std::vector<int> pin_particle(kept_pins);
+    std::vector<float2> pin_offset(kept_pins);
+    std::vector<double2> static_pins(kept_static);
+    std::vector<int> net_start(static_cast<std::size_t>(kept_nets) + 1);
+    std::vector<float> net_weight(static_cast<std::size_t>(kept_nets));
+    bucket_net_weight_.assign(static_cast<std::size_t>(kept_nets), 0.0);
+    std::size_t write = 0, write_static = 0;
+    net_start[0] = 0;
+    for (int k = 0; k < kept_nets; ++k) {
+        const int n = order[static_cast<std::size_t>(k)];
+        for (int64_t pin = p.net_pin_start[n]; pin < p.net_pin_start[n + 1]; ++pin, ++write) {
+            const int particle = p.pin_particle[pin];
+            if (particle >= 0) {
+                pin_particle[write] = particle;
+                pin_offset[write] = make_float2(static_cast<float>(p.pin_x[pin]), static_cast<float>(p.pin_y[pin]));
+            } else {
+                pin_particle[write] = -static_cast<int>(write_static) - 1;
+                pin_offset[write] = make_float2(0.0f, 0.0f);
+                static_pins[write_static++] = make_double2(p.pin_x[pin], p.pin_y[pin]);
+            }
+        }
+        net_start[static_cast<std::size_t>(k) + 1] = static_cast<int>(write);
+        net_weight[static_cast<std::size_t>(k)] = static_cast<float>(p.net_weight[n]);
+        bucket_net_weight_[static_cast<std::size_t>(k)] = p.net_weight[n];
+    }
     // Pins and nets are laid out bucket by bucket; the blocks run heaviest bucket
     // first (one round of the block's lanes each), so the long warp-loop nets do
     // not form the kernel's tail.
-    std::vector<int4> bucket_work[6];
-    for (int b = 0; b < 6; ++b) {
+    std::vector<int4> work;
+    for (int b = 5; b >= 0; --b) {
         const int group = kGroups[b];
         const int nets_per_block = group == 0 ? kThreads / 32 : group == 1 ? kThreads : kThreads / group;
-        const int first_net = static_cast<int>(net_weight.size());
-        for (const int n : bucket[b]) {
-            for (int64_t pin = p.net_pin_start[n]; pin < p.net_pin_start[n + 1]; ++pin) {
-                const int particle = p.pin_particle[pin];
-                if (particle >= 0) {
-                    pin_particle.push_back(particle);
-                    pin_offset.push_back(make_float2(static_cast<float>(p.pin_x[pin]), static_cast<float>(p.pin_y[pin])));
-                } else {
-                    pin_particle.push_back(-static_cast<int>(static_pins.size()) - 1);
-                    pin_offset.push_back(make_float2(0.0f, 0.0f));
-                    static_pins.push_back(make_double2(p.pin_x[pin], p.pin_y[pin]));
-                }
-            }
-            net_start.push_back(static_cast<int>(pin_particle.size()));
-            net_weight.push_back(static_cast<float>(p.net_weight[n]));
-            bucket_net_weight_.push_back(p.net_weight[n]);
-        }
-        const int count = static_cast<int>(bucket[b].size());
+        const int first_net = bucket_nets[b];
+        const int count = bucket_nets[b + 1] - bucket_nets[b];
         for (int off = 0; off < count; off += nets_per_block) {
-            bucket_work[b].push_back(make_int4(group, first_net + off, std::min(nets_per_block, count - off), 0));
+            work.push_back(make_int4(group, first_net + off, std::min(nets_per_block, count - off), 0));
         }
     }
-    for (int b = 5; b >= 0; --b) work.insert(work.end(), bucket_work[b].begin(), bucket_work[b].end());
     wl_blocks_ = static_cast<int>(work.size());
     wl_net_count_ = static_cast<int>(net_weight.size());
     wl_pin_count_ = static_cast<int>(pin_particle.size());
@@ -277,31 +288,6 @@ void Engine::buildNetLayout(const Problem& p) {
 void Engine::buildBasis() {
     const int nx = bins_x_, ny = bins_y_;
     const double width = region_.width(), height = region_.height();
-    // K-major operands of C = A * B^T (runDct), in FP64 before the bf16 split:
-    //   cx[k][c] = 2 cos(pi k (2c+1) / 2nx)          (DCT-II, REDFT10)
-    //   dxc[c][k] = 2 cos(...), k = 0 -> 1            (DCT-III, REDFT01)
-    //   sxwt[c][k] = kx 2 sin(pi k (2c+1) / 2nx)      (DST-III, RODFT01, times the wave number)
-    // and the same along y.
-    std::vector<double> cx(static_cast<std::size_t>(nx) * nx), dxc(cx.size()), sxwt(cx.size());
-    std::vector<double> cy(static_cast<std::size_t>(ny) * ny), dy(cy.size()), syw(cy.size());
-    for (int c = 0; c < nx; ++c) {
-        for (int k = 0; k < nx; ++k) {
-            const long long m = static_cast<long long>(k) * (2 * c + 1);
-            const double wave = kPi * static_cast<double>(k) / width;
-            cx[static_cast<std::size_t>(k) * nx + c] = 2.0 * cosQuarter(m, nx);
-            dxc[static_cast<std::size_t>(c) * nx + k] = k == 0 ? 1.0 : 2.0 * cosQuarter(m, nx);
-            sxwt[static_cast<std::size_t>(c) * nx + k] = k == 0 ? 0.0 : wave * 2.0 * sinQuarter(m, nx);
-        }
-    }
-    for (int r = 0; r < ny; ++r) {
-        for (int l = 0; l < ny; ++l) {
-            const long long m = static_cast<long long>(l) * (2 * r + 1);
-            const double wave = kPi * static_cast<double>(l) / height;
-            cy[static_cast<std::size_t>(l) * ny + r] = 2.0 * cosQuarter(m, ny);
-            dy[static_cast<std::size_t>(r) * ny + l] = l == 0 ? 1.0 : 2.0 * cosQuarter(m, ny);
-            syw[static_cast<std::size_t>(r) * ny + l] = l == 0 ? 0.0 : wave * 2.0 * sinQuarter(m, ny);
-        }
-    }
     // Spectral divide (ElectrostaticField.cpp:212-221): 1/(4 Nx Ny) / (kx^2 + ky^2), DC removed.
     std::vector<float> scale(static_cast<std::size_t>(ny) * nx);
     const double normalization = 1.0 / (4.0 * static_cast<double>(nx) * static_cast<double>(ny));
@@ -328,7 +314,7 @@ void Engine::buildBasis() {
     upload(weight_x_, wx, stream_);
     double max_scale = 0.0;
     for (float v : scale) max_scale = std::max(max_scale, static_cast<double>(v));
-    buildTensorCoreBasis(cx, cy, dy, dxc, sxwt, syw, max_scale);
+    buildTensorCoreBasis(max_scale);
     checkCuda(cudaStreamSynchronize(stream_), "basis upload");
 }
 
@@ -342,41 +328,23 @@ SplitMatrix Engine::newSplit(int rows, int cols, const char* what) {
     return m;
 }
 
-namespace {
 
-// Largest row sum of |values| (rows x cols, row-major): |A x| <= this * max |x|.
-double maxRowL1(const std::vector<double>& values, int rows, int cols) {
-    double top = 0.0;
-    for (int r = 0; r < rows; ++r) {
-        double sum = 0.0;
-        for (int c = 0; c < cols; ++c) sum += std::fabs(values[static_cast<std::size_t>(r) * cols + c]);
-        top = std::max(top, sum);
-    }
-    return top;
-}
-
-}  // namespace
-
-void Engine::buildTensorCoreBasis(const std::vector<double>& cx, const std::vector<double>& cy,
-                                  const std::vector<double>& dy, const std::vector<double>& dxc,
-                                  const std::vector<double>& sxwt, const std::vector<double>& syw,
-                                  double max_scale) {
+void Engine::buildTensorCoreBasis(double max_scale) {
     const int nx = bins_x_, ny = bins_y_;
     TcScales host_scales{};
-    const auto splitUpload = [&](const std::vector<double>& values, int rows, int cols, int slot, const char* what) {
-        SplitMatrix m = newSplit(rows, cols, what);
-        std::vector<__half> planes;
-        host_scales.exp_basis[slot] = splitHost(values, rows, cols, m.ld, planes);
-        upload(m.data, planes, stream_);
-        return m;
-    };
     enum { kCx = 0, kCy, kDy, kDxc, kSxwt, kSyw };
-    tc_cx_ = splitUpload(cx, nx, nx, kCx, "DCT basis planes");
-    tc_cy_ = splitUpload(cy, ny, ny, kCy, "DCT basis planes");
-    tc_dy_ = splitUpload(dy, ny, ny, kDy, "DCT basis planes");
-    tc_dxc_ = splitUpload(dxc, nx, nx, kDxc, "DCT basis planes");
-    tc_sxwt_ = splitUpload(sxwt, nx, nx, kSxwt, "DST basis planes");
-    tc_syw_ = splitUpload(syw, ny, ny, kSyw, "DST basis planes");
+    tc_cx_ = newSplit(nx, nx, "DCT basis planes");
+    tc_cy_ = newSplit(ny, ny, "DCT basis planes");
+    tc_dy_ = newSplit(ny, ny, "DCT basis planes");
+    tc_dxc_ = newSplit(nx, nx, "DCT basis planes");
+    tc_sxwt_ = newSplit(nx, nx, "DST basis planes");
+    tc_syw_ = newSplit(ny, ny, "DST basis planes");
+    const SplitMatrix basis_planes[kBasisCount] = {tc_cx_, tc_cy_, tc_dy_, tc_dxc_, tc_sxwt_, tc_syw_};
+    unsigned long long* ranges = arena_.array<unsigned long long>(2 * kBasisCount, "basis ranges");
+    int exponents[kBasisCount] = {};
+    double row_l1[kBasisCount] = {};
+    buildBasisPlanes(nx, ny, region_.width(), region_.height(), basis_planes, ranges, exponents, row_l1, stream_);
+    for (int t = 0; t < kBasisCount; ++t) host_scales.exp_basis[t] = exponents[t];
     tc_source_ = newSplit(ny, nx, "source planes");
     tc_x1t_ = newSplit(nx, ny, "DCT stage planes");
     tc_phi_ = newSplit(ny, nx, "potential coefficient planes");
@@ -410,7 +378,7 @@ void Engine::buildTensorCoreBasis(const std::vector<double>& cx, const std::vect
     tc_fwd1_.task[0].row_exp_a = tc_row_exp_;
     tc_fwd1_.task[0].exp_b = &sc->exp_basis[kCx];
     tc_fwd1_.task[0].ref_max = &sc->max_source;
-    tc_fwd1_.task[0].gain = static_cast<float>(maxRowL1(cx, nx, nx) * kMargin);
+    tc_fwd1_.task[0].gain = static_cast<float>(row_l1[kCx] * kMargin);
     tc_fwd1_.task[0].out_exp = &sc->exp_x;
     tc_fwd1_.task[0].out_max = &sc->max_x;
     tc_fwd1_.task[0].out_t = tc_x1t_.data;
@@ -421,7 +389,7 @@ void Engine::buildTensorCoreBasis(const std::vector<double>& cx, const std::vect
     tc_fwd2_.task[0].exp_a = &sc->exp_basis[kCy];
     tc_fwd2_.task[0].exp_b = &sc->exp_x;
     tc_fwd2_.task[0].ref_max = &sc->max_x;
-    tc_fwd2_.task[0].gain = static_cast<float>(maxRowL1(cy, ny, ny) * max_scale * kMargin);
+    tc_fwd2_.task[0].gain = static_cast<float>(row_l1[kCy] * max_scale * kMargin);
     tc_fwd2_.task[0].out_exp = &sc->exp_phi;
     tc_fwd2_.task[0].out_max = &sc->max_phi;
     tc_fwd2_.task[0].clear = &sc->max_source;
@@ -439,7 +407,7 @@ void Engine::buildTensorCoreBasis(const std::vector<double>& cx, const std::vect
     tc_inv1_.task[0].exp_a = &sc->exp_basis[kDy];
     tc_inv1_.task[0].exp_b = &sc->exp_phi;
     tc_inv1_.task[0].ref_max = &sc->max_phi;
-    tc_inv1_.task[0].gain = static_cast<float>(maxRowL1(dy, ny, ny) * kMargin);
+    tc_inv1_.task[0].gain = static_cast<float>(row_l1[kDy] * kMargin);
     tc_inv1_.task[0].out_exp = &sc->exp_t;
     tc_inv1_.task[0].out = tc_t_.data;
     tc_inv1_.task[0].out_ld = tc_t_.ld;
@@ -448,7 +416,7 @@ void Engine::buildTensorCoreBasis(const std::vector<double>& cx, const std::vect
     tc_inv1_.task[1].exp_a = &sc->exp_phi;
     tc_inv1_.task[1].exp_b = &sc->exp_basis[kDxc];
     tc_inv1_.task[1].ref_max = &sc->max_phi;
-    tc_inv1_.task[1].gain = static_cast<float>(maxRowL1(dxc, nx, nx) * kMargin);
+    tc_inv1_.task[1].gain = static_cast<float>(row_l1[kDxc] * kMargin);
     tc_inv1_.task[1].out_exp = &sc->exp_u;
     tc_inv1_.task[1].out_t = tc_ut_.data;
     tc_inv1_.task[1].out_t_ld = tc_ut_.ld;
@@ -538,24 +506,11 @@ void Engine::collectTimings() {
 //   gradient: T = Dy * phi_hat, U = phi_hat * Dx^T, Ex = T * (Sx diag(kx))^T, Ey = (Sy diag(ky)) * U
 //   potential (parity hook only): phi = T * Dx^T.
 void Engine::allocateGroups() {
-    const auto groups = [](int blocks) { return std::max(1, ceilDiv(std::max(1, blocks), 32)); };
-    const auto counters = [this](int count, const char* what) {
-        unsigned int* c = arena_.array<unsigned int>(static_cast<std::size_t>(count) + 1, what);
-        checkCuda(cudaMemsetAsync(c, 0, (static_cast<std::size_t>(count) + 1) * sizeof(unsigned int), stream_), what);
-        return c;
-    };
-    wl_groups_ = groups(wl_blocks_);
-    sc_groups_ = groups(scatter_blocks_);
-    g_groups_ = groups(gather_blocks_);
+    wl_groups_ = std::max(1, ceilDiv(std::max(1, wl_blocks_), 32));
     wl_group_ = arena_.array<double>(2 * static_cast<std::size_t>(wl_groups_), "wirelength group partials");
-    sc_group_ = arena_.array<double>(2 * static_cast<std::size_t>(sc_groups_), "scatter group partials");
-    g_group_ = arena_.array<double>(8 * static_cast<std::size_t>(g_groups_), "gather group partials");
-    m_groups_ = groups(metrics_blocks_);
-    m_group_ = arena_.array<double>(9 * static_cast<std::size_t>(m_groups_), "metric group partials");
-    m_counters_ = counters(m_groups_, "metric group counters");
-    wl_counters_ = counters(wl_groups_, "wirelength group counters");
-    sc_counters_ = counters(sc_groups_, "scatter group counters");
-    g_counters_ = counters(g_groups_, "gather group counters");
+    const std::size_t counters = static_cast<std::size_t>(wl_groups_) + 1;
+    wl_counters_ = arena_.array<unsigned int>(counters, "wirelength group counters");
+    checkCuda(cudaMemsetAsync(wl_counters_, 0, counters * sizeof(unsigned int), stream_), "wirelength group counters");
 }
 
 void Engine::runDct(bool gradient, bool potential, bool forward, bool split_source) {
@@ -620,8 +575,6 @@ void Engine::launch(const EvalRequest& q) {
     sa.layers = layers_;
     sa.totals = totals_;
     sa.partials = partials_sc_;
-    sa.group_partials = sc_group_;
-    sa.group_counters = sc_counters_;
     if (q.mode == kGiven) checkCuda(cudaEventRecord(fork_, stream_), "fork");
     if (!q.reuse_density) {
         beginKernel(kKindScatter);
@@ -686,8 +639,6 @@ void Engine::launch(const EvalRequest& q) {
             ma.split_plane = tc_source_.plane();
             ma.row_exp = tc_row_exp_;
             ma.scales = tc_scales_;
-            ma.group_partials = m_group_;
-            ma.group_counters = m_counters_;
             launchMetricsSplit(ma, stream_);
         } else {
             launchMetrics(ma, metrics_blocks_, stream_);
@@ -704,29 +655,28 @@ void Engine::launch(const EvalRequest& q) {
     const auto add = [&](const double* partials, int rows, int stride, int column, bool is_max, int target) {
         ra.sources[s++] = ReduceSource{partials, rows, stride, column, is_max ? 1 : 0, target};
     };
-    add(wl_group_, wl_blocks_ > 0 ? wl_groups_ : 0, 2, 0, false, kSmooth);
-    add(wl_group_, wl_blocks_ > 0 ? wl_groups_ : 0, 2, 1, false, kHpwl);
-    const int scatter_rows = particle_count_ > 0 && q.mode == kPropose ? sc_groups_ : 0;
+    add(wl_group_, wl_blocks_ > 0 ? wl_groups_ : 0, 1, 0, false, kSmooth);
+    add(wl_group_, wl_blocks_ > 0 ? wl_groups_ : 0, 1, wl_groups_, false, kHpwl);
+    const int scatter_rows = particle_count_ > 0 && q.mode == kPropose ? scatter_blocks_ : 0;
     if (!q.reuse_density) {  // otherwise the density scalars of the previous evaluation stand
-        add(sc_group_, scatter_rows, 2, 0, false, kPredicted);
-        add(sc_group_, scatter_rows, 2, 1, true, kMaxDisplacement);
+        add(partials_sc_, scatter_rows, 1, 0, false, kPredicted);
+        add(partials_sc_, scatter_rows, 1, scatter_rows, true, kMaxDisplacement);
         for (int k = 0; k < 9; ++k) {
-            if (metrics_fused_) {
-                add(m_group_, m_groups_, 9, k, k >= 7, kOverflowWith + k);
-            } else {
-                add(partials_m_, metrics_blocks_, 9, k, k >= 7, kOverflowWith + k);
-            }
+            add(partials_m_, metrics_blocks_, 1, k * metrics_blocks_, k >= 7, kOverflowWith + k);
         }
         add(partials_e_, energy_blocks_, 1, 0, false, kEnergy);
     }
     for (int k = 0; k < 5; ++k) {
-        add(rudy_main_.partials, q.rudy ? rudy_main_.blocks : 0, 5, k, k == 4, kRudyEnergy + k);
+        add(rudy_main_.partials, q.rudy ? rudy_main_.blocks : 0, 1, k * rudy_main_.blocks, k == 4, kRudyEnergy + k);
     }
     const bool gather = q.gradient && particle_count_ > 0;
     if (q.gradient) {
-        for (int k = 0; k < 8; ++k) add(g_group_, gather ? g_groups_ : 0, 8, k, false, kWireL1 + k);
+        for (int k = 0; k < 8; ++k) add(partials_g_, gather ? gather_blocks_ : 0, 1, k * gather_blocks_, false, kWireL1 + k);
     }
     ra.source_count = s;
+    ra.offsets[0] = 0;
+    for (int k = 0; k < s; ++k) ra.offsets[k + 1] = ra.offsets[k] + ra.sources[k].rows;
+    ra.staged_capacity = kReduceStaged;
     ra.scalars = scalars_;
     ra.totals = totals_;
     ra.host_slots = host_slots_;
@@ -736,7 +686,6 @@ void Engine::launch(const EvalRequest& q) {
     expected_mask_ = 0;
     for (int k = 0; k < s; ++k) expected_mask_ |= 1U << ra.sources[k].target;
     if (gather) {
-        // The gather's last group finisher also reduces every scalar (no reduce launch).
         GatherArgs ga{};
         ga.particle_count = static_cast<int>(particle_count_);
         ga.movable_count = static_cast<int>(movable_count_);
@@ -767,19 +716,15 @@ void Engine::launch(const EvalRequest& q) {
         ga.rudy_gradient = q.rudy ? rudy_pin_gradient_ : nullptr;
         ga.rudy_weight = q.rudy ? q.rudy_weight : 0.0;
         ga.partials = partials_g_;
-        ga.group_partials = g_group_;
-        ga.group_counters = g_counters_;
-        ga.reduce = ra;
         beginKernel(kKindGather);
         launchGather(ga, gather_blocks_, stream_);
         endKernel();
         kernels += 1;
-    } else {
-        beginKernel(kKindReduce);
-        launchReduce(ra, stream_);
-        endKernel();
-        kernels += 1;
     }
+    beginKernel(kKindReduce);
+    launchReduce(ra, stream_);
+    endKernel();
+    kernels += 1;
 
 
     d2h_bytes_ += static_cast<uint64_t>(s) * sizeof(double) + sizeof(int) + sizeof(unsigned long long);
@@ -969,8 +914,10 @@ RudyReport Engine::rudyEvaluate(const double2* positions, bool validation) {
     launchRudyDeposit(ra, stream_);
     launchRudyMetrics(ra, g.blocks, stream_);
     ReduceArgs rr{};
-    for (int k = 0; k < 5; ++k) rr.sources[k] = ReduceSource{g.partials, g.blocks, 5, k, k == 4 ? 1 : 0, k};
+    for (int k = 0; k < 5; ++k) rr.sources[k] = ReduceSource{g.partials, g.blocks, 1, k * g.blocks, k == 4 ? 1 : 0, k};
     rr.source_count = 5;
+    for (int k = 0; k < 5; ++k) rr.offsets[k + 1] = rr.offsets[k] + g.blocks;
+    rr.staged_capacity = kReduceStaged;
     rr.scalars = rudy_scalars_;
     rr.totals = nullptr;
     launchReduce(rr, stream_);

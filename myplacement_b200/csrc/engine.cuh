@@ -260,18 +260,16 @@ private:
     unsigned long long* host_slots_ = nullptr;
     uint32_t expected_mask_ = 0;
     unsigned long long sequence_ = 0;
-    void buildTensorCoreBasis(const std::vector<double>& cx, const std::vector<double>& cy,
-                              const std::vector<double>& dy, const std::vector<double>& dxc,
-                              const std::vector<double>& sxwt, const std::vector<double>& syw, double max_scale);
+    void buildTensorCoreBasis(double max_scale);
     SplitMatrix newSplit(int rows, int cols, const char* what);
 
     // partials and scalars
     int scatter_blocks_ = 0, metrics_blocks_ = 0, gather_blocks_ = 0, energy_blocks_ = 0;
     bool metrics_fused_ = false;  // metrics pass writes the first contraction's operand planes
-    // Second-level (per 32 blocks) partials and their counters (reduceGroups).
-    double *wl_group_ = nullptr, *sc_group_ = nullptr, *g_group_ = nullptr, *m_group_ = nullptr;
-    unsigned int *wl_counters_ = nullptr, *sc_counters_ = nullptr, *g_counters_ = nullptr, *m_counters_ = nullptr;
-    int wl_groups_ = 0, sc_groups_ = 0, g_groups_ = 0, m_groups_ = 0;
+    // Second-level (per 32 blocks) wirelength partials and their counters (reduceGroups).
+    double* wl_group_ = nullptr;
+    unsigned int* wl_counters_ = nullptr;
+    int wl_groups_ = 0;
     void allocateGroups();
     double* partials_wl_ = nullptr;
     double* partials_sc_ = nullptr;

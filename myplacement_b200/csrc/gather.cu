@@ -19,6 +19,7 @@
 // scalar block in a fixed order (deterministic) and clears the integer layer
 // totals for the next scatter.
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -74,6 +75,21 @@ __device__ __forceinline__ void publishScalar(unsigned long long* slots, int tar
     slot[1] = tag | (bits >> 32);
 }
 
+// Thread 0 resets the layer totals and publishes the error flag.
+__device__ __forceinline__ void finishReduce(const ReduceArgs& a) {
+    if (threadIdx.x != 0) return;
+    if (a.totals != nullptr) {
+        a.totals[0] = 0ULL;
+        a.totals[1] = 0ULL;
+        a.totals[2] = 0ULL;
+    }
+    if (a.host_slots != nullptr) {
+        const unsigned int error = static_cast<unsigned int>(*reinterpret_cast<const volatile int*>(a.device_error));
+        const unsigned long long tag = static_cast<unsigned long long>(a.sequence) << 32;
+        reinterpret_cast<volatile unsigned long long*>(a.host_slots)[2 * kScalarCount] = tag | error;
+    }
+}
+
 // Every source of `a` reduced by the calling block: warp w takes sources w,
 // w + warps, ... (four at a time, their first rows loaded together); lane l
 // sums rows l, l + 32, ... in order, then a fixed shuffle tree, so the scalars
@@ -118,16 +134,7 @@ __device__ void reduceAllSources(const ReduceArgs& a) {
             }
         }
     }
-    if (threadIdx.x == 0 && a.totals != nullptr) {
-        a.totals[0] = 0ULL;
-        a.totals[1] = 0ULL;
-        a.totals[2] = 0ULL;
-    }
-    if (a.host_slots != nullptr && threadIdx.x == 0) {
-        const unsigned int error = static_cast<unsigned int>(*reinterpret_cast<const volatile int*>(a.device_error));
-        const unsigned long long tag = static_cast<unsigned long long>(a.sequence) << 32;
-        reinterpret_cast<volatile unsigned long long*>(a.host_slots)[2 * kScalarCount] = tag | error;
-    }
+    finishReduce(a);
 }
 
 __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
@@ -193,20 +200,72 @@ __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
     blockReduce<8>(v, is_max);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) a.partials[8 * blockIdx.x + k] = v[k];
-    }
-    if (a.group_counters != nullptr) {
-        // The block that finishes the last group reduces every partial of the
-        // evaluation (the other passes completed before this grid started).
-        const bool sums[8] = {false, false, false, false, false, false, false, false};
-        if (reduceGroups<8>(a.partials, a.group_partials, a.group_counters, sums) == 2) reduceAllSources(a.reduce);
+        for (int k = 0; k < 8; ++k) a.partials[k * gridDim.x + blockIdx.x] = v[k];
     }
 }
 
-__global__ void __launch_bounds__(kThreads) reduceKernel(ReduceArgs a) {
+// The scalar reduction as its own kernel: every partial of every source is
+// first staged in shared memory with all loads in flight together (eight per
+// thread at a time), then warp w sums sources w, w + 32, ... from shared memory,
+// lane l taking rows l, l + 32, ... in order and a fixed shuffle tree.
+__global__ void __launch_bounds__(kReduceThreads) reduceKernel(ReduceArgs a) {
     releaseNext();
     waitForPrior();
-    reduceAllSources(a);
+    extern __shared__ double staged[];
+    const int total = a.offsets[a.source_count];
+    if (total > a.staged_capacity) {
+        reduceAllSources(a);
+        return;
+    }
+    // The source table in shared memory: lanes look up different sources at once,
+    // which the parameter bank would serialise.
+    __shared__ const double* base_of[kScalarCount];
+    __shared__ int stride_of[kScalarCount];
+    __shared__ int offset_of[kScalarCount + 1];
+    if (threadIdx.x < a.source_count) {
+        const ReduceSource src = a.sources[threadIdx.x];
+        base_of[threadIdx.x] = src.partials + src.column;
+        stride_of[threadIdx.x] = src.stride;
+    }
+    if (threadIdx.x <= a.source_count) offset_of[threadIdx.x] = a.offsets[threadIdx.x];
+    __syncthreads();
+    constexpr int kBatch = 8;
+    int s = 0;  // the source of element e; e only grows, so the search resumes where it stopped
+    for (int base = threadIdx.x; base < total; base += kBatch * kReduceThreads) {
+        double x[kBatch];
+#pragma unroll
+        for (int j = 0; j < kBatch; ++j) {
+            const int e = base + j * kReduceThreads;
+            x[j] = 0.0;
+            if (e < total) {
+                while (e >= offset_of[s + 1]) ++s;
+                x[j] = __ldcg(base_of[s] + static_cast<size_t>(e - offset_of[s]) * stride_of[s]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kBatch; ++j) {
+            const int e = base + j * kReduceThreads;
+            if (e < total) staged[e] = x[j];
+        }
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    for (int s = threadIdx.x >> 5; s < a.source_count; s += kReduceThreads / 32) {
+        const ReduceSource& src = a.sources[s];
+        const int first = offset_of[s];
+        double value = src.is_max ? -1.0e308 : 0.0;
+        for (int row = lane; row < src.rows; row += 32) {
+            const double y = staged[first + row];
+            value = src.is_max ? fmax(value, y) : value + y;
+        }
+        value = src.is_max ? warpMax(value) : warpSum(value);
+        if (lane == 0) {
+            const double result = src.rows > 0 ? value : 0.0;
+            a.scalars[src.target] = result;
+            if (a.host_slots != nullptr) publishScalar(a.host_slots, src.target, result, a.sequence);
+        }
+    }
+    finishReduce(a);
 }
 
 }  // namespace
@@ -226,7 +285,20 @@ void launchGather(const GatherArgs& args, int blocks, cudaStream_t stream) {
 
 void launchReduce(const ReduceArgs& args, cudaStream_t stream) {
     if (args.source_count <= 0) return;
-    launchChained("Launch the scalar reduction", reduceKernel, dim3(1), dim3(kThreads), 0, stream, args);
+    constexpr int kMaxDevices = 64;
+    static std::once_flag once[kMaxDevices];
+    static cudaError_t attribute[kMaxDevices] = {};
+    int device = 0;
+    checkCuda(cudaGetDevice(&device), "Query the current device");
+    require(device >= 0 && device < kMaxDevices, "Device index out of range.");
+    std::call_once(once[device], [device] {
+        attribute[device] = cudaFuncSetAttribute(reduceKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 kReduceStaged * static_cast<int>(sizeof(double)));
+    });
+    checkCuda(attribute[device], "Configure the scalar reduction");
+    const int total = args.offsets[args.source_count];
+    const size_t smem = total <= args.staged_capacity ? static_cast<size_t>(total) * sizeof(double) : 0;
+    launchChained("Launch the scalar reduction", reduceKernel, dim3(1), dim3(kReduceThreads), smem, stream, args);
 }
 
 }  // namespace mpgp

@@ -104,8 +104,6 @@ struct ScatterArgs {
     unsigned long long* layers; // 3 * B fixed-point accumulators (movable, macro, filler)
     unsigned long long* totals; // 3 exact layer totals
     double* partials;           // per block: predicted, max displacement
-    double* group_partials;     // proposal mode: per 32 blocks (reduceGroups)
-    unsigned int* group_counters;
 };
 void launchScatter(const ScatterArgs& args, int blocks, cudaStream_t stream);
 
@@ -129,8 +127,6 @@ struct MetricsArgs {
     size_t split_plane;
     int* row_exp;
     TcScales* scales;
-    double* group_partials;            // fused form: per 32 rows (reduceGroups)
-    unsigned int* group_counters;
 };
 void launchMetrics(const MetricsArgs& args, int blocks, cudaStream_t stream);
 // The fused metrics-and-split pass takes one block per bin row and keeps a
@@ -171,17 +167,22 @@ void launchRudyMetrics(const RudyArgs& args, int blocks, cudaStream_t stream);
 void launchRudyGradient(const RudyArgs& args, cudaStream_t stream);
 
 // ---- deterministic reduction of all partials into the scalar block ----------------------
+// Source row r is partials[r * stride + column]; the producers write their
+// partials column-major (partial k of block b at k * grid + b), so stride is 1
+// and column is k * grid, and a source's rows are contiguous.
 struct ReduceSource {
     const double* partials;
     int rows;    // number of blocks that wrote partials
-    int stride;  // doubles per block
-    int column;  // which partial
+    int stride;  // doubles between consecutive rows
+    int column;  // offset of row 0
     int is_max;
     int target;  // Scalar slot
 };
 struct ReduceArgs {
     ReduceSource sources[kScalarCount];
     int source_count;
+    int offsets[kScalarCount + 1];  // prefix sums of the sources' rows (the staged layout)
+    int staged_capacity;            // doubles of dynamic shared memory the reduction kernel has
     double* scalars;             // kScalarCount
     unsigned long long* totals;  // reset to zero after use (may be null)
     // Optional completion record in mapped pinned host memory, written without
@@ -195,6 +196,8 @@ struct ReduceArgs {
 };
 static_assert(kScalarCount < 32, "the expected-scalar mask is 32 bits wide");
 // One block reduces every source (one warp per source, rows in a fixed order).
+constexpr int kReduceThreads = 1024;
+constexpr int kReduceStaged = 24576;  // doubles staged in shared memory (192 KiB)
 void launchReduce(const ReduceArgs& args, cudaStream_t stream);
 
 // ---- field gather + gradient combine (the fused update pass) ----------------------------
@@ -224,9 +227,6 @@ struct GatherArgs {
     double* partials;               // per block: 8 partials (kWireL1 .. kRudyL1)
     // Optional fused reduction: the last block to finish reduces `reduce`
     // (counted on reduce_counter, which is zero between launches).
-    double* group_partials;         // per 32 blocks: the 8 partials (reduceGroups)
-    unsigned int* group_counters;
-    ReduceArgs reduce;              // reduced by the block that finishes the last group
 };
 void launchGather(const GatherArgs& args, int blocks, cudaStream_t stream);
 // The gather's grid: one resident wave of blocks (grid-stride over the particles).

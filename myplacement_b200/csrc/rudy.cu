@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(kThreads) rudyMetricsKernel(RudyArgs a) {
     blockReduce<5>(v, is_max);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < 5; ++k) a.partials[5 * blockIdx.x + k] = v[k];
+        for (int k = 0; k < 5; ++k) a.partials[k * gridDim.x + blockIdx.x] = v[k];
     }
 }
 

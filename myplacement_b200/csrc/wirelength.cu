@@ -257,8 +257,8 @@ __global__ void __launch_bounds__(kThreads) wirelengthKernel(WirelengthArgs a) {
     const bool is_max[2] = {false, false};
     blockReduce<2>(values, is_max);
     if (threadIdx.x == 0) {
-        a.partials[2 * blockIdx.x + 0] = values[0];
-        a.partials[2 * blockIdx.x + 1] = values[1];
+        a.partials[blockIdx.x] = values[0];
+        a.partials[gridDim.x + blockIdx.x] = values[1];
     }
     reduceGroups<2>(a.partials, a.group_partials, a.group_counters, is_max);
 }
