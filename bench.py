@@ -51,6 +51,9 @@ def parse_args():
     p.add_argument("--workload", default=WORKLOAD)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--rudy", action="store_true",
+                   help="routability term on (hinge L2, capacity 1.2 x the activation mean demand), as the "
+                        "precision configuration runs it")
     p.add_argument("--form", choices=["plain", "batched", "serving"], default="plain",
                    help="plain: the one-design metric; batched: many small instances at once; "
                         "serving: an open-loop stream of jobs")
@@ -184,6 +187,26 @@ def reference_cpu_sample(design, bins: int, warmup: int, steps: int, variant: st
             "completed": long.completed_iterations, "hpwl_after": long.hpwl_after}
 
 
+def rudy_options(args) -> dict:
+    """The routability options of the precision configuration (none unless --rudy)."""
+    if not getattr(args, "rudy", False):
+        return {}
+    return {"rudy_penalty_model": 1, "rudy_capacity_factor": 1.2}
+
+
+def workload_text(args, design, bins: int) -> str:
+    import myplacement_b200 as mp
+
+    spec = mp.design.WORKLOADS[args.workload]
+    macros, terminals = spec.get("macros", 0), spec.get("terminals", 0)
+    text = (f"{args.workload}: {design.module_count - macros - terminals} cells, {macros} fixed macros, "
+            f"{terminals} terminals, {design.net_count} nets, {design.pin_count} pins, {bins}x{bins} bins, "
+            "target density 0.9")
+    if getattr(args, "rudy", False):
+        text += ", RUDY hinge L2 at capacity 1.2 x mean demand"
+    return text
+
+
 def make_workload(name: str, seed: int):
     import myplacement_b200 as mp
 
@@ -204,7 +227,8 @@ def run_mine(args) -> None:
     design, bins = make_workload(args.workload, replicas.replica_seed(args.seed, rank))
     iterations = args.warmup + args.steps
     options = mp.default_options(bins_x=bins, bins_y=bins, target_density=0.9, cuda_device=local,
-                                 iterations=max(280, iterations), feasible_refinement_iterations=10 ** 9)
+                                 iterations=max(280, iterations), feasible_refinement_iterations=10 ** 9,
+                                 **rudy_options(args))
     session = mp.Session(design, options)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     stream_ptr = session.stream
@@ -281,7 +305,8 @@ def run_mine(args) -> None:
 
     e2e = None
     if not args.no_e2e:
-        e2e_options = mp.default_options(bins_x=bins, bins_y=bins, target_density=0.9, cuda_device=local)
+        e2e_options = mp.default_options(bins_x=bins, bins_y=bins, target_density=0.9, cuda_device=local,
+                                         **rudy_options(args))
         replicas.barrier()
         t0 = time.perf_counter()
         s2 = mp.Session(design, e2e_options)
@@ -316,9 +341,7 @@ def run_mine(args) -> None:
             "metric": METRIC, "value": value, "unit": "iterations/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {design.module_count - 1600} cells, 400 fixed macros, "
-                                   f"1200 terminals, {design.net_count} nets, {design.pin_count} pins, "
-                                   f"{bins}x{bins} bins, target density 0.9",
+            "config": {"workload": workload_text(args, design, bins),
                        "particles": particles, "step": "one adaptive controller iteration",
                        "early_stop": "off in the timed run (fixed iteration count)",
                        "l2": "flushed between timed steps (256 MiB device write, outside the timing)",

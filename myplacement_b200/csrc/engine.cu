@@ -611,8 +611,12 @@ void Engine::launch(const EvalRequest& q) {
         const RudyArgs ra = rudyArgs(rudy_main_, positions, true);
         beginKernel(kKindRudy, stream_wl_);
         launchRudyDeposit(ra, stream_wl_);
+        launchRudyPrefix(ra, stream_wl_);
         launchRudyMetrics(ra, rudy_main_.blocks, stream_wl_);
-        if (q.gradient) launchRudyGradient(ra, stream_wl_);
+        if (q.gradient) {
+            launchRudyTables(ra, stream_wl_);
+            launchRudyGradient(ra, stream_wl_);
+        }
         endKernel(stream_wl_);
     }
     checkCuda(cudaEventRecord(join_, stream_wl_), "join");
@@ -728,7 +732,7 @@ void Engine::launch(const EvalRequest& q) {
 
 
     d2h_bytes_ += static_cast<uint64_t>(s) * sizeof(double) + sizeof(int) + sizeof(unsigned long long);
-    if (q.rudy) kernels += q.gradient ? 3 : 2;
+    if (q.rudy) kernels += q.gradient ? 7 : 4;
     launches_ += kernels;
     last_gradient_ = q.gradient;
     last_propose_ = q.mode == kPropose;
@@ -832,6 +836,11 @@ void Engine::allocateRudyGrid(RudyGrid& g, int columns, int rows, const char* wh
     g.adjoint_h = arena_.array<double>(bins, what);
     g.adjoint_v = arena_.array<double>(bins, what);
     g.utilization = arena_.array<double>(bins, what);
+    const std::size_t padded = static_cast<std::size_t>(columns + 1) * static_cast<std::size_t>(rows + 1);
+    g.diff = arena_.array<unsigned long long>(2 * padded, what);
+    g.table = arena_.array<double>(2 * padded, what);
+    checkCuda(cudaMemsetAsync(g.diff, 0, 2 * padded * sizeof(unsigned long long), stream_), what);
+    checkCuda(cudaMemsetAsync(g.table, 0, 2 * padded * sizeof(double), stream_), what);
     g.blocks = std::max(1, std::min(ceilDiv(static_cast<long long>(bins), kThreads), 148 * 2));
     g.partials = arena_.array<double>(5 * static_cast<std::size_t>(g.blocks), what);
     checkCuda(cudaMemsetAsync(g.horizontal, 0, bins * sizeof(unsigned long long), stream_), what);
@@ -886,8 +895,10 @@ RudyArgs Engine::rudyArgs(const RudyGrid& g, const double2* positions, bool with
     a.minimum_y_span = g.min_y_span;
     a.inv_unit_h = 4294967296.0 / g.bin_w;
     a.inv_unit_v = 4294967296.0 / g.bin_h;
+    a.diff = g.diff;
     a.horizontal = g.horizontal;
     a.vertical = g.vertical;
+    a.table = g.table;
     a.capacity_h = with_capacity ? g.capacity_h : 0.0;
     a.capacity_v = with_capacity ? g.capacity_v : 0.0;
     a.model = rudy_model_;
@@ -912,6 +923,7 @@ RudyReport Engine::rudyEvaluate(const double2* positions, bool validation) {
     const bool with_capacity = g.capacity_h > 0.0 && g.capacity_v > 0.0;
     const RudyArgs ra = rudyArgs(g, positions, with_capacity);
     launchRudyDeposit(ra, stream_);
+    launchRudyPrefix(ra, stream_);
     launchRudyMetrics(ra, g.blocks, stream_);
     ReduceArgs rr{};
     for (int k = 0; k < 5; ++k) rr.sources[k] = ReduceSource{g.partials, g.blocks, 1, k * g.blocks, k == 4 ? 1 : 0, k};
@@ -921,7 +933,7 @@ RudyReport Engine::rudyEvaluate(const double2* positions, bool validation) {
     rr.scalars = rudy_scalars_;
     rr.totals = nullptr;
     launchReduce(rr, stream_);
-    launches_ += 3;
+    launches_ += 5;
     checkCuda(cudaMemcpyAsync(host_rudy_, rudy_scalars_, 5 * sizeof(double), cudaMemcpyDeviceToHost, stream_),
               "Download RUDY scalars");
     const std::size_t bins = static_cast<std::size_t>(g.columns) * static_cast<std::size_t>(g.rows);

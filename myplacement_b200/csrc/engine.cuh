@@ -169,8 +169,10 @@ private:
         int columns = 0, rows = 0;
         double bin_w = 0.0, bin_h = 0.0, min_x_span = 0.0, min_y_span = 0.0;
         double capacity_h = 0.0, capacity_v = 0.0;
+        unsigned long long* diff = nullptr;
         unsigned long long* horizontal = nullptr;
         unsigned long long* vertical = nullptr;
+        double* table = nullptr;
         double* adjoint_h = nullptr;
         double* adjoint_v = nullptr;
         double* utilization = nullptr;

@@ -151,7 +151,8 @@ struct RudyArgs {
     int columns, rows;
     double minimum_x_span, minimum_y_span;
     double inv_unit_h, inv_unit_v;  // fixed point: 2^32 / bin_w, 2^32 / bin_h
-    unsigned long long* horizontal; // columns * rows, read and cleared by the metrics pass
+    unsigned long long* diff;       // 2 x (rows + 1) x (columns + 1) difference arrays (H, V), zero between uses
+    unsigned long long* horizontal; // rows x columns demand maps, written by the prefix pass
     unsigned long long* vertical;
     double capacity_h, capacity_v;  // 0: maps and totals only
     int model;                      // MPGP_RUDY_*
@@ -159,11 +160,14 @@ struct RudyArgs {
     double* adjoint_h;
     double* adjoint_v;
     double* utilization;            // per bin max(uh, uv), or null
+    double* table;                  // 2 x (rows + 1) x (columns + 1) summed-area tables of the adjoints
     double* partials;               // per block: energy, H total, V total, proxy, max utilisation
 };
 int rudyBlocks(int count);
 void launchRudyDeposit(const RudyArgs& args, cudaStream_t stream);
+void launchRudyPrefix(const RudyArgs& args, cudaStream_t stream);
 void launchRudyMetrics(const RudyArgs& args, int blocks, cudaStream_t stream);
+void launchRudyTables(const RudyArgs& args, cudaStream_t stream);
 void launchRudyGradient(const RudyArgs& args, cudaStream_t stream);
 
 // ---- deterministic reduction of all partials into the scalar block ----------------------

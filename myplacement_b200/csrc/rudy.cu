@@ -1,26 +1,36 @@
 // RUDY routing-demand map, hotspot penalty and its subgradient on the device.
 //
 // Restates evaluateRudy (Rudy.cpp:227-456) for the adaptive controller's
-// routability term (AdaptiveGlobalPlacer.cpp:149-172, 201-331):
-//   deposit   one thread per net: the pin bounding box, expanded to
-//             minimum_span_in_bins where a net is thinner (calculateNetBox,
-//             Rudy.cpp:120-152), clipped to the core, and its exact rectangle
-//             overlap with every covered bin added as horizontal demand
-//             w * overlap / y_span and vertical demand w * overlap / x_span.
-//             As in the density scatter the terms are quantized to int64 (units
-//             of bin_w * 2^-32 and bin_h * 2^-32) and added with integer
-//             atomics, so the maps are bit-exact run to run.
+// routability term (AdaptiveGlobalPlacer.cpp:149-172, 201-331).  A net's
+// rectangle-overlap demand is separable: the overlap of its (expanded, clipped)
+// box with bin (c, r) is ox(c) * oy(r), where ox is a partial width in the box's
+// first and last columns and the bin width in between, and the same along y.
+// So a net's demand is at most 3 x 3 constant blocks, and the passes are:
+//   deposit   one thread per net: the pin box, expanded to minimum_span_in_bins
+//             where a net is thinner (calculateNetBox, Rudy.cpp:120-152), each
+//             block's horizontal demand w * overlap / y_span and vertical demand
+//             w * overlap / x_span quantized to int64 (units of bin_w * 2^-32 and
+//             bin_h * 2^-32) and added at the block's four corners of a 2-D
+//             difference array with integer atomics: at most 72 atomics a net
+//             instead of two per covered bin, and the maps stay bit-exact.
+//   prefix    two scans (rows, then columns) turn the difference arrays into the
+//             demand maps and clear them.
 //   metrics   one thread per bin: utilisation against the frozen capacities,
 //             the penalty model (hinge L2 / softplus L2 / hinge L4,
 //             evaluatePenalty Rudy.cpp:83-100), its adjoint, the energy, the
 //             proxy overflow, the maximum utilisation and the demand totals
-//             (FP64 block partials, reduced in a fixed order); the maps are
-//             cleared for the next deposit.
-//   gradient  one thread per net: the Clarke subgradient of the overlap map
-//             with respect to the four box edges (Rudy.cpp:320-400), split over
-//             the pins that sit on each extremal edge (Rudy.cpp:402-452) and
-//             written to the pins' particle-ordered slots for the gather.
-// Arithmetic is FP64 in the reference's order.
+//             (FP64 block partials, reduced in a fixed order).
+//   tables    two scans build summed-area tables of the two adjoints.
+//   gradient  one thread per net: the Clarke subgradient with respect to the
+//             four box edges (Rudy.cpp:320-400).  An edge's term only involves
+//             the one or two columns (rows) its derivative is non-zero in, and
+//             the span terms a box-weighted adjoint sum: with the tables each is
+//             O(1), not O(box area).  The edge gradients are split over the pins
+//             on each extremal edge (Rudy.cpp:402-452) and written to the pins'
+//             particle-ordered slots for the gather.
+// Arithmetic is FP64; interior bins take the bin width and height as their
+// overlap, which the reference's per-bin differences reproduce to the last bit
+// or one unit in it.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -132,9 +142,56 @@ __device__ __forceinline__ bool clippedRange(const RudyArgs& a, const Box& b, in
     return true;
 }
 
+// The parts of a clipped box along one axis: the first cell (partial), the
+// interior cells (full), the last cell (partial); lo / hi index ranges and overlaps.
+struct AxisParts {
+    int count;
+    int lo[3], hi[3];
+    double overlap[3];
+};
+
+__device__ __forceinline__ AxisParts axisParts(double lower, double upper, double origin, double length, int first,
+                                               int last) {
+    AxisParts p;
+    const auto cell = [&](int i) {
+        const double begin = origin + static_cast<double>(i) * length;
+        return overlapLength(lower, upper, begin, begin + length);
+    };
+    p.count = 0;
+    p.lo[0] = p.hi[0] = first;
+    p.overlap[0] = cell(first);
+    p.count = 1;
+    if (last > first) {
+        if (last > first + 1) {
+            p.lo[1] = first + 1;
+            p.hi[1] = last - 1;
+            p.overlap[1] = length;
+            p.count = 2;
+        }
+        p.lo[p.count] = p.hi[p.count] = last;
+        p.overlap[p.count] = cell(last);
+        ++p.count;
+    }
+    return p;
+}
+
+__device__ __forceinline__ void addCorners(unsigned long long* diff, int stride, int r0, int r1, int c0, int c1,
+                                           long long q) {
+    if (q == 0) return;
+    const unsigned long long up = static_cast<unsigned long long>(q);
+    const unsigned long long down = static_cast<unsigned long long>(-q);
+    atomicAdd(diff + static_cast<size_t>(r0) * stride + c0, up);
+    atomicAdd(diff + static_cast<size_t>(r0) * stride + c1 + 1, down);
+    atomicAdd(diff + static_cast<size_t>(r1 + 1) * stride + c0, down);
+    atomicAdd(diff + static_cast<size_t>(r1 + 1) * stride + c1 + 1, up);
+}
+
 __global__ void __launch_bounds__(kThreads) rudyDepositKernel(RudyArgs a) {
     releaseNext();
     waitForPrior();
+    const int stride = a.columns + 1;
+    unsigned long long* diff_h = a.diff;
+    unsigned long long* diff_v = a.diff + static_cast<size_t>(a.rows + 1) * stride;
     for (int net = blockIdx.x * blockDim.x + threadIdx.x; net < a.net_count; net += gridDim.x * blockDim.x) {
         const int begin = a.net_start[net];
         const int end = a.net_start[net + 1];
@@ -143,21 +200,104 @@ __global__ void __launch_bounds__(kThreads) rudyDepositKernel(RudyArgs a) {
         const Box b = netBox(a, begin, end);
         int c0, c1, r0, r1;
         if (!clippedRange(a, b, c0, c1, r0, r1)) continue;
-        for (int row = r0; row <= r1; ++row) {
-            const double bin_bottom = a.lly + static_cast<double>(row) * a.bin_h;
-            const double overlap_y = overlapLength(b.bottom, b.top, bin_bottom, bin_bottom + a.bin_h);
+        const AxisParts cols = axisParts(b.left, b.right, a.llx, a.bin_w, c0, c1);
+        const AxisParts rows = axisParts(b.bottom, b.top, a.lly, a.bin_h, r0, r1);
+        for (int i = 0; i < rows.count; ++i) {
+            const double overlap_y = rows.overlap[i];
             if (overlap_y <= kEpsilon) continue;
-            for (int column = c0; column <= c1; ++column) {
-                const double bin_left = a.llx + static_cast<double>(column) * a.bin_w;
-                const double overlap = overlapLength(b.left, b.right, bin_left, bin_left + a.bin_w) * overlap_y;
+            for (int j = 0; j < cols.count; ++j) {
+                const double overlap = cols.overlap[j] * overlap_y;
                 if (overlap <= kEpsilon) continue;
-                const size_t index = static_cast<size_t>(row) * a.columns + column;
                 const long long qh = __double2ll_rn(weight * overlap / b.y_span * a.inv_unit_h);
                 const long long qv = __double2ll_rn(weight * overlap / b.x_span * a.inv_unit_v);
-                atomicAdd(a.horizontal + index, static_cast<unsigned long long>(qh));
-                atomicAdd(a.vertical + index, static_cast<unsigned long long>(qv));
+                addCorners(diff_h, stride, rows.lo[i], rows.hi[i], cols.lo[j], cols.hi[j], qh);
+                addCorners(diff_v, stride, rows.lo[i], rows.hi[i], cols.lo[j], cols.hi[j], qv);
             }
         }
+    }
+}
+
+// Inclusive scan of `length` values (load(i) / store(i, v)) by the whole block,
+// in chunks of blockDim.x, always in index order (the sums are deterministic).
+template <typename T, class Load, class Store>
+__device__ void scanLine(int length, Load load, Store store) {
+    __shared__ T warp_sums[32];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int warps = blockDim.x >> 5;
+    T carry = T(0);
+    for (int base = 0; base < length; base += blockDim.x) {
+        const int i = base + static_cast<int>(threadIdx.x);
+        T v = i < length ? load(i) : T(0);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const T u = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += u;
+        }
+        if (lane == 31) warp_sums[warp] = v;
+        __syncthreads();
+        if (warp == 0) {
+            T w = lane < warps ? warp_sums[lane] : T(0);
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const T u = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += u;
+            }
+            if (lane < warps) warp_sums[lane] = w;
+        }
+        __syncthreads();
+        const T before = warp > 0 ? warp_sums[warp - 1] : T(0);
+        if (i < length) store(i, carry + before + v);
+        carry += warp_sums[warps - 1];
+        __syncthreads();
+    }
+}
+
+// Difference arrays -> demand maps.  Pass 0 scans each row of both arrays in
+// place; pass 1 scans each column, writes the map and clears the array.
+__global__ void __launch_bounds__(kThreads) rudyPrefixKernel(RudyArgs a, int pass) {
+    releaseNext();
+    waitForPrior();
+    const int stride = a.columns + 1;
+    unsigned long long* diff = a.diff + static_cast<size_t>(blockIdx.y) * (a.rows + 1) * stride;
+    unsigned long long* map = blockIdx.y == 0 ? a.horizontal : a.vertical;
+    if (pass == 0) {
+        unsigned long long* row = diff + static_cast<size_t>(blockIdx.x) * stride;
+        scanLine<unsigned long long>(
+            stride, [&](int i) { return row[i]; }, [&](int i, unsigned long long v) { row[i] = v; });
+    } else {
+        const int c = blockIdx.x;
+        scanLine<unsigned long long>(
+            a.rows + 1,
+            [&](int i) {
+                const unsigned long long v = diff[static_cast<size_t>(i) * stride + c];
+                diff[static_cast<size_t>(i) * stride + c] = 0ULL;
+                return v;
+            },
+            [&](int i, unsigned long long v) {
+                if (i < a.rows && c < a.columns) map[static_cast<size_t>(i) * a.columns + c] = v;
+            });
+    }
+}
+
+// Summed-area tables of the two adjoints: table[(r + 1) * (columns + 1) + c + 1]
+// = sum over r' <= r, c' <= c (row 0 and column 0 stay zero).
+__global__ void __launch_bounds__(kThreads) rudyTableKernel(RudyArgs a, int pass) {
+    releaseNext();
+    waitForPrior();
+    const int stride = a.columns + 1;
+    double* table = a.table + static_cast<size_t>(blockIdx.y) * (a.rows + 1) * stride;
+    const double* adjoint = blockIdx.y == 0 ? a.adjoint_h : a.adjoint_v;
+    if (pass == 0) {
+        const int r = blockIdx.x;
+        const double* in = adjoint + static_cast<size_t>(r) * a.columns;
+        double* out = table + static_cast<size_t>(r + 1) * stride + 1;
+        scanLine<double>(a.columns, [&](int i) { return in[i]; }, [&](int i, double v) { out[i] = v; });
+    } else {
+        const int c = blockIdx.x + 1;
+        scanLine<double>(
+            a.rows, [&](int i) { return table[static_cast<size_t>(i + 1) * stride + c]; },
+            [&](int i, double v) { table[static_cast<size_t>(i + 1) * stride + c] = v; });
     }
 }
 
@@ -196,8 +336,6 @@ __global__ void __launch_bounds__(kThreads) rudyMetricsKernel(RudyArgs a) {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < bins; b += gridDim.x * blockDim.x) {
         const double h = static_cast<double>(static_cast<long long>(a.horizontal[b])) * unit_h;
         const double w = static_cast<double>(static_cast<long long>(a.vertical[b])) * unit_v;
-        a.horizontal[b] = 0ULL;
-        a.vertical[b] = 0ULL;
         v[1] += h;
         v[2] += w;
         if (!with_capacity) continue;
@@ -241,38 +379,81 @@ __global__ void __launch_bounds__(kThreads) rudyGradientKernel(RudyArgs a) {
         const int g1 = min(a.columns - 1, c1 + (onInteriorGridLine(b.right, a.llx, a.bin_w, a.columns) ? 1 : 0));
         const int h0 = max(0, r0 - (onInteriorGridLine(b.bottom, a.lly, a.bin_h, a.rows) ? 1 : 0));
         const int h1 = min(a.rows - 1, r1 + (onInteriorGridLine(b.top, a.lly, a.bin_h, a.rows) ? 1 : 0));
+        const AxisParts cols = axisParts(b.left, b.right, a.llx, a.bin_w, c0, c1);
+        const AxisParts rows = axisParts(b.bottom, b.top, a.lly, a.bin_h, r0, r1);
+        const int stride = a.columns + 1;
+        const double* table_h = a.table;
+        const double* table_v = a.table + static_cast<size_t>(a.rows + 1) * stride;
+        // Sum of one adjoint over rows [rl, rh] x columns [cl, ch] (inclusive).
+        const auto rect = [&](const double* t, int rl, int rh, int cl, int ch) {
+            if (rl > rh || cl > ch) return 0.0;
+            return t[static_cast<size_t>(rh + 1) * stride + ch + 1] - t[static_cast<size_t>(rl) * stride + ch + 1] -
+                   t[static_cast<size_t>(rh + 1) * stride + cl] + t[static_cast<size_t>(rl) * stride + cl];
+        };
+        // sum over the box's rows of oy(r) * adjoint(c, r), and the same along a row.
+        const auto column_sum = [&](const double* t, int c) {
+            double sum = 0.0;
+            for (int i = 0; i < rows.count; ++i) sum += rows.overlap[i] * rect(t, rows.lo[i], rows.hi[i], c, c);
+            return sum;
+        };
+        const auto row_sum = [&](const double* t, int r) {
+            double sum = 0.0;
+            for (int j = 0; j < cols.count; ++j) sum += cols.overlap[j] * rect(t, r, r, cols.lo[j], cols.hi[j]);
+            return sum;
+        };
+        // sum over the box of ox(c) oy(r) adjoint(c, r).
+        const auto box_sum = [&](const double* t) {
+            double sum = 0.0;
+            for (int i = 0; i < rows.count; ++i) {
+                for (int j = 0; j < cols.count; ++j) {
+                    sum += rows.overlap[i] * cols.overlap[j] * rect(t, rows.lo[i], rows.hi[i], cols.lo[j], cols.hi[j]);
+                }
+            }
+            return sum;
+        };
+        // Edge terms: the columns (rows) next to an edge are the only ones whose
+        // derivative can be non-zero; each adds d * (adj_h / y_span + adj_v / x_span)
+        // weighted by the other axis' overlaps (Rudy.cpp:360-400).
         double g_left = 0.0, g_right = 0.0, g_bottom = 0.0, g_top = 0.0;
-        for (int row = h0; row <= h1; ++row) {
-            const double bin_bottom = a.lly + static_cast<double>(row) * a.bin_h;
-            const double bin_top = bin_bottom + a.bin_h;
-            const double overlap_y = overlapLength(b.bottom, b.top, bin_bottom, bin_top);
-            const double d_bottom = lowerDerivative(b.bottom, bin_bottom, bin_top, overlap_y);
-            const double d_top = upperDerivative(b.top, bin_bottom, bin_top, overlap_y);
-            if (overlap_y <= kEpsilon && d_bottom == 0.0 && d_top == 0.0) continue;
-            for (int column = g0; column <= g1; ++column) {
-                const double bin_left = a.llx + static_cast<double>(column) * a.bin_w;
+        const auto column_edge = [&](double edge, bool lower) {
+            double sum = 0.0;
+            const int near = static_cast<int>(floor((edge - a.llx) / a.bin_w));
+            for (int c = max(g0, near - 1); c <= min(g1, near + 1); ++c) {
+                const double bin_left = a.llx + static_cast<double>(c) * a.bin_w;
                 const double bin_right = bin_left + a.bin_w;
                 const double overlap_x = overlapLength(b.left, b.right, bin_left, bin_right);
-                const double overlap = overlap_x * overlap_y;
-                const double d_left = lowerDerivative(b.left, bin_left, bin_right, overlap_x);
-                const double d_right = upperDerivative(b.right, bin_left, bin_right, overlap_x);
-                if (overlap_x <= kEpsilon && d_left == 0.0 && d_right == 0.0) continue;
-                const size_t index = static_cast<size_t>(row) * a.columns + column;
-                const double adj_h = a.adjoint_h[index];
-                const double adj_v = a.adjoint_v[index];
-                const double o_left = d_left * overlap_y;
-                const double o_right = d_right * overlap_y;
-                const double o_bottom = overlap_x * d_bottom;
-                const double o_top = overlap_x * d_top;
-                const double x_left = b.x_physical ? overlap / (b.x_span * b.x_span) : 0.0;
-                const double x_right = b.x_physical ? -overlap / (b.x_span * b.x_span) : 0.0;
-                const double y_bottom = b.y_physical ? overlap / (b.y_span * b.y_span) : 0.0;
-                const double y_top = b.y_physical ? -overlap / (b.y_span * b.y_span) : 0.0;
-                g_left += adj_h * weight * o_left / b.y_span + adj_v * weight * (o_left / b.x_span + x_left);
-                g_right += adj_h * weight * o_right / b.y_span + adj_v * weight * (o_right / b.x_span + x_right);
-                g_bottom += adj_h * weight * (o_bottom / b.y_span + y_bottom) + adj_v * weight * o_bottom / b.x_span;
-                g_top += adj_h * weight * (o_top / b.y_span + y_top) + adj_v * weight * o_top / b.x_span;
+                const double d = lower ? lowerDerivative(edge, bin_left, bin_right, overlap_x)
+                                       : upperDerivative(edge, bin_left, bin_right, overlap_x);
+                if (d != 0.0) sum += d * (column_sum(table_h, c) / b.y_span + column_sum(table_v, c) / b.x_span);
             }
+            return sum;
+        };
+        const auto row_edge = [&](double edge, bool lower) {
+            double sum = 0.0;
+            const int near = static_cast<int>(floor((edge - a.lly) / a.bin_h));
+            for (int r = max(h0, near - 1); r <= min(h1, near + 1); ++r) {
+                const double bin_bottom = a.lly + static_cast<double>(r) * a.bin_h;
+                const double bin_top = bin_bottom + a.bin_h;
+                const double overlap_y = overlapLength(b.bottom, b.top, bin_bottom, bin_top);
+                const double d = lower ? lowerDerivative(edge, bin_bottom, bin_top, overlap_y)
+                                       : upperDerivative(edge, bin_bottom, bin_top, overlap_y);
+                if (d != 0.0) sum += d * (row_sum(table_h, r) / b.y_span + row_sum(table_v, r) / b.x_span);
+            }
+            return sum;
+        };
+        g_left = weight * column_edge(b.left, true);
+        g_right = weight * column_edge(b.right, false);
+        g_bottom = weight * row_edge(b.bottom, true);
+        g_top = weight * row_edge(b.top, false);
+        if (b.x_physical) {
+            const double span_term = weight * box_sum(table_v) / (b.x_span * b.x_span);
+            g_left += span_term;
+            g_right -= span_term;
+        }
+        if (b.y_physical) {
+            const double span_term = weight * box_sum(table_h) / (b.y_span * b.y_span);
+            g_bottom += span_term;
+            g_top -= span_term;
         }
         int n_left = 0, n_right = 0, n_bottom = 0, n_top = 0;
         for (int pin = begin; pin < end; ++pin) {
@@ -315,6 +496,20 @@ void launchRudyDeposit(const RudyArgs& args, cudaStream_t stream) {
     if (args.net_count <= 0) return;
     launchChained("Launch the RUDY deposit", rudyDepositKernel, dim3(rudyBlocks(args.net_count)), dim3(kThreads), 0,
                   stream, args);
+}
+
+void launchRudyPrefix(const RudyArgs& args, cudaStream_t stream) {
+    launchChained("Launch the RUDY row scan", rudyPrefixKernel, dim3(args.rows + 1, 2), dim3(kThreads), 0, stream,
+                  args, 0);
+    launchChained("Launch the RUDY column scan", rudyPrefixKernel, dim3(args.columns + 1, 2), dim3(kThreads), 0,
+                  stream, args, 1);
+}
+
+void launchRudyTables(const RudyArgs& args, cudaStream_t stream) {
+    launchChained("Launch the RUDY adjoint row scan", rudyTableKernel, dim3(args.rows, 2), dim3(kThreads), 0, stream,
+                  args, 0);
+    launchChained("Launch the RUDY adjoint column scan", rudyTableKernel, dim3(args.columns, 2), dim3(kThreads), 0,
+                  stream, args, 1);
 }
 
 void launchRudyMetrics(const RudyArgs& args, int blocks, cudaStream_t stream) {
