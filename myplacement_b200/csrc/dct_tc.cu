@@ -64,7 +64,9 @@ constexpr int kTilePitch = kTileN + 1;  // floats per staged row (odd pitch: no 
 constexpr int kStagedOffset = kParkBytes;
 constexpr int kReceiveOffset = kRingBytes;
 constexpr int kBarrierOffset = kReceiveOffset + kParkBytes;
-constexpr int kSmemBytes = kBarrierOffset + 256 + 1024 /* alignment slack */;
+constexpr int kPrefetchOffset = kBarrierOffset + 256;  // epilogue inputs fetched right after the dependency wait
+constexpr int kPrefetchInts = 4 + kTileM;              // exp_a, exp_b, out_exp, -, then the tile's row exponents
+constexpr int kSmemBytes = kPrefetchOffset + kPrefetchInts * 4 + 1024 /* alignment slack */;
 constexpr uint32_t kTmemColumns = 4 * kTileN;  // two buffers x (main, correction) accumulators
 constexpr long kSpinLimit = 1L << 22;
 static_assert(kStagedOffset + kTileM * kTilePitch * 4 <= kRingBytes, "the parked and staged tiles must fit in the ring");
@@ -276,6 +278,31 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
     }
     __syncthreads();
     clusterArrive();  // this CTA's barriers are initialised; peers wait for it before sending
+    // The spectral scale of this CTA's output rows (a fixed table) goes to the slot of
+    // the receive area that no peer writes (a CTA's own split), before the wait.
+    float* scale_tile = reinterpret_cast<float*>(smem + kReceiveOffset +
+                                                 static_cast<size_t>(split) * rows_per * kParkPitch * 8);
+    if (t.mode == kTcSpectral && threadIdx.x >= 64) {
+        // The four epilogue warps, eight loads in flight per thread.
+        constexpr int kBatch = 8;
+        const int count = rows_per * kTileN;
+        for (int base = static_cast<int>(threadIdx.x) - 64; base < count; base += kBatch * (kTcThreads - 64)) {
+            float v[kBatch];
+#pragma unroll
+            for (int j = 0; j < kBatch; ++j) {
+                const int e = base + j * (kTcThreads - 64);
+                const int grow = m0 + row_begin + e / kTileN;
+                const int gcol = n0 + e % kTileN;
+                v[j] = e < count && grow < t.m && gcol < t.n ? __ldg(t.scale + static_cast<size_t>(grow) * t.n + gcol)
+                                                             : 0.0f;
+            }
+#pragma unroll
+            for (int j = 0; j < kBatch; ++j) {
+                const int e = base + j * (kTcThreads - 64);
+                if (e < count) scale_tile[e] = v[j];
+            }
+        }
+    }
     // The first stages' basis tiles do not depend on the previous kernels: issue them
     // now, so that only the data operand's latency follows the dependency wait.
     const int prefetched = t.constant_operand != 0 ? min(k_blocks, kStages) : 0;
@@ -324,6 +351,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
                 // Drain: wait (bounded) for every issued stage so no copy lands after exit.
                 for (int kb = max(0, issued - kStages); kb < issued; ++kb) {
                     mbarWait(full0 + 8 * (kb % kStages), (kb / kStages) & 1, nullptr);
+                }
+            }
+        } else {
+            // The epilogue's scalar inputs (written by the previous kernels), fetched
+            // now so that their latency hides behind the main loop.
+            int* early = reinterpret_cast<int*>(smem + kPrefetchOffset);
+            if (lane == 1) {
+                early[0] = t.exp_a != nullptr ? *t.exp_a : 0;
+                early[1] = *t.exp_b;
+                early[2] = t.mode != kTcField ? planeExponent(t.ref_max, t.gain) : 0;
+            }
+            if (t.row_exp_a != nullptr) {
+                for (int r = lane - 1; r < rows_per; r += 31) {
+                    early[4 + r] = __ldg(t.row_exp_a + min(m0 + row_begin + r, t.m - 1));
                 }
             }
         }
@@ -436,31 +477,42 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
     // Fused sum and output, one (row, eight columns) unit per thread and pass: the
     // fixed-order sum over the splits, the unscaling, then the row-major output
     // (planes, field, or spectral divide + planes) and the staged copy for the
-    // transposed pass.  A warp's lanes run along the columns.
-    const int exp_b = *t.exp_b;
-    const int exp_a = t.exp_a != nullptr ? *t.exp_a : 0;
+    // transposed pass.
+    const int* early = reinterpret_cast<const int*>(smem + kPrefetchOffset);
+    const int exp_a = early[0];
+    const int exp_b = early[1];
     const bool split_out = t.mode != kTcField;
-    const int out_exp = split_out ? planeExponent(t.ref_max, t.gain) : 0;
+    const int out_exp = early[2];
     const float inv_scale = static_cast<float>(pow2(-out_exp));
     const bool staging = t.mode == kTcSplitTransposed || t.mode == kTcSpectral;
     double energy = 0.0;
     float magnitude = 0.0f;
     if (tile_ok) {
         for (int u = threadIdx.x; u < rows_per * (kTileN / 8); u += kTcThreads) {
-            const int r_local = u / (kTileN / 8);
-            const int c0 = (u % (kTileN / 8)) * 8;
+            // Lanes run down the rows: their shared-memory rows are a pitch apart,
+            // so the pieces' 16-byte loads and the staged stores hit distinct banks.
+            const int r_local = u % rows_per;
+            const int c0 = (u / rows_per) * 8;
             const int r = row_begin + r_local;
             const int grow = m0 + r;
             const int gcol0 = n0 + c0;
             const bool row_in = grow < t.m;
             const int valid = row_in ? max(0, min(8, t.n - gcol0)) : 0;
             // Global inputs first, so their latency overlaps the shared-memory sum.
-            const int shift = exp_b + (t.row_exp_a != nullptr ? __ldg(t.row_exp_a + min(grow, t.m - 1)) : exp_a);
+            const int shift = exp_b + (t.row_exp_a != nullptr ? early[4 + r_local] : exp_a);
             float sc[8];
             if (t.mode == kTcSpectral) {
-                const float* scale = t.scale + static_cast<size_t>(min(grow, t.m - 1)) * t.n + gcol0;
-#pragma unroll
-                for (int i = 0; i < 8; ++i) sc[i] = i < valid ? __ldg(scale + i) : 0.0f;
+                // The spectral divide (ElectrostaticField.cpp:212-221), from the staged table.
+                const float4 lo4 = *reinterpret_cast<const float4*>(scale_tile + r_local * kTileN + c0);
+                const float4 hi4 = *reinterpret_cast<const float4*>(scale_tile + r_local * kTileN + c0 + 4);
+                sc[0] = lo4.x;
+                sc[1] = lo4.y;
+                sc[2] = lo4.z;
+                sc[3] = lo4.w;
+                sc[4] = hi4.x;
+                sc[5] = hi4.y;
+                sc[6] = hi4.z;
+                sc[7] = hi4.w;
             }
             double sum[8];
 #pragma unroll
@@ -532,8 +584,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
         // Transposed pass: eight consecutive rows of one column per thread.
         const int groups = rows_per / 8;
         for (int g = threadIdx.x; g < groups * kTileN && tile_ok; g += kTcThreads) {
-            const int r0 = row_begin + (g % groups) * 8;
-            const int c = g / groups;
+            const int r0 = row_begin + (g / kTileN) * 8;  // lanes along the columns: conflict-free reads
+            const int c = g % kTileN;
             const int grow0 = m0 + r0;
             const int gcol = n0 + c;
             if (gcol >= t.n || grow0 >= t.m) continue;

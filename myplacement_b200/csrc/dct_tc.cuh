@@ -83,6 +83,7 @@ struct alignas(64) TcTask {
     const float* scale;
     const float* weight_r;
     const float* weight_c;
+
     double* energy_partials;  // one per CTA of the launch (tcBlocks)
 };
 

@@ -400,6 +400,7 @@ void Engine::buildTensorCoreBasis(double max_scale) {
     tc_fwd2_.task[0].out_t_ld = tc_phit_.ld;
     tc_fwd2_.task[0].out_t_plane = tc_phit_.plane();
     tc_fwd2_.task[0].scale = spectral_scale_;
+
     tc_fwd2_.task[0].weight_r = weight_y_;
     tc_fwd2_.task[0].weight_c = weight_x_;
     // T = Dy * phi_hat and U = phi_hat * Dx^T (stored transposed), one launch.
