@@ -307,23 +307,29 @@ def run_mine(args) -> None:
     if not args.no_e2e:
         e2e_options = mp.default_options(bins_x=bins, bins_y=bins, target_density=0.9, cuda_device=local,
                                          **rudy_options(args))
-        replicas.barrier()
-        t0 = time.perf_counter()
-        s2 = mp.Session(design, e2e_options)
-        while not s2.step(64)[1]:
-            pass
-        placed = s2.finish()
-        t1 = time.perf_counter()
-        h2d, d2h = s2.transfer_bytes()
-        s2.close()
+        # Three whole runs through the public API; the median one is reported (a single
+        # run of ~0.15 s is at the mercy of the shared host).
+        runs = []
+        for _ in range(3):
+            replicas.barrier()
+            t0 = time.perf_counter()
+            s2 = mp.Session(design, e2e_options)
+            while not s2.step(64)[1]:
+                pass
+            placed = s2.finish()
+            t1 = time.perf_counter()
+            h2d, d2h = s2.transfer_bytes()
+            s2.close()
+            runs.append((replicas.reduce_max(t1 - t0), placed, h2d, d2h))
+        e2e_time, placed, h2d, d2h = sorted(runs, key=lambda r: r[0])[1]
         it = placed.completed_iterations
-        e2e_time = replicas.reduce_max(t1 - t0)
         e2e_iters = replicas.reduce_sum(it)
         e2e = {"value": e2e_iters / e2e_time, "unit": "iterations/s",
                "h2d_bytes_per_step": int(h2d / max(it, 1)), "d2h_bytes_per_step": int(d2h / max(it, 1)),
-               "api": "Session create/step/finish (= GlobalPlacer.run) on host arrays, early stop on",
-               "completed_iterations": it, "seconds": t1 - t0, "hpwl_after": placed.hpwl_after,
-               "overflow_after": placed.overflow_after}
+               "api": "Session create/step/finish (= GlobalPlacer.run) on host arrays, early stop on; "
+                      "median of three runs",
+               "completed_iterations": it, "seconds": e2e_time, "seconds_of_runs": [r[0] for r in runs],
+               "hpwl_after": placed.hpwl_after, "overflow_after": placed.overflow_after}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
