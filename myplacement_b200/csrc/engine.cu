@@ -20,6 +20,7 @@
 #include <thread>
 
 #include "common.cuh"
+#include "ingest.cuh"
 
 namespace mpgp {
 
@@ -173,115 +174,42 @@ void Engine::uploadStatic(const Problem& p) {
 }
 
 void Engine::buildNetLayout(const Problem& p) {
-    const int net_count = static_cast<int>(p.net_weight.size());
+    // The bucketed layout and the particle pin lists are built on the device
+    // (ingest.cu); the host only turns the bucket sizes into the work list.
+    const NetLayout layout = buildNetLayoutOnDevice(
+        p, static_cast<int>(movable_count_),
+        [this](std::size_t bytes, const char* what) { return arena_.allocate(bytes, what); }, stream_);
+    pin_particle_ = layout.pin_particle;
+    pin_offset_ = layout.pin_offset;
+    static_pins_ = layout.static_pins;
+    net_start_ = layout.net_start;
+    net_weight_ = layout.net_weight;
+    rudy_net_weight_ = layout.net_weight64;
+    particle_pin_start_ = layout.particle_pin_start;
+    pin_slot_ = layout.pin_slot;
+    wl_net_count_ = layout.kept_nets;
+    wl_pin_count_ = layout.kept_pins;
     // Degree buckets: one thread per two-pin net, G lanes per net for degree <= G,
-    // a warp loop above 32.  Nets are ordered bucket by bucket (a stable counting
-    // sort), and every output array is sized before it is filled.
+    // a warp loop above 32.  The blocks run heaviest bucket first (one round of the
+    // block's lanes each), so the long warp-loop nets do not form the kernel's tail.
     const int kGroups[6] = {1, 4, 8, 16, 32, 0};
-    std::vector<int8_t> bucket_of(static_cast<std::size_t>(net_count), -1);
-    int bucket_nets[7] = {0, 0, 0, 0, 0, 0, 0};
-    std::size_t kept_pins = 0, kept_static = 0;
-    for (int n = 0; n < net_count; ++n) {
-        const int64_t degree = p.net_pin_start[n + 1] - p.net_pin_start[n];
-        if (degree < 2) continue;  // nets with fewer than two pins contribute nothing
-        const int b = degree <= 2 ? 0 : degree <= 4 ? 1 : degree <= 8 ? 2 : degree <= 16 ? 3 : degree <= 32 ? 4 : 5;
-        bucket_of[static_cast<std::size_t>(n)] = static_cast<int8_t>(b);
-        ++bucket_nets[b + 1];
-        kept_pins += static_cast<std::size_t>(degree);
-        for (int64_t pin = p.net_pin_start[n]; pin < p.net_pin_start[n + 1]; ++pin) {
-            if (p.pin_particle[pin] < 0) ++kept_static;
-        }
-    }
-    for (int b = 0; b < 6; ++b) bucket_nets[b + 1] += bucket_nets[b];
-    const int kept_nets = bucket_nets[6];
-    std::vector<int> order(static_cast<std::size_t>(kept_nets));
-    {
-        int next[6];
-        for (int b = 0; b < 6; ++b) next[b] = bucket_nets[b];
-        for (int n = 0; n < net_count; ++n) {
-            const int b = bucket_of[static_cast<std::size_t>(n)];
-            if (b >= 0) order[static_cast<std::size_t>(next[b]++)] = n;
-        }
-    }
-    std::vector<int> pin_particle(kept_pins);
-    std::vector<float2> pin_offset(kept_pins);
-    std::vector<double2> static_pins(kept_static);
-    std::vector<int> net_start(static_cast<std::size_t>(kept_nets) + 1);
-    std::vector<float> net_weight(static_cast<std::size_t>(kept_nets));
-    bucket_net_weight_.assign(static_cast<std::size_t>(kept_nets), 0.0);
-    std::size_t write = 0, write_static = 0;
-    net_start[0] = 0;
-    for (int k = 0; k < kept_nets; ++k) {
-        const int n = order[static_cast<std::size_t>(k)];
-        for (int64_t pin = p.net_pin_start[n]; pin < p.net_pin_start[n + 1]; ++pin, ++write) {
-            const int particle = p.pin_particle[pin];
-            if (particle >= 0) {
-                pin_particle[write] = particle;
-                pin_offset[write] = make_float2(static_cast<float>(p.pin_x[pin]), static_cast<float>(p.pin_y[pin]));
-            } else {
-                pin_particle[write] = -static_cast<int>(write_static) - 1;
-                pin_offset[write] = make_float2(0.0f, 0.0f);
-                static_pins[write_static++] = make_double2(p.pin_x[pin], p.pin_y[pin]);
-            }
-        }
-        net_start[static_cast<std::size_t>(k) + 1] = static_cast<int>(write);
-        net_weight[static_cast<std::size_t>(k)] = static_cast<float>(p.net_weight[n]);
-        bucket_net_weight_[static_cast<std::size_t>(k)] = p.net_weight[n];
-    }
-    // Pins and nets are laid out bucket by bucket; the blocks run heaviest bucket
-    // first (one round of the block's lanes each), so the long warp-loop nets do
-    // not form the kernel's tail.
     std::vector<int4> work;
     for (int b = 5; b >= 0; --b) {
         const int group = kGroups[b];
         const int nets_per_block = group == 0 ? kThreads / 32 : group == 1 ? kThreads : kThreads / group;
-        const int first_net = bucket_nets[b];
-        const int count = bucket_nets[b + 1] - bucket_nets[b];
+        const int first_net = layout.bucket_first[b];
+        const int count = layout.bucket_first[b + 1] - layout.bucket_first[b];
         for (int off = 0; off < count; off += nets_per_block) {
             work.push_back(make_int4(group, first_net + off, std::min(nets_per_block, count - off), 0));
         }
     }
     wl_blocks_ = static_cast<int>(work.size());
-    wl_net_count_ = static_cast<int>(net_weight.size());
-    wl_pin_count_ = static_cast<int>(pin_particle.size());
-    const std::size_t pins = std::max<std::size_t>(1, pin_particle.size());
-    pin_particle_ = arena_.array<int>(pins, "pin particles");
-    pin_offset_ = arena_.array<float2>(pins, "pin offsets");
-    static_pins_ = arena_.array<double2>(std::max<std::size_t>(1, static_pins.size()), "static pins");
-    net_start_ = arena_.array<int>(net_start.size(), "net offsets");
-    net_weight_ = arena_.array<float>(std::max<std::size_t>(1, net_weight.size()), "net weights");
+    const std::size_t pins = std::max<std::size_t>(1, static_cast<std::size_t>(layout.kept_pins));
     block_work_ = arena_.array<int4>(std::max<std::size_t>(1, work.size()), "wirelength work");
     pin_gradient_ = arena_.array<float2>(pins, "pin gradients");
     partials_wl_ = arena_.array<double>(2 * std::max<std::size_t>(1, work.size()), "wirelength partials");
-    upload(pin_particle_, pin_particle, stream_);
-    upload(pin_offset_, pin_offset, stream_);
-    upload(static_pins_, static_pins, stream_);
-    upload(net_start_, net_start, stream_);
-    upload(net_weight_, net_weight, stream_);
     upload(block_work_, work, stream_);
     checkCuda(cudaMemsetAsync(pin_gradient_, 0, pins * sizeof(float2), stream_), "clear pin gradients");
-
-    // Particle-ordered gradient slots: particle i's pins (ascending bucketed pin
-    // index) own slots count[i] .. count[i + 1] - 1, so the gather reads one
-    // contiguous range per particle in a fixed order.
-    const std::size_t movable = static_cast<std::size_t>(movable_count_);
-    std::vector<int> count(movable + 1, 0);
-    for (std::size_t i = 0; i < pin_particle.size(); ++i) {
-        const int particle = pin_particle[i];
-        require(particle < 0 || static_cast<std::size_t>(particle) < movable, "A pin refers to a non-movable particle.");
-        if (particle >= 0) ++count[particle + 1];
-    }
-    for (std::size_t i = 0; i < movable; ++i) count[i + 1] += count[i];
-    std::vector<int> slot(pin_particle.size(), -1);
-    std::vector<int> fill(count.begin(), count.end() - 1);
-    for (std::size_t i = 0; i < pin_particle.size(); ++i) {
-        const int particle = pin_particle[i];
-        if (particle >= 0) slot[i] = fill[particle]++;
-    }
-    particle_pin_start_ = arena_.array<int>(count.size(), "particle pin offsets");
-    pin_slot_ = arena_.array<int>(std::max<std::size_t>(1, slot.size()), "pin gradient slots");
-    upload(particle_pin_start_, count, stream_);
-    upload(pin_slot_, slot, stream_);
     checkCuda(cudaStreamSynchronize(stream_), "net layout upload");
 }
 
@@ -864,8 +792,6 @@ void Engine::enableRudy(const mpgp_options& o) {
     if (o.rudy_validation_bins > 0) {
         allocateRudyGrid(rudy_validation_, o.rudy_validation_bins, o.rudy_validation_bins, "RUDY validation maps");
     }
-    rudy_net_weight_ = arena_.array<double>(std::max<std::size_t>(1, bucket_net_weight_.size()), "RUDY net weights");
-    upload(rudy_net_weight_, bucket_net_weight_, stream_);
     rudy_pin_gradient_ =
         arena_.array<double2>(std::max<std::size_t>(1, static_cast<std::size_t>(wl_pin_count_)), "RUDY pin gradients");
     rudy_scalars_ = arena_.array<double>(5, "RUDY scalars");

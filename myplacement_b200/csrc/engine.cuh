@@ -189,7 +189,6 @@ private:
     double2* rudy_pin_gradient_ = nullptr;
     double* rudy_scalars_ = nullptr;
     double* host_rudy_ = nullptr;
-    std::vector<double> bucket_net_weight_;
     int wl_net_count_ = 0;
     int wl_pin_count_ = 0;
 
