@@ -83,7 +83,7 @@ __device__ void netPairs(const WirelengthArgs& a, int first, int count, double& 
     const int local = static_cast<int>(threadIdx.x);
     if (local >= count) return;  // the caller's block reduction follows; every thread still reaches it
     const int net = first + local;
-    const int begin = a.net_start[net];
+    const int begin = 2 * net;  // two-pin nets lead the layout: net k's pins are 2k and 2k + 1
     const PinPoint p = loadPin(a, begin);
     const PinPoint q = loadPin(a, begin + 1);
     const float weight = a.net_weight[net];
