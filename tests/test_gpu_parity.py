@@ -130,6 +130,24 @@ def test_evaluation_parity_against_reference_session(gpu, ref, name, scale):
     assert _rel(ev["density_gradient"], comp["density_gradient"]) <= GRADIENT_TOL
 
 
+def test_wide_grid_evaluation_matches_reference(gpu, ref):
+    """A grid wider than the fused metrics-and-split pass takes (4096 x 8 bins): the
+    separate metrics and source-split kernels, against the reference session."""
+    design, _ = _session_case(ref, "small_5k", 1.0)
+    bins_x, bins_y = 4096, 8
+    session = ref.session(design, ref_options(bins_x=bins_x, bins_y=bins_y, target_density=0.9))
+    layout = mp.build_layout(design, session.width, session.height, session.layer, session.pin_count,
+                             session.movable_count, bins_x, bins_y, 0.9, *session.static_density())
+    backend, reason = mp.try_create_backend(layout, 0)
+    assert backend is not None, reason
+    smoothing = 0.75 * max((design.core[2] - design.core[0]) / bins_x, (design.core[3] - design.core[1]) / bins_y)
+    comp = session.components(session.positions, smoothing)
+    ev = backend.evaluate(session.positions, smoothing, True)
+    assert ev["electrostatic_energy"] == pytest.approx(comp["energy"], rel=SCALAR_TOL)
+    assert _rel(ev["density_gradient"], comp["density_gradient"]) <= GRADIENT_TOL
+    assert _rel(ev["wire_gradient"], comp["wire_gradient"]) <= GRADIENT_TOL
+
+
 def _nudged(design: Design, bins: int, k: int) -> Design:
     """The same placement with every movable centre moved by at most 1e-6 bin widths."""
     rng = np.random.default_rng(1000 + k)
