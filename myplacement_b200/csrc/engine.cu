@@ -178,7 +178,8 @@ void Engine::buildNetLayout(const Problem& p) {
     // (ingest.cu); the host only turns the bucket sizes into the work list.
     const NetLayout layout = buildNetLayoutOnDevice(
         p, static_cast<int>(movable_count_),
-        [this](std::size_t bytes, const char* what) { return arena_.allocate(bytes, what); }, stream_);
+        [this](std::size_t bytes, const char* what) { return arena_.allocate(bytes, what); },
+        [this]() { return arena_.headroom(); }, stream_);
     pin_particle_ = layout.pin_particle;
     pin_offset_ = layout.pin_offset;
     static_pins_ = layout.static_pins;

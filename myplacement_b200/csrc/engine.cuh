@@ -29,6 +29,7 @@ public:
         return static_cast<T*>(allocate(count * sizeof(T), what));
     }
     [[nodiscard]] uint64_t reserved() const { return reserved_; }
+    [[nodiscard]] uint64_t headroom() const { return limit_ - std::min(limit_, reserved_); }
 
 private:
     uint64_t limit_;

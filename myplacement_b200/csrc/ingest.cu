@@ -111,24 +111,36 @@ int bitsFor(int value) {
     return bits;
 }
 
-// Stream-ordered scratch, released when the ingest returns.
+// Stream-ordered scratch, released when the ingest returns.  While it lives it
+// counts against the engine's device-memory budget like the lasting arrays.
 class Scratch {
 public:
-    explicit Scratch(cudaStream_t stream) : stream_(stream) {}
+    Scratch(cudaStream_t stream, const BudgetHeadroom& headroom) : stream_(stream), headroom_(headroom) {}
     ~Scratch() {
         for (void* p : blocks_) cudaFreeAsync(p, stream_);
     }
+    // Fails unless `bytes` more fit in the budget beside the scratch held now.
+    void check(std::size_t bytes) const {
+        if (held_ + bytes > headroom_()) {
+            fail(MPGP_ERR_BUDGET, "CUDA allocation budget exceeded while ingesting the design.");
+        }
+    }
     template <typename T>
     T* array(std::size_t count) {
+        const std::size_t bytes = std::max<std::size_t>(1, count) * sizeof(T);
+        check(bytes);
         void* p = nullptr;
-        checkCuda(cudaMallocAsync(&p, std::max<std::size_t>(1, count) * sizeof(T), stream_), "ingest scratch");
+        checkCuda(cudaMallocAsync(&p, bytes, stream_), "ingest scratch");
         blocks_.push_back(p);
+        held_ += bytes;
         return static_cast<T*>(p);
     }
 
 private:
     cudaStream_t stream_;
+    const BudgetHeadroom& headroom_;
     std::vector<void*> blocks_;
+    uint64_t held_ = 0;
 };
 
 template <typename T>
@@ -141,12 +153,17 @@ void uploadVector(T* device, const std::vector<T>& host, cudaStream_t stream) {
 
 }  // namespace
 
-NetLayout buildNetLayoutOnDevice(const Problem& p, int movable, const DeviceAllocator& allocate,
-                                 cudaStream_t stream) {
+NetLayout buildNetLayoutOnDevice(const Problem& p, int movable, const DeviceAllocator& lasting,
+                                 const BudgetHeadroom& headroom, cudaStream_t stream) {
     const int nets = static_cast<int>(p.net_weight.size());
     const int pins_in = static_cast<int>(p.pin_particle.size());
     NetLayout out;
-    Scratch scratch(stream);
+    Scratch scratch(stream, headroom);
+    // The layout's lasting arrays, checked against the budget beside the scratch.
+    const auto allocate = [&](std::size_t bytes, const char* what) {
+        scratch.check(bytes);
+        return lasting(bytes, what);
+    };
 
     // The flat CSR on the device.
     long long* net_pin_start = scratch.array<long long>(static_cast<std::size_t>(nets) + 1);

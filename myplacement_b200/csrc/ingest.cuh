@@ -13,6 +13,8 @@ namespace mpgp {
 
 // Device memory for the layout's lasting arrays (the engine's budgeted arena).
 using DeviceAllocator = std::function<void*(std::size_t bytes, const char* what)>;
+// Bytes the budget still allows (transient scratch counts against it while it lives).
+using BudgetHeadroom = std::function<uint64_t()>;
 
 struct NetLayout {
     int kept_nets = 0;            // nets with two or more pins, in bucket order
@@ -30,6 +32,6 @@ struct NetLayout {
 };
 
 NetLayout buildNetLayoutOnDevice(const Problem& problem, int movable, const DeviceAllocator& allocate,
-                                 cudaStream_t stream);
+                                 const BudgetHeadroom& headroom, cudaStream_t stream);
 
 }  // namespace mpgp

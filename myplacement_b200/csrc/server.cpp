@@ -60,8 +60,10 @@ uint64_t estimateSessionBytes(const mpgp_design& design, const mpgp_options& opt
     const uint64_t split = 4ull * 3ull * (nx * ldx + ny * ldy + ny * ldx + nx * ldy);
     // 12 session vectors + sizes, charge, preconditioner, layer, upload scratch (per particle);
     // particle, offset, slot, gradient and a possible static copy (per pin); CSR, weight,
-    // work and partials (per net); layers, static charge, source, scale, field, potential (per bin).
-    const uint64_t bytes = 256ull * particles + 40ull * pins + 16ull * nets + 64ull * bins + split;
+    // work and partials (per net); layers, static charge, source, scale, field, potential (per bin);
+    // and the set-up's transient sorting and scanning scratch (per pin and per net), which
+    // is freed before the iterations start but must fit while it lives.
+    const uint64_t bytes = 256ull * particles + (40ull + 80ull) * pins + (16ull + 48ull) * nets + 64ull * bins + split;
     return bytes + (256ull << 10) /* partials, scalars, rounding of ~60 allocations */;
 }
 
