@@ -83,10 +83,28 @@ __device__ void netPairs(const WirelengthArgs& a, int first, int count, double& 
     const int local = static_cast<int>(threadIdx.x);
     if (local >= count) return;  // the caller's block reduction follows; every thread still reaches it
     const int net = first + local;
-    const int begin = 2 * net;  // two-pin nets lead the layout: net k's pins are 2k and 2k + 1
-    const PinPoint p = loadPin(a, begin);
-    const PinPoint q = loadPin(a, begin + 1);
+    // Two-pin nets lead the layout: net k's pins are 2k and 2k + 1, so each of the
+    // pin arrays is read as one vector (the arrays start 256-byte aligned).
+    const int2 particle = reinterpret_cast<const int2*>(a.pin_particle)[net];
+    const float4 offset = reinterpret_cast<const float4*>(a.pin_offset)[net];
+    const int2 slot = a.gradient ? reinterpret_cast<const int2*>(a.pin_slot)[net] : make_int2(0, 0);
     const float weight = a.net_weight[net];
+    const auto place = [&](int index, float ox, float oy) {
+        PinPoint pin;
+        pin.particle = index;
+        if (index >= 0) {
+            const double2 c = a.positions[index];
+            pin.x = c.x + static_cast<double>(ox);
+            pin.y = c.y + static_cast<double>(oy);
+        } else {
+            const double2 s = a.static_pins[-index - 1];
+            pin.x = s.x;
+            pin.y = s.y;
+        }
+        return pin;
+    };
+    const PinPoint p = place(particle.x, offset.x, offset.y);
+    const PinPoint q = place(particle.y, offset.z, offset.w);
     const float dx = static_cast<float>(p.x - q.x);
     const float dy = static_cast<float>(p.y - q.y);
     const float ax = fabsf(dx), ay = fabsf(dy);
@@ -99,8 +117,8 @@ __device__ void netPairs(const WirelengthArgs& a, int first, int count, double& 
     if (a.gradient) {
         const float gx = copysignf(weight * __fdividef(1.0f - tx, 1.0f + tx), dx);
         const float gy = copysignf(weight * __fdividef(1.0f - ty, 1.0f + ty), dy);
-        if (p.particle >= 0) a.pin_gradient[a.pin_slot[begin]] = make_float2(gx, gy);
-        if (q.particle >= 0) a.pin_gradient[a.pin_slot[begin + 1]] = make_float2(-gx, -gy);
+        if (p.particle >= 0) a.pin_gradient[slot.x] = make_float2(gx, gy);
+        if (q.particle >= 0) a.pin_gradient[slot.y] = make_float2(-gx, -gy);
     }
 }
 
