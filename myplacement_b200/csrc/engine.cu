@@ -111,6 +111,15 @@ Engine::~Engine() {
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
 }
 
+void Engine::newParticleArrays(int count, double2** out, const char* what) {
+    // Each array starts on a 256-byte boundary, like a separate allocation would.
+    const std::size_t stride = ((static_cast<std::size_t>(std::max<int64_t>(1, particle_count_)) * sizeof(double2) +
+                                 255) / 256) * 256 / sizeof(double2);
+    double2* base = arena_.array<double2>(stride * static_cast<std::size_t>(count), what);
+    checkCuda(cudaMemsetAsync(base, 0, stride * static_cast<std::size_t>(count) * sizeof(double2), stream_), what);
+    for (int k = 0; k < count; ++k) out[k] = base + stride * static_cast<std::size_t>(k);
+}
+
 double2* Engine::newParticleArray(const char* what) {
     double2* p = arena_.array<double2>(static_cast<std::size_t>(std::max<int64_t>(1, particle_count_)), what);
     checkCuda(cudaMemsetAsync(p, 0, sizeof(double2) * std::max<int64_t>(1, particle_count_), stream_), what);

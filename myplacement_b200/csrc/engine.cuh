@@ -141,6 +141,8 @@ public:
     [[nodiscard]] double2* scratchPositions() const { return scratch_positions_; }
 
     [[nodiscard]] double2* newParticleArray(const char* what);
+    // `count` zeroed particle arrays from one allocation: out[k] = base + k * stride.
+    void newParticleArrays(int count, double2** out, const char* what);
     [[nodiscard]] cudaStream_t stream() const { return stream_; }
     [[nodiscard]] int device() const { return device_; }
     [[nodiscard]] uint64_t reservedBytes() const { return arena_.reserved(); }

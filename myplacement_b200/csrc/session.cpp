@@ -131,18 +131,22 @@ Session::Session(const mpgp_design& design, const mpgp_options& options) : optio
     min_bin_ = std::min(bin_w, bin_h);
     max_bin_ = std::max(bin_w, bin_h);
 
-    cur_ = engine_->newParticleArray("current positions");
-    look_ = engine_->newParticleArray("lookahead positions");
-    cand_ = engine_->newParticleArray("candidate positions");
-    prev_pos_ = engine_->newParticleArray("previous positions");
-    velocity_ = engine_->newParticleArray("velocity");
-    raw_cur_ = engine_->newParticleArray("raw gradient");
-    pre_cur_ = engine_->newParticleArray("preconditioned gradient");
-    raw_look_ = engine_->newParticleArray("lookahead raw gradient");
-    pre_look_ = engine_->newParticleArray("lookahead preconditioned gradient");
-    prev_grad_ = engine_->newParticleArray("previous gradient");
-    best_feasible_.positions = engine_->newParticleArray("best feasible checkpoint");
-    best_fallback_.positions = engine_->newParticleArray("best fallback checkpoint");
+    // The controller's twelve particle vectors (positions, lookahead, candidate, previous,
+    // velocity, the gradients and the two checkpoints), from one allocation.
+    double2* vectors[12] = {};
+    engine_->newParticleArrays(12, vectors, "controller vectors");
+    cur_ = vectors[0];
+    look_ = vectors[1];
+    cand_ = vectors[2];
+    prev_pos_ = vectors[3];
+    velocity_ = vectors[4];
+    raw_cur_ = vectors[5];
+    pre_cur_ = vectors[6];
+    raw_look_ = vectors[7];
+    pre_look_ = vectors[8];
+    prev_grad_ = vectors[9];
+    best_feasible_.positions = vectors[10];
+    best_fallback_.positions = vectors[11];
     result_.cuda_reserved_memory_bytes = engine_->reservedBytes();
 
     // capturePositions (AdaptiveGlobalPlacer.cpp:174-183): movable centres, then fillers.

@@ -11,6 +11,7 @@
 #include <numeric>
 #include <random>
 #include <string>
+#include <thread>
 
 #include "common.cuh"
 
@@ -356,6 +357,40 @@ Problem buildProblem(const mpgp_design& d, const DerivedDesign& derived, const m
     problem.bins_y = options.bins_y;
     problem.region = derived.core;
     problem.target_density = options.target_density;
+    // The pin CSR (buildHostLayout, CudaPlacementBackend.cu:815-837) depends only on
+    // the movable list, so a second thread forms it while this one builds the static
+    // layers, the fillers and the particle arrays.
+    std::vector<int32_t> module_particle(static_cast<std::size_t>(d.module_count), -1);
+    for (std::size_t index = 0; index < derived.movable.size(); ++index) {
+        module_particle[derived.movable[index]] = static_cast<int32_t>(index);
+    }
+    problem.net_weight.assign(d.net_weight, d.net_weight + d.net_count);
+    problem.net_pin_start.assign(d.net_pin_start, d.net_pin_start + d.net_count + 1);
+    problem.pin_particle.resize(static_cast<std::size_t>(d.pin_count));
+    problem.pin_x.resize(static_cast<std::size_t>(d.pin_count));
+    problem.pin_y.resize(static_cast<std::size_t>(d.pin_count));
+    std::thread pins([&] {
+        for (int64_t p = 0; p < d.pin_count; ++p) {
+            const int32_t m = d.pin_module[p];
+            double ox, oy;
+            transformOffset(d.pin_offset_x[p], d.pin_offset_y[p], orientationOf(d, m), ox, oy);
+            const int32_t particle = module_particle[m];
+            problem.pin_particle[p] = particle;
+            if (particle >= 0) {
+                problem.pin_x[p] = ox;
+                problem.pin_y[p] = oy;
+            } else {
+                problem.pin_x[p] = d.module_x[m] + ox;  // pinPosition (PlacementDatabase.cpp:138-142)
+                problem.pin_y[p] = d.module_y[m] + oy;
+            }
+        }
+    });
+    struct Join {
+        std::thread& t;
+        ~Join() {
+            if (t.joinable()) t.join();
+        }
+    } join{pins};
     staticDensity(d, derived, options.bins_x, options.bins_y, options.target_density, problem.static_fixed,
                   problem.static_dark);
     fillers = createFillers(d, derived, problem.static_fixed, problem.static_dark, options.bins_x, options.bins_y,
@@ -373,10 +408,8 @@ Problem buildProblem(const mpgp_design& d, const DerivedDesign& derived, const m
     problem.charge.reserve(particles);
     problem.pin_count.reserve(particles);
     const double t = options.target_density;
-    std::vector<int32_t> module_particle(static_cast<std::size_t>(d.module_count), -1);
     for (std::size_t index = 0; index < movable; ++index) {
         const int32_t m = derived.movable[index];
-        module_particle[m] = static_cast<int32_t>(index);
         problem.width.push_back(d.module_width[m]);
         problem.height.push_back(d.module_height[m]);
         problem.layer.push_back(derived.is_macro[m] ? MPGP_LAYER_MACRO : MPGP_LAYER_STANDARD);
@@ -406,26 +439,7 @@ Problem buildProblem(const mpgp_design& d, const DerivedDesign& derived, const m
         problem.precond_base.push_back(1.0 / (pin_factor * area_factor));
     }
 
-    // buildHostLayout pin CSR (CudaPlacementBackend.cu:815-837).
-    problem.net_weight.assign(d.net_weight, d.net_weight + d.net_count);
-    problem.net_pin_start.assign(d.net_pin_start, d.net_pin_start + d.net_count + 1);
-    problem.pin_particle.resize(static_cast<std::size_t>(d.pin_count));
-    problem.pin_x.resize(static_cast<std::size_t>(d.pin_count));
-    problem.pin_y.resize(static_cast<std::size_t>(d.pin_count));
-    for (int64_t p = 0; p < d.pin_count; ++p) {
-        const int32_t m = d.pin_module[p];
-        double ox, oy;
-        transformOffset(d.pin_offset_x[p], d.pin_offset_y[p], orientationOf(d, m), ox, oy);
-        const int32_t particle = module_particle[m];
-        problem.pin_particle[p] = particle;
-        if (particle >= 0) {
-            problem.pin_x[p] = ox;
-            problem.pin_y[p] = oy;
-        } else {
-            problem.pin_x[p] = d.module_x[m] + ox;  // pinPosition (PlacementDatabase.cpp:138-142)
-            problem.pin_y[p] = d.module_y[m] + oy;
-        }
-    }
+    pins.join();
     return problem;
 }
 
