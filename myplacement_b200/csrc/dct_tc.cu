@@ -17,9 +17,9 @@
 // exponents follow the data: the source gets one exponent per row, every later
 // stage a bound from the measured maximum of its input (TcScales).
 //
-// A 128 x kTileN output tile is computed by a cluster of `ksplit` CTAs, each
-// owning a contiguous share of the K-blocks, so that a 512 x 512 contraction
-// (32 tiles) still occupies ~128 SMs.  Per CTA, six warps:
+// A 128 x kTileN output tile is computed by a cluster of `ksplit` (at most
+// kMaxSplit) CTAs, each owning a contiguous share of the K-blocks, so that a
+// 512 x 512 contraction (32 tiles) spreads over more SMs.  Per CTA, six warps:
 //   warp 0 lane 0  TMA producer: K-blocks of 64 elements of both planes of A
 //                  and B into a kStages-deep shared-memory ring (3-D tensor
 //                  maps: K, rows, plane; 128-byte swizzle; zero fill past edges).
@@ -761,7 +761,7 @@ int tcBlocks(const TcBatch& batch, int task_count) {
 void launchTcGemm(const TcBatch& batch, int task_count, cudaStream_t stream) {
     configureKernel();
     require(batch.ksplit >= 1 && batch.ksplit <= kMaxSplit && (batch.ksplit & (batch.ksplit - 1)) == 0,
-            "Contraction K split must be a power of two up to 8.");
+            "Contraction K split must be a power of two up to kMaxSplit.");
     cudaLaunchAttribute attribute[2] = {};
     const cudaLaunchConfig_t config =
         launchConfig(dim3(static_cast<unsigned>(tcBlocks(batch, task_count)), static_cast<unsigned>(task_count)),
