@@ -16,6 +16,7 @@
  *     stream owned by the handle.
  *   - Status codes map onto the reference's error conventions:
  *     MPGP_ERR_INVALID_ARGUMENT  <-> std::invalid_argument
+ *     MPGP_ERR_PARSE             <-> myplacement::ParseError (BookShelf input)
  *     MPGP_ERR_RUNTIME / _CUDA / _NON_FINITE / _BUDGET <-> std::runtime_error
  *     MPGP_ERR_UNAVAILABLE       <-> tryCreateCudaPlacementBackend returning
  *                                    nullptr with a populated reason.
@@ -40,7 +41,8 @@ enum {
     MPGP_ERR_BUDGET = 4,
     MPGP_ERR_NON_FINITE = 5,
     MPGP_ERR_UNAVAILABLE = 6,
-    MPGP_ERR_TIMEOUT = 7
+    MPGP_ERR_TIMEOUT = 7,
+    MPGP_ERR_PARSE = 8
 };
 
 /* Module flag bits (PlacementDatabase.hpp Module::is_terminal / is_fixed). */
@@ -360,6 +362,39 @@ int mpgp_wirelength_noalloc(const double* positions, const int32_t* net_pin_star
                             const int32_t* particle_pin_start, const int32_t* particle_pins,
                             int32_t particle_count, double smoothing, double* wire_gradient, double* totals,
                             void* stream);
+
+/* ---- BookShelf input ----------------------------------------------------------- */
+
+/* BookshelfParser::parseAux (include/myplacement/io/BookshelfParser.hpp:16-19;
+ * src/io/BookshelfParser.cpp:313-348 with the readers of :62-278 and
+ * validateCounts :280-299): reads the design an .aux file names (.nodes, .scl,
+ * .pl, .nets, and .wts when present) into a flattened PlacementDatabase.  The
+ * records, values and error texts are the reference reader's, and so is which
+ * error comes first; its ParseError is MPGP_ERR_PARSE and the database's
+ * std::invalid_argument (duplicate names, negative sizes) is
+ * MPGP_ERR_INVALID_ARGUMENT.  The files are read whole and parsed by `threads`
+ * host threads (<= 0: one per hardware thread); the result does not depend on
+ * the thread count.  No GPU is used. */
+typedef struct mpgp_bookshelf mpgp_bookshelf;
+
+typedef struct mpgp_bookshelf_view {
+    mpgp_design design;               /* arrays owned by the handle; module_orientation is set */
+    const char* module_names;         /* the names back to back, no separators */
+    const int64_t* module_name_start; /* module_count + 1 offsets into module_names */
+    const char* net_names;
+    const int64_t* net_name_start;    /* net_count + 1 offsets into net_names */
+    const int8_t* pin_direction;      /* PinDirection order: 0 input, 1 output, 2 bidirectional, 3 unknown */
+    const int32_t* row_orientation;   /* Orientation order, 8 = unknown */
+    int64_t declared_nodes;           /* NumNodes, NumTerminals, NumNets, NumPins as declared; -1 if absent */
+    int64_t declared_terminals;
+    int64_t declared_nets;
+    int64_t declared_pins;
+} mpgp_bookshelf_view;
+
+int mpgp_bookshelf_read(const char* aux_path, int32_t threads, mpgp_bookshelf** out);
+/* Pointers into the handle, valid until mpgp_bookshelf_destroy. */
+int mpgp_bookshelf_get(const mpgp_bookshelf* book, mpgp_bookshelf_view* view);
+void mpgp_bookshelf_destroy(mpgp_bookshelf* book);
 
 /* ---- host setup restated from the reference ----------------------------------- */
 

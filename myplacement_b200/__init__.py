@@ -5,14 +5,16 @@ hand-written sm_100a CUDA kernels); this package is its host-side mirror of the
 reference's GlobalPlacer / CudaPlacementBackend interface plus the seeded
 synthetic designs the engine is measured on.
 """
-from ._abi import EngineError, load_library
+from ._abi import EngineError, ParseError, load_library
+from .bookshelf import BookshelfParser, read_bookshelf, write_bookshelf
 from .design import Design, synthetic_design, workload
 from .placer import (BackendLayout, CudaPlacementBackend, GlobalPlacer, PlacementResult, PlacementServer, Session,
                      batch_place, build_layout, default_options, estimate_bytes, host_setup, random_placement,
                      try_create_backend)
 
 __all__ = [
-    "BackendLayout", "CudaPlacementBackend", "Design", "EngineError", "GlobalPlacer", "PlacementResult",
-    "PlacementServer", "Session", "batch_place", "build_layout", "estimate_bytes", "default_options", "host_setup", "load_library", "random_placement", "synthetic_design", "try_create_backend",
-    "workload",
+    "BackendLayout", "BookshelfParser", "CudaPlacementBackend", "Design", "EngineError", "GlobalPlacer",
+    "ParseError", "PlacementResult", "PlacementServer", "Session", "batch_place", "build_layout", "estimate_bytes",
+    "default_options", "host_setup", "load_library", "random_placement", "read_bookshelf", "synthetic_design",
+    "try_create_backend", "workload", "write_bookshelf",
 ]

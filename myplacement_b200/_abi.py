@@ -21,6 +21,7 @@ MPGP_ERR_BUDGET = 4
 MPGP_ERR_NON_FINITE = 5
 MPGP_ERR_UNAVAILABLE = 6
 MPGP_ERR_TIMEOUT = 7
+MPGP_ERR_PARSE = 8
 
 MODULE_TERMINAL = 1
 MODULE_FIXED = 2
@@ -56,6 +57,22 @@ class Design(C.Structure):
         ("row_site_spacing", _d),
         ("row_x_start", _d),
         ("row_site_count", _i64),
+    ]
+
+
+class BookshelfView(C.Structure):
+    _fields_ = [
+        ("design", Design),
+        ("module_names", C.c_void_p),
+        ("module_name_start", _i64),
+        ("net_names", C.c_void_p),
+        ("net_name_start", _i64),
+        ("pin_direction", C.POINTER(C.c_int8)),
+        ("row_orientation", _i32),
+        ("declared_nodes", C.c_int64),
+        ("declared_terminals", C.c_int64),
+        ("declared_nets", C.c_int64),
+        ("declared_pins", C.c_int64),
     ]
 
 
@@ -287,6 +304,9 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "mpgp_backend_field_solve": (C.c_int, [vp, _d, _d, _d, _d]),
         "mpgp_backend_rudy": (C.c_int, [vp, C.POINTER(Options), _d, C.c_double, C.c_double, C.c_int, _d, _d, _d]),
         "mpgp_random_placement": (C.c_int, [C.POINTER(Design), C.c_uint64, _d, _d]),
+        "mpgp_bookshelf_read": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(vp)]),
+        "mpgp_bookshelf_get": (C.c_int, [vp, C.POINTER(BookshelfView)]),
+        "mpgp_bookshelf_destroy": (None, [vp]),
         "mpgp_wirelength_noalloc": (C.c_int, [vp, vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, C.c_int32,
                                               C.c_double, vp, vp, vp]),
         "mpgp_global_place": (C.c_int, [C.POINTER(Design), C.POINTER(Options), _d, _d, C.POINTER(Result),
@@ -351,6 +371,11 @@ class EngineError(RuntimeError):
         self.status = status
 
 
+class ParseError(EngineError):
+    """Malformed BookShelf input: the reference's myplacement::ParseError."""
+
+
 def check(status: int) -> None:
     if status != MPGP_OK:
-        raise EngineError(status, load_library().mpgp_last_error().decode(errors="replace"))
+        message = load_library().mpgp_last_error().decode(errors="replace")
+        raise (ParseError if status == MPGP_ERR_PARSE else EngineError)(status, message)

@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "bookshelf.hpp"
 #include "common.cuh"
 #include "engine.cuh"
 #include "mpgp.h"
@@ -62,6 +63,10 @@ struct mpgp_session {
 
 struct mpgp_server {
     std::unique_ptr<mpgp::Server> server;
+};
+
+struct mpgp_bookshelf {
+    mpgp::Bookshelf book;
 };
 
 struct mpgp_setup {
@@ -289,6 +294,58 @@ int mpgp_wirelength_noalloc(const double* positions, const int32_t* net_pin_star
         mpgp::launchWirelengthNoAlloc(args);
     });
 }
+
+int mpgp_bookshelf_read(const char* aux_path, int32_t threads, mpgp_bookshelf** out) {
+    return guarded([&] {
+        mpgp::require(aux_path != nullptr && out != nullptr, "Arguments are required.");
+        *out = nullptr;
+        auto b = std::make_unique<mpgp_bookshelf>();
+        b->book = mpgp::readBookshelf(aux_path, threads);
+        *out = b.release();
+    });
+}
+
+int mpgp_bookshelf_get(const mpgp_bookshelf* b, mpgp_bookshelf_view* view) {
+    return guarded([&] {
+        mpgp::require(b != nullptr && view != nullptr, "Arguments are required.");
+        const mpgp::Bookshelf& k = b->book;
+        *view = mpgp_bookshelf_view{};
+        mpgp_design& d = view->design;
+        d.module_count = static_cast<int32_t>(k.width.size());
+        d.module_width = k.width.data();
+        d.module_height = k.height.data();
+        d.module_x = k.x.data();
+        d.module_y = k.y.data();
+        d.module_flags = k.flags.data();
+        d.module_orientation = k.orientation.data();
+        d.net_count = static_cast<int32_t>(k.net_weight.size());
+        d.net_weight = k.net_weight.data();
+        d.net_pin_start = k.net_pin_start.data();
+        d.pin_count = static_cast<int64_t>(k.pin_module.size());
+        d.pin_module = k.pin_module.data();
+        d.pin_offset_x = k.pin_offset_x.data();
+        d.pin_offset_y = k.pin_offset_y.data();
+        d.row_count = static_cast<int32_t>(k.row_bottom.size());
+        d.row_bottom = k.row_bottom.data();
+        d.row_height = k.row_height.data();
+        d.row_site_width = k.row_site_width.data();
+        d.row_site_spacing = k.row_site_spacing.data();
+        d.row_x_start = k.row_x_start.data();
+        d.row_site_count = k.row_site_count.data();
+        view->module_names = k.module_names.data();
+        view->module_name_start = k.module_name_start.data();
+        view->net_names = k.net_names.data();
+        view->net_name_start = k.net_name_start.data();
+        view->pin_direction = k.pin_direction.data();
+        view->row_orientation = k.row_orientation.data();
+        view->declared_nodes = k.declared[0];
+        view->declared_terminals = k.declared[1];
+        view->declared_nets = k.declared[2];
+        view->declared_pins = k.declared[3];
+    });
+}
+
+void mpgp_bookshelf_destroy(mpgp_bookshelf* b) { delete b; }
 
 int mpgp_random_placement(const mpgp_design* design, uint64_t seed, double* module_x, double* module_y) {
     return guarded([&] {

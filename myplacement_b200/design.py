@@ -45,6 +45,9 @@ class Design:
     row_site_count: np.ndarray
     module_orientation: np.ndarray | None = None
     name: str = "design"
+    # Names, pin directions, row orientations and declared counts of a design
+    # read from BookShelf files (myplacement_b200.bookshelf.BookshelfInfo).
+    bookshelf: object | None = None
     _keep: list = field(default_factory=list, repr=False)
 
     def __post_init__(self) -> None:
@@ -125,7 +128,7 @@ class Design:
     # ---- persistence -----------------------------------------------------------------
     def save(self, path: str | Path) -> None:
         arrays = {k: getattr(self, k) for k in self.__dataclass_fields__
-                  if not k.startswith("_") and k != "name" and getattr(self, k) is not None}
+                  if not k.startswith("_") and isinstance(getattr(self, k), np.ndarray)}
         np.savez_compressed(path, name=np.array(self.name), **arrays)
 
     @staticmethod

@@ -13,10 +13,13 @@ the GPU host with the rest of the working tree):
     of the stub, and ``oracle/policy_override`` replacing the shared-server GPU
     allow-list so device 0 is accepted.
 ``libref_dropin.so``
-    The reference controller linked against this project's drop-in adapter
-    (myplacement_b200/adapter/mpgp_placement_backend.cpp) and ``libmpgp.so``
-    in place of the CUDA backend: the reference's own AdaptiveGlobalPlacer
-    driving the B200 engine through the C ABI.
+    The reference controller linked against this project's drop-in adapters
+    and ``libmpgp.so``: myplacement_b200/adapter/mpgp_placement_backend.cpp in
+    place of the CUDA backend (the reference's own AdaptiveGlobalPlacer
+    driving the B200 engine through the C ABI) and
+    myplacement_b200/adapter/mpgp_bookshelf_parser.cpp in place of
+    src/io/BookshelfParser.cpp (the reference's BookshelfParser API over the
+    native reader).
 
 ``oracle/liboracle.so`` is the project's own C restatement (fixed-point density).
 
@@ -39,6 +42,7 @@ OUT = ORACLE / "_ref"
 OBJ = OUT / "obj"
 
 CPU_SOURCES = [
+    "src/io/BookshelfParser.cpp",
     "src/model/PlacementDatabase.cpp",
     "src/metrics/Metrics.cpp",
     "src/metrics/Rudy.cpp",
@@ -116,14 +120,15 @@ def build_reference(dropin: bool = True, cuda: bool = True) -> list[Path]:
     shim = ORACLE / "fftw_shim" / "fftw_shim.cpp"
     capi = ORACLE / "ref_capi.cpp"
     jobs = [(s, "ref") for s in cpu_sources] + [(shim, "ref"), (capi, "ref"), (REF_ROOT / STUB_SOURCE, "ref")]
-    adapter = REPO / "myplacement_b200" / "adapter" / "mpgp_placement_backend.cpp"
+    adapters = [REPO / "myplacement_b200" / "adapter" / name
+                for name in ("mpgp_placement_backend.cpp", "mpgp_bookshelf_parser.cpp")]
     with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as pool:
         futures = [pool.submit(_compile_cxx, s, t) for s, t in jobs]
         cuda_future = pool.submit(_compile_cuda, REF_ROOT / CUDA_SOURCE, "ref") if cuda else None
-        adapter_future = pool.submit(_compile_cxx, adapter, "dropin") if dropin and adapter.exists() else None
+        adapter_futures = [pool.submit(_compile_cxx, a, "dropin") for a in adapters] if dropin else []
         objects = [f.result() for f in futures]
         cuda_object = cuda_future.result() if cuda_future else None
-        adapter_object = adapter_future.result() if adapter_future else None
+        adapter_objects = [f.result() for f in adapter_futures]
 
     common = objects[:-1]  # everything but the stub
     stub = objects[-1]
@@ -137,11 +142,14 @@ def build_reference(dropin: bool = True, cuda: bool = True) -> list[Path]:
         _run(["g++", "-shared", "-o", str(cuda_lib), *map(str, common), str(cuda_object),
               f"-L{cuda_home / 'lib64'}", "-lcufft", "-lcudart", f"-Wl,-rpath,{cuda_home / 'lib64'}"])
         built.append(cuda_lib)
-    if adapter_object is not None:
+    if adapter_objects:
         engine = REPO / "myplacement_b200" / "libmpgp.so"
         if engine.exists():
+            # The reference's BookShelf reader gives way to the adapter's.
+            reader = _object(REF_ROOT / CPU_SOURCES[0], "ref")
+            kept = [o for o in common if o != reader]
             dropin_lib = OUT / "libref_dropin.so"
-            _run(["g++", "-shared", "-o", str(dropin_lib), *map(str, common), str(adapter_object),
+            _run(["g++", "-shared", "-o", str(dropin_lib), *map(str, kept), *map(str, adapter_objects),
                   f"-L{engine.parent}", "-lmpgp", "-Wl,-rpath,$ORIGIN/../../myplacement_b200"])
             built.append(dropin_lib)
     return built

@@ -31,6 +31,15 @@ def _ptr(array: np.ndarray | None, kind):
     return None if array is None else array.ctypes.data_as(kind)
 
 
+class ReferenceFailure(RuntimeError):
+    """An exception thrown by the reference code, as (status, message)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"reference status {status}: {message}")
+        self.status = status
+        self.message = message
+
+
 class ReferenceLibrary:
     """One of libref_cpu.so / libref_cuda.so / libref_dropin.so."""
 
@@ -65,6 +74,14 @@ class ReferenceLibrary:
                                           C.POINTER(_abi.DensityMetrics)]),
             "ref_design_metrics": (C.c_int, [C.POINTER(_abi.Design), C.c_int32, C.c_int32, C.c_double, _d,
                                              C.POINTER(_abi.DensityMetrics)]),
+            "ref_bookshelf_read": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
+            "ref_bookshelf_destroy": (None, [_vp]),
+            "ref_bookshelf_counts": (C.c_int, [_vp, _i64, _i64, _d]),
+            "ref_bookshelf_modules": (C.c_int, [_vp, _d, _d, _d, _d, _i32, _i32, _i64, _i64]),
+            "ref_bookshelf_nets": (C.c_int, [_vp, _d, _i64, _i64, _i32, _i64, _d, _d, _i32]),
+            "ref_bookshelf_rows": (C.c_int, [_vp, _d, _d, _d, _d, _d, _i64, _i32]),
+            "ref_bookshelf_module_name": (C.c_char_p, [_vp, C.c_int64]),
+            "ref_bookshelf_net_name": (C.c_char_p, [_vp, C.c_int64]),
         }
         for name, (restype, argtypes) in sig.items():
             fn = getattr(lib, name)
@@ -104,6 +121,53 @@ class ReferenceLibrary:
         return hpwl.value, metrics.as_dict()
 
     # ---- single evaluations ------------------------------------------------------------
+    def read_bookshelf(self, aux_path) -> dict:
+        """BookshelfParser().parseAux(aux_path) of the linked reader, flattened.
+
+        Raises ReferenceFailure with the status (MPGP_ERR_PARSE for ParseError)
+        and the message when the reader throws."""
+        lib = self.lib
+        handle = _vp()
+        status = lib.ref_bookshelf_read(str(aux_path).encode(), C.byref(handle))
+        if status != 0:
+            raise ReferenceFailure(status, lib.ref_last_error().decode(errors="replace"))
+        try:
+            counts = np.zeros(5, np.int64)
+            declared = np.zeros(4, np.int64)
+            regions = np.zeros(9)
+            lib.ref_bookshelf_counts(handle, _ptr(counts, _i64), _ptr(declared, _i64), _ptr(regions, _d))
+            modules, nets, pins, rows, movable = (int(c) for c in counts)
+            out = {"declared": declared, "regions": regions, "movable_count": movable}
+            f64 = lambda n: np.zeros(n)
+            m = {k: f64(modules) for k in ("width", "height", "x", "y")}
+            m["flags"] = np.zeros(modules, np.int32)
+            m["orientation"] = np.zeros(modules, np.int32)
+            m["pin_start"] = np.zeros(modules + 1, np.int64)
+            m["pins"] = np.zeros(pins, np.int64)
+            lib.ref_bookshelf_modules(handle, *(_ptr(m[k], _d) for k in ("width", "height", "x", "y")),
+                                      _ptr(m["flags"], _i32), _ptr(m["orientation"], _i32),
+                                      _ptr(m["pin_start"], _i64), _ptr(m["pins"], _i64))
+            n = {"weight": f64(nets), "pin_start": np.zeros(nets + 1, np.int64), "pins": np.zeros(pins, np.int64),
+                 "pin_module": np.zeros(pins, np.int32), "pin_net": np.zeros(pins, np.int64),
+                 "offset_x": f64(pins), "offset_y": f64(pins), "direction": np.zeros(pins, np.int32)}
+            lib.ref_bookshelf_nets(handle, _ptr(n["weight"], _d), _ptr(n["pin_start"], _i64), _ptr(n["pins"], _i64),
+                                   _ptr(n["pin_module"], _i32), _ptr(n["pin_net"], _i64), _ptr(n["offset_x"], _d),
+                                   _ptr(n["offset_y"], _d), _ptr(n["direction"], _i32))
+            r = {k: f64(rows) for k in ("bottom", "height", "site_width", "site_spacing", "x_start")}
+            r["site_count"] = np.zeros(rows, np.int64)
+            r["orientation"] = np.zeros(rows, np.int32)
+            lib.ref_bookshelf_rows(handle, *(_ptr(r[k], _d) for k in ("bottom", "height", "site_width",
+                                                                      "site_spacing", "x_start")),
+                                   _ptr(r["site_count"], _i64), _ptr(r["orientation"], _i32))
+            out["modules"], out["nets"], out["rows"] = m, n, r
+            out["module_names"] = [lib.ref_bookshelf_module_name(handle, i).decode("utf-8", "surrogateescape")
+                                   for i in range(modules)]
+            out["net_names"] = [lib.ref_bookshelf_net_name(handle, i).decode("utf-8", "surrogateescape")
+                                for i in range(nets)]
+            return out
+        finally:
+            lib.ref_bookshelf_destroy(handle)
+
     def session(self, design, options: _abi.Options) -> "ReferenceSession":
         return ReferenceSession(self, design, options)
 

@@ -12,6 +12,7 @@
 #include "AdaptiveGlobalPlacer.cpp"
 
 #include "mpgp.h"
+#include "myplacement/io/BookshelfParser.hpp"
 
 #include <cstring>
 #include <exception>
@@ -131,6 +132,10 @@ void copyMetrics(const DensityMetrics& in, mpgp_density_metrics* out) {
     out->placeable_area = in.placeable_area;
     out->dark_area = in.dark_area;
 }
+
+struct RefBook {
+    PlacementDatabase database;
+};
 
 struct RefSession {
     PlacementDatabase database;
@@ -564,6 +569,112 @@ int ref_design_metrics(const mpgp_design* design, int32_t columns, int32_t rows,
     } catch (const std::exception& error) {
         return fail(error);
     }
+}
+
+// BookshelfParser::parseAux (src/io/BookshelfParser.cpp:313-348) through the
+// reader linked into this library: the reference's own in libref_cpu.so, the
+// adapter over libmpgp.so's reader in libref_dropin.so.  ParseError returns
+// MPGP_ERR_PARSE.
+int ref_bookshelf_read(const char* aux_path, void** out) {
+    *out = nullptr;
+    try {
+        auto book = std::make_unique<RefBook>();
+        book->database = BookshelfParser().parseAux(aux_path);
+        *out = book.release();
+        return MPGP_OK;
+    } catch (const ParseError& error) {
+        g_ref_error = error.what();
+        return MPGP_ERR_PARSE;
+    } catch (const std::exception& error) {
+        return fail(error);
+    }
+}
+
+void ref_bookshelf_destroy(void* handle) { delete static_cast<RefBook*>(handle); }
+
+// counts: modules, nets, pins, rows, movable modules; declared: NumNodes,
+// NumTerminals, NumNets, NumPins (-1 when absent); regions: core (ll, ur),
+// chip (ll, ur), nominal row height.
+int ref_bookshelf_counts(void* handle, int64_t* counts, int64_t* declared, double* regions) {
+    const PlacementDatabase& d = static_cast<RefBook*>(handle)->database;
+    counts[0] = static_cast<int64_t>(d.modules.size());
+    counts[1] = static_cast<int64_t>(d.nets.size());
+    counts[2] = static_cast<int64_t>(d.pins.size());
+    counts[3] = static_cast<int64_t>(d.rows.size());
+    counts[4] = static_cast<int64_t>(d.movableModules().size());
+    const std::optional<std::size_t>* values[4] = {&d.declared_nodes, &d.declared_terminals, &d.declared_nets,
+                                                   &d.declared_pins};
+    for (int k = 0; k < 4; ++k) declared[k] = *values[k] ? static_cast<int64_t>(**values[k]) : -1;
+    const double r[9] = {d.core_region.ll.x, d.core_region.ll.y, d.core_region.ur.x, d.core_region.ur.y,
+                         d.chip_region.ll.x, d.chip_region.ll.y, d.chip_region.ur.x, d.chip_region.ur.y,
+                         d.nominalRowHeight()};
+    std::memcpy(regions, r, sizeof(r));
+    return MPGP_OK;
+}
+
+// flags: bit 0 terminal, bit 1 fixed, bit 2 macro.  pin_start / pins: each
+// module's pin list (Module::pins).
+int ref_bookshelf_modules(void* handle, double* width, double* height, double* x, double* y, int32_t* flags,
+                          int32_t* orientation, int64_t* pin_start, int64_t* pins) {
+    const PlacementDatabase& d = static_cast<RefBook*>(handle)->database;
+    pin_start[0] = 0;
+    for (std::size_t m = 0; m < d.modules.size(); ++m) {
+        const Module& module = d.modules[m];
+        width[m] = module.width;
+        height[m] = module.height;
+        x[m] = module.center.x;
+        y[m] = module.center.y;
+        flags[m] = (module.is_terminal ? 1 : 0) | (module.is_fixed ? 2 : 0) | (module.is_macro ? 4 : 0);
+        orientation[m] = static_cast<int32_t>(module.orientation);
+        pin_start[m + 1] = pin_start[m] + static_cast<int64_t>(module.pins.size());
+        for (std::size_t k = 0; k < module.pins.size(); ++k) pins[pin_start[m] + k] = static_cast<int64_t>(module.pins[k]);
+    }
+    return MPGP_OK;
+}
+
+// Nets with their pin lists (Net::pins), and the pins in PlacementDatabase order.
+int ref_bookshelf_nets(void* handle, double* weight, int64_t* net_pin_start, int64_t* net_pins, int32_t* pin_module,
+                       int64_t* pin_net, double* offset_x, double* offset_y, int32_t* direction) {
+    const PlacementDatabase& d = static_cast<RefBook*>(handle)->database;
+    net_pin_start[0] = 0;
+    for (std::size_t n = 0; n < d.nets.size(); ++n) {
+        weight[n] = d.nets[n].weight;
+        net_pin_start[n + 1] = net_pin_start[n] + static_cast<int64_t>(d.nets[n].pins.size());
+        for (std::size_t k = 0; k < d.nets[n].pins.size(); ++k) {
+            net_pins[net_pin_start[n] + k] = static_cast<int64_t>(d.nets[n].pins[k]);
+        }
+    }
+    for (std::size_t p = 0; p < d.pins.size(); ++p) {
+        pin_module[p] = static_cast<int32_t>(d.pins[p].module);
+        pin_net[p] = static_cast<int64_t>(d.pins[p].net);
+        offset_x[p] = d.pins[p].offset.x;
+        offset_y[p] = d.pins[p].offset.y;
+        direction[p] = static_cast<int32_t>(d.pins[p].direction);
+    }
+    return MPGP_OK;
+}
+
+int ref_bookshelf_rows(void* handle, double* bottom, double* height, double* site_width, double* site_spacing,
+                       double* x_start, int64_t* site_count, int32_t* orientation) {
+    const PlacementDatabase& d = static_cast<RefBook*>(handle)->database;
+    for (std::size_t r = 0; r < d.rows.size(); ++r) {
+        bottom[r] = d.rows[r].bottom;
+        height[r] = d.rows[r].height;
+        site_width[r] = d.rows[r].site_width;
+        site_spacing[r] = d.rows[r].site_spacing;
+        x_start[r] = d.rows[r].x_start;
+        site_count[r] = static_cast<int64_t>(d.rows[r].site_count);
+        orientation[r] = static_cast<int32_t>(d.rows[r].orientation);
+    }
+    return MPGP_OK;
+}
+
+const char* ref_bookshelf_module_name(void* handle, int64_t module) {
+    return static_cast<RefBook*>(handle)->database.modules[static_cast<std::size_t>(module)].name.c_str();
+}
+
+const char* ref_bookshelf_net_name(void* handle, int64_t net) {
+    return static_cast<RefBook*>(handle)->database.nets[static_cast<std::size_t>(net)].name.c_str();
 }
 
 }  // extern "C"
