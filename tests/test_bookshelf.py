@@ -25,6 +25,7 @@ import myplacement_b200 as mp
 from myplacement_b200 import _abi
 from oracle.build_oracle import REF_ROOT
 from oracle.ref import ReferenceFailure, ReferenceLibrary
+from oracle.ref import default_options as ref_options
 
 THREADS = (1, 5)
 
@@ -389,3 +390,40 @@ def test_seeded_mutations_match_reference(readers, tmp_path):
 def test_view_layout_matches_header():
     import ctypes
     assert ctypes.sizeof(_abi.BookshelfView) == ctypes.sizeof(_abi.Design) + 10 * 8
+
+
+# ---- read, then place on the device ------------------------------------------------------------------
+
+
+def _design_from_reference(theirs: dict) -> mp.Design:
+    m, n, r = theirs["modules"], theirs["nets"], theirs["rows"]
+    return mp.Design(module_width=m["width"], module_height=m["height"], module_x=m["x"], module_y=m["y"],
+                     module_flags=m["flags"] & 3, module_orientation=m["orientation"], net_weight=n["weight"],
+                     net_pin_start=n["pin_start"], pin_module=n["pin_module"], pin_offset_x=n["offset_x"],
+                     pin_offset_y=n["offset_y"], row_bottom=r["bottom"], row_height=r["height"],
+                     row_site_width=r["site_width"], row_site_spacing=r["site_spacing"], row_x_start=r["x_start"],
+                     row_site_count=r["site_count"])
+
+
+@pytest.mark.gpu
+def test_read_design_places_like_reference(gpu, readers, tmp_path):
+    """BookShelf files -> native reader -> the engine on the device, against the
+    same files -> the reference reader -> the reference CPU placer: the first 25
+    iterations take the same accept / backtrack / restart decisions, with HPWL
+    and overflow within 1e-4."""
+    design, bins = mp.workload("small_5k")
+    x, y = mp.random_placement(design, 2026)
+    aux = mp.write_bookshelf(design.copy_with_positions(x, y), tmp_path, "placed")
+    ref, _ = readers
+    theirs = _design_from_reference(ref.read_bookshelf(aux))
+    mine = mp.read_bookshelf(aux)
+    fixed = dict(bins_x=bins, bins_y=bins, target_density=0.9, iterations=30, feasible_refinement_iterations=100000)
+    _, _, ref_result, ref_history = ref.global_place(theirs, ref_options(**fixed))
+    result = mp.GlobalPlacer().run(mine, mp.default_options(**fixed))
+    assert result.completed_iterations == ref_result.completed_iterations == 30
+    assert result.hpwl_before == pytest.approx(ref_result.hpwl_before, rel=1e-6)
+    for row, ref_row in zip(result.history[:25], ref_history[:25]):
+        for key in ("accepted", "backtracks", "momentum_restarted"):
+            assert row[key] == ref_row[key], (row["iteration"], key)
+        assert row["hpwl"] == pytest.approx(ref_row["hpwl"], rel=1e-4)
+        assert row["overflow"] == pytest.approx(ref_row["overflow"], rel=1e-4)
