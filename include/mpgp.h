@@ -396,6 +396,56 @@ int mpgp_bookshelf_read(const char* aux_path, int32_t threads, mpgp_bookshelf** 
 int mpgp_bookshelf_get(const mpgp_bookshelf* book, mpgp_bookshelf_view* view);
 void mpgp_bookshelf_destroy(mpgp_bookshelf* book);
 
+/* ---- detailed placement ---------------------------------------------------------- */
+
+/* DetailedPlacementMethod (include/myplacement/placement/DetailedPlacer.hpp:14). */
+enum { MPGP_DETAILED_NONE = 0, MPGP_DETAILED_ADJACENT_SWAP = 1, MPGP_DETAILED_WINDOW_REORDER = 2 };
+
+/* DetailedPlacementOptions (DetailedPlacer.hpp:23-44) for the device backend;
+ * mpgp_detailed_options_default() fills the reference defaults with the
+ * window-reorder method. */
+typedef struct mpgp_detailed_options {
+    int32_t method;
+    int32_t passes;
+    int32_t window_size;
+    int32_t cuda_device;
+    uint64_t maximum_net_degree;
+    double improvement_epsilon;
+    uint64_t maximum_cuda_memory_bytes;
+} mpgp_detailed_options;
+
+/* DetailedPlacementResult (DetailedPlacer.hpp:46-57). */
+typedef struct mpgp_detailed_result {
+    double hpwl_before;
+    double hpwl_after;
+    double elapsed_seconds;
+    uint64_t evaluated_windows;
+    uint64_t evaluated_permutations;
+    uint64_t accepted_operations;
+    int32_t completed_passes;
+    int32_t cuda_device_used;
+    uint64_t cuda_reserved_memory_bytes;
+} mpgp_detailed_result;
+
+void mpgp_detailed_options_default(mpgp_detailed_options* options);
+
+/* tryRunCudaDetailedPlacement (src/placement/CudaDetailedPlacementBackend.hpp:
+ * 13-16; src/placement/cuda/CudaDetailedPlacementBackend.cu:491-709): window
+ * reordering of four consecutive cells of each row segment, every ordering
+ * evaluated on the device, the reference's acceptance rule and order of
+ * application, on a legal placement.  The design's module_x / module_y /
+ * module_orientation are the placement on entry; the result goes to
+ * module_x / module_y / module_orientation (module_count each; orientation
+ * may be NULL).  row_orientation (row_count, Orientation order, 8 = unknown;
+ * NULL = all N) is the SiteRow orientation a moved cell takes.  Where the
+ * reference backend declines (options other than a four-cell window reorder,
+ * options out of range, no usable device) the call returns
+ * MPGP_ERR_UNAVAILABLE with the reason and changes nothing. */
+int mpgp_detailed_place(const mpgp_design* design, const int32_t* row_orientation,
+                        const mpgp_detailed_options* options, double* module_x, double* module_y,
+                        int32_t* module_orientation, mpgp_detailed_result* result, char* reason,
+                        size_t reason_capacity);
+
 /* ---- host setup restated from the reference ----------------------------------- */
 
 /* randomPlacement (src/placement/InitialPlacer.cpp:102-121): writes the module

@@ -60,6 +60,38 @@ class Design(C.Structure):
     ]
 
 
+DETAILED_NONE, DETAILED_ADJACENT_SWAP, DETAILED_WINDOW_REORDER = 0, 1, 2
+
+
+class DetailedOptions(C.Structure):
+    _fields_ = [
+        ("method", C.c_int32),
+        ("passes", C.c_int32),
+        ("window_size", C.c_int32),
+        ("cuda_device", C.c_int32),
+        ("maximum_net_degree", C.c_uint64),
+        ("improvement_epsilon", C.c_double),
+        ("maximum_cuda_memory_bytes", C.c_uint64),
+    ]
+
+
+class DetailedResult(C.Structure):
+    _fields_ = [
+        ("hpwl_before", C.c_double),
+        ("hpwl_after", C.c_double),
+        ("elapsed_seconds", C.c_double),
+        ("evaluated_windows", C.c_uint64),
+        ("evaluated_permutations", C.c_uint64),
+        ("accepted_operations", C.c_uint64),
+        ("completed_passes", C.c_int32),
+        ("cuda_device_used", C.c_int32),
+        ("cuda_reserved_memory_bytes", C.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class BookshelfView(C.Structure):
     _fields_ = [
         ("design", Design),
@@ -304,6 +336,9 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "mpgp_backend_field_solve": (C.c_int, [vp, _d, _d, _d, _d]),
         "mpgp_backend_rudy": (C.c_int, [vp, C.POINTER(Options), _d, C.c_double, C.c_double, C.c_int, _d, _d, _d]),
         "mpgp_random_placement": (C.c_int, [C.POINTER(Design), C.c_uint64, _d, _d]),
+        "mpgp_detailed_options_default": (None, [C.POINTER(DetailedOptions)]),
+        "mpgp_detailed_place": (C.c_int, [C.POINTER(Design), _i32, C.POINTER(DetailedOptions), _d, _d, _i32,
+                                          C.POINTER(DetailedResult), C.c_char_p, C.c_size_t]),
         "mpgp_bookshelf_read": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(vp)]),
         "mpgp_bookshelf_get": (C.c_int, [vp, C.POINTER(BookshelfView)]),
         "mpgp_bookshelf_destroy": (None, [vp]),

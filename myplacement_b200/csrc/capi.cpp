@@ -13,6 +13,7 @@
 
 #include "bookshelf.hpp"
 #include "common.cuh"
+#include "detailed.hpp"
 #include "engine.cuh"
 #include "mpgp.h"
 #include "session.hpp"
@@ -346,6 +347,43 @@ int mpgp_bookshelf_get(const mpgp_bookshelf* b, mpgp_bookshelf_view* view) {
 }
 
 void mpgp_bookshelf_destroy(mpgp_bookshelf* b) { delete b; }
+
+void mpgp_detailed_options_default(mpgp_detailed_options* options) {
+    if (options == nullptr) return;
+    // DetailedPlacementOptions (DetailedPlacer.hpp:23-44) with the window reorder
+    // selected and device 0.
+    options->method = MPGP_DETAILED_WINDOW_REORDER;
+    options->passes = 2;
+    options->window_size = 4;
+    options->cuda_device = 0;
+    options->maximum_net_degree = 64;
+    options->improvement_epsilon = 1e-9;
+    options->maximum_cuda_memory_bytes = 2ULL * 1024ULL * 1024ULL * 1024ULL;
+}
+
+int mpgp_detailed_place(const mpgp_design* design, const int32_t* row_orientation,
+                        const mpgp_detailed_options* options, double* module_x, double* module_y,
+                        int32_t* module_orientation, mpgp_detailed_result* result, char* reason,
+                        size_t reason_capacity) {
+    std::string why;
+    const int status = guarded([&] {
+        mpgp::require(design != nullptr && options != nullptr && module_x != nullptr && module_y != nullptr &&
+                          result != nullptr,
+                      "Arguments are required.");
+        mpgp_detailed_result out{};
+        if (!mpgp::detailedPlace(*design, row_orientation, *options, module_x, module_y, module_orientation, out,
+                                 why)) {
+            mpgp::fail(MPGP_ERR_UNAVAILABLE, why);
+        }
+        *result = out;
+    });
+    if (status != MPGP_OK && reason != nullptr && reason_capacity > 0) {
+        const std::size_t n = std::min(g_last_error.size(), reason_capacity - 1);
+        std::memcpy(reason, g_last_error.data(), n);
+        reason[n] = '\0';
+    }
+    return status;
+}
 
 int mpgp_random_placement(const mpgp_design* design, uint64_t seed, double* module_x, double* module_y) {
     return guarded([&] {

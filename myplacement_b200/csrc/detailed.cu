@@ -1,0 +1,720 @@
+// Detailed placement by window reordering, the orderings evaluated on the
+// device: the reference's CUDA detailed-placement backend
+// (src/placement/cuda/CudaDetailedPlacementBackend.cu:144-709) with the CPU rule
+// it keeps for the windows the device does not take (:328-354).
+//
+// Each pass cuts the rows into segments of abutting standard cells and the
+// segments into windows of four consecutive cells, staggered by two cells on
+// odd passes.  One warp evaluates one window: lanes 0..23 each place the cells
+// in one of the 24 orders (lexicographic, the order std::next_permutation
+// visits) and sum the weighted HPWL of the window's nets; lane 24 sums it for
+// the placement as it is.  Every lane accumulates twice: with fused
+// multiply-adds, which is what the reference's kernel compiles to and what
+// picks the best order, and with separately rounded products and sums, the host
+// arithmetic with which the reference accepts an order.  The windows are then
+// accepted in the reference's order.  A window none of whose nets an earlier
+// accepted window moved takes the device's values as they are; the others are
+// re-evaluated on the host against the placement as it stands, which is what
+// the reference does for every window.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "detailed.hpp"
+#include "setup.hpp"
+
+namespace mpgp {
+namespace {
+
+constexpr int kWindow = 4;
+constexpr int kOrders = 24;
+constexpr int kCurrentLane = kOrders;  // the lane that evaluates the placement as it is
+constexpr int kWindowsPerBlock = 8;
+constexpr int kOrientationUnknown = 8;
+constexpr double kLargest = std::numeric_limits<double>::max();
+
+// Order k (0..23) of four cells in lexicographic order, as four 4-bit fields:
+// field i is the window cell placed i-th.  The Lehmer digits of k are k / 6,
+// k % 6 / 2 and k % 2; each picks a field of the cells not yet placed (`pool`,
+// packed the same way) and removes it.
+__host__ __device__ inline unsigned orderCode(int k) {
+    const unsigned digit[kWindow - 1] = {static_cast<unsigned>(k / 6), static_cast<unsigned>((k % 6) / 2),
+                                         static_cast<unsigned>(k % 2)};
+    unsigned pool = 0x3210u;
+    unsigned code = 0u;
+#pragma unroll
+    for (int i = 0; i < kWindow - 1; ++i) {
+        const unsigned d = digit[i];
+        code |= ((pool >> (4u * d)) & 0xFu) << (4u * static_cast<unsigned>(i));
+        pool = (pool & ((1u << (4u * d)) - 1u)) | ((pool >> (4u * (d + 1u))) << (4u * d));
+    }
+    return code | ((pool & 0xFu) << 12u);
+}
+
+inline void orderOf(int k, int order[kWindow]) {
+    const unsigned code = orderCode(k);
+    for (int i = 0; i < kWindow; ++i) order[i] = static_cast<int>((code >> (4u * static_cast<unsigned>(i))) & 0xFu);
+}
+
+// alignUp(width, 0, spacing) (DetailedPlacer.cpp:67-70), products and sums
+// rounded separately.
+__device__ inline double roundedWidthDevice(double width, double spacing) {
+    return spacing <= kEpsilon ? width : __dmul_rn(ceil((width - kEpsilon) / spacing), spacing);
+}
+
+struct WindowArrays {
+    const int4* modules;
+    const double* start_x;  // lower-left x of the window's first cell
+    const double* bottom;
+    const double* spacing;
+    const int* net_start;   // windows + 1
+    const int* nets;
+};
+
+__global__ void __launch_bounds__(32 * kWindowsPerBlock)
+    windowOrdersKernel(const double2* __restrict__ center, const double2* __restrict__ size,
+                       const int* __restrict__ pin_module, const double2* __restrict__ pin_offset,
+                       const int* __restrict__ net_pin_start, const double* __restrict__ net_weight,
+                       WindowArrays windows, int window_count, int* __restrict__ best_order,
+                       double* __restrict__ value_before, double* __restrict__ value_after) {
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x * kWindowsPerBlock + static_cast<int>(threadIdx.x >> 5);
+    if (w >= window_count) return;  // whole warps leave together
+    const int4 m4 = windows.modules[w];
+    const int module[kWindow] = {m4.x, m4.y, m4.z, m4.w};
+
+    // The window's cells where this lane puts them (registers only: the cell of
+    // each slot is picked by comparisons, never by a computed index).
+    double cx[kWindow];
+    double cy[kWindow];
+#pragma unroll
+    for (int i = 0; i < kWindow; ++i) {
+        const double2 c = center[module[i]];
+        cx[i] = c.x;
+        cy[i] = c.y;
+    }
+    if (lane < kOrders) {
+        const unsigned code = orderCode(lane);
+        double cursor = windows.start_x[w];
+        const double bottom = windows.bottom[w];
+        const double spacing = windows.spacing[w];
+#pragma unroll
+        for (int i = 0; i < kWindow; ++i) {
+            const unsigned local = (code >> (4u * static_cast<unsigned>(i))) & 0xFu;
+            int placed = module[0];
+#pragma unroll
+            for (int j = 1; j < kWindow; ++j) placed = local == static_cast<unsigned>(j) ? module[j] : placed;
+            const double2 s = size[placed];
+            const double x = __dadd_rn(cursor, __dmul_rn(s.x, 0.5));
+            const double y = __dadd_rn(bottom, __dmul_rn(s.y, 0.5));
+#pragma unroll
+            for (int j = 0; j < kWindow; ++j) {
+                if (local == static_cast<unsigned>(j)) {
+                    cx[j] = x;
+                    cy[j] = y;
+                }
+            }
+            cursor = __dadd_rn(cursor, roundedWidthDevice(s.x, spacing));
+        }
+    }
+
+    double fused = 0.0;
+    double plain = 0.0;
+    if (lane <= kCurrentLane) {
+        for (int e = windows.net_start[w]; e < windows.net_start[w + 1]; ++e) {
+            const int net = windows.nets[e];
+            double fmin_x = kLargest, fmax_x = -kLargest, fmin_y = kLargest, fmax_y = -kLargest;
+            double min_x = kLargest, max_x = -kLargest, min_y = kLargest, max_y = -kLargest;
+            for (int p = net_pin_start[net]; p < net_pin_start[net + 1]; ++p) {
+                const int m = pin_module[p];
+                double2 c = center[m];
+#pragma unroll
+                for (int i = 0; i < kWindow; ++i) {  // a window's cells are distinct: one match at most
+                    if (module[i] == m) c = make_double2(cx[i], cy[i]);
+                }
+                const double2 o = pin_offset[p];
+                const double x = c.x + o.x;
+                const double y = c.y + o.y;
+                fmin_x = fmin(fmin_x, x);
+                fmax_x = fmax(fmax_x, x);
+                fmin_y = fmin(fmin_y, y);
+                fmax_y = fmax(fmax_y, y);
+                min_x = x < min_x ? x : min_x;  // std::min / std::max
+                max_x = max_x < x ? x : max_x;
+                min_y = y < min_y ? y : min_y;
+                max_y = max_y < y ? y : max_y;
+            }
+            const double weight = net_weight[net];
+            fused = fma(weight, (fmax_x - fmin_x) + (fmax_y - fmin_y), fused);
+            plain = __dadd_rn(plain, __dmul_rn(weight, (max_x - min_x) + (max_y - min_y)));
+        }
+    }
+
+    // The smallest fused value, the lowest order on ties, to every lane.
+    double best = lane < kOrders ? fused : kLargest;
+    int index = lane;
+    for (int offset = 16; offset > 0; offset >>= 1) {
+        const double other = __shfl_xor_sync(0xffffffffu, best, offset);
+        const int other_index = __shfl_xor_sync(0xffffffffu, index, offset);
+        if (other < best || (other == best && other_index < index)) {
+            best = other;
+            index = other_index;
+        }
+    }
+    const double before = __shfl_sync(0xffffffffu, plain, kCurrentLane);
+    const double after = __shfl_sync(0xffffffffu, plain, index);
+    if (lane == 0) {
+        best_order[w] = index;
+        value_before[w] = before;
+        value_after[w] = after;
+    }
+}
+
+// ---- host ---------------------------------------------------------------------------------
+
+// transformOffset (PlacementDatabase.cpp:55-68).
+inline void transform(double x, double y, int orientation, double& ox, double& oy) {
+    switch (orientation) {
+        case 1: ox = -x; oy = -y; return;
+        case 2: ox = -y; oy = x; return;
+        case 3: ox = y; oy = -x; return;
+        case 4: ox = -x; oy = y; return;
+        case 5: ox = x; oy = -y; return;
+        case 6: ox = y; oy = x; return;
+        case 7: ox = -y; oy = -x; return;
+        default: ox = x; oy = y; return;
+    }
+}
+
+// alignUp(width, 0, spacing) (CudaDetailedPlacementBackend.cu:229-236).
+inline double roundedWidth(double width, double spacing) {
+    if (spacing <= kEpsilon) return width;
+    return 0.0 + std::ceil((width - 0.0 - kEpsilon) / spacing) * spacing;
+}
+
+template <typename T>
+class DeviceArray {
+public:
+    DeviceArray() = default;
+    DeviceArray(const DeviceArray&) = delete;
+    DeviceArray& operator=(const DeviceArray&) = delete;
+    ~DeviceArray() {
+        if (data_ != nullptr) cudaFree(data_);
+    }
+    void allocate(std::size_t count, uint64_t& reserved, uint64_t limit, const char* what) {
+        const uint64_t bytes = static_cast<uint64_t>(std::max<std::size_t>(count, 1)) * sizeof(T);
+        if (bytes > limit - std::min(limit, reserved)) {
+            fail(MPGP_ERR_BUDGET, std::string("CUDA detailed-placement budget exceeded while reserving ") + what + ".");
+        }
+        checkCuda(cudaMalloc(reinterpret_cast<void**>(&data_), bytes), what);
+        reserved += bytes;
+    }
+    void upload(const std::vector<T>& values, cudaStream_t stream) {
+        if (!values.empty()) {
+            checkCuda(cudaMemcpyAsync(data_, values.data(), values.size() * sizeof(T), cudaMemcpyHostToDevice, stream),
+                      "detailed-placement upload");
+        }
+    }
+    void download(std::vector<T>& values, cudaStream_t stream) const {
+        if (!values.empty()) {
+            checkCuda(cudaMemcpyAsync(values.data(), data_, values.size() * sizeof(T), cudaMemcpyDeviceToHost, stream),
+                      "detailed-placement download");
+        }
+    }
+    [[nodiscard]] T* get() const { return data_; }
+
+private:
+    T* data_ = nullptr;
+};
+
+class Stream {
+public:
+    Stream() { checkCuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate"); }
+    ~Stream() { cudaStreamDestroy(stream_); }
+    Stream(const Stream&) = delete;
+    Stream& operator=(const Stream&) = delete;
+    [[nodiscard]] cudaStream_t get() const { return stream_; }
+
+private:
+    cudaStream_t stream_ = nullptr;
+};
+
+// The placement state the passes change, with the design's fixed data.
+struct Placement {
+    const mpgp_design& d;
+    std::vector<double> cx, cy;
+    std::vector<int32_t> orientation;
+    std::vector<int32_t> pin_net;
+    std::vector<int64_t> module_pin_start;  // module -> its pins, in pin order
+    std::vector<int32_t> module_pins;
+
+    explicit Placement(const mpgp_design& design) : d(design) {
+        const std::size_t m = static_cast<std::size_t>(d.module_count);
+        cx.assign(d.module_x, d.module_x + m);
+        cy.assign(d.module_y, d.module_y + m);
+        orientation.assign(m, 0);
+        if (d.module_orientation != nullptr) orientation.assign(d.module_orientation, d.module_orientation + m);
+        pin_net.resize(static_cast<std::size_t>(d.pin_count));
+        for (int32_t n = 0; n < d.net_count; ++n) {
+            for (int64_t p = d.net_pin_start[n]; p < d.net_pin_start[n + 1]; ++p) pin_net[p] = n;
+        }
+        module_pin_start.assign(m + 1, 0);
+        for (int64_t p = 0; p < d.pin_count; ++p) ++module_pin_start[d.pin_module[p] + 1];
+        for (std::size_t k = 0; k < m; ++k) module_pin_start[k + 1] += module_pin_start[k];
+        module_pins.resize(static_cast<std::size_t>(d.pin_count));
+        std::vector<int64_t> fill(module_pin_start.begin(), module_pin_start.end() - 1);
+        for (int64_t p = 0; p < d.pin_count; ++p) module_pins[fill[d.pin_module[p]]++] = static_cast<int32_t>(p);
+    }
+
+    [[nodiscard]] double lowerLeftX(int m) const { return cx[m] - d.module_width[m] * 0.5; }
+    [[nodiscard]] double lowerLeftY(int m) const { return cy[m] - d.module_height[m] * 0.5; }
+
+    // localHpwl (CudaDetailedPlacementBackend.cu:282-302) with the window's cells
+    // at (wx, wy).
+    double windowHpwl(const int32_t* modules, int count, const int32_t* nets, int net_count, const double* wx,
+                      const double* wy) const {
+        double result = 0.0;
+        for (int e = 0; e < net_count; ++e) {
+            const int32_t net = nets[e];
+            double min_x = std::numeric_limits<double>::infinity();
+            double max_x = -std::numeric_limits<double>::infinity();
+            double min_y = std::numeric_limits<double>::infinity();
+            double max_y = -std::numeric_limits<double>::infinity();
+            for (int64_t p = d.net_pin_start[net]; p < d.net_pin_start[net + 1]; ++p) {
+                const int32_t m = d.pin_module[p];
+                double x = cx[m];
+                double y = cy[m];
+                for (int i = 0; i < count; ++i) {
+                    if (modules[i] == m) {
+                        x = wx[i];
+                        y = wy[i];
+                        break;
+                    }
+                }
+                double ox = 0.0;
+                double oy = 0.0;
+                transform(d.pin_offset_x[p], d.pin_offset_y[p], orientation[m], ox, oy);
+                x = x + ox;
+                y = y + oy;
+                min_x = std::min(min_x, x);
+                max_x = std::max(max_x, x);
+                min_y = std::min(min_y, y);
+                max_y = std::max(max_y, y);
+            }
+            result += d.net_weight[net] * ((max_x - min_x) + (max_y - min_y));
+        }
+        return result;
+    }
+
+    // centersForOrder (:304-315).
+    void centersForOrder(const int32_t* modules, const int* order, int count, double bottom, double spacing,
+                         double* wx, double* wy) const {
+        double cursor = lowerLeftX(modules[0]);
+        for (int i = 0; i < count; ++i) {
+            const int local = order[i];
+            const int32_t m = modules[local];
+            wx[local] = cursor + d.module_width[m] * 0.5;
+            wy[local] = bottom + d.module_height[m] * 0.5;
+            cursor += roundedWidth(d.module_width[m], spacing);
+        }
+    }
+
+    // applyOrder (:317-326): setLowerLeft, then the row's orientation when known.
+    void applyOrder(const int32_t* modules, const int* order, int count, double bottom, double spacing,
+                    int row_orientation) {
+        double cursor = lowerLeftX(modules[0]);
+        for (int i = 0; i < count; ++i) {
+            const int32_t m = modules[order[i]];
+            cx[m] = cursor + d.module_width[m] * 0.5;
+            cy[m] = bottom + d.module_height[m] * 0.5;
+            if (row_orientation != kOrientationUnknown) orientation[m] = row_orientation;
+            cursor += roundedWidth(d.module_width[m], spacing);
+        }
+    }
+
+    // calculateHpwl (Metrics.cpp:128-147).
+    [[nodiscard]] double hpwl() const {
+        double result = 0.0;
+        for (int32_t n = 0; n < d.net_count; ++n) {
+            if (d.net_pin_start[n + 1] - d.net_pin_start[n] < 2) continue;
+            double min_x = std::numeric_limits<double>::infinity();
+            double max_x = -std::numeric_limits<double>::infinity();
+            double min_y = std::numeric_limits<double>::infinity();
+            double max_y = -std::numeric_limits<double>::infinity();
+            for (int64_t p = d.net_pin_start[n]; p < d.net_pin_start[n + 1]; ++p) {
+                const int32_t m = d.pin_module[p];
+                double ox = 0.0;
+                double oy = 0.0;
+                transform(d.pin_offset_x[p], d.pin_offset_y[p], orientation[m], ox, oy);
+                const double x = cx[m] + ox;
+                const double y = cy[m] + oy;
+                min_x = std::min(min_x, x);
+                max_x = std::max(max_x, x);
+                min_y = std::min(min_y, y);
+                max_y = std::max(max_y, y);
+            }
+            result += d.net_weight[n] * ((max_x - min_x) + (max_y - min_y));
+        }
+        return result;
+    }
+};
+
+// A window: up to four consecutive cells of a segment and the nets they touch.
+struct Windows {
+    std::vector<int32_t> row;
+    std::vector<int32_t> count;
+    std::vector<int32_t> modules;  // kWindow per window (unused slots -1)
+    std::vector<int64_t> net_start{0};
+    std::vector<int32_t> nets;     // sorted, unique per window
+    std::vector<uint8_t> device;   // evaluated on the device (gpu_eligible)
+
+    void clear() {
+        row.clear();
+        count.clear();
+        modules.clear();
+        net_start.assign(1, 0);
+        nets.clear();
+        device.clear();
+    }
+};
+
+// buildRowSegments (:238-274) and makeWindow (:276-293) for one pass: the
+// windows in the reference's order, whichever list they go to.
+void buildWindows(const Placement& s, const std::vector<uint8_t>& standard, int phase, uint64_t maximum_net_degree,
+                  Windows& out) {
+    const mpgp_design& d = s.d;
+    out.clear();
+    if (d.row_count == 0) return;
+    std::vector<std::size_t> sorted_rows(static_cast<std::size_t>(d.row_count));
+    std::iota(sorted_rows.begin(), sorted_rows.end(), 0U);
+    std::sort(sorted_rows.begin(), sorted_rows.end(),
+              [&](std::size_t a, std::size_t b) { return d.row_bottom[a] < d.row_bottom[b]; });
+    const auto centre = [&](std::size_t r) { return d.row_bottom[r] + d.row_height[r] * 0.5; };
+    const auto nearestRow = [&](double coordinate) {
+        const auto it = std::lower_bound(sorted_rows.begin(), sorted_rows.end(), coordinate,
+                                         [&](std::size_t r, double value) { return centre(r) < value; });
+        if (it == sorted_rows.begin()) return *it;
+        if (it == sorted_rows.end()) return sorted_rows.back();
+        const std::size_t right = *it;
+        const std::size_t left = *(it - 1);
+        return std::abs(centre(left) - coordinate) <= std::abs(centre(right) - coordinate) ? left : right;
+    };
+    constexpr double kSegmentEpsilon = 1e-6;
+    std::vector<std::vector<int32_t>> cells_by_row(static_cast<std::size_t>(d.row_count));
+    for (int32_t m = 0; m < d.module_count; ++m) {
+        if (standard[m] == 0) continue;
+        const std::size_t r = nearestRow(s.cy[m]);
+        if (std::abs(s.lowerLeftY(m) - d.row_bottom[r]) <= kSegmentEpsilon) cells_by_row[r].push_back(m);
+    }
+    std::vector<int32_t> segment;
+    std::vector<int32_t> window_nets;
+    const auto emitWindows = [&](int32_t r) {
+        if (segment.size() < 2U) return;
+        for (std::size_t start = static_cast<std::size_t>(phase); start + 1U < segment.size(); start += kWindow) {
+            const std::size_t count = std::min<std::size_t>(kWindow, segment.size() - start);
+            if (count < 2U) break;
+            window_nets.clear();
+            for (std::size_t i = 0; i < count; ++i) {
+                const int32_t m = segment[start + i];
+                for (int64_t k = s.module_pin_start[m]; k < s.module_pin_start[m + 1]; ++k) {
+                    window_nets.push_back(s.pin_net[s.module_pins[k]]);
+                }
+            }
+            std::sort(window_nets.begin(), window_nets.end());
+            window_nets.erase(std::unique(window_nets.begin(), window_nets.end()), window_nets.end());
+            bool device = count == static_cast<std::size_t>(kWindow) && !window_nets.empty();
+            for (const int32_t n : window_nets) {
+                if (static_cast<uint64_t>(d.net_pin_start[n + 1] - d.net_pin_start[n]) > maximum_net_degree) {
+                    device = false;
+                }
+            }
+            out.row.push_back(r);
+            out.count.push_back(static_cast<int32_t>(count));
+            for (std::size_t i = 0; i < kWindow; ++i) out.modules.push_back(i < count ? segment[start + i] : -1);
+            out.nets.insert(out.nets.end(), window_nets.begin(), window_nets.end());
+            out.net_start.push_back(static_cast<int64_t>(out.nets.size()));
+            out.device.push_back(device ? 1 : 0);
+        }
+    };
+    for (int32_t r = 0; r < d.row_count; ++r) {
+        std::vector<int32_t>& cells = cells_by_row[r];
+        if (cells.size() < 2U) continue;
+        std::sort(cells.begin(), cells.end(),
+                  [&](int32_t a, int32_t b) { return s.lowerLeftX(a) < s.lowerLeftX(b); });
+        segment.clear();
+        for (const int32_t m : cells) {
+            if (!segment.empty()) {
+                const int32_t previous = segment.back();
+                const double expected =
+                    s.lowerLeftX(previous) + roundedWidth(d.module_width[previous], d.row_site_spacing[r]);
+                if (std::abs(s.lowerLeftX(m) - expected) > kSegmentEpsilon) {
+                    emitWindows(r);
+                    segment.clear();
+                }
+            }
+            segment.push_back(m);
+        }
+        emitWindows(r);
+    }
+}
+
+}  // namespace
+
+bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const mpgp_detailed_options& options,
+                   double* module_x, double* module_y, int32_t* module_orientation, mpgp_detailed_result& result,
+                   std::string& reason) {
+    reason.clear();
+    // The checks of tryRunCudaDetailedPlacement (:493-523), without the home
+    // server's device allow-list and free-memory reserve.
+    if (options.method != MPGP_DETAILED_WINDOW_REORDER || options.window_size != kWindow) {
+        reason = "CUDA detailed placement currently supports window reordering with a four-cell window only.";
+        return false;
+    }
+    if (options.passes <= 0 || options.maximum_net_degree < 2U || options.improvement_epsilon < 0.0 ||
+        options.maximum_cuda_memory_bytes == 0U) {
+        reason = "CUDA detailed-placement options are outside their valid range.";
+        return false;
+    }
+    int device_count = 0;
+    if (cudaGetDeviceCount(&device_count) != cudaSuccess || options.cuda_device < 0 ||
+        options.cuda_device >= device_count) {
+        cudaGetLastError();
+        reason = "Requested CUDA device is unavailable on this host.";
+        return false;
+    }
+    int previous_device = 0;
+    cudaGetDevice(&previous_device);
+    if (cudaSetDevice(options.cuda_device) != cudaSuccess) {
+        cudaGetLastError();
+        reason = "Unable to select the requested CUDA device.";
+        return false;
+    }
+    struct RestoreDevice {
+        int device;
+        ~RestoreDevice() { cudaSetDevice(device); }
+    } restore{previous_device};
+    cudaDeviceProp properties{};
+    if (cudaGetDeviceProperties(&properties, options.cuda_device) != cudaSuccess || properties.major < 6) {
+        reason = "Requested CUDA device lacks required double-precision support.";
+        return false;
+    }
+    std::size_t free_bytes = 0;
+    std::size_t total_bytes = 0;
+    checkCuda(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
+    const uint64_t limit = std::min<uint64_t>(options.maximum_cuda_memory_bytes, free_bytes);
+
+    validateDesign(d);
+    const DerivedDesign derived = deriveDesign(d);
+    std::vector<uint8_t> standard(static_cast<std::size_t>(d.module_count));
+    for (int32_t m = 0; m < d.module_count; ++m) standard[m] = derived.is_fixed[m] == 0 && derived.is_macro[m] == 0;
+    const auto rowOrientation = [&](int r) { return row_orientation != nullptr ? row_orientation[r] : 0; };
+
+    Placement s(d);
+    result = mpgp_detailed_result{};
+    result.hpwl_before = s.hpwl();
+    result.cuda_device_used = options.cuda_device;
+    const auto started = std::chrono::steady_clock::now();
+
+    // Device copies of the design: sizes, pin modules and net CSR once; centres
+    // and orientation-transformed pin offsets at the start of every pass.
+    const std::size_t modules = static_cast<std::size_t>(d.module_count);
+    const std::size_t pins = static_cast<std::size_t>(d.pin_count);
+    const std::size_t nets = static_cast<std::size_t>(d.net_count);
+    const std::size_t window_capacity = modules / kWindow + 1;
+    uint64_t reserved = 0;
+    DeviceArray<double2> center, size, pin_offset;
+    DeviceArray<int> pin_module, net_pin_start;
+    DeviceArray<double> net_weight;
+    DeviceArray<int4> window_modules;
+    DeviceArray<double> window_start, window_bottom, window_spacing, value_before, value_after;
+    DeviceArray<int> window_net_start, window_nets, best_order;
+    center.allocate(modules, reserved, limit, "CUDA detailed module centers");
+    size.allocate(modules, reserved, limit, "CUDA detailed module sizes");
+    pin_offset.allocate(pins, reserved, limit, "CUDA detailed pin offsets");
+    pin_module.allocate(pins, reserved, limit, "CUDA detailed pin modules");
+    net_pin_start.allocate(nets + 1, reserved, limit, "CUDA detailed net offsets");
+    net_weight.allocate(nets, reserved, limit, "CUDA detailed net weights");
+    window_modules.allocate(window_capacity, reserved, limit, "CUDA detailed window modules");
+    window_start.allocate(window_capacity, reserved, limit, "CUDA detailed window start x");
+    window_bottom.allocate(window_capacity, reserved, limit, "CUDA detailed window bottoms");
+    window_spacing.allocate(window_capacity, reserved, limit, "CUDA detailed window spacing");
+    window_net_start.allocate(window_capacity + 1, reserved, limit, "CUDA detailed window net offsets");
+    window_nets.allocate(std::max<std::size_t>(pins, 1), reserved, limit, "CUDA detailed window net ids");
+    best_order.allocate(window_capacity, reserved, limit, "CUDA detailed best orders");
+    value_before.allocate(window_capacity, reserved, limit, "CUDA detailed window values");
+    value_after.allocate(window_capacity, reserved, limit, "CUDA detailed window values");
+    result.cuda_reserved_memory_bytes = reserved;
+
+    Stream stream;
+    {
+        std::vector<double2> sizes(modules);
+        for (std::size_t m = 0; m < modules; ++m) sizes[m] = make_double2(d.module_width[m], d.module_height[m]);
+        const std::vector<int> modules_of_pins(d.pin_module, d.pin_module + pins);
+        std::vector<int> starts(nets + 1);
+        for (std::size_t n = 0; n <= nets; ++n) starts[n] = static_cast<int>(d.net_pin_start[n]);
+        const std::vector<double> weights(d.net_weight, d.net_weight + nets);
+        size.upload(sizes, stream.get());
+        pin_module.upload(modules_of_pins, stream.get());
+        net_pin_start.upload(starts, stream.get());
+        net_weight.upload(weights, stream.get());
+        checkCuda(cudaStreamSynchronize(stream.get()), "detailed-placement upload");
+    }
+
+    Windows windows;
+    std::vector<double2> host_center(modules);
+    std::vector<double2> host_offset(pins);
+    std::vector<int4> host_modules;
+    std::vector<double> host_start, host_bottom, host_spacing, before, after;
+    std::vector<int> host_net_start, host_nets, best;
+    std::vector<uint8_t> moved(nets);
+    for (int pass = 0; pass < options.passes; ++pass) {
+        buildWindows(s, standard, (pass % 2) * (kWindow / 2), options.maximum_net_degree, windows);
+        const std::size_t total = windows.row.size();
+        host_modules.clear();
+        host_start.clear();
+        host_bottom.clear();
+        host_spacing.clear();
+        host_net_start.assign(1, 0);
+        host_nets.clear();
+        std::vector<std::size_t> on_device;
+        for (std::size_t k = 0; k < total; ++k) {
+            if (windows.device[k] == 0) continue;
+            on_device.push_back(k);
+            const int32_t* m = &windows.modules[k * kWindow];
+            host_modules.push_back(make_int4(m[0], m[1], m[2], m[3]));
+            host_start.push_back(s.lowerLeftX(m[0]));
+            host_bottom.push_back(d.row_bottom[windows.row[k]]);
+            host_spacing.push_back(d.row_site_spacing[windows.row[k]]);
+            for (int64_t e = windows.net_start[k]; e < windows.net_start[k + 1]; ++e) host_nets.push_back(windows.nets[e]);
+            host_net_start.push_back(static_cast<int>(host_nets.size()));
+        }
+        const std::size_t count = on_device.size();
+        require(count <= window_capacity && host_nets.size() <= std::max<std::size_t>(pins, 1),
+                "Detailed-placement window arrays exceed their capacity.");
+        best.assign(count, 0);
+        before.assign(count, 0.0);
+        after.assign(count, 0.0);
+        if (count > 0) {
+            for (std::size_t m = 0; m < modules; ++m) host_center[m] = make_double2(s.cx[m], s.cy[m]);
+            for (std::size_t p = 0; p < pins; ++p) {
+                double ox = 0.0;
+                double oy = 0.0;
+                transform(d.pin_offset_x[p], d.pin_offset_y[p], s.orientation[d.pin_module[p]], ox, oy);
+                host_offset[p] = make_double2(ox, oy);
+            }
+            center.upload(host_center, stream.get());
+            pin_offset.upload(host_offset, stream.get());
+            window_modules.upload(host_modules, stream.get());
+            window_start.upload(host_start, stream.get());
+            window_bottom.upload(host_bottom, stream.get());
+            window_spacing.upload(host_spacing, stream.get());
+            window_net_start.upload(host_net_start, stream.get());
+            window_nets.upload(host_nets, stream.get());
+            const WindowArrays arrays{window_modules.get(), window_start.get(), window_bottom.get(),
+                                      window_spacing.get(), window_net_start.get(), window_nets.get()};
+            const unsigned blocks = static_cast<unsigned>((count + kWindowsPerBlock - 1) / kWindowsPerBlock);
+            windowOrdersKernel<<<blocks, 32 * kWindowsPerBlock, 0, stream.get()>>>(
+                center.get(), size.get(), pin_module.get(), pin_offset.get(), net_pin_start.get(), net_weight.get(),
+                arrays, static_cast<int>(count), best_order.get(), value_before.get(), value_after.get());
+            checkCuda(cudaGetLastError(), "windowOrdersKernel launch");
+            best_order.download(best, stream.get());
+            value_before.download(before, stream.get());
+            value_after.download(after, stream.get());
+            checkCuda(cudaStreamSynchronize(stream.get()), "windowOrdersKernel");
+        }
+
+        // The device's windows in order (:649-677), then the host's (:680-688).
+        std::fill(moved.begin(), moved.end(), 0);
+        double wx[kWindow];
+        double wy[kWindow];
+        for (std::size_t j = 0; j < count; ++j) {
+            const std::size_t k = on_device[j];
+            ++result.evaluated_windows;
+            result.evaluated_permutations += kOrders;
+            const int order_index = best[j];
+            if (order_index <= 0 || order_index >= kOrders) continue;
+            const int32_t* m = &windows.modules[k * kWindow];
+            const int32_t* window_nets_k = &windows.nets[windows.net_start[k]];
+            const int net_count = static_cast<int>(windows.net_start[k + 1] - windows.net_start[k]);
+            int order[kWindow];
+            orderOf(order_index, order);
+            const int r = windows.row[k];
+            double value_now = before[j];
+            double value_then = after[j];
+            bool stale = false;
+            for (int e = 0; e < net_count && !stale; ++e) stale = moved[window_nets_k[e]] != 0;
+            if (stale) {
+                for (int i = 0; i < kWindow; ++i) {
+                    wx[i] = s.cx[m[i]];
+                    wy[i] = s.cy[m[i]];
+                }
+                value_now = s.windowHpwl(m, kWindow, window_nets_k, net_count, wx, wy);
+                s.centersForOrder(m, order, kWindow, d.row_bottom[r], d.row_site_spacing[r], wx, wy);
+                value_then = s.windowHpwl(m, kWindow, window_nets_k, net_count, wx, wy);
+            }
+            if (value_then < value_now - options.improvement_epsilon) {
+                s.applyOrder(m, order, kWindow, d.row_bottom[r], d.row_site_spacing[r], rowOrientation(r));
+                ++result.accepted_operations;
+                for (int e = 0; e < net_count; ++e) moved[window_nets_k[e]] = 1;
+            }
+        }
+        for (std::size_t k = 0; k < total; ++k) {
+            if (windows.device[k] != 0) continue;
+            ++result.evaluated_windows;
+            // optimizeCpuWindow (:328-354).
+            const int32_t* m = &windows.modules[k * kWindow];
+            const int n = windows.count[k];
+            const int32_t* window_nets_k = &windows.nets[windows.net_start[k]];
+            const int net_count = static_cast<int>(windows.net_start[k + 1] - windows.net_start[k]);
+            if (net_count == 0) continue;
+            bool too_wide = false;
+            for (int e = 0; e < net_count; ++e) {
+                const int32_t net = window_nets_k[e];
+                too_wide |= static_cast<uint64_t>(d.net_pin_start[net + 1] - d.net_pin_start[net]) >
+                            options.maximum_net_degree;
+            }
+            if (too_wide) continue;
+            const int r = windows.row[k];
+            for (int i = 0; i < n; ++i) {
+                wx[i] = s.cx[m[i]];
+                wy[i] = s.cy[m[i]];
+            }
+            double best_value = s.windowHpwl(m, n, window_nets_k, net_count, wx, wy);
+            int order[kWindow] = {0, 1, 2, 3};
+            int best_order_found[kWindow] = {0, 1, 2, 3};
+            bool improved = false;
+            do {
+                s.centersForOrder(m, order, n, d.row_bottom[r], d.row_site_spacing[r], wx, wy);
+                const double value = s.windowHpwl(m, n, window_nets_k, net_count, wx, wy);
+                ++result.evaluated_permutations;
+                if (value < best_value - options.improvement_epsilon) {
+                    best_value = value;
+                    std::copy(order, order + n, best_order_found);
+                    improved = true;
+                }
+            } while (std::next_permutation(order, order + n));
+            if (improved) {
+                s.applyOrder(m, best_order_found, n, d.row_bottom[r], d.row_site_spacing[r], rowOrientation(r));
+                ++result.accepted_operations;
+            }
+        }
+        result.completed_passes = pass + 1;
+    }
+    result.hpwl_after = s.hpwl();
+    result.elapsed_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count();
+    std::copy(s.cx.begin(), s.cx.end(), module_x);
+    std::copy(s.cy.begin(), s.cy.end(), module_y);
+    if (module_orientation != nullptr) std::copy(s.orientation.begin(), s.orientation.end(), module_orientation);
+    return true;
+}
+
+}  // namespace mpgp

@@ -381,6 +381,46 @@ def workload(name: str, seed: int = 2026, scale: float = 1.0) -> tuple[Design, i
     return design, bins
 
 
+def packed_placement(design: Design, seed: int, gap_probability: float = 0.05) -> Design:
+    """A seeded legal placement of the standard cells, the input detailed placement expects.
+
+    Standard cells (neither fixed nor taller than the median row) are shuffled
+    and packed left to right into the rows, bottom row first: each takes its
+    width rounded up to whole sites (alignUp, as the detailed placer measures
+    it), and with probability `gap_probability` one free site follows it.
+    Other modules keep their positions.  Raises ValueError if the cells do not
+    fit the rows.
+    """
+    rng = np.random.Generator(np.random.PCG64(seed))
+    rows = np.argsort(design.row_bottom, kind="stable")
+    nominal = float(np.sort(design.row_height)[design.row_height.shape[0] // 2])
+    fixed = (design.module_flags & (_abi.MODULE_TERMINAL | _abi.MODULE_FIXED)) != 0
+    standard = ~fixed & (np.abs(design.module_height - nominal) <= 1e-9)
+    cells = rng.permutation(np.nonzero(standard)[0])
+    gaps = rng.random(cells.shape[0]) < gap_probability
+    x = design.module_x.copy()
+    y = design.module_y.copy()
+    r = 0
+    cursor = float(design.row_x_start[rows[0]])
+    for cell, gap in zip(cells.tolist(), gaps.tolist()):
+        width = float(design.module_width[cell])
+        while True:
+            row = rows[r]
+            spacing = float(design.row_site_spacing[row])
+            taken = width if spacing <= 1e-9 else math.ceil((width - 1e-9) / spacing) * spacing
+            end = float(design.row_x_start[row] + design.row_site_count[row] * spacing)
+            if cursor + taken <= end + 1e-9:
+                break
+            r += 1
+            if r == rows.shape[0]:
+                raise ValueError("the standard cells do not fit the rows")
+            cursor = float(design.row_x_start[rows[r]])
+        x[cell] = cursor + width * 0.5
+        y[cell] = float(design.row_bottom[row]) + float(design.module_height[cell]) * 0.5
+        cursor += taken + (spacing if gap else 0.0)
+    return design.copy_with_positions(x, y)
+
+
 def small_instance(cells: int, seed: int) -> tuple[Design, int]:
     """A small-design-structured instance (no macros) of `cells` cells; bins = power of two nearest sqrt(cells)."""
     nets = int(round(cells * 5_200 / 5_000))

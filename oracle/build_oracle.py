@@ -8,10 +8,11 @@ the GPU host with the rest of the working tree):
     reference sources, with ``oracle/fftw_shim`` standing in for FFTW3 and
     ``oracle/ref_capi.cpp`` exposing a C ABI.
 ``libref_cuda.so``
-    The same, with the reference CUDA backend
-    (src/placement/cuda/CudaPlacementBackend.cu) compiled for sm_100a in place
-    of the stub, and ``oracle/policy_override`` replacing the shared-server GPU
-    allow-list so device 0 is accepted.
+    The same, with the reference CUDA backends
+    (src/placement/cuda/CudaPlacementBackend.cu and
+    CudaDetailedPlacementBackend.cu) compiled for sm_100a in place of the stubs,
+    and ``oracle/policy_override`` replacing the shared-server GPU allow-list so
+    device 0 is accepted.
 ``libref_dropin.so``
     The reference controller linked against this project's drop-in adapters
     and ``libmpgp.so``: myplacement_b200/adapter/mpgp_placement_backend.cpp in
@@ -19,7 +20,9 @@ the GPU host with the rest of the working tree):
     driving the B200 engine through the C ABI) and
     myplacement_b200/adapter/mpgp_bookshelf_parser.cpp in place of
     src/io/BookshelfParser.cpp (the reference's BookshelfParser API over the
-    native reader).
+    native reader), and myplacement_b200/adapter/mpgp_detailed_placement_backend.cpp
+    in place of the CUDA detailed-placement backend (DetailedPlacer::run with the
+    cuda backend over the engine's window reorder).
 
 ``oracle/liboracle.so`` is the project's own C restatement (fixed-point density).
 
@@ -50,9 +53,11 @@ CPU_SOURCES = [
     "src/placement/ElectrostaticField.cpp",
     "src/placement/GlobalPlacer.cpp",
     "src/placement/LegacyGlobalPlacer.cpp",
+    "src/placement/DetailedPlacer.cpp",
 ]
-STUB_SOURCE = "src/placement/CudaPlacementBackendStub.cpp"
-CUDA_SOURCE = "src/placement/cuda/CudaPlacementBackend.cu"
+STUB_SOURCES = ["src/placement/CudaPlacementBackendStub.cpp", "src/placement/CudaDetailedPlacementBackendStub.cpp"]
+CUDA_SOURCES = ["src/placement/cuda/CudaPlacementBackend.cu", "src/placement/cuda/CudaDetailedPlacementBackend.cu"]
+ADAPTERS = ["mpgp_placement_backend.cpp", "mpgp_bookshelf_parser.cpp", "mpgp_detailed_placement_backend.cpp"]
 
 CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off"]
 
@@ -116,30 +121,28 @@ def build_reference(dropin: bool = True, cuda: bool = True) -> list[Path]:
     if not reference_available():
         return []
     OBJ.mkdir(parents=True, exist_ok=True)
-    cpu_sources = [REF_ROOT / s for s in CPU_SOURCES]
     shim = ORACLE / "fftw_shim" / "fftw_shim.cpp"
     capi = ORACLE / "ref_capi.cpp"
-    jobs = [(s, "ref") for s in cpu_sources] + [(shim, "ref"), (capi, "ref"), (REF_ROOT / STUB_SOURCE, "ref")]
-    adapters = [REPO / "myplacement_b200" / "adapter" / name
-                for name in ("mpgp_placement_backend.cpp", "mpgp_bookshelf_parser.cpp")]
+    common_jobs = [REF_ROOT / s for s in CPU_SOURCES] + [shim, capi]
+    adapters = [REPO / "myplacement_b200" / "adapter" / name for name in ADAPTERS]
     with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as pool:
-        futures = [pool.submit(_compile_cxx, s, t) for s, t in jobs]
-        cuda_future = pool.submit(_compile_cuda, REF_ROOT / CUDA_SOURCE, "ref") if cuda else None
+        futures = [pool.submit(_compile_cxx, s, "ref") for s in common_jobs]
+        stub_futures = [pool.submit(_compile_cxx, REF_ROOT / s, "ref") for s in STUB_SOURCES]
+        cuda_futures = [pool.submit(_compile_cuda, REF_ROOT / s, "ref") for s in CUDA_SOURCES] if cuda else []
         adapter_futures = [pool.submit(_compile_cxx, a, "dropin") for a in adapters] if dropin else []
-        objects = [f.result() for f in futures]
-        cuda_object = cuda_future.result() if cuda_future else None
+        common = [f.result() for f in futures]
+        stubs = [f.result() for f in stub_futures]
+        cuda_objects = [f.result() for f in cuda_futures]
         adapter_objects = [f.result() for f in adapter_futures]
 
-    common = objects[:-1]  # everything but the stub
-    stub = objects[-1]
     built = []
     cpu_lib = OUT / "libref_cpu.so"
-    _run(["g++", "-shared", "-o", str(cpu_lib), *map(str, common), str(stub)])
+    _run(["g++", "-shared", "-o", str(cpu_lib), *map(str, common), *map(str, stubs)])
     built.append(cpu_lib)
-    if cuda_object is not None:
+    if cuda_objects:
         cuda_lib = OUT / "libref_cuda.so"
         cuda_home = Path(shutil.which("nvcc")).resolve().parent.parent
-        _run(["g++", "-shared", "-o", str(cuda_lib), *map(str, common), str(cuda_object),
+        _run(["g++", "-shared", "-o", str(cuda_lib), *map(str, common), *map(str, cuda_objects),
               f"-L{cuda_home / 'lib64'}", "-lcufft", "-lcudart", f"-Wl,-rpath,{cuda_home / 'lib64'}"])
         built.append(cuda_lib)
     if adapter_objects:

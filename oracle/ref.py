@@ -74,6 +74,8 @@ class ReferenceLibrary:
                                           C.POINTER(_abi.DensityMetrics)]),
             "ref_design_metrics": (C.c_int, [C.POINTER(_abi.Design), C.c_int32, C.c_int32, C.c_double, _d,
                                              C.POINTER(_abi.DensityMetrics)]),
+            "ref_detailed_place": (C.c_int, [C.POINTER(_abi.Design), _i32, C.POINTER(_abi.DetailedOptions),
+                                             C.c_int32, _d, _d, _i32, C.POINTER(_abi.DetailedResult)]),
             "ref_bookshelf_read": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
             "ref_bookshelf_destroy": (None, [_vp]),
             "ref_bookshelf_counts": (C.c_int, [_vp, _i64, _i64, _d]),
@@ -121,6 +123,22 @@ class ReferenceLibrary:
         return hpwl.value, metrics.as_dict()
 
     # ---- single evaluations ------------------------------------------------------------
+    def detailed_place(self, design, options: _abi.DetailedOptions, backend: int, row_orientation=None):
+        """DetailedPlacer::run with `backend` (0 cpu, 1 cuda, 2 auto) of the linked
+        backend; returns (x, y, orientation, result dict, backend used) or raises
+        ReferenceFailure."""
+        x = np.empty(design.module_count)
+        y = np.empty(design.module_count)
+        orientation = np.empty(design.module_count, np.int32)
+        rows = None if row_orientation is None else np.ascontiguousarray(row_orientation, dtype=np.int32)
+        result = _abi.DetailedResult()
+        s = design.as_c()
+        used = self.lib.ref_detailed_place(C.byref(s), _ptr(rows, _i32), C.byref(options), backend, _ptr(x, _d),
+                                           _ptr(y, _d), _ptr(orientation, _i32), C.byref(result))
+        if used < 0:
+            raise ReferenceFailure(-used, self.lib.ref_last_error().decode(errors="replace"))
+        return x, y, orientation, result.as_dict(), used
+
     def read_bookshelf(self, aux_path) -> dict:
         """BookshelfParser().parseAux(aux_path) of the linked reader, flattened.
 

@@ -13,6 +13,7 @@
 
 #include "mpgp.h"
 #include "myplacement/io/BookshelfParser.hpp"
+#include "myplacement/placement/DetailedPlacer.hpp"
 
 #include <cstring>
 #include <exception>
@@ -675,6 +676,51 @@ const char* ref_bookshelf_module_name(void* handle, int64_t module) {
 
 const char* ref_bookshelf_net_name(void* handle, int64_t net) {
     return static_cast<RefBook*>(handle)->database.nets[static_cast<std::size_t>(net)].name.c_str();
+}
+
+// DetailedPlacer::run (src/placement/DetailedPlacer.cpp:262-338) on a flattened
+// design with the rows' orientations (NULL: N) and `backend` (0 cpu, 1 cuda,
+// 2 auto): the reference's CPU placer, or its CUDA backend in libref_cuda.so, or
+// the engine's in libref_dropin.so.  Writes the centres and orientations.
+int ref_detailed_place(const mpgp_design* design, const int32_t* row_orientation, const mpgp_detailed_options* flat,
+                       int32_t backend, double* x, double* y, int32_t* orientation, mpgp_detailed_result* out) {
+    try {
+        PlacementDatabase database = buildDatabase(design);
+        if (row_orientation != nullptr) {
+            for (std::size_t r = 0; r < database.rows.size(); ++r) {
+                database.rows[r].orientation = static_cast<Orientation>(row_orientation[r]);
+            }
+        }
+        DetailedPlacementOptions options;
+        options.method = static_cast<DetailedPlacementMethod>(flat->method);
+        options.passes = flat->passes;
+        options.window_size = flat->window_size;
+        options.maximum_net_degree = static_cast<std::size_t>(flat->maximum_net_degree);
+        options.improvement_epsilon = flat->improvement_epsilon;
+        options.compute_backend = static_cast<DetailedPlacementBackend>(backend);
+        options.cuda_device = flat->cuda_device;
+        options.maximum_cuda_memory_bytes = static_cast<std::size_t>(flat->maximum_cuda_memory_bytes);
+        const DetailedPlacementResult result = DetailedPlacer().run(database, options);
+        for (std::size_t m = 0; m < database.modules.size(); ++m) {
+            x[m] = database.modules[m].center.x;
+            y[m] = database.modules[m].center.y;
+            orientation[m] = static_cast<int32_t>(database.modules[m].orientation);
+        }
+        out->hpwl_before = result.hpwl_before;
+        out->hpwl_after = result.hpwl_after;
+        out->elapsed_seconds = result.elapsed_seconds;
+        out->evaluated_windows = result.evaluated_windows;
+        out->evaluated_permutations = result.evaluated_permutations;
+        out->accepted_operations = result.accepted_operations;
+        out->completed_passes = result.completed_passes;
+        out->cuda_device_used = result.cuda_device_used;
+        out->cuda_reserved_memory_bytes = result.cuda_reserved_memory_bytes;
+        return static_cast<int>(result.compute_backend_used) == 1 ? 1 : 0;  // >= 0: the backend used
+    } catch (const std::exception& error) {
+        g_ref_error = error.what();
+        return -(dynamic_cast<const std::invalid_argument*>(&error) != nullptr ? MPGP_ERR_INVALID_ARGUMENT
+                                                                              : MPGP_ERR_RUNTIME);
+    }
 }
 
 }  // extern "C"
