@@ -484,6 +484,15 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
         reason = "CUDA detailed-placement options are outside their valid range.";
         return false;
     }
+    validateDesign(d);
+    for (int32_t m = 0; d.module_orientation != nullptr && m < d.module_count; ++m) {
+        require(d.module_orientation[m] >= 0 && d.module_orientation[m] <= kOrientationUnknown,
+                "Module orientations must be Orientation values (0-8).");
+    }
+    for (int32_t r = 0; row_orientation != nullptr && r < d.row_count; ++r) {
+        require(row_orientation[r] >= 0 && row_orientation[r] <= kOrientationUnknown,
+                "Row orientations must be Orientation values (0-8).");
+    }
     int device_count = 0;
     if (cudaGetDeviceCount(&device_count) != cudaSuccess || options.cuda_device < 0 ||
         options.cuda_device >= device_count) {
@@ -512,7 +521,6 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
     checkCuda(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
     const uint64_t limit = std::min<uint64_t>(options.maximum_cuda_memory_bytes, free_bytes);
 
-    validateDesign(d);
     const DerivedDesign derived = deriveDesign(d);
     std::vector<uint8_t> standard(static_cast<std::size_t>(d.module_count));
     for (int32_t m = 0; m < d.module_count; ++m) standard[m] = derived.is_fixed[m] == 0 && derived.is_macro[m] == 0;

@@ -102,6 +102,17 @@ def test_declines_like_reference_without_running(libraries):
         assert theirs.value.message.endswith(str(mine.value).split(": ", 1)[1])
 
 
+def test_invalid_orientations_are_rejected():
+    design = _fixture()
+    design.module_orientation = np.array([0, 9, 0, 0], np.int32)
+    with pytest.raises(mp.EngineError) as error:
+        mp.DetailedPlacer().run(design)
+    assert error.value.status == _abi.MPGP_ERR_INVALID_ARGUMENT
+    with pytest.raises(mp.EngineError) as error:
+        mp.DetailedPlacer().run(_fixture(), row_orientation=np.array([-1], np.int32))
+    assert error.value.status == _abi.MPGP_ERR_INVALID_ARGUMENT
+
+
 def test_no_cpu_fallback_without_gpu():
     from conftest import GPU_PRESENT
     if GPU_PRESENT:
