@@ -42,6 +42,7 @@
 
 #include "common.cuh"
 #include "mpgp.h"
+#include "workers.hpp"
 
 namespace mpgp {
 namespace {
@@ -326,55 +327,6 @@ int64_t lineNumberAt(Text text, size_t offset) {
     return 1 + static_cast<int64_t>(std::count(text.data(), text.data() + offset, '\n'));
 }
 
-class Workers {
-public:
-    explicit Workers(int threads) : threads_(std::max(1, threads)) {}
-    [[nodiscard]] int threads() const { return threads_; }
-
-    // body(i) for every i in [0, count); the first exception is rethrown after
-    // every thread has stopped.
-    template <typename F>
-    void run(size_t count, const F& body) const {
-        const size_t helpers = std::min<size_t>(static_cast<size_t>(threads_), count);
-        if (helpers <= 1) {
-            for (size_t i = 0; i < count; ++i) body(i);
-            return;
-        }
-        std::atomic<size_t> next{0};
-        std::exception_ptr error;
-        std::mutex lock;
-        const auto work = [&] {
-            try {
-                for (size_t i; (i = next.fetch_add(1)) < count;) body(i);
-            } catch (...) {
-                const std::lock_guard<std::mutex> guard(lock);
-                if (!error) error = std::current_exception();
-                next.store(count);
-            }
-        };
-        std::vector<std::thread> pool;
-        pool.reserve(helpers - 1);
-        try {
-            for (size_t t = 1; t < helpers; ++t) pool.emplace_back(work);
-        } catch (...) {
-            next.store(count);
-            for (std::thread& thread : pool) thread.join();
-            throw;
-        }
-        work();
-        for (std::thread& thread : pool) thread.join();
-        if (error) std::rethrow_exception(error);
-    }
-
-    template <typename F>
-    void blocks(size_t count, const F& body) const {
-        run((count + kBlock - 1) / kBlock, [&](size_t b) { body(b * kBlock, std::min(count, (b + 1) * kBlock)); });
-    }
-
-private:
-    int threads_;
-};
-
 // ---- names --------------------------------------------------------------------------
 
 uint64_t hashName(Text s) {
@@ -410,10 +362,10 @@ public:
         while (capacity < 2 * names.size()) capacity <<= 1;
         mask_ = capacity - 1;
         slots_.reset(new std::atomic<uint64_t>[capacity]);
-        workers.blocks(capacity, [&](size_t b, size_t e) {
+        workers.blocks(capacity, kBlock, [&](size_t b, size_t e) {
             for (size_t i = b; i < e; ++i) slots_[i].store(kEmpty, std::memory_order_relaxed);
         });
-        workers.blocks(names.size(), [&](size_t b, size_t e) {
+        workers.blocks(names.size(), kBlock, [&](size_t b, size_t e) {
             for (size_t i = b; i < e; ++i) insert(static_cast<uint32_t>(i));
         });
     }
@@ -509,7 +461,7 @@ void storeNames(const std::vector<Text>& names, const Workers& workers, std::str
     start.assign(names.size() + 1, 0);
     for (size_t i = 0; i < names.size(); ++i) start[i + 1] = start[i] + static_cast<int64_t>(names[i].size());
     blob.resize(static_cast<size_t>(start.back()));
-    workers.blocks(names.size(), [&](size_t b, size_t e) {
+    workers.blocks(names.size(), kBlock, [&](size_t b, size_t e) {
         for (size_t i = b; i < e; ++i) {
             if (!names[i].empty()) std::memcpy(blob.data() + start[i], names[i].data(), names[i].size());
         }
@@ -915,7 +867,7 @@ void parseNets(const fs::path& path, Text text, const Workers& workers, const Na
     book.pin_direction.resize(static_cast<size_t>(pins));
     std::mutex failure_lock;
     PinFailure failure;
-    workers.blocks(nets, [&](size_t b, size_t e) {
+    workers.blocks(nets, kBlock, [&](size_t b, size_t e) {
         // The block's pins are contiguous: read every line up to the first
         // malformed one, then look the module names up together.
         const int64_t first_pin = book.net_pin_start[b];

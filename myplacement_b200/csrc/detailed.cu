@@ -31,6 +31,7 @@
 #include "common.cuh"
 #include "detailed.hpp"
 #include "setup.hpp"
+#include "workers.hpp"
 
 namespace mpgp {
 namespace {
@@ -39,6 +40,7 @@ constexpr int kWindow = 4;
 constexpr int kOrders = 24;
 constexpr int kCurrentLane = kOrders;  // the lane that evaluates the placement as it is
 constexpr int kWindowsPerBlock = 8;
+constexpr int kSpeculations = 3;  // rounds of speculative re-decision on the device
 constexpr int kOrientationUnknown = 8;
 constexpr double kLargest = std::numeric_limits<double>::max();
 
@@ -84,8 +86,8 @@ __global__ void __launch_bounds__(32 * kWindowsPerBlock)
     windowOrdersKernel(const double2* __restrict__ center, const double2* __restrict__ size,
                        const int* __restrict__ pin_module, const double2* __restrict__ pin_offset,
                        const int* __restrict__ net_pin_start, const double* __restrict__ net_weight,
-                       WindowArrays windows, int window_count, int* __restrict__ best_order,
-                       double* __restrict__ value_before, double* __restrict__ value_after) {
+                       WindowArrays windows, int window_count, double epsilon, int* __restrict__ best_order,
+                       uint8_t* __restrict__ decided, double2* __restrict__ moved_center) {
     const int lane = threadIdx.x & 31;
     const int w = blockIdx.x * kWindowsPerBlock + static_cast<int>(threadIdx.x >> 5);
     if (w >= window_count) return;  // whole warps leave together
@@ -174,9 +176,96 @@ __global__ void __launch_bounds__(32 * kWindowsPerBlock)
     const double after = __shfl_sync(0xffffffffu, plain, index);
     if (lane == 0) {
         best_order[w] = index;
-        value_before[w] = before;
-        value_after[w] = after;
+        decided[w] = index > 0 && index < kOrders && after < before - epsilon ? 1 : 0;
     }
+    if (lane == index) {  // where the best order puts the window's cells (applyOrder's arithmetic)
+#pragma unroll
+        for (int i = 0; i < kWindow; ++i) moved_center[module[i]] = make_double2(cx[i], cy[i]);
+    }
+}
+
+// transformOffset (PlacementDatabase.cpp:55-68).
+__host__ __device__ inline double2 transformed(double2 o, int orientation) {
+    switch (orientation) {
+        case 1: return make_double2(-o.x, -o.y);
+        case 2: return make_double2(-o.y, o.x);
+        case 3: return make_double2(o.y, -o.x);
+        case 4: return make_double2(-o.x, o.y);
+        case 5: return make_double2(o.x, -o.y);
+        case 6: return make_double2(o.y, o.x);
+        case 7: return make_double2(-o.y, -o.x);
+        default: return o;
+    }
+}
+
+// The host's before / after values of every window (its best order against
+// its current placement) on the assumption that each earlier window decided as
+// `decided_in` says, and the decisions they give.  A cell of an earlier window
+// assumed accepted sits where that window's best order puts it, with the
+// orientation of its row; every other cell is where the pass found it.  One
+// thread per window folds its nets in order, products and sums rounded
+// separately, as the host does.
+__global__ void __launch_bounds__(256)
+    speculativeValuesKernel(const double2* __restrict__ center, const double2* __restrict__ moved_center,
+                            const int* __restrict__ owner, const int8_t* __restrict__ moved_orientation,
+                            const double2* __restrict__ raw_offset, const double2* __restrict__ pin_offset,
+                            const int* __restrict__ pin_module, const int* __restrict__ net_pin_start,
+                            const double* __restrict__ net_weight, WindowArrays windows, int window_count,
+                            const int* __restrict__ best_order, double epsilon, const uint8_t* __restrict__ decided_in,
+                            uint8_t* __restrict__ decided_out, double* __restrict__ value_before,
+                            double* __restrict__ value_after) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= window_count) return;
+    const int best = best_order[w];
+    if (best <= 0 || best >= kOrders) {
+        decided_out[w] = 0;
+        return;
+    }
+    const int4 m4 = windows.modules[w];
+    double before = 0.0;
+    double after = 0.0;
+    for (int e = windows.net_start[w]; e < windows.net_start[w + 1]; ++e) {
+        const int net = windows.nets[e];
+        double min_b = kLargest, max_b = -kLargest, min_by = kLargest, max_by = -kLargest;
+        double min_a = kLargest, max_a = -kLargest, min_ay = kLargest, max_ay = -kLargest;
+        for (int p = net_pin_start[net]; p < net_pin_start[net + 1]; ++p) {
+            const int m = pin_module[p];
+            double2 offset = pin_offset[p];
+            double2 now_c;   // the cell now (before)
+            double2 then_c;  // the cell with this window's best order applied (after)
+            if (m == m4.x || m == m4.y || m == m4.z || m == m4.w) {
+                now_c = center[m];
+                then_c = moved_center[m];  // its orientation changes only once accepted
+            } else {
+                const int j = owner[m];
+                if (j >= 0 && j < w && decided_in[j] != 0) {
+                    now_c = moved_center[m];
+                    offset = transformed(raw_offset[p], moved_orientation[m]);
+                } else {
+                    now_c = center[m];
+                }
+                then_c = now_c;
+            }
+            const double bx = now_c.x + offset.x;
+            const double by = now_c.y + offset.y;
+            const double ax = then_c.x + offset.x;
+            const double ay = then_c.y + offset.y;
+            min_b = bx < min_b ? bx : min_b;
+            max_b = max_b < bx ? bx : max_b;
+            min_by = by < min_by ? by : min_by;
+            max_by = max_by < by ? by : max_by;
+            min_a = ax < min_a ? ax : min_a;
+            max_a = max_a < ax ? ax : max_a;
+            min_ay = ay < min_ay ? ay : min_ay;
+            max_ay = max_ay < ay ? ay : max_ay;
+        }
+        const double weight = net_weight[net];
+        before = __dadd_rn(before, __dmul_rn(weight, (max_b - min_b) + (max_by - min_by)));
+        after = __dadd_rn(after, __dmul_rn(weight, (max_a - min_a) + (max_ay - min_ay)));
+    }
+    value_before[w] = before;
+    value_after[w] = after;
+    decided_out[w] = after < before - epsilon ? 1 : 0;
 }
 
 // ---- host ---------------------------------------------------------------------------------
@@ -341,30 +430,39 @@ struct Placement {
         }
     }
 
-    // calculateHpwl (Metrics.cpp:128-147).
-    [[nodiscard]] double hpwl() const {
+    // calculateHpwl (Metrics.cpp:128-147): the nets' terms on several threads,
+    // summed in net order.
+    [[nodiscard]] double hpwl(const Workers& workers) const {
+        std::vector<double> term(static_cast<std::size_t>(d.net_count), 0.0);
+        workers.blocks(term.size(), 8192, [&](std::size_t b, std::size_t e) {
+            for (std::size_t n = b; n < e; ++n) term[n] = netTerm(static_cast<int32_t>(n));
+        });
         double result = 0.0;
         for (int32_t n = 0; n < d.net_count; ++n) {
-            if (d.net_pin_start[n + 1] - d.net_pin_start[n] < 2) continue;
-            double min_x = std::numeric_limits<double>::infinity();
-            double max_x = -std::numeric_limits<double>::infinity();
-            double min_y = std::numeric_limits<double>::infinity();
-            double max_y = -std::numeric_limits<double>::infinity();
-            for (int64_t p = d.net_pin_start[n]; p < d.net_pin_start[n + 1]; ++p) {
-                const int32_t m = d.pin_module[p];
-                double ox = 0.0;
-                double oy = 0.0;
-                transform(d.pin_offset_x[p], d.pin_offset_y[p], orientation[m], ox, oy);
-                const double x = cx[m] + ox;
-                const double y = cy[m] + oy;
-                min_x = std::min(min_x, x);
-                max_x = std::max(max_x, x);
-                min_y = std::min(min_y, y);
-                max_y = std::max(max_y, y);
-            }
-            result += d.net_weight[n] * ((max_x - min_x) + (max_y - min_y));
+            if (d.net_pin_start[n + 1] - d.net_pin_start[n] >= 2) result += term[n];
         }
         return result;
+    }
+
+    // One net's weighted HPWL at the current placement.
+    [[nodiscard]] double netTerm(int32_t n) const {
+        double min_x = std::numeric_limits<double>::infinity();
+        double max_x = -std::numeric_limits<double>::infinity();
+        double min_y = std::numeric_limits<double>::infinity();
+        double max_y = -std::numeric_limits<double>::infinity();
+        for (int64_t p = d.net_pin_start[n]; p < d.net_pin_start[n + 1]; ++p) {
+            const int32_t m = d.pin_module[p];
+            double ox = 0.0;
+            double oy = 0.0;
+            transform(d.pin_offset_x[p], d.pin_offset_y[p], orientation[m], ox, oy);
+            const double x = cx[m] + ox;
+            const double y = cy[m] + oy;
+            min_x = std::min(min_x, x);
+            max_x = std::max(max_x, x);
+            min_y = std::min(min_y, y);
+            max_y = std::max(max_y, y);
+        }
+        return d.net_weight[n] * ((max_x - min_x) + (max_y - min_y));
     }
 };
 
@@ -388,9 +486,12 @@ struct Windows {
 };
 
 // buildRowSegments (:238-274) and makeWindow (:276-293) for one pass: the
-// windows in the reference's order, whichever list they go to.
+// windows in the reference's order, whichever list they go to.  Rows are
+// independent: each sorts its cells (in module order before the sort, as the
+// reference collects them, so std::sort leaves ties as the reference's does)
+// and cuts its segments and windows on a thread of its own.
 void buildWindows(const Placement& s, const std::vector<uint8_t>& standard, int phase, uint64_t maximum_net_degree,
-                  Windows& out) {
+                  const Workers& workers, Windows& out) {
     const mpgp_design& d = s.d;
     out.clear();
     if (d.row_count == 0) return;
@@ -409,61 +510,95 @@ void buildWindows(const Placement& s, const std::vector<uint8_t>& standard, int 
         return std::abs(centre(left) - coordinate) <= std::abs(centre(right) - coordinate) ? left : right;
     };
     constexpr double kSegmentEpsilon = 1e-6;
-    std::vector<std::vector<int32_t>> cells_by_row(static_cast<std::size_t>(d.row_count));
-    for (int32_t m = 0; m < d.module_count; ++m) {
-        if (standard[m] == 0) continue;
-        const std::size_t r = nearestRow(s.cy[m]);
-        if (std::abs(s.lowerLeftY(m) - d.row_bottom[r]) <= kSegmentEpsilon) cells_by_row[r].push_back(m);
+    const std::size_t modules = static_cast<std::size_t>(d.module_count);
+    const std::size_t rows = static_cast<std::size_t>(d.row_count);
+    std::vector<int32_t> row_of(modules, -1);
+    workers.blocks(modules, 16384, [&](std::size_t b, std::size_t e) {
+        for (std::size_t m = b; m < e; ++m) {
+            if (standard[m] == 0) continue;
+            const std::size_t r = nearestRow(s.cy[m]);
+            if (std::abs(s.lowerLeftY(static_cast<int>(m)) - d.row_bottom[r]) <= kSegmentEpsilon) {
+                row_of[m] = static_cast<int32_t>(r);
+            }
+        }
+    });
+    std::vector<std::size_t> row_start(rows + 1, 0);
+    for (const int32_t r : row_of) {
+        if (r >= 0) ++row_start[static_cast<std::size_t>(r) + 1];
     }
-    std::vector<int32_t> segment;
-    std::vector<int32_t> window_nets;
-    const auto emitWindows = [&](int32_t r) {
-        if (segment.size() < 2U) return;
-        for (std::size_t start = static_cast<std::size_t>(phase); start + 1U < segment.size(); start += kWindow) {
-            const std::size_t count = std::min<std::size_t>(kWindow, segment.size() - start);
-            if (count < 2U) break;
-            window_nets.clear();
-            for (std::size_t i = 0; i < count; ++i) {
-                const int32_t m = segment[start + i];
-                for (int64_t k = s.module_pin_start[m]; k < s.module_pin_start[m + 1]; ++k) {
-                    window_nets.push_back(s.pin_net[s.module_pins[k]]);
-                }
-            }
-            std::sort(window_nets.begin(), window_nets.end());
-            window_nets.erase(std::unique(window_nets.begin(), window_nets.end()), window_nets.end());
-            bool device = count == static_cast<std::size_t>(kWindow) && !window_nets.empty();
-            for (const int32_t n : window_nets) {
-                if (static_cast<uint64_t>(d.net_pin_start[n + 1] - d.net_pin_start[n]) > maximum_net_degree) {
-                    device = false;
-                }
-            }
-            out.row.push_back(r);
-            out.count.push_back(static_cast<int32_t>(count));
-            for (std::size_t i = 0; i < kWindow; ++i) out.modules.push_back(i < count ? segment[start + i] : -1);
-            out.nets.insert(out.nets.end(), window_nets.begin(), window_nets.end());
-            out.net_start.push_back(static_cast<int64_t>(out.nets.size()));
-            out.device.push_back(device ? 1 : 0);
+    for (std::size_t r = 0; r < rows; ++r) row_start[r + 1] += row_start[r];
+    std::vector<int32_t> cells(row_start[rows]);
+    {
+        std::vector<std::size_t> fill(row_start.begin(), row_start.end() - 1);
+        for (std::size_t m = 0; m < modules; ++m) {
+            if (row_of[m] >= 0) cells[fill[static_cast<std::size_t>(row_of[m])]++] = static_cast<int32_t>(m);
         }
+    }
+
+    struct RowWindows {
+        std::vector<int32_t> count, modules, nets;
+        std::vector<int64_t> net_end;
+        std::vector<uint8_t> device;
     };
-    for (int32_t r = 0; r < d.row_count; ++r) {
-        std::vector<int32_t>& cells = cells_by_row[r];
-        if (cells.size() < 2U) continue;
-        std::sort(cells.begin(), cells.end(),
+    std::vector<RowWindows> per_row(rows);
+    workers.run(rows, [&](std::size_t r) {
+        if (row_start[r + 1] - row_start[r] < 2U) return;
+        std::vector<int32_t> row_cells(cells.begin() + static_cast<std::ptrdiff_t>(row_start[r]),
+                                       cells.begin() + static_cast<std::ptrdiff_t>(row_start[r + 1]));
+        std::sort(row_cells.begin(), row_cells.end(),
                   [&](int32_t a, int32_t b) { return s.lowerLeftX(a) < s.lowerLeftX(b); });
-        segment.clear();
-        for (const int32_t m : cells) {
-            if (!segment.empty()) {
-                const int32_t previous = segment.back();
-                const double expected =
-                    s.lowerLeftX(previous) + roundedWidth(d.module_width[previous], d.row_site_spacing[r]);
-                if (std::abs(s.lowerLeftX(m) - expected) > kSegmentEpsilon) {
-                    emitWindows(r);
-                    segment.clear();
+        RowWindows& mine = per_row[r];
+        std::vector<int32_t> window_nets;
+        const auto emit = [&](std::size_t first, std::size_t size) {
+            if (size < 2U) return;
+            for (std::size_t start = static_cast<std::size_t>(phase); start + 1U < size; start += kWindow) {
+                const std::size_t count = std::min<std::size_t>(kWindow, size - start);
+                if (count < 2U) break;
+                window_nets.clear();
+                for (std::size_t i = 0; i < count; ++i) {
+                    const int32_t m = row_cells[first + start + i];
+                    for (int64_t k = s.module_pin_start[m]; k < s.module_pin_start[m + 1]; ++k) {
+                        window_nets.push_back(s.pin_net[s.module_pins[k]]);
+                    }
                 }
+                std::sort(window_nets.begin(), window_nets.end());
+                window_nets.erase(std::unique(window_nets.begin(), window_nets.end()), window_nets.end());
+                bool device = count == static_cast<std::size_t>(kWindow) && !window_nets.empty();
+                for (const int32_t n : window_nets) {
+                    if (static_cast<uint64_t>(d.net_pin_start[n + 1] - d.net_pin_start[n]) > maximum_net_degree) {
+                        device = false;
+                    }
+                }
+                mine.count.push_back(static_cast<int32_t>(count));
+                for (std::size_t i = 0; i < kWindow; ++i) {
+                    mine.modules.push_back(i < count ? row_cells[first + start + i] : -1);
+                }
+                mine.nets.insert(mine.nets.end(), window_nets.begin(), window_nets.end());
+                mine.net_end.push_back(static_cast<int64_t>(mine.nets.size()));
+                mine.device.push_back(device ? 1 : 0);
             }
-            segment.push_back(m);
+        };
+        std::size_t first = 0;
+        for (std::size_t i = 1; i < row_cells.size(); ++i) {
+            const int32_t previous = row_cells[i - 1];
+            const double expected =
+                s.lowerLeftX(previous) + roundedWidth(d.module_width[previous], d.row_site_spacing[r]);
+            if (std::abs(s.lowerLeftX(row_cells[i]) - expected) > kSegmentEpsilon) {
+                emit(first, i - first);
+                first = i;
+            }
         }
-        emitWindows(r);
+        emit(first, row_cells.size() - first);
+    });
+    for (std::size_t r = 0; r < rows; ++r) {
+        const RowWindows& mine = per_row[r];
+        const int64_t base = static_cast<int64_t>(out.nets.size());
+        out.row.insert(out.row.end(), mine.count.size(), static_cast<int32_t>(r));
+        out.count.insert(out.count.end(), mine.count.begin(), mine.count.end());
+        out.modules.insert(out.modules.end(), mine.modules.begin(), mine.modules.end());
+        out.nets.insert(out.nets.end(), mine.nets.begin(), mine.nets.end());
+        for (const int64_t end : mine.net_end) out.net_start.push_back(base + end);
+        out.device.insert(out.device.end(), mine.device.begin(), mine.device.end());
     }
 }
 
@@ -526,9 +661,10 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
     for (int32_t m = 0; m < d.module_count; ++m) standard[m] = derived.is_fixed[m] == 0 && derived.is_macro[m] == 0;
     const auto rowOrientation = [&](int r) { return row_orientation != nullptr ? row_orientation[r] : 0; };
 
+    const Workers workers = Workers::all();
     Placement s(d);
     result = mpgp_detailed_result{};
-    result.hpwl_before = s.hpwl();
+    result.hpwl_before = s.hpwl(workers);
     result.cuda_device_used = options.cuda_device;
     const auto started = std::chrono::steady_clock::now();
 
@@ -539,15 +675,21 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
     const std::size_t nets = static_cast<std::size_t>(d.net_count);
     const std::size_t window_capacity = modules / kWindow + 1;
     uint64_t reserved = 0;
-    DeviceArray<double2> center, size, pin_offset;
-    DeviceArray<int> pin_module, net_pin_start;
+    DeviceArray<double2> center, moved_center, size, pin_offset, raw_offset;
+    DeviceArray<int> pin_module, net_pin_start, owner;
+    DeviceArray<int8_t> moved_orientation;
     DeviceArray<double> net_weight;
     DeviceArray<int4> window_modules;
     DeviceArray<double> window_start, window_bottom, window_spacing, value_before, value_after;
     DeviceArray<int> window_net_start, window_nets, best_order;
+    DeviceArray<uint8_t> decided[2];
     center.allocate(modules, reserved, limit, "CUDA detailed module centers");
+    moved_center.allocate(modules, reserved, limit, "CUDA detailed moved centers");
+    owner.allocate(modules, reserved, limit, "CUDA detailed window owners");
+    moved_orientation.allocate(modules, reserved, limit, "CUDA detailed moved orientations");
     size.allocate(modules, reserved, limit, "CUDA detailed module sizes");
     pin_offset.allocate(pins, reserved, limit, "CUDA detailed pin offsets");
+    raw_offset.allocate(pins, reserved, limit, "CUDA detailed raw pin offsets");
     pin_module.allocate(pins, reserved, limit, "CUDA detailed pin modules");
     net_pin_start.allocate(nets + 1, reserved, limit, "CUDA detailed net offsets");
     net_weight.allocate(nets, reserved, limit, "CUDA detailed net weights");
@@ -560,6 +702,8 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
     best_order.allocate(window_capacity, reserved, limit, "CUDA detailed best orders");
     value_before.allocate(window_capacity, reserved, limit, "CUDA detailed window values");
     value_after.allocate(window_capacity, reserved, limit, "CUDA detailed window values");
+    decided[0].allocate(window_capacity, reserved, limit, "CUDA detailed decisions");
+    decided[1].allocate(window_capacity, reserved, limit, "CUDA detailed decisions");
     result.cuda_reserved_memory_bytes = reserved;
 
     Stream stream;
@@ -570,6 +714,9 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
         std::vector<int> starts(nets + 1);
         for (std::size_t n = 0; n <= nets; ++n) starts[n] = static_cast<int>(d.net_pin_start[n]);
         const std::vector<double> weights(d.net_weight, d.net_weight + nets);
+        std::vector<double2> raw(pins);
+        for (std::size_t q = 0; q < pins; ++q) raw[q] = make_double2(d.pin_offset_x[q], d.pin_offset_y[q]);
+        raw_offset.upload(raw, stream.get());
         size.upload(sizes, stream.get());
         pin_module.upload(modules_of_pins, stream.get());
         net_pin_start.upload(starts, stream.get());
@@ -582,10 +729,11 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
     std::vector<double2> host_offset(pins);
     std::vector<int4> host_modules;
     std::vector<double> host_start, host_bottom, host_spacing, before, after;
-    std::vector<int> host_net_start, host_nets, best;
-    std::vector<uint8_t> moved(nets);
+    std::vector<int> host_net_start, host_nets, best, host_owner(modules);
+    std::vector<int8_t> host_moved_orientation(modules);
+    std::vector<uint8_t> assumed, divergent(nets);
     for (int pass = 0; pass < options.passes; ++pass) {
-        buildWindows(s, standard, (pass % 2) * (kWindow / 2), options.maximum_net_degree, windows);
+        buildWindows(s, standard, (pass % 2) * (kWindow / 2), options.maximum_net_degree, workers, windows);
         const std::size_t total = windows.row.size();
         host_modules.clear();
         host_start.clear();
@@ -611,16 +759,33 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
         best.assign(count, 0);
         before.assign(count, 0.0);
         after.assign(count, 0.0);
+        assumed.assign(count, 0);
         if (count > 0) {
             for (std::size_t m = 0; m < modules; ++m) host_center[m] = make_double2(s.cx[m], s.cy[m]);
-            for (std::size_t p = 0; p < pins; ++p) {
-                double ox = 0.0;
-                double oy = 0.0;
-                transform(d.pin_offset_x[p], d.pin_offset_y[p], s.orientation[d.pin_module[p]], ox, oy);
-                host_offset[p] = make_double2(ox, oy);
+            workers.blocks(pins, 65536, [&](std::size_t b, std::size_t e) {
+                for (std::size_t p = b; p < e; ++p) {
+                    double ox = 0.0;
+                    double oy = 0.0;
+                    transform(d.pin_offset_x[p], d.pin_offset_y[p], s.orientation[d.pin_module[p]], ox, oy);
+                    host_offset[p] = make_double2(ox, oy);
+                }
+            });
+            std::fill(host_owner.begin(), host_owner.end(), -1);
+            for (std::size_t m = 0; m < modules; ++m) host_moved_orientation[m] = static_cast<int8_t>(s.orientation[m]);
+            for (std::size_t j = 0; j < count; ++j) {
+                const int32_t* m = &windows.modules[on_device[j] * kWindow];
+                const int r = windows.row[on_device[j]];
+                for (int i = 0; i < kWindow; ++i) {
+                    host_owner[m[i]] = static_cast<int>(j);
+                    if (rowOrientation(r) != kOrientationUnknown) {
+                        host_moved_orientation[m[i]] = static_cast<int8_t>(rowOrientation(r));
+                    }
+                }
             }
             center.upload(host_center, stream.get());
             pin_offset.upload(host_offset, stream.get());
+            owner.upload(host_owner, stream.get());
+            moved_orientation.upload(host_moved_orientation, stream.get());
             window_modules.upload(host_modules, stream.get());
             window_start.upload(host_start, stream.get());
             window_bottom.upload(host_bottom, stream.get());
@@ -629,19 +794,32 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
             window_nets.upload(host_nets, stream.get());
             const WindowArrays arrays{window_modules.get(), window_start.get(), window_bottom.get(),
                                       window_spacing.get(), window_net_start.get(), window_nets.get()};
+            const int n = static_cast<int>(count);
             const unsigned blocks = static_cast<unsigned>((count + kWindowsPerBlock - 1) / kWindowsPerBlock);
             windowOrdersKernel<<<blocks, 32 * kWindowsPerBlock, 0, stream.get()>>>(
                 center.get(), size.get(), pin_module.get(), pin_offset.get(), net_pin_start.get(), net_weight.get(),
-                arrays, static_cast<int>(count), best_order.get(), value_before.get(), value_after.get());
+                arrays, n, options.improvement_epsilon, best_order.get(), decided[0].get(), moved_center.get());
             checkCuda(cudaGetLastError(), "windowOrdersKernel launch");
+            // Each iteration re-decides every window on the previous iteration's
+            // decisions; the last one's input is the assumption its values rest on.
+            int in = 0;
+            for (int iteration = 0; iteration < kSpeculations; ++iteration, in ^= 1) {
+                speculativeValuesKernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0, stream.get()>>>(
+                    center.get(), moved_center.get(), owner.get(), moved_orientation.get(), raw_offset.get(),
+                    pin_offset.get(), pin_module.get(), net_pin_start.get(), net_weight.get(), arrays, n,
+                    best_order.get(), options.improvement_epsilon, decided[in].get(), decided[in ^ 1].get(),
+                    value_before.get(), value_after.get());
+                checkCuda(cudaGetLastError(), "speculativeValuesKernel launch");
+            }
             best_order.download(best, stream.get());
+            decided[in ^ 1].download(assumed, stream.get());
             value_before.download(before, stream.get());
             value_after.download(after, stream.get());
             checkCuda(cudaStreamSynchronize(stream.get()), "windowOrdersKernel");
         }
 
         // The device's windows in order (:649-677), then the host's (:680-688).
-        std::fill(moved.begin(), moved.end(), 0);
+        std::fill(divergent.begin(), divergent.end(), 0);
         double wx[kWindow];
         double wy[kWindow];
         for (std::size_t j = 0; j < count; ++j) {
@@ -656,10 +834,13 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
             int order[kWindow];
             orderOf(order_index, order);
             const int r = windows.row[k];
+            // The device's values rest on the assumed decisions of the earlier
+            // windows; they are exact unless one whose cells sit on these nets
+            // decided otherwise.
             double value_now = before[j];
             double value_then = after[j];
             bool stale = false;
-            for (int e = 0; e < net_count && !stale; ++e) stale = moved[window_nets_k[e]] != 0;
+            for (int e = 0; e < net_count && !stale; ++e) stale = divergent[window_nets_k[e]] != 0;
             if (stale) {
                 for (int i = 0; i < kWindow; ++i) {
                     wx[i] = s.cx[m[i]];
@@ -669,10 +850,13 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
                 s.centersForOrder(m, order, kWindow, d.row_bottom[r], d.row_site_spacing[r], wx, wy);
                 value_then = s.windowHpwl(m, kWindow, window_nets_k, net_count, wx, wy);
             }
-            if (value_then < value_now - options.improvement_epsilon) {
+            const bool accept = value_then < value_now - options.improvement_epsilon;
+            if (accept) {
                 s.applyOrder(m, order, kWindow, d.row_bottom[r], d.row_site_spacing[r], rowOrientation(r));
                 ++result.accepted_operations;
-                for (int e = 0; e < net_count; ++e) moved[window_nets_k[e]] = 1;
+            }
+            if (accept != (assumed[j] != 0)) {
+                for (int e = 0; e < net_count; ++e) divergent[window_nets_k[e]] = 1;
             }
         }
         for (std::size_t k = 0; k < total; ++k) {
@@ -717,7 +901,7 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
         }
         result.completed_passes = pass + 1;
     }
-    result.hpwl_after = s.hpwl();
+    result.hpwl_after = s.hpwl(workers);
     result.elapsed_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count();
     std::copy(s.cx.begin(), s.cx.end(), module_x);
     std::copy(s.cy.begin(), s.cy.end(), module_y);
