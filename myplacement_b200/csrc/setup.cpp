@@ -5,6 +5,7 @@
 #include "setup.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -14,6 +15,7 @@
 #include <thread>
 
 #include "common.cuh"
+#include "workers.hpp"
 
 namespace mpgp {
 namespace {
@@ -78,6 +80,56 @@ struct Grid {
 
 bool finite(double value) { return std::isfinite(value); }
 
+// Host threads for a set-up step over `items` elements: one below `from`
+// (small designs, many of which the batched and served forms set up at once),
+// else up to eight.
+Workers setupWorkers(std::size_t items, std::size_t from = std::size_t{1} << 17) {
+    if (items < from) return Workers(1);
+    return Workers(static_cast<int>(std::min(8u, std::max(1u, std::thread::hardware_concurrency()))));
+}
+
+// std::sort's result on several threads: pieces sorted apart, then merged
+// pairwise (a sorted sequence of doubles is unique, so it is the same).
+void sortAscending(std::vector<double>& values) {
+    const Workers workers = setupWorkers(values.size(), std::size_t{1} << 16);
+    const std::size_t pieces = static_cast<std::size_t>(workers.threads());
+    if (pieces <= 1) {
+        std::sort(values.begin(), values.end());
+        return;
+    }
+    std::vector<std::size_t> bound(pieces + 1);
+    for (std::size_t k = 0; k <= pieces; ++k) bound[k] = values.size() * k / pieces;
+    const auto at = [&](std::size_t k) { return values.begin() + static_cast<std::ptrdiff_t>(bound[k]); };
+    workers.run(pieces, [&](std::size_t k) { std::sort(at(k), at(k + 1)); });
+    for (std::size_t width = 1; width < pieces; width *= 2) {
+        const std::size_t merges = (pieces + 2 * width - 1) / (2 * width);
+        workers.run(merges, [&](std::size_t m) {
+            const std::size_t first = 2 * width * m;
+            const std::size_t middle = std::min(first + width, pieces);
+            const std::size_t last = std::min(first + 2 * width, pieces);
+            if (middle < last) std::inplace_merge(at(first), at(middle), at(last));
+        });
+    }
+}
+
+
+// The first index in [0, count) at which `bad` holds, or count; the checks of
+// long ranges run on several threads.
+template <typename F>
+std::size_t firstBad(std::size_t count, const F& bad) {
+    std::atomic<std::size_t> first{count};
+    setupWorkers(count).blocks(count, 65536, [&](std::size_t b, std::size_t e) {
+        for (std::size_t i = b; i < e && i < first.load(std::memory_order_relaxed); ++i) {
+            if (!bad(i)) continue;
+            std::size_t seen = first.load(std::memory_order_relaxed);
+            while (i < seen && !first.compare_exchange_weak(seen, i, std::memory_order_relaxed)) {
+            }
+            return;
+        }
+    });
+    return first.load();
+}
+
 }  // namespace
 
 void defaultOptions(mpgp_options& o) {
@@ -141,13 +193,21 @@ void validateDesign(const mpgp_design& d) {
             "net_pin_start must begin at 0 and end at pin_count.");
     require(d.pin_count < static_cast<int64_t>(std::numeric_limits<int32_t>::max()),
             "The engine indexes pins with 32-bit integers.");
-    for (int32_t n = 0; n < d.net_count; ++n) {
-        require(d.net_pin_start[n + 1] >= d.net_pin_start[n], "net_pin_start must be non-decreasing.");
-        require(finite(d.net_weight[n]), "Net weights must be finite.");
+    // The first net, then the first pin, that fails a check fails with that check's message.
+    const std::size_t net = firstBad(static_cast<std::size_t>(d.net_count), [&](std::size_t n) {
+        return !(d.net_pin_start[n + 1] >= d.net_pin_start[n]) || !finite(d.net_weight[n]);
+    });
+    if (net < static_cast<std::size_t>(d.net_count)) {
+        require(d.net_pin_start[net + 1] >= d.net_pin_start[net], "net_pin_start must be non-decreasing.");
+        require(finite(d.net_weight[net]), "Net weights must be finite.");
     }
-    for (int64_t p = 0; p < d.pin_count; ++p) {
-        require(d.pin_module[p] >= 0 && d.pin_module[p] < d.module_count, "Pin refers to an unknown module.");
-        require(finite(d.pin_offset_x[p]) && finite(d.pin_offset_y[p]), "Pin offsets must be finite.");
+    const std::size_t pin = firstBad(static_cast<std::size_t>(d.pin_count), [&](std::size_t p) {
+        return !(d.pin_module[p] >= 0 && d.pin_module[p] < d.module_count) || !finite(d.pin_offset_x[p]) ||
+               !finite(d.pin_offset_y[p]);
+    });
+    if (pin < static_cast<std::size_t>(d.pin_count)) {
+        require(d.pin_module[pin] >= 0 && d.pin_module[pin] < d.module_count, "Pin refers to an unknown module.");
+        require(finite(d.pin_offset_x[pin]) && finite(d.pin_offset_y[pin]), "Pin offsets must be finite.");
     }
     for (int32_t m = 0; m < d.module_count; ++m) {
         require(d.module_width[m] >= 0.0 && d.module_height[m] >= 0.0, "A module cannot have a negative size.");
@@ -322,7 +382,7 @@ std::vector<Filler> createFillers(const mpgp_design& d, const DerivedDesign& der
     const double filler_area = required_filler_charge_area / std::max(t, kEpsilon);
     if (filler_area <= kEpsilon || areas.empty() || options.maximum_fillers == 0U) return {};
 
-    std::sort(areas.begin(), areas.end());
+    sortAscending(areas);
     const std::size_t lower = areas.size() / 10U;
     const std::size_t upper = std::max(lower + 1U, areas.size() - areas.size() / 10U);
     const double representative_area =
@@ -364,25 +424,33 @@ Problem buildProblem(const mpgp_design& d, const DerivedDesign& derived, const m
     for (std::size_t index = 0; index < derived.movable.size(); ++index) {
         module_particle[derived.movable[index]] = static_cast<int32_t>(index);
     }
-    problem.net_weight.assign(d.net_weight, d.net_weight + d.net_count);
-    problem.net_pin_start.assign(d.net_pin_start, d.net_pin_start + d.net_count + 1);
-    problem.pin_particle.resize(static_cast<std::size_t>(d.pin_count));
-    problem.pin_x.resize(static_cast<std::size_t>(d.pin_count));
-    problem.pin_y.resize(static_cast<std::size_t>(d.pin_count));
+    std::exception_ptr pins_error;
     std::thread pins([&] {
-        for (int64_t p = 0; p < d.pin_count; ++p) {
-            const int32_t m = d.pin_module[p];
-            double ox, oy;
-            transformOffset(d.pin_offset_x[p], d.pin_offset_y[p], orientationOf(d, m), ox, oy);
-            const int32_t particle = module_particle[m];
-            problem.pin_particle[p] = particle;
-            if (particle >= 0) {
-                problem.pin_x[p] = ox;
-                problem.pin_y[p] = oy;
-            } else {
-                problem.pin_x[p] = d.module_x[m] + ox;  // pinPosition (PlacementDatabase.cpp:138-142)
-                problem.pin_y[p] = d.module_y[m] + oy;
-            }
+        try {
+            problem.net_weight.assign(d.net_weight, d.net_weight + d.net_count);
+            problem.net_pin_start.assign(d.net_pin_start, d.net_pin_start + d.net_count + 1);
+            const std::size_t count = static_cast<std::size_t>(d.pin_count);
+            problem.pin_particle.resize(count);
+            problem.pin_x.resize(count);
+            problem.pin_y.resize(count);
+            setupWorkers(count).blocks(count, 65536, [&](std::size_t b, std::size_t e) {
+                for (std::size_t p = b; p < e; ++p) {
+                    const int32_t m = d.pin_module[p];
+                    double ox, oy;
+                    transformOffset(d.pin_offset_x[p], d.pin_offset_y[p], orientationOf(d, m), ox, oy);
+                    const int32_t particle = module_particle[m];
+                    problem.pin_particle[p] = particle;
+                    if (particle >= 0) {
+                        problem.pin_x[p] = ox;
+                        problem.pin_y[p] = oy;
+                    } else {
+                        problem.pin_x[p] = d.module_x[m] + ox;  // pinPosition (PlacementDatabase.cpp:138-142)
+                        problem.pin_y[p] = d.module_y[m] + oy;
+                    }
+                }
+            });
+        } catch (...) {
+            pins_error = std::current_exception();
         }
     });
     struct Join {
@@ -402,44 +470,46 @@ Problem buildProblem(const mpgp_design& d, const DerivedDesign& derived, const m
             "The engine indexes particles with 32-bit integers.");
     problem.particle_count = static_cast<int64_t>(particles);
     problem.movable_count = static_cast<int64_t>(movable);
-    problem.width.reserve(particles);
-    problem.height.reserve(particles);
-    problem.layer.reserve(particles);
-    problem.charge.reserve(particles);
-    problem.pin_count.reserve(particles);
+    problem.width.resize(particles);
+    problem.height.resize(particles);
+    problem.layer.resize(particles);
+    problem.charge.resize(particles);
+    problem.pin_count.resize(particles);
+    problem.precond_base.resize(particles);
     const double t = options.target_density;
-    for (std::size_t index = 0; index < movable; ++index) {
-        const int32_t m = derived.movable[index];
-        problem.width.push_back(d.module_width[m]);
-        problem.height.push_back(d.module_height[m]);
-        problem.layer.push_back(derived.is_macro[m] ? MPGP_LAYER_MACRO : MPGP_LAYER_STANDARD);
-        const double area = d.module_width[m] * d.module_height[m];
-        problem.charge.push_back(derived.is_macro[m] ? t * area : area);  // densityChargeArea (Support.cpp:105-107)
-        problem.pin_count.push_back(derived.pin_count[m]);
-    }
-    for (const Filler& filler : fillers) {
-        problem.width.push_back(filler.width);
-        problem.height.push_back(filler.height);
-        problem.layer.push_back(MPGP_LAYER_FILLER);
-        problem.charge.push_back(t * (filler.width * filler.height));  // Support.cpp:109-111
-        problem.pin_count.push_back(0);
-    }
-
-    // initializePreconditioner (AdaptiveGlobalPlacer.cpp:358-375).
+    // initializePreconditioner (AdaptiveGlobalPlacer.cpp:358-375): the area sum in module order.
     double total_movable_area = 0.0;
     for (const int32_t m : derived.movable) total_movable_area += d.module_width[m] * d.module_height[m];
     const double average_movable_area =
         total_movable_area / static_cast<double>(std::max<std::size_t>(1U, movable));
-    problem.precond_base.reserve(particles);
-    for (std::size_t index = 0; index < particles; ++index) {
-        const double area = problem.width[index] * problem.height[index];
-        const double area_ratio = std::max(area / std::max(average_movable_area, kEpsilon), 0.1);
-        const double pin_factor = std::sqrt(1.0 + static_cast<double>(problem.pin_count[index]));
-        const double area_factor = 1.0 + std::sqrt(area_ratio);
-        problem.precond_base.push_back(1.0 / (pin_factor * area_factor));
-    }
+    setupWorkers(particles).blocks(particles, 32768, [&](std::size_t b, std::size_t e) {
+        for (std::size_t index = b; index < e; ++index) {
+            if (index < movable) {
+                const int32_t m = derived.movable[index];
+                problem.width[index] = d.module_width[m];
+                problem.height[index] = d.module_height[m];
+                problem.layer[index] = derived.is_macro[m] ? MPGP_LAYER_MACRO : MPGP_LAYER_STANDARD;
+                const double area = d.module_width[m] * d.module_height[m];
+                problem.charge[index] = derived.is_macro[m] ? t * area : area;  // densityChargeArea (Support.cpp:105-107)
+                problem.pin_count[index] = derived.pin_count[m];
+            } else {
+                const Filler& filler = fillers[index - movable];
+                problem.width[index] = filler.width;
+                problem.height[index] = filler.height;
+                problem.layer[index] = MPGP_LAYER_FILLER;
+                problem.charge[index] = t * (filler.width * filler.height);  // Support.cpp:109-111
+                problem.pin_count[index] = 0;
+            }
+            const double area = problem.width[index] * problem.height[index];
+            const double area_ratio = std::max(area / std::max(average_movable_area, kEpsilon), 0.1);
+            const double pin_factor = std::sqrt(1.0 + static_cast<double>(problem.pin_count[index]));
+            const double area_factor = 1.0 + std::sqrt(area_ratio);
+            problem.precond_base[index] = 1.0 / (pin_factor * area_factor);
+        }
+    });
 
     pins.join();
+    if (pins_error) std::rethrow_exception(pins_error);
     return problem;
 }
 
