@@ -8,14 +8,18 @@
 // odd passes.  One warp evaluates one window: lanes 0..23 each place the cells
 // in one of the 24 orders (lexicographic, the order std::next_permutation
 // visits) and sum the weighted HPWL of the window's nets; lane 24 sums it for
-// the placement as it is.  Every lane accumulates twice: with fused
-// multiply-adds, which is what the reference's kernel compiles to and what
-// picks the best order, and with separately rounded products and sums, the host
-// arithmetic with which the reference accepts an order.  The windows are then
-// accepted in the reference's order.  A window none of whose nets an earlier
-// accepted window moved takes the device's values as they are; the others are
-// re-evaluated on the host against the placement as it stands, which is what
-// the reference does for every window.
+// the placement as it is.  The sum with fused multiply-adds (what the
+// reference's kernel compiles to) picks the best order.
+//
+// The reference then accepts the windows one after another, each by its host
+// arithmetic (products and sums rounded separately) against the placement the
+// earlier acceptances left.  A second kernel evaluates that rule
+// speculatively: every window's before and after values on the assumption
+// that each earlier window decided as the previous round said, for a few
+// rounds.  The host walks the windows in the reference's order and takes the
+// device's values unless a net of the window belongs to an earlier window
+// whose actual decision differed from the assumption; only those windows are
+// re-evaluated on the host.  The result is the reference's exactly.
 #include <cuda_runtime.h>
 
 #include <algorithm>
