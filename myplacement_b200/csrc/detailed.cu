@@ -48,27 +48,33 @@ constexpr int kSpeculations = 3;  // rounds of speculative re-decision on the de
 constexpr int kOrientationUnknown = 8;
 constexpr double kLargest = std::numeric_limits<double>::max();
 
-// Order k (0..23) of four cells in lexicographic order, as four 4-bit fields:
-// field i is the window cell placed i-th.  The Lehmer digits of k are k / 6,
-// k % 6 / 2 and k % 2; each picks a field of the cells not yet placed (`pool`,
-// packed the same way) and removes it.
-__host__ __device__ inline unsigned orderCode(int k) {
-    const unsigned digit[kWindow - 1] = {static_cast<unsigned>(k / 6), static_cast<unsigned>((k % 6) / 2),
-                                         static_cast<unsigned>(k % 2)};
+// Order k (0..n!-1) of n <= 4 cells in lexicographic order (the order
+// std::next_permutation visits from 0, 1, ..., n - 1), as 4-bit fields: field
+// i is the window cell placed i-th.  The Lehmer digits of k (k / (n-1)!, then
+// the remainder's digit for (n-2)!, ...) each pick a field of the cells not yet
+// placed (`pool`, packed the same way) and remove it.
+__host__ __device__ inline unsigned orderCode(int k, int n = kWindow) {
     unsigned pool = 0x3210u;
     unsigned code = 0u;
+    int rest = k;
 #pragma unroll
     for (int i = 0; i < kWindow - 1; ++i) {
-        const unsigned d = digit[i];
+        if (i >= n - 1) break;
+        const int place = n - 1 - i;
+        const int factorial = place == 3 ? 6 : place == 2 ? 2 : 1;
+        const unsigned d = static_cast<unsigned>(rest / factorial);
+        rest %= factorial;
         code |= ((pool >> (4u * d)) & 0xFu) << (4u * static_cast<unsigned>(i));
         pool = (pool & ((1u << (4u * d)) - 1u)) | ((pool >> (4u * (d + 1u))) << (4u * d));
     }
-    return code | ((pool & 0xFu) << 12u);
+    return code | ((pool & 0xFu) << (4u * static_cast<unsigned>(n - 1)));
 }
 
-inline void orderOf(int k, int order[kWindow]) {
-    const unsigned code = orderCode(k);
-    for (int i = 0; i < kWindow; ++i) order[i] = static_cast<int>((code >> (4u * static_cast<unsigned>(i))) & 0xFu);
+__host__ __device__ inline int factorialOf(int n) { return n == 4 ? 24 : n == 3 ? 6 : n == 2 ? 2 : 1; }
+
+inline void orderOf(int k, int order[kWindow], int n = kWindow) {
+    const unsigned code = orderCode(k, n);
+    for (int i = 0; i < n; ++i) order[i] = static_cast<int>((code >> (4u * static_cast<unsigned>(i))) & 0xFu);
 }
 
 // alignUp(width, 0, spacing) (DetailedPlacer.cpp:67-70), products and sums
@@ -270,6 +276,133 @@ __global__ void __launch_bounds__(256)
     value_before[w] = before;
     value_after[w] = after;
     decided_out[w] = after < before - epsilon ? 1 : 0;
+}
+
+// The windows the reference keeps on the host (segment ends of two or three
+// cells), those with nets to evaluate, in the reference's order.
+struct TailArrays {
+    const int4* modules;  // unused slots -1
+    const int* count;
+    const double* start_x;
+    const double* bottom;
+    const double* spacing;
+    const int* net_start;
+    const int* nets;
+};
+
+// Where each tail window's assumed order (-1: none) puts its cells.
+__global__ void __launch_bounds__(256)
+    tailPlacementKernel(TailArrays tail, int tail_count, const double2* __restrict__ size,
+                        const int8_t* __restrict__ assumed, double2* __restrict__ moved_center) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tail_count || assumed[t] < 0) return;
+    const int n = tail.count[t];
+    const int4 m4 = tail.modules[t];
+    const int module[kWindow] = {m4.x, m4.y, m4.z, m4.w};
+    const unsigned code = orderCode(assumed[t], n);
+    double cursor = tail.start_x[t];
+    for (int i = 0; i < n; ++i) {
+        const unsigned local = (code >> (4u * static_cast<unsigned>(i))) & 0xFu;
+        int placed = module[0];
+#pragma unroll
+        for (int j = 1; j < kWindow; ++j) placed = local == static_cast<unsigned>(j) ? module[j] : placed;
+        const double2 s = size[placed];
+        moved_center[placed] = make_double2(__dadd_rn(cursor, __dmul_rn(s.x, 0.5)),
+                                            __dadd_rn(tail.bottom[t], __dmul_rn(s.y, 0.5)));
+        cursor = __dadd_rn(cursor, roundedWidthDevice(s.x, tail.spacing[t]));
+    }
+}
+
+// optimizeCpuWindow (CudaDetailedPlacementBackend.cu:328-354) for every tail
+// window on the assumption that each earlier tail window took the order
+// `assumed_in` says: every order in lexicographic order, each taken when it
+// beats the best so far by more than epsilon, from the placement as it is.
+// Writes the order taken, or -1.  A cell of an earlier tail window assumed
+// reordered sits where that order puts it, with its row's orientation; every
+// other cell is where the four-cell windows left it.
+__global__ void __launch_bounds__(256)
+    tailOrdersKernel(const double2* __restrict__ center, const int8_t* __restrict__ orientation,
+                     const double2* __restrict__ moved_center, const int* __restrict__ owner, int tail_base,
+                     const int8_t* __restrict__ moved_orientation, const double2* __restrict__ raw_offset,
+                     const double2* __restrict__ size, const int* __restrict__ pin_module,
+                     const int* __restrict__ net_pin_start, const double* __restrict__ net_weight, TailArrays tail,
+                     int tail_count, double epsilon, const int8_t* __restrict__ assumed_in,
+                     int8_t* __restrict__ order_out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tail_count) return;
+    const int n = tail.count[t];
+    const int4 m4 = tail.modules[t];
+    const int module[kWindow] = {m4.x, m4.y, m4.z, m4.w};
+    double cx[kWindow];
+    double cy[kWindow];
+    // The window's weighted HPWL with its own cells at (cx, cy).
+    const auto value = [&]() {
+        double sum = 0.0;
+        for (int e = tail.net_start[t]; e < tail.net_start[t + 1]; ++e) {
+            const int net = tail.nets[e];
+            double min_x = kLargest, max_x = -kLargest, min_y = kLargest, max_y = -kLargest;
+            for (int p = net_pin_start[net]; p < net_pin_start[net + 1]; ++p) {
+                const int m = pin_module[p];
+                double2 c = center[m];
+                int turn = orientation[m];
+#pragma unroll
+                for (int i = 0; i < kWindow; ++i) {
+                    if (module[i] == m) c = make_double2(cx[i], cy[i]);
+                }
+                if (m != module[0] && m != module[1] && m != module[2] && m != module[3]) {
+                    const int j = owner[m] - tail_base;
+                    if (j >= 0 && j < t && assumed_in[j] >= 0) {
+                        c = moved_center[m];
+                        turn = moved_orientation[m];
+                    }
+                }
+                const double2 o = transformed(raw_offset[p], turn);
+                const double x = c.x + o.x;
+                const double y = c.y + o.y;
+                min_x = x < min_x ? x : min_x;
+                max_x = max_x < x ? x : max_x;
+                min_y = y < min_y ? y : min_y;
+                max_y = max_y < y ? y : max_y;
+            }
+            sum = __dadd_rn(sum, __dmul_rn(net_weight[net], (max_x - min_x) + (max_y - min_y)));
+        }
+        return sum;
+    };
+#pragma unroll
+    for (int i = 0; i < kWindow; ++i) {
+        const double2 c = module[i] >= 0 ? center[module[i]] : make_double2(0.0, 0.0);
+        cx[i] = c.x;
+        cy[i] = c.y;
+    }
+    double best = value();
+    int taken = -1;
+    for (int k = 0; k < factorialOf(n); ++k) {
+        const unsigned code = orderCode(k, n);
+        double cursor = tail.start_x[t];
+        for (int i = 0; i < n; ++i) {
+            const unsigned local = (code >> (4u * static_cast<unsigned>(i))) & 0xFu;
+            int placed = module[0];
+#pragma unroll
+            for (int j = 1; j < kWindow; ++j) placed = local == static_cast<unsigned>(j) ? module[j] : placed;
+            const double2 s = size[placed];
+            const double x = __dadd_rn(cursor, __dmul_rn(s.x, 0.5));
+            const double y = __dadd_rn(tail.bottom[t], __dmul_rn(s.y, 0.5));
+#pragma unroll
+            for (int j = 0; j < kWindow; ++j) {
+                if (local == static_cast<unsigned>(j)) {
+                    cx[j] = x;
+                    cy[j] = y;
+                }
+            }
+            cursor = __dadd_rn(cursor, roundedWidthDevice(s.x, tail.spacing[t]));
+        }
+        const double v = value();
+        if (v < best - epsilon) {
+            best = v;
+            taken = k;
+        }
+    }
+    order_out[t] = static_cast<int8_t>(taken);
 }
 
 // ---- host ---------------------------------------------------------------------------------
@@ -708,6 +841,20 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
     value_after.allocate(window_capacity, reserved, limit, "CUDA detailed window values");
     decided[0].allocate(window_capacity, reserved, limit, "CUDA detailed decisions");
     decided[1].allocate(window_capacity, reserved, limit, "CUDA detailed decisions");
+    const std::size_t tail_capacity = modules / 2 + 1;  // every window holds two cells at least
+    DeviceArray<int4> tail_modules;
+    DeviceArray<int> tail_count, tail_net_start;
+    DeviceArray<double> tail_start, tail_bottom, tail_spacing;
+    DeviceArray<int8_t> tail_decided[2], orientation_now;
+    tail_modules.allocate(tail_capacity, reserved, limit, "CUDA detailed tail windows");
+    tail_count.allocate(tail_capacity, reserved, limit, "CUDA detailed tail windows");
+    tail_start.allocate(tail_capacity, reserved, limit, "CUDA detailed tail windows");
+    tail_bottom.allocate(tail_capacity, reserved, limit, "CUDA detailed tail windows");
+    tail_spacing.allocate(tail_capacity, reserved, limit, "CUDA detailed tail windows");
+    tail_net_start.allocate(tail_capacity + 1, reserved, limit, "CUDA detailed tail window net offsets");
+    tail_decided[0].allocate(tail_capacity, reserved, limit, "CUDA detailed tail orders");
+    tail_decided[1].allocate(tail_capacity, reserved, limit, "CUDA detailed tail orders");
+    orientation_now.allocate(modules, reserved, limit, "CUDA detailed orientations");
     result.cuda_reserved_memory_bytes = reserved;
 
     Stream stream;
@@ -736,6 +883,10 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
     std::vector<int> host_net_start, host_nets, best, host_owner(modules);
     std::vector<int8_t> host_moved_orientation(modules);
     std::vector<uint8_t> assumed, divergent(nets);
+    std::vector<int4> tail_host_modules;
+    std::vector<int> tail_host_count, tail_host_net_start, tail_host_nets, tail_of_window;
+    std::vector<double> tail_host_start, tail_host_bottom, tail_host_spacing;
+    std::vector<int8_t> tail_result, tail_assumed, host_orientation_now(modules);
     for (int pass = 0; pass < options.passes; ++pass) {
         buildWindows(s, standard, (pass % 2) * (kWindow / 2), options.maximum_net_degree, workers, windows);
         const std::size_t total = windows.row.size();
@@ -760,6 +911,62 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
         const std::size_t count = on_device.size();
         require(count <= window_capacity && host_nets.size() <= std::max<std::size_t>(pins, 1),
                 "Detailed-placement window arrays exceed their capacity.");
+        // The host-rule windows with nets to evaluate (optimizeCpuWindow returns
+        // at once for the others).
+        tail_host_modules.clear();
+        tail_host_count.clear();
+        tail_host_start.clear();
+        tail_host_bottom.clear();
+        tail_host_spacing.clear();
+        tail_host_net_start.assign(1, 0);
+        tail_host_nets.clear();
+        tail_of_window.assign(total, -1);
+        for (std::size_t k = 0; k < total; ++k) {
+            if (windows.device[k] != 0 || windows.net_start[k + 1] == windows.net_start[k]) continue;
+            bool too_wide = false;
+            for (int64_t e = windows.net_start[k]; e < windows.net_start[k + 1]; ++e) {
+                const int32_t net = windows.nets[e];
+                too_wide |= static_cast<uint64_t>(d.net_pin_start[net + 1] - d.net_pin_start[net]) >
+                            options.maximum_net_degree;
+            }
+            if (too_wide) continue;
+            tail_of_window[k] = static_cast<int>(tail_host_count.size());
+            const int32_t* m = &windows.modules[k * kWindow];
+            tail_host_modules.push_back(make_int4(m[0], m[1], m[2], m[3]));
+            tail_host_count.push_back(windows.count[k]);
+            tail_host_start.push_back(s.lowerLeftX(m[0]));
+            tail_host_bottom.push_back(d.row_bottom[windows.row[k]]);
+            tail_host_spacing.push_back(d.row_site_spacing[windows.row[k]]);
+            for (int64_t e = windows.net_start[k]; e < windows.net_start[k + 1]; ++e) {
+                tail_host_nets.push_back(windows.nets[e]);
+            }
+            tail_host_net_start.push_back(static_cast<int>(tail_host_nets.size()));
+        }
+        const std::size_t tails = tail_host_count.size();
+        require(tails <= tail_capacity && tail_host_nets.size() <= std::max<std::size_t>(pins, 1),
+                "Detailed-placement tail window arrays exceed their capacity.");
+        if (count > 0 || tails > 0) {
+            // Owners: device window j as j, tail window t as count + t; and the
+            // orientation a moved cell takes.
+            std::fill(host_owner.begin(), host_owner.end(), -1);
+            for (std::size_t m = 0; m < modules; ++m) host_moved_orientation[m] = static_cast<int8_t>(s.orientation[m]);
+            const auto own = [&](std::size_t k, int value) {
+                const int32_t* m = &windows.modules[k * kWindow];
+                const int r = windows.row[k];
+                for (int i = 0; i < windows.count[k]; ++i) {
+                    host_owner[m[i]] = value;
+                    if (rowOrientation(r) != kOrientationUnknown) {
+                        host_moved_orientation[m[i]] = static_cast<int8_t>(rowOrientation(r));
+                    }
+                }
+            };
+            for (std::size_t j = 0; j < count; ++j) own(on_device[j], static_cast<int>(j));
+            for (std::size_t k = 0; k < total; ++k) {
+                if (tail_of_window[k] >= 0) own(k, static_cast<int>(count) + tail_of_window[k]);
+            }
+            owner.upload(host_owner, stream.get());
+            moved_orientation.upload(host_moved_orientation, stream.get());
+        }
         best.assign(count, 0);
         before.assign(count, 0.0);
         after.assign(count, 0.0);
@@ -774,22 +981,8 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
                     host_offset[p] = make_double2(ox, oy);
                 }
             });
-            std::fill(host_owner.begin(), host_owner.end(), -1);
-            for (std::size_t m = 0; m < modules; ++m) host_moved_orientation[m] = static_cast<int8_t>(s.orientation[m]);
-            for (std::size_t j = 0; j < count; ++j) {
-                const int32_t* m = &windows.modules[on_device[j] * kWindow];
-                const int r = windows.row[on_device[j]];
-                for (int i = 0; i < kWindow; ++i) {
-                    host_owner[m[i]] = static_cast<int>(j);
-                    if (rowOrientation(r) != kOrientationUnknown) {
-                        host_moved_orientation[m[i]] = static_cast<int8_t>(rowOrientation(r));
-                    }
-                }
-            }
             center.upload(host_center, stream.get());
             pin_offset.upload(host_offset, stream.get());
-            owner.upload(host_owner, stream.get());
-            moved_orientation.upload(host_moved_orientation, stream.get());
             window_modules.upload(host_modules, stream.get());
             window_start.upload(host_start, stream.get());
             window_bottom.upload(host_bottom, stream.get());
@@ -863,44 +1056,89 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
                 for (int e = 0; e < net_count; ++e) divergent[window_nets_k[e]] = 1;
             }
         }
+        // The host-rule windows: evaluated on the device the same speculative
+        // way, from the placement the four-cell windows left.
+        tail_result.assign(tails, -1);
+        tail_assumed.assign(tails, -1);
+        if (tails > 0) {
+            for (std::size_t m = 0; m < modules; ++m) {
+                host_center[m] = make_double2(s.cx[m], s.cy[m]);
+                host_orientation_now[m] = static_cast<int8_t>(s.orientation[m]);
+            }
+            center.upload(host_center, stream.get());
+            orientation_now.upload(host_orientation_now, stream.get());
+            tail_modules.upload(tail_host_modules, stream.get());
+            tail_count.upload(tail_host_count, stream.get());
+            tail_start.upload(tail_host_start, stream.get());
+            tail_bottom.upload(tail_host_bottom, stream.get());
+            tail_spacing.upload(tail_host_spacing, stream.get());
+            tail_net_start.upload(tail_host_net_start, stream.get());
+            window_nets.upload(tail_host_nets, stream.get());
+            checkCuda(cudaMemsetAsync(tail_decided[0].get(), 0xFF, tails, stream.get()), "tail orders");
+            const TailArrays tail{tail_modules.get(), tail_count.get(), tail_start.get(), tail_bottom.get(),
+                                  tail_spacing.get(), tail_net_start.get(), window_nets.get()};
+            const int n = static_cast<int>(tails);
+            const unsigned blocks = static_cast<unsigned>((tails + 255) / 256);
+            int in = 0;
+            for (int iteration = 0; iteration < kSpeculations; ++iteration, in ^= 1) {
+                if (iteration > 0) {
+                    tailPlacementKernel<<<blocks, 256, 0, stream.get()>>>(tail, n, size.get(), tail_decided[in].get(),
+                                                                         moved_center.get());
+                    checkCuda(cudaGetLastError(), "tailPlacementKernel launch");
+                }
+                tailOrdersKernel<<<blocks, 256, 0, stream.get()>>>(
+                    center.get(), orientation_now.get(), moved_center.get(), owner.get(), static_cast<int>(count),
+                    moved_orientation.get(), raw_offset.get(), size.get(), pin_module.get(), net_pin_start.get(),
+                    net_weight.get(), tail, n, options.improvement_epsilon, tail_decided[in].get(),
+                    tail_decided[in ^ 1].get());
+                checkCuda(cudaGetLastError(), "tailOrdersKernel launch");
+            }
+            tail_decided[in].download(tail_result, stream.get());
+            tail_decided[in ^ 1].download(tail_assumed, stream.get());
+            checkCuda(cudaStreamSynchronize(stream.get()), "tailOrdersKernel");
+        }
+        std::fill(divergent.begin(), divergent.end(), 0);
         for (std::size_t k = 0; k < total; ++k) {
             if (windows.device[k] != 0) continue;
             ++result.evaluated_windows;
+            const int t = tail_of_window[k];
+            if (t < 0) continue;  // no nets, or one above the degree limit: nothing to evaluate
             // optimizeCpuWindow (:328-354).
             const int32_t* m = &windows.modules[k * kWindow];
             const int n = windows.count[k];
             const int32_t* window_nets_k = &windows.nets[windows.net_start[k]];
             const int net_count = static_cast<int>(windows.net_start[k + 1] - windows.net_start[k]);
-            if (net_count == 0) continue;
-            bool too_wide = false;
-            for (int e = 0; e < net_count; ++e) {
-                const int32_t net = window_nets_k[e];
-                too_wide |= static_cast<uint64_t>(d.net_pin_start[net + 1] - d.net_pin_start[net]) >
-                            options.maximum_net_degree;
-            }
-            if (too_wide) continue;
             const int r = windows.row[k];
-            for (int i = 0; i < n; ++i) {
-                wx[i] = s.cx[m[i]];
-                wy[i] = s.cy[m[i]];
-            }
-            double best_value = s.windowHpwl(m, n, window_nets_k, net_count, wx, wy);
-            int order[kWindow] = {0, 1, 2, 3};
-            int best_order_found[kWindow] = {0, 1, 2, 3};
-            bool improved = false;
-            do {
-                s.centersForOrder(m, order, n, d.row_bottom[r], d.row_site_spacing[r], wx, wy);
-                const double value = s.windowHpwl(m, n, window_nets_k, net_count, wx, wy);
-                ++result.evaluated_permutations;
-                if (value < best_value - options.improvement_epsilon) {
-                    best_value = value;
-                    std::copy(order, order + n, best_order_found);
-                    improved = true;
+            result.evaluated_permutations += static_cast<uint64_t>(factorialOf(n));
+            bool stale = false;
+            for (int e = 0; e < net_count && !stale; ++e) stale = divergent[window_nets_k[e]] != 0;
+            int taken = tail_result[t];
+            if (stale) {
+                for (int i = 0; i < n; ++i) {
+                    wx[i] = s.cx[m[i]];
+                    wy[i] = s.cy[m[i]];
                 }
-            } while (std::next_permutation(order, order + n));
-            if (improved) {
-                s.applyOrder(m, best_order_found, n, d.row_bottom[r], d.row_site_spacing[r], rowOrientation(r));
+                double best_value = s.windowHpwl(m, n, window_nets_k, net_count, wx, wy);
+                taken = -1;
+                for (int candidate = 0; candidate < factorialOf(n); ++candidate) {
+                    int order[kWindow];
+                    orderOf(candidate, order, n);
+                    s.centersForOrder(m, order, n, d.row_bottom[r], d.row_site_spacing[r], wx, wy);
+                    const double value = s.windowHpwl(m, n, window_nets_k, net_count, wx, wy);
+                    if (value < best_value - options.improvement_epsilon) {
+                        best_value = value;
+                        taken = candidate;
+                    }
+                }
+            }
+            if (taken >= 0) {
+                int order[kWindow];
+                orderOf(taken, order, n);
+                s.applyOrder(m, order, n, d.row_bottom[r], d.row_site_spacing[r], rowOrientation(r));
                 ++result.accepted_operations;
+            }
+            if (taken != tail_assumed[t]) {
+                for (int e = 0; e < net_count; ++e) divergent[window_nets_k[e]] = 1;
             }
         }
         result.completed_passes = pass + 1;
