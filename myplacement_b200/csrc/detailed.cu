@@ -19,7 +19,10 @@
 // rounds.  The host walks the windows in the reference's order and takes the
 // device's values unless a net of the window belongs to an earlier window
 // whose actual decision differed from the assumption; only those windows are
-// re-evaluated on the host.  The result is the reference's exactly.
+// re-evaluated on the host.  The segment ends the reference keeps on the host
+// (two or three cells, every order by its exhaustive rule) go through a tail
+// kernel the same way, after the four-cell windows.  The result is the
+// reference's exactly.
 #include <cuda_runtime.h>
 
 #include <algorithm>
