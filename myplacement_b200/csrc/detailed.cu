@@ -216,9 +216,9 @@ __host__ __device__ inline double2 transformed(double2 o, int orientation) {
 // `decided_in` says, and the decisions they give.  A cell of an earlier window
 // assumed accepted sits where that window's best order puts it, with the
 // orientation of its row; every other cell is where the pass found it.  One
-// thread per window folds its nets in order, products and sums rounded
-// separately, as the host does.
-__global__ void __launch_bounds__(256)
+// warp per window: each lane takes one net and forms its two terms (products
+// rounded separately), and the warp adds them in net order, as the host does.
+__global__ void __launch_bounds__(32 * kWindowsPerBlock)
     speculativeValuesKernel(const double2* __restrict__ center, const double2* __restrict__ moved_center,
                             const int* __restrict__ owner, const int8_t* __restrict__ moved_orientation,
                             const double2* __restrict__ raw_offset, const double2* __restrict__ pin_offset,
@@ -227,58 +227,73 @@ __global__ void __launch_bounds__(256)
                             const int* __restrict__ best_order, double epsilon, const uint8_t* __restrict__ decided_in,
                             uint8_t* __restrict__ decided_out, double* __restrict__ value_before,
                             double* __restrict__ value_after) {
-    const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= window_count) return;
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x * kWindowsPerBlock + static_cast<int>(threadIdx.x >> 5);
+    if (w >= window_count) return;  // whole warps leave together
     const int best = best_order[w];
     if (best <= 0 || best >= kOrders) {
-        decided_out[w] = 0;
+        if (lane == 0) decided_out[w] = 0;
         return;
     }
     const int4 m4 = windows.modules[w];
+    const int first = windows.net_start[w];
+    const int last = windows.net_start[w + 1];
     double before = 0.0;
     double after = 0.0;
-    for (int e = windows.net_start[w]; e < windows.net_start[w + 1]; ++e) {
-        const int net = windows.nets[e];
-        double min_b = kLargest, max_b = -kLargest, min_by = kLargest, max_by = -kLargest;
-        double min_a = kLargest, max_a = -kLargest, min_ay = kLargest, max_ay = -kLargest;
-        for (int p = net_pin_start[net]; p < net_pin_start[net + 1]; ++p) {
-            const int m = pin_module[p];
-            double2 offset = pin_offset[p];
-            double2 now_c;   // the cell now (before)
-            double2 then_c;  // the cell with this window's best order applied (after)
-            if (m == m4.x || m == m4.y || m == m4.z || m == m4.w) {
-                now_c = center[m];
-                then_c = moved_center[m];  // its orientation changes only once accepted
-            } else {
-                const int j = owner[m];
-                if (j >= 0 && j < w && decided_in[j] != 0) {
-                    now_c = moved_center[m];
-                    offset = transformed(raw_offset[p], moved_orientation[m]);
-                } else {
+    for (int base = first; base < last; base += 32) {
+        double term_before = 0.0;
+        double term_after = 0.0;
+        const int e = base + lane;
+        if (e < last) {
+            const int net = windows.nets[e];
+            double min_b = kLargest, max_b = -kLargest, min_by = kLargest, max_by = -kLargest;
+            double min_a = kLargest, max_a = -kLargest, min_ay = kLargest, max_ay = -kLargest;
+            for (int p = net_pin_start[net]; p < net_pin_start[net + 1]; ++p) {
+                const int m = pin_module[p];
+                double2 offset = pin_offset[p];
+                double2 now_c;   // the cell now (before)
+                double2 then_c;  // the cell with this window's best order applied (after)
+                if (m == m4.x || m == m4.y || m == m4.z || m == m4.w) {
                     now_c = center[m];
+                    then_c = moved_center[m];  // its orientation changes only once accepted
+                } else {
+                    const int j = owner[m];
+                    if (j >= 0 && j < w && decided_in[j] != 0) {
+                        now_c = moved_center[m];
+                        offset = transformed(raw_offset[p], moved_orientation[m]);
+                    } else {
+                        now_c = center[m];
+                    }
+                    then_c = now_c;
                 }
-                then_c = now_c;
+                const double bx = now_c.x + offset.x;
+                const double by = now_c.y + offset.y;
+                const double ax = then_c.x + offset.x;
+                const double ay = then_c.y + offset.y;
+                min_b = bx < min_b ? bx : min_b;
+                max_b = max_b < bx ? bx : max_b;
+                min_by = by < min_by ? by : min_by;
+                max_by = max_by < by ? by : max_by;
+                min_a = ax < min_a ? ax : min_a;
+                max_a = max_a < ax ? ax : max_a;
+                min_ay = ay < min_ay ? ay : min_ay;
+                max_ay = max_ay < ay ? ay : max_ay;
             }
-            const double bx = now_c.x + offset.x;
-            const double by = now_c.y + offset.y;
-            const double ax = then_c.x + offset.x;
-            const double ay = then_c.y + offset.y;
-            min_b = bx < min_b ? bx : min_b;
-            max_b = max_b < bx ? bx : max_b;
-            min_by = by < min_by ? by : min_by;
-            max_by = max_by < by ? by : max_by;
-            min_a = ax < min_a ? ax : min_a;
-            max_a = max_a < ax ? ax : max_a;
-            min_ay = ay < min_ay ? ay : min_ay;
-            max_ay = max_ay < ay ? ay : max_ay;
+            const double weight = net_weight[net];
+            term_before = __dmul_rn(weight, (max_b - min_b) + (max_by - min_by));
+            term_after = __dmul_rn(weight, (max_a - min_a) + (max_ay - min_ay));
         }
-        const double weight = net_weight[net];
-        before = __dadd_rn(before, __dmul_rn(weight, (max_b - min_b) + (max_by - min_by)));
-        after = __dadd_rn(after, __dmul_rn(weight, (max_a - min_a) + (max_ay - min_ay)));
+        const int terms = min(32, last - base);
+        for (int j = 0; j < terms; ++j) {
+            before = __dadd_rn(before, __shfl_sync(0xffffffffu, term_before, j));
+            after = __dadd_rn(after, __shfl_sync(0xffffffffu, term_after, j));
+        }
     }
-    value_before[w] = before;
-    value_after[w] = after;
-    decided_out[w] = after < before - epsilon ? 1 : 0;
+    if (lane == 0) {
+        value_before[w] = before;
+        value_after[w] = after;
+        decided_out[w] = after < before - epsilon ? 1 : 0;
+    }
 }
 
 // The windows the reference keeps on the host (segment ends of two or three
@@ -322,8 +337,10 @@ __global__ void __launch_bounds__(256)
 // beats the best so far by more than epsilon, from the placement as it is.
 // Writes the order taken, or -1.  A cell of an earlier tail window assumed
 // reordered sits where that order puts it, with its row's orientation; every
-// other cell is where the four-cell windows left it.
-__global__ void __launch_bounds__(256)
+// other cell is where the four-cell windows left it.  One warp per window:
+// lane k < n! evaluates order k, lane n! the placement as it is, and every lane
+// then runs the same selection over the lanes' values in order.
+__global__ void __launch_bounds__(32 * kWindowsPerBlock)
     tailOrdersKernel(const double2* __restrict__ center, const int8_t* __restrict__ orientation,
                      const double2* __restrict__ moved_center, const int* __restrict__ owner, int tail_base,
                      const int8_t* __restrict__ moved_orientation, const double2* __restrict__ raw_offset,
@@ -331,9 +348,11 @@ __global__ void __launch_bounds__(256)
                      const int* __restrict__ net_pin_start, const double* __restrict__ net_weight, TailArrays tail,
                      int tail_count, double epsilon, const int8_t* __restrict__ assumed_in,
                      int8_t* __restrict__ order_out) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= tail_count) return;
+    const int lane = threadIdx.x & 31;
+    const int t = blockIdx.x * kWindowsPerBlock + static_cast<int>(threadIdx.x >> 5);
+    if (t >= tail_count) return;  // whole warps leave together
     const int n = tail.count[t];
+    const int orders = factorialOf(n);
     const int4 m4 = tail.modules[t];
     const int module[kWindow] = {m4.x, m4.y, m4.z, m4.w};
     double cx[kWindow];
@@ -377,10 +396,8 @@ __global__ void __launch_bounds__(256)
         cx[i] = c.x;
         cy[i] = c.y;
     }
-    double best = value();
-    int taken = -1;
-    for (int k = 0; k < factorialOf(n); ++k) {
-        const unsigned code = orderCode(k, n);
+    if (lane < orders) {
+        const unsigned code = orderCode(lane, n);
         double cursor = tail.start_x[t];
         for (int i = 0; i < n; ++i) {
             const unsigned local = (code >> (4u * static_cast<unsigned>(i))) & 0xFu;
@@ -399,13 +416,18 @@ __global__ void __launch_bounds__(256)
             }
             cursor = __dadd_rn(cursor, roundedWidthDevice(s.x, tail.spacing[t]));
         }
-        const double v = value();
+    }
+    const double mine = lane <= orders ? value() : 0.0;
+    double best = __shfl_sync(0xffffffffu, mine, orders);
+    int taken = -1;
+    for (int k = 0; k < orders; ++k) {
+        const double v = __shfl_sync(0xffffffffu, mine, k);
         if (v < best - epsilon) {
             best = v;
             taken = k;
         }
     }
-    order_out[t] = static_cast<int8_t>(taken);
+    if (lane == 0) order_out[t] = static_cast<int8_t>(taken);
 }
 
 // ---- host ---------------------------------------------------------------------------------
@@ -1004,7 +1026,7 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
             // decisions; the last one's input is the assumption its values rest on.
             int in = 0;
             for (int iteration = 0; iteration < kSpeculations; ++iteration, in ^= 1) {
-                speculativeValuesKernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0, stream.get()>>>(
+                speculativeValuesKernel<<<blocks, 32 * kWindowsPerBlock, 0, stream.get()>>>(
                     center.get(), moved_center.get(), owner.get(), moved_orientation.get(), raw_offset.get(),
                     pin_offset.get(), pin_module.get(), net_pin_start.get(), net_weight.get(), arrays, n,
                     best_order.get(), options.improvement_epsilon, decided[in].get(), decided[in ^ 1].get(),
@@ -1082,6 +1104,7 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
                                   tail_spacing.get(), tail_net_start.get(), window_nets.get()};
             const int n = static_cast<int>(tails);
             const unsigned blocks = static_cast<unsigned>((tails + 255) / 256);
+            const unsigned warp_blocks = static_cast<unsigned>((tails + kWindowsPerBlock - 1) / kWindowsPerBlock);
             int in = 0;
             for (int iteration = 0; iteration < kSpeculations; ++iteration, in ^= 1) {
                 if (iteration > 0) {
@@ -1089,7 +1112,7 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
                                                                          moved_center.get());
                     checkCuda(cudaGetLastError(), "tailPlacementKernel launch");
                 }
-                tailOrdersKernel<<<blocks, 256, 0, stream.get()>>>(
+                tailOrdersKernel<<<warp_blocks, 32 * kWindowsPerBlock, 0, stream.get()>>>(
                     center.get(), orientation_now.get(), moved_center.get(), owner.get(), static_cast<int>(count),
                     moved_orientation.get(), raw_offset.get(), size.get(), pin_module.get(), net_pin_start.get(),
                     net_weight.get(), tail, n, options.improvement_epsilon, tail_decided[in].get(),
