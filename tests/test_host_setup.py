@@ -39,25 +39,36 @@ def test_random_placement_identical(ref, golden_dir):
 
 def test_session_setup_identical(ref, golden_dir):
     for design, bins, t, fillers in _cases(golden_dir):
-        x, y = mp.random_placement(design, 11)
-        design = design.copy_with_positions(x, y)
-        rs = ref.session(design, ref_options(bins_x=bins, bins_y=bins, target_density=t, maximum_fillers=fillers))
-        mine = mp.host_setup(design, mp.default_options(bins_x=bins, bins_y=bins, target_density=t,
-                                                        maximum_fillers=fillers))
-        assert mine["particle_count"] == rs.particle_count
-        assert mine["movable_count"] == rs.movable_count
-        fixed, dark = rs.static_density()
-        assert np.array_equal(mine["static_fixed"], fixed)
-        assert np.array_equal(mine["static_dark"], dark)
-        m = rs.movable_count
-        assert np.array_equal(mine["x"][m:], rs.x[m:]) and np.array_equal(mine["y"][m:], rs.y[m:])
-        assert np.array_equal(mine["width"], rs.width) and np.array_equal(mine["height"], rs.height)
-        assert np.array_equal(mine["layer"], rs.layer)
-        # The preconditioner base: pre / raw = base / sqrt(1 + penalty / reference_penalty).
-        ev = rs.evaluate(rs.positions, 4.0, 2.0, 1.0, True)
-        raw, pre = ev["raw_gradient"][:, 0], ev["preconditioned_gradient"][:, 0]
-        ok = np.abs(raw) > 1e-12
-        np.testing.assert_allclose(pre[ok] / raw[ok] * np.sqrt(3.0), mine["preconditioner"][ok], rtol=1e-14)
+        _check_setup(ref, design, bins, t, fillers)
+
+
+def test_session_setup_identical_at_full_size(ref):
+    """The 210k-cell design (848k pins, 260k particles): every set-up loop runs
+    on several host threads at this size, and must still match bit for bit."""
+    design, bins = mp.workload("mid_210k")
+    _check_setup(ref, design, bins, 0.9, 50_000)
+
+
+def _check_setup(ref, design, bins, t, fillers):
+    x, y = mp.random_placement(design, 11)
+    design = design.copy_with_positions(x, y)
+    rs = ref.session(design, ref_options(bins_x=bins, bins_y=bins, target_density=t, maximum_fillers=fillers))
+    mine = mp.host_setup(design, mp.default_options(bins_x=bins, bins_y=bins, target_density=t,
+                                                    maximum_fillers=fillers))
+    assert mine["particle_count"] == rs.particle_count
+    assert mine["movable_count"] == rs.movable_count
+    fixed, dark = rs.static_density()
+    assert np.array_equal(mine["static_fixed"], fixed)
+    assert np.array_equal(mine["static_dark"], dark)
+    m = rs.movable_count
+    assert np.array_equal(mine["x"][m:], rs.x[m:]) and np.array_equal(mine["y"][m:], rs.y[m:])
+    assert np.array_equal(mine["width"], rs.width) and np.array_equal(mine["height"], rs.height)
+    assert np.array_equal(mine["layer"], rs.layer)
+    # The preconditioner base: pre / raw = base / sqrt(1 + penalty / reference_penalty).
+    ev = rs.evaluate(rs.positions, 4.0, 2.0, 1.0, True)
+    raw, pre = ev["raw_gradient"][:, 0], ev["preconditioned_gradient"][:, 0]
+    ok = np.abs(raw) > 1e-12
+    np.testing.assert_allclose(pre[ok] / raw[ok] * np.sqrt(3.0), mine["preconditioner"][ok], rtol=1e-14)
 
 
 @pytest.mark.parametrize("override,message", [
