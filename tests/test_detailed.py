@@ -102,6 +102,14 @@ def test_declines_like_reference_without_running(libraries):
         assert theirs.value.message.endswith(str(mine.value).split(": ", 1)[1])
 
 
+def test_defaults_follow_the_reference():
+    """DetailedPlacementOptions (DetailedPlacer.hpp:23-44): the reference's defaults,
+    with the window reorder selected and device 0."""
+    o = mp.default_detailed_options()
+    assert (o.method, o.passes, o.window_size, o.maximum_net_degree) == (_abi.DETAILED_WINDOW_REORDER, 2, 4, 64)
+    assert o.improvement_epsilon == 1e-9 and o.maximum_cuda_memory_bytes == 2 << 30 and o.cuda_device == 0
+
+
 def test_invalid_orientations_are_rejected():
     design = _fixture()
     design.module_orientation = np.array([0, 9, 0, 0], np.int32)
