@@ -54,9 +54,11 @@ def parse_args():
     p.add_argument("--rudy", action="store_true",
                    help="routability term on (hinge L2, capacity 1.2 x the activation mean demand), as the "
                         "precision configuration runs it")
-    p.add_argument("--form", choices=["plain", "batched", "serving"], default="plain",
+    p.add_argument("--form", choices=["plain", "batched", "serving", "detailed", "bookshelf"], default="plain",
                    help="plain: the one-design metric; batched: many small instances at once; "
-                        "serving: an open-loop stream of jobs")
+                        "serving: an open-loop stream of jobs; detailed: window-reorder detailed placement "
+                        "of the workload packed legally, against the reference CUDA backend; bookshelf: "
+                        "reading the workload as BookShelf files (host only), against the reference reader")
     p.add_argument("--instances", type=int, default=256, help="batched form: instance count")
     p.add_argument("--jobs", type=int, default=240, help="serving form: job count")
     p.add_argument("--workers", type=int, default=32, help="batched / serving forms: worker threads")
@@ -530,6 +532,92 @@ def run_serving(args) -> None:
     print(json.dumps(line))
 
 
+def run_detailed(args) -> None:
+    """Detailed placement (two passes of the four-cell window reorder) of the workload's cells packed
+    legally in shuffled order: seconds for this engine and for the reference CUDA backend rebuilt for
+    sm_100a (oracle/_ref/libref_cuda.so through DetailedPlacer::run) on the same device, and whether the
+    two placements are bit-identical."""
+    import numpy as np
+
+    import myplacement_b200 as mp
+    from myplacement_b200.design import packed_placement
+    from oracle.ref import ReferenceLibrary
+
+    design, _ = mp.workload(args.workload, seed=args.seed)
+    placed = packed_placement(design, 7)
+    options = mp.default_detailed_options(passes=2)
+    runs = []
+    for _ in range(3):
+        out, result = mp.DetailedPlacer().run(placed, options)
+        runs.append(result["elapsed_seconds"])
+    reference = ReferenceLibrary("cuda")
+    ref_runs = []
+    for _ in range(2):
+        x, y, orientation, theirs, used = reference.detailed_place(placed, options, 1)
+        ref_runs.append(theirs["elapsed_seconds"])
+    same = (np.array_equal(out.module_x.view(np.int64), x.view(np.int64)) and
+            np.array_equal(out.module_y.view(np.int64), y.view(np.int64)) and
+            np.array_equal(out.module_orientation, orientation) and
+            all(result[k] == theirs[k] for k in ("evaluated_windows", "evaluated_permutations",
+                                                 "accepted_operations", "hpwl_after")))
+    line = {
+        "form": "detailed", "metric": "detailed placement seconds (two window-reorder passes)",
+        "value": statistics.median(runs), "unit": "s", "n_gpus": 1, "higher_is_better": False,
+        "runs_s": runs, "reference_cuda_runs_s": ref_runs, "reference_backend_used": used,
+        "speedup_vs_reference_cuda": statistics.median(ref_runs) / statistics.median(runs),
+        "identical_to_reference_cuda": bool(same),
+        "windows": result["evaluated_windows"], "accepted": result["accepted_operations"],
+        "hpwl_before": result["hpwl_before"], "hpwl_after": result["hpwl_after"],
+        "data": f"synthetic: {args.workload} (seed {args.seed}) with its standard cells packed legally in "
+                "shuffled order (packed_placement, seed 7)",
+    }
+    print(json.dumps(line))
+
+
+def run_bookshelf(args) -> None:
+    """Reading the workload written as BookShelf files (host only): seconds for the native reader on one
+    and on all host threads, and for the reference reader (oracle/_ref/libref_cpu.so), and whether the
+    two read the same design."""
+    import os as _os
+    import tempfile
+
+    import numpy as np
+
+    import myplacement_b200 as mp
+    from oracle.ref import ReferenceLibrary
+
+    design, _ = mp.workload(args.workload, seed=args.seed)
+    x, y = mp.random_placement(design, args.seed)
+    with tempfile.TemporaryDirectory() as directory:
+        aux = mp.write_bookshelf(design.copy_with_positions(x, y), directory, args.workload)
+        size = sum(f.stat().st_size for f in Path(directory).iterdir())
+        timings = {}
+        for threads in (1, 0):
+            best = math.inf
+            for _ in range(3):
+                t0 = time.perf_counter()
+                mine = mp.read_bookshelf(aux, threads)
+                best = min(best, time.perf_counter() - t0)
+            timings["one_thread" if threads == 1 else "all_threads"] = best
+        t0 = time.perf_counter()
+        theirs = ReferenceLibrary("cpu").read_bookshelf(aux)
+        reference_seconds = time.perf_counter() - t0
+    same = (np.array_equal(mine.module_x, theirs["modules"]["x"]) and
+            np.array_equal(mine.pin_module, theirs["nets"]["pin_module"]) and
+            np.array_equal(mine.pin_offset_x, theirs["nets"]["offset_x"]) and
+            list(mine.bookshelf.net_names) == theirs["net_names"])
+    line = {
+        "form": "bookshelf", "metric": "BookShelf read seconds", "value": timings["all_threads"], "unit": "s",
+        "higher_is_better": False, "threads": _os.cpu_count(), "one_thread_s": timings["one_thread"],
+        "reference_reader_s": reference_seconds,
+        "speedup_vs_reference": reference_seconds / timings["all_threads"], "bytes": size,
+        "modules": mine.module_count, "nets": mine.net_count, "pins": mine.pin_count,
+        "identical_to_reference": bool(same),
+        "data": f"synthetic: {args.workload} (seed {args.seed}) written by write_bookshelf",
+    }
+    print(json.dumps(line))
+
+
 def main() -> int:
     args = parse_args()
     if args.impl == "reference":
@@ -538,6 +626,10 @@ def main() -> int:
         run_batched(args)
     elif args.form == "serving":
         run_serving(args)
+    elif args.form == "detailed":
+        run_detailed(args)
+    elif args.form == "bookshelf":
+        run_bookshelf(args)
     else:
         run_mine(args)
     return 0
