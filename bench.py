@@ -361,6 +361,13 @@ def run_mine(args) -> None:
             "quality": {"hpwl_after": result.hpwl_after, "overflow_after": result.overflow_after,
                         "iterations": result.completed_iterations},
         }
+        if result.completed_iterations > 0 and result.evaluations > 0:
+            # An iteration holds one or more objective evaluations (candidates,
+            # backtracks, the accepted point's gradient).
+            per_iteration = result.evaluations / result.completed_iterations
+            line["evaluations"] = {"per_iteration": per_iteration, "per_s": value * per_iteration,
+                                   "us_per_evaluation": 1e6 / (value * per_iteration),
+                                   "counted_over": "the whole run (initial evaluations, warm-up and timed steps)"}
         print(json.dumps(line), flush=True)
     replicas.shutdown()
 
