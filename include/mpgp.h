@@ -373,8 +373,8 @@ int mpgp_wirelength_noalloc(const double* positions, const int32_t* net_pin_star
  * error comes first; its ParseError is MPGP_ERR_PARSE and the database's
  * std::invalid_argument (duplicate names, negative sizes) is
  * MPGP_ERR_INVALID_ARGUMENT.  The files are read whole and parsed by `threads`
- * host threads (<= 0: one per hardware thread); the result does not depend on
- * the thread count.  No GPU is used. */
+ * host threads (<= 0: one per hardware thread, at most 32); the result does not
+ * depend on the thread count.  No GPU is used. */
 typedef struct mpgp_bookshelf mpgp_bookshelf;
 
 typedef struct mpgp_bookshelf_view {

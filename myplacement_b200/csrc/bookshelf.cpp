@@ -54,6 +54,7 @@ constexpr double kEpsilon = 1e-9;  // myplacement/core/Geometry.hpp
 constexpr int kOrientationUnknown = 8;
 constexpr size_t kPieceBytes = 4096;  // smallest piece worth a thread
 constexpr size_t kBlock = 4096;       // records per parallel task
+constexpr unsigned kDefaultThreads = 32;  // threads <= 0: one per hardware thread, at most this many
 
 [[noreturn]] void parseError(const std::string& message) { fail(MPGP_ERR_PARSE, message); }
 [[noreturn]] void invalidArgument(const std::string& message) { fail(MPGP_ERR_INVALID_ARGUMENT, message); }
@@ -969,7 +970,7 @@ void parseWeights(Text text, const Workers& workers, const NameTable& nets, Book
 // refreshDerivedData's terminal => fixed and validateCounts (:280-299).  The
 // named files are read on their own threads while the earlier ones parse.
 Bookshelf readBookshelf(const std::string& aux_name, int threads) {
-    const Workers workers(threads > 0 ? threads : static_cast<int>(std::max(1u, std::thread::hardware_concurrency())));
+    const Workers workers = threads > 0 ? Workers(threads) : Workers::all(kDefaultThreads);
     const fs::path aux_path(aux_name);
     const FileText aux = readWhole(aux_path);
     if (!aux.opened) parseError("Unable to open BookShelf file: " + aux_path.string());

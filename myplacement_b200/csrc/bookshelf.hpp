@@ -36,8 +36,8 @@ struct Bookshelf {
 // Reads the design named by a BookShelf .aux file.  Same grammar, records and
 // error texts as the reference reader: its ParseError becomes Error with
 // MPGP_ERR_PARSE, the database's std::invalid_argument (duplicate names,
-// negative sizes) MPGP_ERR_INVALID_ARGUMENT.  `threads` <= 0 uses every
-// hardware thread; the result does not depend on the thread count.
+// negative sizes) MPGP_ERR_INVALID_ARGUMENT.  `threads` <= 0 uses one per
+// hardware thread, at most 32; the result does not depend on the thread count.
 Bookshelf readBookshelf(const std::string& aux_path, int threads);
 
 }  // namespace mpgp

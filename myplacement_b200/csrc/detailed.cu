@@ -823,7 +823,7 @@ bool detailedPlace(const mpgp_design& d, const int32_t* row_orientation, const m
     for (int32_t m = 0; m < d.module_count; ++m) standard[m] = derived.is_fixed[m] == 0 && derived.is_macro[m] == 0;
     const auto rowOrientation = [&](int r) { return row_orientation != nullptr ? row_orientation[r] : 0; };
 
-    const Workers workers = Workers::all();
+    const Workers workers = Workers::all(16);
     Placement s(d);
     result = mpgp_detailed_result{};
     result.hpwl_before = s.hpwl(workers);

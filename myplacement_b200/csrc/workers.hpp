@@ -18,8 +18,11 @@ class Workers {
 public:
     explicit Workers(int threads) : threads_(std::max(1, threads)) {}
 
-    // One per hardware thread.
-    static Workers all() { return Workers(static_cast<int>(std::max(1u, std::thread::hardware_concurrency()))); }
+    // One per hardware thread, at most `cap`: a fork-join region costs a thread
+    // start per helper, and large hosts have hundreds of hardware threads.
+    static Workers all(unsigned cap) {
+        return Workers(static_cast<int>(std::min(cap, std::max(1u, std::thread::hardware_concurrency()))));
+    }
 
     [[nodiscard]] int threads() const { return threads_; }
 
