@@ -371,6 +371,45 @@ def _mutate(lines: list[str], rng: random.Random) -> list[str]:
     return lines
 
 
+JUNK_BYTES = [b"\x00", b"#", b":", b"\r", b"\t", b" ", b"\xff", b"\xc3\xa9", b"-", b"+", b".", b"e", b"\n", b"1"]
+
+
+def _mutate_bytes(data: bytes, rng: random.Random) -> bytes:
+    out = bytearray(data)
+    for _ in range(rng.randint(1, 4)):
+        if not out:
+            break
+        at = rng.randrange(len(out))
+        kind = rng.randrange(3)
+        if kind == 0:
+            del out[at]
+        elif kind == 1:
+            out[at:at] = rng.choice(JUNK_BYTES)
+        else:
+            out[at:at + 1] = rng.choice(JUNK_BYTES)
+    return bytes(out)
+
+
+def test_seeded_byte_mutations_match_reference(readers, tmp_path):
+    """100 seeded byte-level edits (NUL, '#', ':', CR, tabs, bytes above 0x7f,
+    signs, points, exponents, newlines) of a written 300-cell design: the
+    readers agree on each."""
+    base = _synthetic_files(tmp_path, cells=300)
+    outcomes = {"ok": 0, "error": 0}
+    for case in range(100):
+        rng = random.Random(70000 + case)
+        suffix = rng.choice([".nets", ".nets", ".nodes", ".pl", ".wts", ".scl"])
+        directory = tmp_path / f"b{case}"
+        directory.mkdir()
+        for s, lines in base.items():
+            data = ("\n".join(lines) + "\n").encode()
+            (directory / f"m{s}").write_bytes(_mutate_bytes(data, rng) if s == suffix else data)
+        names = " ".join(f"m{s}" for s in (".nodes", ".nets", ".wts", ".pl", ".scl"))
+        (directory / "m.aux").write_text(f"RowBasedPlacement : {names}\n")
+        outcomes["ok" if _check(readers, directory / "m.aux") == "ok" else "error"] += 1
+    assert outcomes["ok"] > 10 and outcomes["error"] > 10, outcomes
+
+
 def test_seeded_mutations_match_reference(readers, tmp_path):
     """200 seeded edits of a written 800-cell design (deleted, repeated, swapped and
     junk lines and tokens, truncations, in every file): the readers agree on each."""
