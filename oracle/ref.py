@@ -82,8 +82,8 @@ class ReferenceLibrary:
             "ref_bookshelf_modules": (C.c_int, [_vp, _d, _d, _d, _d, _i32, _i32, _i64, _i64]),
             "ref_bookshelf_nets": (C.c_int, [_vp, _d, _i64, _i64, _i32, _i64, _d, _d, _i32]),
             "ref_bookshelf_rows": (C.c_int, [_vp, _d, _d, _d, _d, _d, _i64, _i32]),
-            "ref_bookshelf_module_name": (C.c_char_p, [_vp, C.c_int64]),
-            "ref_bookshelf_net_name": (C.c_char_p, [_vp, C.c_int64]),
+            "ref_bookshelf_module_name": (C.c_void_p, [_vp, C.c_int64, _i64]),
+            "ref_bookshelf_net_name": (C.c_void_p, [_vp, C.c_int64, _i64]),
         }
         for name, (restype, argtypes) in sig.items():
             fn = getattr(lib, name)
@@ -178,10 +178,14 @@ class ReferenceLibrary:
                                                                       "site_spacing", "x_start")),
                                    _ptr(r["site_count"], _i64), _ptr(r["orientation"], _i32))
             out["modules"], out["nets"], out["rows"] = m, n, r
-            out["module_names"] = [lib.ref_bookshelf_module_name(handle, i).decode("utf-8", "surrogateescape")
-                                   for i in range(modules)]
-            out["net_names"] = [lib.ref_bookshelf_net_name(handle, i).decode("utf-8", "surrogateescape")
-                                for i in range(nets)]
+            length = C.c_int64()
+
+            def name(fn, i):
+                data = fn(handle, i, C.byref(length))
+                return C.string_at(data, length.value).decode("utf-8", "surrogateescape") if length.value else ""
+
+            out["module_names"] = [name(lib.ref_bookshelf_module_name, i) for i in range(modules)]
+            out["net_names"] = [name(lib.ref_bookshelf_net_name, i) for i in range(nets)]
             return out
         finally:
             lib.ref_bookshelf_destroy(handle)

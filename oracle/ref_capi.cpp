@@ -670,12 +670,17 @@ int ref_bookshelf_rows(void* handle, double* bottom, double* height, double* sit
     return MPGP_OK;
 }
 
-const char* ref_bookshelf_module_name(void* handle, int64_t module) {
-    return static_cast<RefBook*>(handle)->database.modules[static_cast<std::size_t>(module)].name.c_str();
+// A name's bytes and length (names may hold any byte but blanks, NUL included).
+const char* ref_bookshelf_module_name(void* handle, int64_t module, int64_t* length) {
+    const std::string& name = static_cast<RefBook*>(handle)->database.modules[static_cast<std::size_t>(module)].name;
+    *length = static_cast<int64_t>(name.size());
+    return name.data();
 }
 
-const char* ref_bookshelf_net_name(void* handle, int64_t net) {
-    return static_cast<RefBook*>(handle)->database.nets[static_cast<std::size_t>(net)].name.c_str();
+const char* ref_bookshelf_net_name(void* handle, int64_t net, int64_t* length) {
+    const std::string& name = static_cast<RefBook*>(handle)->database.nets[static_cast<std::size_t>(net)].name;
+    *length = static_cast<int64_t>(name.size());
+    return name.data();
 }
 
 // DetailedPlacer::run (src/placement/DetailedPlacer.cpp:262-338) on a flattened
