@@ -131,8 +131,9 @@ def test_no_cpu_fallback_without_gpu():
     assert "unavailable on this host" in str(error.value)
 
 
-def test_packed_placement_is_legal():
-    design, _ = _legal_case(3, 2000)
+@pytest.mark.parametrize("spacing,fractional", [(1.0, False), (0.19, True), (0.5, True)])
+def test_packed_placement_is_legal(spacing, fractional):
+    design, _ = _legal_case(3, 2000, spacing=spacing, fractional=fractional)
     _assert_legal(design, design.module_x, design.module_y)
 
 
