@@ -130,7 +130,7 @@ class ClockSampler:
 def algorithmic_units(design, particles: int, bins_x: int, bins_y: int) -> dict:
     """Per-launch algorithmic bytes (HBM-bound families) or FLOPs (DCT) of each kernel family.
 
-    Bytes per unit follow the per-unit figures of the design notes: wirelength
+    Bytes per unit are the compulsory bytes of each pass (each array counted once per pass): wirelength
     20 B/pin + 8 B/net + 8 B/particle; scatter 20 B/particle + 24 B/bin; metrics
     36 B/bin; gather + update 80 B/particle.  A DCT launch is one (forward) or
     two (inverse) M x N x K contractions at 2 flops per multiply-add (the transform's
@@ -209,12 +209,36 @@ def workload_text(args, design, bins: int) -> str:
     return text
 
 
-def make_workload(name: str, seed: int):
+def make_workload(name: str, seed: int, placer=None):
+    """The seeded synthetic design with its random initial placement (randomPlacement,
+    InitialPlacer.cpp:102-121).  `placer` draws the placement; the reference arm passes
+    the reference's own, so that it loads nothing of this engine."""
     import myplacement_b200 as mp
 
     design, bins = mp.workload(name)
-    x, y = mp.random_placement(design, seed)
+    x, y = (placer or mp.random_placement)(design, seed)
     return design.copy_with_positions(x, y), bins
+
+
+def bench_config(args, design, bins: int, world: int) -> dict:
+    """The `config` object both arms print (the same workload, step and timing rules)."""
+    return {"workload": workload_text(args, design, bins), "step": "one adaptive controller iteration",
+            "early_stop": "off in the timed run (fixed iteration count)",
+            "l2": "flushed between timed steps (256 MiB device write, outside the timing)",
+            "parallelism": f"replicas x{world}", "seed": args.seed}
+
+
+def native_libraries() -> list[str]:
+    """The shared objects of this repository mapped into the process (from /proc/self/maps)."""
+    found = set()
+    try:
+        for line in Path("/proc/self/maps").read_text().splitlines():
+            path = line.split()[-1] if line.split() else ""
+            if path.endswith(".so") and str(REPO) in path:
+                found.add(str(Path(path).relative_to(REPO)))
+    except OSError:
+        pass
+    return sorted(found)
 
 
 def run_mine(args) -> None:
@@ -349,17 +373,15 @@ def run_mine(args) -> None:
             "metric": METRIC, "value": value, "unit": "iterations/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload_text(args, design, bins),
-                       "particles": particles, "step": "one adaptive controller iteration",
-                       "early_stop": "off in the timed run (fixed iteration count)",
-                       "l2": "flushed between timed steps (256 MiB device write, outside the timing)",
-                       "arithmetic": "f32 kernels, int64 fixed-point density, f64 reductions and controller",
-                       "parallelism": f"replicas x{world}", "seed": args.seed,
-                       "wall_seconds_timed_region": wall},
+            "config": bench_config(args, design, bins, world),
+            "details": {"particles": particles,
+                        "arithmetic": "f32 kernels, int64 fixed-point density, f64 reductions and controller",
+                        "wall_seconds_timed_region": wall},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clock_info,
             "quality": {"hpwl_after": result.hpwl_after, "overflow_after": result.overflow_after,
                         "iterations": result.completed_iterations},
+            "native_libraries": native_libraries(),
         }
         if result.completed_iterations > 0 and result.evaluations > 0:
             # An iteration holds one or more objective evaluations (candidates,
@@ -372,13 +394,34 @@ def run_mine(args) -> None:
     replicas.shutdown()
 
 
+def reference_quality(design, bins: int, device: int) -> dict:
+    """One whole run of the reference CUDA backend (rebuilt for sm_100a) with the reference's
+    default options (280-iteration budget, early stop on): the quality the engine's e2e run is
+    compared with."""
+    from oracle.ref import ReferenceLibrary, default_options
+
+    lib = ReferenceLibrary("cuda")
+    options = default_options(bins_x=bins, bins_y=bins, target_density=0.9, compute_backend=1, cuda_device=device)
+    _, _, result, _ = lib.global_place(design, options)
+    return {"hpwl_after": result.hpwl_after, "overflow_after": result.overflow_after,
+            "completed_iterations": result.completed_iterations,
+            "best_checkpoint_iteration": result.best_checkpoint_iteration,
+            "seconds": result.elapsed_seconds,
+            "backend_used": "cuda" if result.compute_backend_used == 1 else "cpu",
+            "what": "reference CUDA backend rebuilt for sm_100a, default options (280-iteration budget, "
+                    "early stop on), same design and initial placement"}
+
+
 def run_reference(args) -> None:
+    """The reference's own CPU path (oracle/_ref/libref_cpu.so, built from the reference sources) on the
+    same workload; the inputs are generated without this engine's library (the reference's randomPlacement)."""
     from myplacement_b200 import replicas
+    from oracle.ref import ReferenceLibrary
 
     rank, world, local = replicas.world()
     if rank != 0:
         return  # the reference CPU path runs on rank 0 only
-    design, bins = make_workload(args.workload, args.seed)
+    design, bins = make_workload(args.workload, args.seed, placer=ReferenceLibrary("cpu").random_placement)
     try:
         cpu = reference_cpu_sample(design, bins, warmup=args.warmup, steps=args.steps)
     except Exception as error:
@@ -394,18 +437,26 @@ def run_reference(args) -> None:
                 "seconds": sample["seconds"], "iterations": sample["iterations"]}
     except Exception as error:
         cuda = {"value": None, "unavailable": str(error)}
+    quality = None
+    if not args.no_e2e:
+        try:
+            quality = reference_quality(design, bins, local)
+        except Exception as error:
+            quality = {"unavailable": str(error)}
     value = cpu["value"]
     line = {
         "metric": METRIC, "value": value, "unit": "iterations/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": f"{args.workload}: {bins}x{bins} bins, target density 0.9",
-                   "step": "one adaptive controller iteration", "early_stop": "off (fixed iteration count)",
-                   "timing": "(T(W + K) - T(W)) / K from the reference's own elapsed_seconds"},
+        "config": bench_config(args, design, bins, world),
+        "timing": "(T(W + K) - T(W)) / K from the reference's own elapsed_seconds",
         "cpu_baseline": {"value": value, "unit": "iterations/s", "cores": 1, "kind": "reference",
-                         "sample": f"reference CPU path, iterations {args.warmup + 1}-{args.warmup + args.steps}"},
+                         "sample": f"reference CPU path (single-threaded, as the reference runs it), iterations "
+                                   f"{args.warmup + 1}-{args.warmup + args.steps}"},
         "e2e": {"value": value, "unit": "iterations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_cuda_backend": cuda,
+        "reference_quality": quality,
+        "native_libraries": native_libraries(),
     }
     print(json.dumps(line), flush=True)
 

@@ -290,6 +290,16 @@ int mpgp_backend_evaluate(mpgp_backend* backend, const double* positions, double
                           int calculate_gradient, mpgp_evaluation* out, double* wire_gradient,
                           double* density_gradient);
 
+/* Failure-detection test hook; no counterpart in the reference, which has no
+ * device-side waits.  With polls > 0 every field contraction of this backend's
+ * later evaluations first waits, for at most `polls` polls, on a barrier that
+ * nothing completes: the wait runs out, the contraction raises the backend's
+ * error flag and returns before it issues any copy or allocates tensor memory,
+ * and the evaluation returns MPGP_ERR_TIMEOUT.  The flag stays raised: every
+ * later evaluation of this backend also fails, and a new backend starts clean.
+ * 0 turns the hook off. */
+int mpgp_backend_set_stall_probe(mpgp_backend* backend, int64_t polls);
+
 /* Replaces CudaPlacementBackend::device() (CudaPlacementBackend.hpp:34). */
 int mpgp_backend_device(const mpgp_backend* backend);
 
@@ -353,8 +363,14 @@ int mpgp_backend_rudy(mpgp_backend* backend, const mpgp_options* options, const 
  * 1,048,576 (larger inputs return MPGP_ERR_INVALID_ARGUMENT and launch
  * nothing).  The first call on each device looks up that array's device
  * address with the device current; make that first call before any stream
- * capture.  All calls share the one array: calls that overlap on the GPU
- * (different streams, or threads) race and must be serialised by the caller.
+ * capture.  The address is looked up again when the current CUDA context
+ * changes (after cudaDeviceReset, or under a caller's own context).  All calls
+ * share the one array, and each call clears the pin slots it uses before its
+ * net pass: a pin that no net of two or more pins covers (including the pins
+ * of a net whose range lies outside [0, pin_count], which is skipped) adds
+ * nothing, and a particle takes the gradient of a listed pin only when
+ * pin_particle names that particle.  Calls that overlap on the GPU (different
+ * streams, or threads) race on the array and must be serialised by the caller.
  * No device memory is allocated or freed.
  */
 int mpgp_wirelength_noalloc(const double* positions, const int32_t* net_pin_start, const int32_t* pin_particle,

@@ -329,6 +329,7 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "mpgp_backend_create": (C.c_int, [C.POINTER(Layout), C.c_int, C.c_uint64, C.POINTER(vp), C.c_char_p,
                                           C.c_size_t]),
         "mpgp_backend_evaluate": (C.c_int, [vp, _d, C.c_double, C.c_int, C.POINTER(Evaluation), _d, _d]),
+        "mpgp_backend_set_stall_probe": (C.c_int, [vp, C.c_int64]),
         "mpgp_backend_device": (C.c_int, [vp]),
         "mpgp_backend_reserved_bytes": (C.c_uint64, [vp]),
         "mpgp_backend_destroy": (None, [vp]),

@@ -189,6 +189,14 @@ int mpgp_backend_evaluate(mpgp_backend* b, const double* positions, double smoot
     });
 }
 
+int mpgp_backend_set_stall_probe(mpgp_backend* b, int64_t polls) {
+    return guarded([&] {
+        mpgp::require(b != nullptr, "mpgp_backend_set_stall_probe requires a backend.");
+        mpgp::require(polls >= 0, "The probe's poll count must be non-negative.");
+        b->engine->setStallProbe(polls);
+    });
+}
+
 int mpgp_backend_device(const mpgp_backend* b) { return b != nullptr ? b->engine->device() : -1; }
 
 uint64_t mpgp_backend_reserved_bytes(const mpgp_backend* b) { return b != nullptr ? b->engine->reservedBytes() : 0; }

@@ -231,6 +231,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
     releaseNext();
     // The whole cluster shares the tile, so the whole cluster leaves together.
     if (tile_index >= tiles_m * tiles_n) return;
+    if (batch.stall_polls > 0) {
+        // Failure-detection probe: a bounded wait on a barrier that nothing completes.
+        // Every CTA of every cluster takes this path before any cluster barrier, copy
+        // or TMEM allocation, so nothing is in flight when it returns.
+        __shared__ __align__(8) uint64_t probe;
+        if (threadIdx.x == 0) {
+            mbarInit(smemAddress(&probe), 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            bool done = false;
+            for (long long i = 0; i < batch.stall_polls && !done; ++i) done = mbarTryWait(smemAddress(&probe), 0);
+            if (!done) atomicExch(batch.error_flag, 1);
+        }
+        waitForPrior();  // the grid completes only after its predecessor, as on the normal path
+        __syncthreads();
+        return;
+    }
     const int split = static_cast<int>(clusterRank());
     const int m0 = (tile_index / tiles_n) * kTileM;
     const int n0 = (tile_index % tiles_n) * kTileN;

@@ -93,6 +93,10 @@ struct alignas(64) TcBatch {
     TcTask task[2];
     int* error_flag;
     int ksplit;
+    // Failure-detection probe (0 = off): every CTA first waits, for at most this many
+    // polls, on an mbarrier that nothing completes, raises error_flag when the wait
+    // runs out and returns before it issues any copy or allocates tensor memory.
+    long long stall_polls;
 };
 
 void makeOperandMap(CUtensorMap* map, const SplitMatrix& m, int box_rows);

@@ -398,6 +398,10 @@ void Engine::buildTensorCoreBasis(double max_scale) {
     tc_fwd2_.task[0].energy_partials = partials_e_;
 }
 
+void Engine::setStallProbe(long long polls) {
+    for (TcBatch* b : {&tc_fwd1_, &tc_fwd2_, &tc_inv1_, &tc_inv2_, &tc_pot_}) b->stall_polls = std::max(0LL, polls);
+}
+
 const char* kernelKindName(int kind) {
     static const char* names[kKindCount] = {"scatter", "wirelength", "metrics", "dct_forward",
                                             "dct_inverse", "gather", "reduce", "vector", "dct_split", "rudy"};

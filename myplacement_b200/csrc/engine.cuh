@@ -139,6 +139,10 @@ public:
     // Runs the fixed-point scatter alone at `positions` and copies the three layers out (parity hook).
     void depositLayers(const double2* positions, int64_t* movable, int64_t* macro, int64_t* filler);
     [[nodiscard]] double2* scratchPositions() const { return scratch_positions_; }
+    // Failure-detection probe: with polls > 0 every later field contraction waits on a
+    // barrier that nothing completes for at most `polls` polls and raises the engine's
+    // error flag (the evaluation then fails with MPGP_ERR_TIMEOUT); 0 turns it off.
+    void setStallProbe(long long polls);
 
     [[nodiscard]] double2* newParticleArray(const char* what);
     // `count` zeroed particle arrays from one allocation: out[k] = base + k * stride.

@@ -305,7 +305,41 @@ constexpr int kNoAllocMaxDevices = 64;
 static __device__ __align__(256) unsigned char g_wirelength_scratch[kNoAllocScratchBytes];
 
 std::mutex g_scratch_mutex;
+// The array's device address per device, and the ID of the CUDA context it was
+// looked up in: a device reset (or a caller's own context) makes a new context,
+// in which the old address is no longer valid, so the address is looked up again.
 void* g_scratch_address[kNoAllocMaxDevices] = {};
+unsigned long long g_scratch_context[kNoAllocMaxDevices] = {};
+
+// The unique ID of the calling thread's current CUDA context (0 if it has none),
+// through the driver entry points the runtime exposes (no libcuda link needed).
+unsigned long long currentContextId() {
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult found{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &found) == cudaSuccess &&
+            found == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<GetCurrent>(fn);
+        }
+        fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &found) == cudaSuccess &&
+            found == cudaDriverEntryPointSuccess) {
+            get_id = reinterpret_cast<GetId>(fn);
+        }
+    });
+    void* context = nullptr;
+    unsigned long long id = 0;
+    if (get_current == nullptr || get_id == nullptr || get_current(&context) != 0 || context == nullptr ||
+        get_id(context, &id) != 0) {
+        return 0;
+    }
+    return id;
+}
 
 // Pins as the caller lays them out: pin_xy is the offset from the particle
 // centre, or the absolute position of a pin whose particle is < 0.
@@ -337,18 +371,13 @@ __global__ void __launch_bounds__(kThreads) noAllocNetKernel(CallerPinLoader loa
     float2* pin_gradient = reinterpret_cast<float2*>(scratch);
     double* partials = reinterpret_cast<double*>(scratch + kNoAllocPinBytes);
     double values[2] = {0.0, 0.0};
-    const int lane = threadIdx.x & 31;
     const int warps_total = static_cast<int>((gridDim.x * blockDim.x) >> 5);
     for (int net = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5); net < net_count;
          net += warps_total) {
         const int begin = net_pin_start[net];
         const int end = net_pin_start[net + 1];
         if (begin < 0 || end > pin_count || end < begin) continue;  // malformed CSR: never write outside scratch
-        if (end - begin < 2) {
-            // Single-pin nets contribute nothing; their slots must read as zero in the gather.
-            for (int pin = begin + lane; pin < end; pin += 32) pin_gradient[pin] = make_float2(0.0f, 0.0f);
-            continue;
-        }
+        if (end - begin < 2) continue;  // single-pin nets contribute nothing; their slots stay zero
         netOnWarp(load, begin, end, static_cast<float>(net_weight[net]), gamma, inv_gamma, true,
                   PinStore{pin_gradient}, values[0], values[1]);
     }
@@ -361,7 +390,8 @@ __global__ void __launch_bounds__(kThreads) noAllocNetKernel(CallerPinLoader loa
 }
 
 __global__ void __launch_bounds__(kThreads) noAllocParticleKernel(const int* particle_pin_start,
-                                                                 const int* particle_pins, int particle_count,
+                                                                 const int* particle_pins, const int* pin_particle,
+                                                                 int particle_count,
                                                                  int pin_count, const unsigned char* scratch,
                                                                  int net_blocks, double2* wire_gradient,
                                                                  double* totals) {
@@ -372,7 +402,10 @@ __global__ void __launch_bounds__(kThreads) noAllocParticleKernel(const int* par
         double gx = 0.0, gy = 0.0;
         for (int j = particle_pin_start[i]; j < particle_pin_start[i + 1]; ++j) {
             const int pin = particle_pins[j];
-            if (pin < 0 || pin >= pin_count) continue;
+            // Only a pin that really belongs to this particle adds its gradient; a pin
+            // listed under another particle (or out of range) would read a slot this
+            // call did not write for it.
+            if (pin < 0 || pin >= pin_count || pin_particle[pin] != i) continue;
             const float2 g = pin_gradient[pin];
             gx += static_cast<double>(g.x);
             gy += static_cast<double>(g.y);
@@ -415,13 +448,17 @@ void launchWirelengthNoAlloc(const NoAllocWirelengthArgs& a) {
     require(device >= 0 && device < kNoAllocMaxDevices, "Device index out of range.");
     void* scratch = nullptr;
     {
-        // Set-up, once per device, with that device current: the host-side name of
-        // the array is not a device address, so ask the runtime for it.
+        // Set-up, once per device and context, with that device current: the
+        // host-side name of the array is not a device address, so ask the runtime
+        // for it.  The lookup makes the device's primary context current when the
+        // thread has none yet, so the context is identified after it.
+        const unsigned long long context = currentContextId();
         std::lock_guard<std::mutex> lock(g_scratch_mutex);
-        if (g_scratch_address[device] == nullptr) {
+        if (g_scratch_address[device] == nullptr || context == 0 || g_scratch_context[device] != context) {
             void* address = nullptr;
             checkCuda(cudaGetSymbolAddress(&address, g_wirelength_scratch), "Locate the wirelength scratch array");
             g_scratch_address[device] = address;
+            g_scratch_context[device] = currentContextId();
         }
         scratch = g_scratch_address[device];
     }
@@ -431,13 +468,20 @@ void launchWirelengthNoAlloc(const NoAllocWirelengthArgs& a) {
     const int net_blocks = std::min(kNoAllocMaxBlocks, std::max(1, ceilDiv(a.net_count, kThreads / 32)));
     const CallerPinLoader load{reinterpret_cast<const double2*>(a.positions), a.pin_particle,
                                reinterpret_cast<const double2*>(a.pin_xy), a.particle_count};
+    // Every pin slot of this call starts at zero: a pin that no well-formed net of
+    // at least two pins covers (a pin outside every net's range, a net skipped as
+    // malformed) then adds nothing, instead of an earlier call's value.
+    if (a.pin_count > 0) {
+        checkCuda(cudaMemsetAsync(scratch, 0, sizeof(float2) * static_cast<std::size_t>(a.pin_count), stream),
+                  "Clear the allocation-free pin slots");
+    }
     noAllocNetKernel<<<net_blocks, kThreads, 0, stream>>>(load, a.net_pin_start, a.net_weight, a.net_count,
                                                           a.pin_count, gamma, inv_gamma,
                                                           static_cast<unsigned char*>(scratch));
     checkCuda(cudaGetLastError(), "Launch the allocation-free net pass");
     const int particle_blocks = std::max(1, ceilDiv(a.particle_count, kThreads));
     noAllocParticleKernel<<<particle_blocks, kThreads, 0, stream>>>(
-        a.particle_pin_start, a.particle_pins, a.particle_count, a.pin_count,
+        a.particle_pin_start, a.particle_pins, a.pin_particle, a.particle_count, a.pin_count,
         static_cast<const unsigned char*>(scratch), net_blocks, reinterpret_cast<double2*>(a.wire_gradient),
         a.totals);
     checkCuda(cudaGetLastError(), "Launch the allocation-free particle pass");

@@ -284,6 +284,10 @@ class CudaPlacementBackend:
             result["density_gradient"] = density.reshape(-1, 2)
         return result
 
+    def set_stall_probe(self, polls: int) -> None:
+        """Failure-detection hook: later field contractions wait out a barrier nothing completes."""
+        check(self.lib.mpgp_backend_set_stall_probe(self.handle, int(polls)))
+
     def density_layers(self, bins_x: int, bins_y: int):
         """The fixed-point layers (movable, macro, filler) of the last evaluated positions."""
         out = [np.empty(bins_x * bins_y, np.int64) for _ in range(3)]

@@ -18,6 +18,7 @@ Only this script reads the reference tree; the tests read the .npz files.
 """
 from __future__ import annotations
 
+import os
 import sys
 from pathlib import Path
 
@@ -31,7 +32,8 @@ from myplacement_b200 import _abi  # noqa: E402
 from myplacement_b200.design import Design, synthetic_design  # noqa: E402
 from oracle.ref import ReferenceLibrary, default_options  # noqa: E402
 
-REFERENCE_FIXTURES = Path("/root/reference/tests/fixtures")
+# The reference tree this recipe reads (MPGP_REFERENCE_ROOT, as oracle/build_oracle.py takes it).
+REFERENCE_FIXTURES = Path(os.environ.get("MPGP_REFERENCE_ROOT", "/root/reference")) / "tests" / "fixtures"
 
 
 def _lines(path: Path):
