@@ -39,6 +39,10 @@ WORKLOAD = "mid_210k"
 PEAKS_FILE = REPO / "MEASURED_PEAKS.json"
 PROFILE_TRAFFIC = REPO / "profiles" / "traffic_mid_210k.md"
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+# Iteration budget of the end-to-end runs (early stop on): large enough that the run stops on its
+# own once the design overflow is <= 0.10 (the reference's default budget of 280 iterations ends
+# this design at overflow 0.13).
+E2E_BUDGET = 1000
 
 
 def parse_args():
@@ -61,7 +65,8 @@ def parse_args():
                         "reading the workload as BookShelf files (host only), against the reference reader")
     p.add_argument("--instances", type=int, default=256, help="batched form: instance count")
     p.add_argument("--jobs", type=int, default=240, help="serving form: job count")
-    p.add_argument("--workers", type=int, default=32, help="batched / serving forms: worker threads")
+    p.add_argument("--workers", type=int, default=64, help="batched / serving forms: worker threads (the most "
+                                                                   "placements running at once)")
     return p.parse_args()
 
 
@@ -332,7 +337,7 @@ def run_mine(args) -> None:
     e2e = None
     if not args.no_e2e:
         e2e_options = mp.default_options(bins_x=bins, bins_y=bins, target_density=0.9, cuda_device=local,
-                                         **rudy_options(args))
+                                         iterations=E2E_BUDGET, **rudy_options(args))
         # Three whole runs through the public API; the median one is reported (a single
         # run of ~0.15 s is at the mercy of the shared host).
         runs = []
@@ -352,8 +357,8 @@ def run_mine(args) -> None:
         e2e_iters = replicas.reduce_sum(it)
         e2e = {"value": e2e_iters / e2e_time, "unit": "iterations/s",
                "h2d_bytes_per_step": int(h2d / max(it, 1)), "d2h_bytes_per_step": int(d2h / max(it, 1)),
-               "api": "Session create/step/finish (= GlobalPlacer.run) on host arrays, early stop on; "
-                      "median of three runs",
+               "api": f"Session create/step/finish (= GlobalPlacer.run) on host arrays, {E2E_BUDGET}-iteration "
+                      "budget with the early stop on (the run ends once overflow <= 0.10); median of three runs",
                "completed_iterations": it, "seconds": e2e_time, "seconds_of_runs": [r[0] for r in runs],
                "hpwl_after": placed.hpwl_after, "overflow_after": placed.overflow_after}
 
@@ -396,20 +401,21 @@ def run_mine(args) -> None:
 
 def reference_quality(design, bins: int, device: int) -> dict:
     """One whole run of the reference CUDA backend (rebuilt for sm_100a) with the reference's
-    default options (280-iteration budget, early stop on): the quality the engine's e2e run is
-    compared with."""
+    default options and the e2e run's iteration budget (early stop on): the quality the engine's
+    e2e run is compared with."""
     from oracle.ref import ReferenceLibrary, default_options
 
     lib = ReferenceLibrary("cuda")
-    options = default_options(bins_x=bins, bins_y=bins, target_density=0.9, compute_backend=1, cuda_device=device)
+    options = default_options(bins_x=bins, bins_y=bins, target_density=0.9, compute_backend=1, cuda_device=device,
+                              iterations=E2E_BUDGET)
     _, _, result, _ = lib.global_place(design, options)
     return {"hpwl_after": result.hpwl_after, "overflow_after": result.overflow_after,
             "completed_iterations": result.completed_iterations,
             "best_checkpoint_iteration": result.best_checkpoint_iteration,
             "seconds": result.elapsed_seconds,
             "backend_used": "cuda" if result.compute_backend_used == 1 else "cpu",
-            "what": "reference CUDA backend rebuilt for sm_100a, default options (280-iteration budget, "
-                    "early stop on), same design and initial placement"}
+            "what": f"reference CUDA backend rebuilt for sm_100a, default options with the e2e run's "
+                    f"{E2E_BUDGET}-iteration budget (early stop on), same design and initial placement"}
 
 
 def run_reference(args) -> None:
@@ -483,7 +489,13 @@ def batched_instances(count: int, seed: int):
 
 
 def run_batched(args) -> None:
-    """Aggregate iterations/s of many independent instances: one at a time vs all through the server."""
+    """Aggregate iterations/s of many independent instances: one at a time (plain) against the server,
+    batched (every round of the running instances' evaluations in one launch per kernel family) and,
+    for comparison, concurrent (every instance launching its own kernels).  Each server mode runs
+    three times; the line reports the median and the spread, and whether every instance's result is
+    bit-identical to its plain run."""
+    import numpy as np
+
     import myplacement_b200 as mp
 
     jobs = batched_instances(args.instances, args.seed)
@@ -492,23 +504,40 @@ def run_batched(args) -> None:
     t0 = time.perf_counter()
     plain = [placer.run(d, o) for d, o in jobs]
     plain_seconds = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    placed, job_stats, server_stats = mp.batch_place([d for d, _ in jobs], [o for _, o in jobs],
-                                                     workers=args.workers)
-    batched_seconds = time.perf_counter() - t0
+    plain_rate = sum(r.completed_iterations for r in plain) / plain_seconds
+
+    def server_runs(batched: bool, repeats: int):
+        rates, last = [], None
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            placed, job_stats, server_stats = mp.batch_place([d for d, _ in jobs], [o for _, o in jobs],
+                                                             workers=args.workers, batched=batched)
+            seconds = time.perf_counter() - t0
+            rates.append(sum(r.completed_iterations for r in placed) / seconds)
+            last = (placed, server_stats, seconds)
+        return rates, last
+
+    batched_rates, (placed, server_stats, batched_seconds) = server_runs(True, 3)
+    concurrent_rates, _ = server_runs(False, 1)
     iterations = sum(r.completed_iterations for r in placed)
-    same = all(a.hpwl_after == b.hpwl_after and a.completed_iterations == b.completed_iterations
+    same = all(np.array_equal(a.module_x, b.module_x) and np.array_equal(a.module_y, b.module_y) and
+               a.hpwl_after == b.hpwl_after and a.completed_iterations == b.completed_iterations
                for a, b in zip(placed, plain))
+    value = statistics.median(batched_rates)
     line = {
         "form": "batched", "metric": "aggregate GP iterations/s, independent instances on one GPU",
-        "value": iterations / batched_seconds, "unit": "iterations/s", "n_gpus": 1, "higher_is_better": True,
-        "plain_one_at_a_time": sum(r.completed_iterations for r in plain) / plain_seconds,
-        "speedup_vs_plain": (iterations / batched_seconds) / (sum(r.completed_iterations for r in plain) / plain_seconds),
+        "value": value, "unit": "iterations/s", "n_gpus": 1, "higher_is_better": True,
+        "runs": batched_rates, "spread": [min(batched_rates), max(batched_rates)],
+        "plain_one_at_a_time": plain_rate, "speedup_vs_plain": value / plain_rate,
+        "concurrent_without_batching": concurrent_rates[0],
         "instances": len(jobs), "workers": args.workers, "iterations": iterations,
         "seconds": batched_seconds, "plain_seconds": plain_seconds,
-        "results_identical_to_plain": same,
+        "results_identical_to_plain": bool(same),
         "overflow_le_0.10": sum(r.overflow_after <= 0.10 for r in placed),
-        "peak_running": server_stats["peak_running"],
+        "hpwl_total": sum(r.hpwl_after for r in placed), "hpwl_total_plain": sum(r.hpwl_after for r in plain),
+        "peak_running": server_stats["peak_running"], "batch_rounds": server_stats["batch_rounds"],
+        "evaluations_per_round": server_stats["batch_evaluations"] / max(1, server_stats["batch_rounds"]),
+        "gpu_launches": server_stats["batch_launches"],
         "data": "synthetic: cells log-normal median 4k in 1k-20k, small-design net law, bins 32^2-256^2, "
                 "early stop on (280-iteration budget)",
     }

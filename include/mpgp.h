@@ -554,11 +554,22 @@ typedef struct mpgp_server_stats {
     uint64_t memory_budget;
     uint64_t peak_reserved;         /* largest sum of admitted footprints */
     double seconds;                 /* since the server was created */
+    int32_t batched;                /* 1: the running jobs' evaluations share batched launches */
+    int32_t batch_peak_round;       /* most evaluations one batched round carried */
+    int64_t batch_rounds;           /* batched rounds launched */
+    int64_t batch_evaluations;      /* evaluations those rounds carried */
+    int64_t batch_launches;         /* kernel launches of those rounds */
 } mpgp_server_stats;
 
 /* Upper bound of the device bytes one placement of `design` reserves. */
 int mpgp_estimate_bytes(const mpgp_design* design, const mpgp_options* options, uint64_t* bytes);
 int mpgp_server_create(int device, uint64_t memory_budget_bytes, int32_t workers, mpgp_server** out);
+/* As mpgp_server_create, choosing the mode: batched != 0 gathers the running
+ * jobs' evaluations into shared rounds, one launch per kernel family for all of
+ * them (mpgp_server_create's mode); batched == 0 lets every job launch its own
+ * kernels on its own streams.  The results are the same either way. */
+int mpgp_server_create_mode(int device, uint64_t memory_budget_bytes, int32_t workers, int32_t batched,
+                            mpgp_server** out);
 /* Copies the design and options (options->cuda_device is replaced by the
  * server's device).  A job whose footprint exceeds the budget is refused with
  * MPGP_ERR_BUDGET. */
@@ -573,10 +584,11 @@ int mpgp_server_stats_get(const mpgp_server* server, mpgp_server_stats* stats);
 /* Finishes the running jobs, abandons the queued ones, joins the workers. */
 void mpgp_server_destroy(mpgp_server* server);
 
-/* The batched form: `count` placements through a server (submit all, take all).
- * module_x[i] / module_y[i] receive design i's positions; history is not kept. */
+/* The batched form: `count` placements through a server (submit all, take all),
+ * in the server's batched mode when batched != 0.  module_x[i] / module_y[i]
+ * receive design i's positions; history is not kept. */
 int mpgp_batch_place(int32_t count, const mpgp_design* designs, const mpgp_options* options, int device,
-                     int32_t workers, uint64_t memory_budget_bytes, double* const* module_x,
+                     int32_t workers, int32_t batched, uint64_t memory_budget_bytes, double* const* module_x,
                      double* const* module_y, mpgp_result* results, mpgp_job_stats* job_stats,
                      mpgp_server_stats* server_stats);
 

@@ -313,6 +313,11 @@ class ServerStats(C.Structure):
         ("memory_budget", C.c_uint64),
         ("peak_reserved", C.c_uint64),
         ("seconds", C.c_double),
+        ("batched", C.c_int32),
+        ("batch_peak_round", C.c_int32),
+        ("batch_rounds", C.c_int64),
+        ("batch_evaluations", C.c_int64),
+        ("batch_launches", C.c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -366,6 +371,7 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "mpgp_session_destroy": (None, [vp]),
         "mpgp_estimate_bytes": (C.c_int, [C.POINTER(Design), C.POINTER(Options), C.POINTER(C.c_uint64)]),
         "mpgp_server_create": (C.c_int, [C.c_int, C.c_uint64, C.c_int32, C.POINTER(vp)]),
+        "mpgp_server_create_mode": (C.c_int, [C.c_int, C.c_uint64, C.c_int32, C.c_int32, C.POINTER(vp)]),
         "mpgp_server_submit": (C.c_int, [vp, C.POINTER(Design), C.POINTER(Options), C.POINTER(C.c_int64)]),
         "mpgp_server_wait": (C.c_int, [vp, C.c_int64, C.c_double, _i32]),
         "mpgp_server_take": (C.c_int, [vp, C.c_int64, _d, _d, C.POINTER(Result), C.POINTER(HistoryRow), C.c_int32,
@@ -373,7 +379,7 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "mpgp_server_stats_get": (C.c_int, [vp, C.POINTER(ServerStats)]),
         "mpgp_server_destroy": (None, [vp]),
         "mpgp_batch_place": (C.c_int, [C.c_int32, C.POINTER(Design), C.POINTER(Options), C.c_int, C.c_int32,
-                                       C.c_uint64, C.POINTER(_d), C.POINTER(_d), C.POINTER(Result),
+                                       C.c_int32, C.c_uint64, C.POINTER(_d), C.POINTER(_d), C.POINTER(Result),
                                        C.POINTER(JobStats), C.POINTER(ServerStats)]),
     }
     for name, (restype, argtypes) in sig.items():

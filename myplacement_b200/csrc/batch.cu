@@ -1,0 +1,284 @@
+// Batched rounds of many engines' evaluations (batch.hpp).
+#include "batch.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+
+#include "common.cuh"
+#include "dct_tc.cuh"
+
+namespace mpgp {
+
+namespace {
+
+std::size_t alignUp(std::size_t value, std::size_t alignment) { return (value + alignment - 1) / alignment * alignment; }
+
+// A round's argument blocks, laid out one after another in one buffer.
+struct RoundLayout {
+    std::size_t bytes = 0;
+    template <typename T>
+    std::size_t add(std::size_t count) {
+        const std::size_t at = alignUp(bytes, 256);
+        bytes = at + std::max<std::size_t>(1, count) * sizeof(T);
+        return at;
+    }
+};
+
+constexpr int kContractionStages = 4;  // forward 1, forward 2, inverse 1, inverse 2
+
+}  // namespace
+
+Batch::Batch(int device, double window_seconds) : device_(device), window_(window_seconds) {
+    require(window_seconds >= 0.0, "The batch window must be non-negative.");
+    checkCuda(cudaSetDevice(device_), "Select CUDA device");
+    checkCuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "Create batch stream");
+    checkCuda(cudaStreamCreateWithFlags(&wirelength_, cudaStreamNonBlocking), "Create batch wirelength stream");
+    checkCuda(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "Create batch event");
+    checkCuda(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "Create batch event");
+    checkCuda(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "Create batch event");
+    reserve(std::size_t{1} << 20);
+    thread_ = std::thread([this] { loop(); });
+}
+
+Batch::~Batch() {
+    {
+        std::lock_guard<std::mutex> lock(mutex_);
+        stopping_ = true;
+    }
+    submitted_.notify_all();
+    if (thread_.joinable()) thread_.join();
+    cudaSetDevice(device_);
+    if (stream_ != nullptr) cudaStreamSynchronize(stream_);
+    if (wirelength_ != nullptr) cudaStreamSynchronize(wirelength_);
+    if (fork_ != nullptr) cudaEventDestroy(fork_);
+    if (join_ != nullptr) cudaEventDestroy(join_);
+    if (done_ != nullptr) cudaEventDestroy(done_);
+    if (host_args_ != nullptr) cudaFreeHost(host_args_);
+    if (device_args_ != nullptr) cudaFree(device_args_);
+    if (wirelength_ != nullptr) cudaStreamDestroy(wirelength_);
+    if (stream_ != nullptr) cudaStreamDestroy(stream_);
+}
+
+void Batch::reserve(std::size_t bytes) {
+    if (bytes <= capacity_) return;
+    const std::size_t grown = std::max(bytes, 2 * capacity_);
+    // The previous round has completed (rounds end with a synchronisation), so
+    // neither buffer is in use.
+    if (host_args_ != nullptr) checkCuda(cudaFreeHost(host_args_), "Free batch staging");
+    if (device_args_ != nullptr) checkCuda(cudaFree(device_args_), "Free batch arguments");
+    host_args_ = nullptr;
+    device_args_ = nullptr;
+    capacity_ = 0;
+    checkCuda(cudaMallocHost(reinterpret_cast<void**>(&host_args_), grown), "Allocate batch staging");
+    checkCuda(cudaMalloc(reinterpret_cast<void**>(&device_args_), grown), "Allocate batch arguments");
+    capacity_ = grown;
+}
+
+void Batch::attach(Engine* engine) {
+    engine->deviceBatches();  // the contraction descriptors the batched launches read
+    std::lock_guard<std::mutex> lock(mutex_);
+    ++attached_;
+}
+
+void Batch::detach(Engine* /*engine*/) {
+    {
+        std::lock_guard<std::mutex> lock(mutex_);
+        --attached_;
+    }
+    submitted_.notify_all();  // a round waiting for this engine can start
+}
+
+void Batch::evaluate(Engine* engine, const EvalPlan& plan) {
+    Request request{engine, &plan, false, std::string(), MPGP_OK};
+    {
+        std::unique_lock<std::mutex> lock(mutex_);
+        require(!stopping_, "The batch is shutting down.");
+        pending_.push_back(&request);
+        submitted_.notify_all();
+        finished_.wait(lock, [&] { return request.done; });
+    }
+    if (request.status != MPGP_OK) fail(request.status, request.error);
+}
+
+BatchStats Batch::stats() const {
+    std::lock_guard<std::mutex> lock(mutex_);
+    return stats_;
+}
+
+void Batch::loop() {
+    cudaSetDevice(device_);
+    for (;;) {
+        std::vector<Request*> round;
+        {
+            std::unique_lock<std::mutex> lock(mutex_);
+            submitted_.wait(lock, [&] { return stopping_ || !pending_.empty(); });
+            if (pending_.empty()) return;  // stopping
+            // Give the attached engines that have not handed in their evaluation a
+            // short window to do so, then launch whatever is there.
+            const auto deadline = std::chrono::steady_clock::now() + std::chrono::duration<double>(window_);
+            submitted_.wait_until(lock, deadline,
+                                  [&] { return stopping_ || static_cast<int>(pending_.size()) >= attached_; });
+            round.swap(pending_);
+        }
+        int status = MPGP_OK;
+        std::string error;
+        try {
+            execute(round);
+        } catch (const Error& e) {
+            status = e.status();
+            error = e.what();
+        } catch (const std::exception& e) {
+            status = MPGP_ERR_RUNTIME;
+            error = e.what();
+        }
+        {
+            std::lock_guard<std::mutex> lock(mutex_);
+            for (Request* r : round) {
+                r->status = status;
+                r->error = error;
+                r->done = true;
+            }
+            stats_.rounds += 1;
+            stats_.evaluations += static_cast<int64_t>(round.size());
+            stats_.peak_round = std::max(stats_.peak_round, static_cast<int>(round.size()));
+        }
+        finished_.notify_all();
+    }
+}
+
+void Batch::execute(const std::vector<Request*>& round) {
+    const int n = static_cast<int>(round.size());
+    std::vector<int> scatter, metrics, gather;
+    std::vector<TcItem> items[kContractionStages][kMaxSplit];
+    int staged = 0;
+    for (int i = 0; i < n; ++i) {
+        const EvalPlan& p = *round[i]->plan;
+        Engine* engine = round[i]->engine;
+        if (p.scatter) scatter.push_back(i);
+        if (p.metrics) metrics.push_back(i);
+        if (p.gather) gather.push_back(i);
+        const int total = p.reduce_args.offsets[p.reduce_args.source_count];
+        if (total <= p.reduce_args.staged_capacity) staged = std::max(staged, total);
+        const TcBatch* device_batches = engine->deviceBatches();
+        for (int stage = 0; stage < kContractionStages; ++stage) {
+            if (stage < 2 ? !p.forward : !p.gradient) continue;
+            const TcBatch& batch = engine->contraction(stage);
+            const int tasks = stage < 2 ? 1 : 2;
+            for (int task = 0; task < tasks; ++task) {
+                const int tiles = taskTiles(batch, task);
+                for (int tile = 0; tile < tiles; ++tile) {
+                    items[stage][batch.ksplit - 1].push_back(TcItem{device_batches + stage, task, tile});
+                }
+            }
+        }
+    }
+
+    RoundLayout layout;
+    const std::size_t at_scatter = layout.add<ScatterArgs>(scatter.size());
+    const std::size_t at_scatter_offsets = layout.add<int>(scatter.size() + 1);
+    const std::size_t at_wirelength = layout.add<WirelengthArgs>(static_cast<std::size_t>(n));
+    const std::size_t at_wirelength_offsets = layout.add<int>(static_cast<std::size_t>(n) + 1);
+    const std::size_t at_metrics = layout.add<MetricsArgs>(metrics.size());
+    const std::size_t at_metrics_offsets = layout.add<int>(metrics.size() + 1);
+    const std::size_t at_gather = layout.add<GatherArgs>(gather.size());
+    const std::size_t at_gather_offsets = layout.add<int>(gather.size() + 1);
+    const std::size_t at_reduce = layout.add<ReduceArgs>(static_cast<std::size_t>(n));
+    std::size_t at_items[kContractionStages][kMaxSplit];
+    for (int stage = 0; stage < kContractionStages; ++stage) {
+        for (int k = 0; k < kMaxSplit; ++k) at_items[stage][k] = layout.add<TcItem>(items[stage][k].size());
+    }
+    reserve(layout.bytes);
+
+    unsigned char* host = host_args_;
+    const auto fill = [&](std::size_t at, const std::vector<int>& members, auto args_of, auto blocks_of,
+                          std::size_t offsets_at) {
+        using Args = std::decay_t<decltype(args_of(*round[0]->plan))>;
+        Args* args = reinterpret_cast<Args*>(host + at);
+        int* offsets = reinterpret_cast<int*>(host + offsets_at);
+        int blocks = 0;
+        for (std::size_t j = 0; j < members.size(); ++j) {
+            const EvalPlan& p = *round[members[j]]->plan;
+            args[j] = args_of(p);
+            offsets[j] = blocks;
+            blocks += blocks_of(p);
+        }
+        offsets[members.size()] = blocks;
+        return blocks;
+    };
+    std::vector<int> everyone(static_cast<std::size_t>(n));
+    for (int i = 0; i < n; ++i) everyone[static_cast<std::size_t>(i)] = i;
+    const int scatter_blocks = fill(
+        at_scatter, scatter, [](const EvalPlan& p) { return p.scatter_args; },
+        [](const EvalPlan& p) { return p.scatter_blocks; }, at_scatter_offsets);
+    const int wirelength_blocks = fill(
+        at_wirelength, everyone, [](const EvalPlan& p) { return p.wirelength_args; },
+        [](const EvalPlan& p) { return p.wirelength_blocks; }, at_wirelength_offsets);
+    const int metrics_blocks = fill(
+        at_metrics, metrics, [](const EvalPlan& p) { return p.metrics_args; },
+        [](const EvalPlan& p) { return p.metrics_blocks; }, at_metrics_offsets);
+    const int gather_blocks = fill(
+        at_gather, gather, [](const EvalPlan& p) { return p.gather_args; },
+        [](const EvalPlan& p) { return p.gather_blocks; }, at_gather_offsets);
+    ReduceArgs* reduce = reinterpret_cast<ReduceArgs*>(host + at_reduce);
+    for (int i = 0; i < n; ++i) reduce[i] = round[i]->plan->reduce_args;
+    for (int stage = 0; stage < kContractionStages; ++stage) {
+        for (int k = 0; k < kMaxSplit; ++k) {
+            if (!items[stage][k].empty()) {
+                std::memcpy(host + at_items[stage][k], items[stage][k].data(), items[stage][k].size() * sizeof(TcItem));
+            }
+        }
+    }
+
+    unsigned char* dev = device_args_;
+    const auto on_device = [&](std::size_t at) { return dev + at; };
+    checkCuda(cudaMemcpyAsync(dev, host, layout.bytes, cudaMemcpyHostToDevice, stream_), "Upload batch arguments");
+    int64_t launches = 0;
+    // The same order as one engine's evaluation (Engine::run): scatter (which forms
+    // proposal and lookahead positions), the wirelength pass beside the density
+    // chain, metrics, the contractions, then the gather and the reduction.
+    if (!scatter.empty()) {
+        launchScatterBatch(reinterpret_cast<const ScatterArgs*>(on_device(at_scatter)),
+                           reinterpret_cast<const int*>(on_device(at_scatter_offsets)), static_cast<int>(scatter.size()),
+                           scatter_blocks, stream_);
+        ++launches;
+    }
+    checkCuda(cudaEventRecord(fork_, stream_), "Batch fork");
+    checkCuda(cudaStreamWaitEvent(wirelength_, fork_, 0), "Batch fork");
+    if (wirelength_blocks > 0) {
+        launchWirelengthBatch(reinterpret_cast<const WirelengthArgs*>(on_device(at_wirelength)),
+                              reinterpret_cast<const int*>(on_device(at_wirelength_offsets)), n, wirelength_blocks,
+                              wirelength_);
+        ++launches;
+    }
+    checkCuda(cudaEventRecord(join_, wirelength_), "Batch join");
+    if (!metrics.empty()) {
+        launchMetricsSplitBatch(reinterpret_cast<const MetricsArgs*>(on_device(at_metrics)),
+                                reinterpret_cast<const int*>(on_device(at_metrics_offsets)),
+                                static_cast<int>(metrics.size()), metrics_blocks, stream_);
+        ++launches;
+    }
+    for (int stage = 0; stage < kContractionStages; ++stage) {
+        for (int k = 0; k < kMaxSplit; ++k) {
+            if (items[stage][k].empty()) continue;
+            launchTcGemmBatch(reinterpret_cast<const TcItem*>(on_device(at_items[stage][k])),
+                              static_cast<int>(items[stage][k].size()), k + 1, stream_);
+            ++launches;
+        }
+    }
+    checkCuda(cudaStreamWaitEvent(stream_, join_, 0), "Batch join");
+    if (!gather.empty()) {
+        launchGatherBatch(reinterpret_cast<const GatherArgs*>(on_device(at_gather)),
+                          reinterpret_cast<const int*>(on_device(at_gather_offsets)), static_cast<int>(gather.size()),
+                          gather_blocks, stream_);
+        ++launches;
+    }
+    launchReduceBatch(reinterpret_cast<const ReduceArgs*>(on_device(at_reduce)), n, staged, stream_);
+    ++launches;
+    checkCuda(cudaEventRecord(done_, stream_), "Batch done");
+    checkCuda(cudaEventSynchronize(done_), "Batched evaluation on the device");
+    std::lock_guard<std::mutex> lock(mutex_);
+    stats_.launches += launches;
+}
+
+}  // namespace mpgp

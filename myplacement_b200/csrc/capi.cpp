@@ -542,14 +542,19 @@ int mpgp_estimate_bytes(const mpgp_design* design, const mpgp_options* options, 
     });
 }
 
-int mpgp_server_create(int device, uint64_t memory_budget_bytes, int32_t workers, mpgp_server** out) {
+int mpgp_server_create_mode(int device, uint64_t memory_budget_bytes, int32_t workers, int32_t batched,
+                            mpgp_server** out) {
     return guarded([&] {
         mpgp::require(out != nullptr, "An output handle is required.");
         *out = nullptr;
         auto handle = std::make_unique<mpgp_server>();
-        handle->server = std::make_unique<mpgp::Server>(device, memory_budget_bytes, workers);
+        handle->server = std::make_unique<mpgp::Server>(device, memory_budget_bytes, workers, batched != 0);
         *out = handle.release();
     });
+}
+
+int mpgp_server_create(int device, uint64_t memory_budget_bytes, int32_t workers, mpgp_server** out) {
+    return mpgp_server_create_mode(device, memory_budget_bytes, workers, 1, out);
 }
 
 int mpgp_server_submit(mpgp_server* s, const mpgp_design* design, const mpgp_options* options, int64_t* job) {
@@ -586,12 +591,13 @@ int mpgp_server_stats_get(const mpgp_server* s, mpgp_server_stats* stats) {
 void mpgp_server_destroy(mpgp_server* s) { delete s; }
 
 int mpgp_batch_place(int32_t count, const mpgp_design* designs, const mpgp_options* options, int device,
-                     int32_t workers, uint64_t memory_budget_bytes, double* const* module_x, double* const* module_y,
-                     mpgp_result* results, mpgp_job_stats* job_stats, mpgp_server_stats* server_stats) {
+                     int32_t workers, int32_t batched, uint64_t memory_budget_bytes, double* const* module_x,
+                     double* const* module_y, mpgp_result* results, mpgp_job_stats* job_stats,
+                     mpgp_server_stats* server_stats) {
     return guarded([&] {
         mpgp::require(count >= 0 && (count == 0 || (designs != nullptr && options != nullptr)),
                       "Designs and options are required.");
-        mpgp::Server server(device, memory_budget_bytes, workers);
+        mpgp::Server server(device, memory_budget_bytes, workers, batched != 0);
         std::vector<int64_t> ids(static_cast<std::size_t>(count));
         for (int32_t i = 0; i < count; ++i) ids[i] = server.submit(designs[i], options[i]);
         int first_failure = MPGP_OK;

@@ -109,22 +109,24 @@ __device__ __forceinline__ unsigned int atomicAddAcqRel(unsigned int* address, u
 }
 
 // Second level of a deterministic grid reduction, called by every block after
-// thread 0 wrote the block's K partials at partials[k * gridDim.x + blockIdx.x]
-// (column-major): the last block of each group of 32 consecutive blocks reduces
-// the group's rows (in block order) into group_partials[k * groups + group].  counters holds 1 + groups
+// thread 0 wrote the block's K partials at partials[k * grid + block]
+// (column-major; block / grid are the block's index and the block count of its
+// launch, or of its instance in a batched launch): the last block of each group
+// of 32 consecutive blocks reduces the group's rows (in block order) into
+// group_partials[k * groups + group].  counters holds 1 + groups
 // zeros and is left zeroed.  Returns 0 in most blocks, 1 in a block that
 // finished a group, 2 in the block that finished the last group (after which
 // every group row is visible to it).  Thread 0 does every global write and
 // counter update, so its release / acquire atomics order all of them.
 template <int K>
 __device__ int reduceGroups(const double* partials, double* group_partials, unsigned int* counters,
-                            const bool (&is_max)[K]) {
+                            const bool (&is_max)[K], unsigned int block, unsigned int grid) {
     __shared__ int state;
     __shared__ double folded[K];
-    const unsigned int group = blockIdx.x / 32U;
-    const unsigned int groups = (gridDim.x + 31U) / 32U;
+    const unsigned int group = block / 32U;
+    const unsigned int groups = (grid + 31U) / 32U;
     const unsigned int first = group * 32U;
-    const unsigned int size = min(32U, gridDim.x - first);
+    const unsigned int size = min(32U, grid - first);
     if (threadIdx.x == 0) state = atomicAddAcqRel(counters + 1 + group, 1U) == size - 1U ? 1 : 0;
     __syncthreads();
     if (state == 0) return 0;
@@ -133,7 +135,7 @@ __device__ int reduceGroups(const double* partials, double* group_partials, unsi
     const int warps = static_cast<int>(blockDim.x >> 5);
     for (int k = warp; k < K; k += warps) {
         double x = is_max[k] ? -1.0e308 : 0.0;
-        if (lane < size) x = __ldcg(partials + static_cast<size_t>(k) * gridDim.x + first + lane);
+        if (lane < size) x = __ldcg(partials + static_cast<size_t>(k) * grid + first + lane);
         x = is_max[k] ? warpMax(x) : warpSum(x);
         if (lane == 0) folded[k] = x;
     }
@@ -147,6 +149,23 @@ __device__ int reduceGroups(const double* partials, double* group_partials, unsi
     }
     __syncthreads();
     return state;
+}
+
+// Batched launches: the blocks of `count` instances one after another, instance k
+// owning blocks [offsets[k], offsets[k + 1]).  Returns (instance, block within the
+// instance, block count of the instance) for block `block` of the launch.
+__device__ __forceinline__ int3 batchSlot(const int* offsets, int count, int block) {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(offsets + mid) <= block) {
+            lo = mid;
+        } else {
+            hi = mid - 1;
+        }
+    }
+    const int first = __ldg(offsets + lo);
+    return make_int3(lo, block - first, __ldg(offsets + lo + 1) - first);
 }
 
 __device__ __forceinline__ long long warpSumI64(long long value) {

@@ -222,13 +222,13 @@ __device__ __forceinline__ float loadShared(uint32_t address) {
 // Parseval weight of a DCT-II index: 1/2 for the DC term, 1 otherwise.
 __device__ __forceinline__ double parsevalWeight(int index) { return index == 0 ? 0.5 : 1.0; }
 
-__global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_constant__ TcBatch batch) {
-    const TcTask& t = batch.task[blockIdx.y];
+// One CTA of the cluster that computes output tile `tile_index` of task `t`;
+// `local_block` = tile_index * ksplit + the CTA's rank (its energy partial and,
+// for block 0, the task's bookkeeping).  The caller has released its successor.
+__device__ __forceinline__ void tcTile(const TcBatch& batch, const TcTask& t, int tile_index, int local_block) {
     const int ksplit = batch.ksplit;
     const int tiles_n = (t.n + kTileN - 1) / kTileN;
     const int tiles_m = (t.m + kTileM - 1) / kTileM;
-    const int tile_index = static_cast<int>(blockIdx.x) / ksplit;
-    releaseNext();
     // The whole cluster shares the tile, so the whole cluster leaves together.
     if (tile_index >= tiles_m * tiles_n) return;
     if (batch.stall_polls > 0) {
@@ -625,9 +625,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
         const bool is_max[2] = {false, true};
         blockReduce<2>(values, is_max);
         if (threadIdx.x == 0) {
-            if (t.mode == kTcSpectral && t.energy_partials != nullptr) t.energy_partials[blockIdx.x] = values[0];
+            if (t.mode == kTcSpectral && t.energy_partials != nullptr) t.energy_partials[local_block] = values[0];
             if (t.out_max != nullptr) atomicMax(t.out_max, __float_as_uint(static_cast<float>(values[1])));
-            if (blockIdx.x == 0) {
+            if (local_block == 0) {
                 if (t.out_exp != nullptr) *t.out_exp = out_exp;
                 if (t.clear != nullptr) *t.clear = 0u;
             }
@@ -639,6 +639,28 @@ __global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_const
         const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tmem_slot);
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemColumns));
     }
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) tcGemmKernel(const __grid_constant__ TcBatch batch) {
+    releaseNext();
+    tcTile(batch, batch.task[blockIdx.y], static_cast<int>(blockIdx.x) / batch.ksplit, static_cast<int>(blockIdx.x));
+}
+
+// Batched: cluster c computes items[c] (an instance's batch, task and tile); every
+// item's batch has the launch's K split.
+__global__ void __launch_bounds__(kTcThreads, 1) tcGemmBatchKernel(const TcItem* items, int ksplit) {
+    releaseNext();
+    const TcItem item = items[blockIdx.x / static_cast<unsigned>(ksplit)];
+    const TcBatch& batch = *item.batch;
+    if (threadIdx.x == 0) {
+        // The tensor maps live in global memory here (uploaded by a copy, possibly into
+        // memory an earlier engine's maps used): make the TMA proxy see their current bytes.
+        const TcTask& t = batch.task[item.task];
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&t.map_a) : "memory");
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&t.map_b) : "memory");
+    }
+    tcTile(batch, batch.task[item.task], item.tile,
+           item.tile * ksplit + static_cast<int>(blockIdx.x % static_cast<unsigned>(ksplit)));
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
@@ -697,6 +719,10 @@ void configureKernel() {
     require(device >= 0 && device < kMaxDevices, "Device index out of range.");
     std::call_once(once[device], [device] {
         attribute[device] = cudaFuncSetAttribute(tcGemmKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        if (attribute[device] == cudaSuccess) {
+            attribute[device] =
+                cudaFuncSetAttribute(tcGemmBatchKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        }
     });
     checkCuda(attribute[device], "Configure the tcgen05 contraction kernel");
 }
@@ -772,6 +798,23 @@ void tcPlan(TcBatch& batch, int task_count) {
 int tcBlocks(const TcBatch& batch, int task_count) {
     (void)task_count;
     return batchTiles(batch, task_count) * batch.ksplit;
+}
+
+int taskTiles(const TcBatch& batch, int task) {
+    const TcTask& t = batch.task[task];
+    return ((t.m + kTileM - 1) / kTileM) * ((t.n + kTileN - 1) / kTileN);
+}
+
+void launchTcGemmBatch(const TcItem* items, int count, int ksplit, cudaStream_t stream) {
+    if (count <= 0) return;
+    configureKernel();
+    require(ksplit >= 1 && ksplit <= kMaxSplit && (ksplit & (ksplit - 1)) == 0,
+            "Contraction K split must be a power of two up to kMaxSplit.");
+    cudaLaunchAttribute attribute[2] = {};
+    const cudaLaunchConfig_t config =
+        launchConfig(dim3(static_cast<unsigned>(count * ksplit)), ksplit, stream, attribute);
+    checkCuda(cudaLaunchKernelEx(&config, tcGemmBatchKernel, items, ksplit),
+              "Launch the batched tcgen05 contraction kernel");
 }
 
 void launchTcGemm(const TcBatch& batch, int task_count, cudaStream_t stream) {

@@ -99,6 +99,18 @@ struct alignas(64) TcBatch {
     long long stall_polls;
 };
 
+// One cluster's work in a batched launch: output tile `tile` of task `task` of
+// `batch` (a TcBatch in device memory, whose tensor maps the TMA reads there).
+struct TcItem {
+    const TcBatch* batch;
+    int task;
+    int tile;
+};
+// Output tiles of task i of a batch.
+int taskTiles(const TcBatch& batch, int task);
+// Launches `count` items (clusters of `ksplit` CTAs) from device memory.
+void launchTcGemmBatch(const TcItem* items, int count, int ksplit, cudaStream_t stream);
+
 void makeOperandMap(CUtensorMap* map, const SplitMatrix& m, int box_rows);
 // Chooses the K split of a batch: the largest cluster size whose clusters all fit
 // on the GPU at once.  Call after the tasks are filled in.

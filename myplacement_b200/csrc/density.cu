@@ -36,10 +36,8 @@ __device__ __forceinline__ double clampCenter(double value, double size, double 
     return lo <= hi ? fmax(lo, fmin(value, hi)) : __dmul_rn(__dadd_rn(low, high), 0.5);
 }
 
-__global__ void __launch_bounds__(kThreads) scatterKernel(ScatterArgs a) {
-    releaseNext();
-    waitForPrior();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void scatterBlock(const ScatterArgs& a, int block, int grid) {
+    const int i = block * blockDim.x + threadIdx.x;
     double predicted = 0.0;
     double displacement = 0.0;
     long long totals[3] = {0, 0, 0};
@@ -136,11 +134,25 @@ __global__ void __launch_bounds__(kThreads) scatterKernel(ScatterArgs a) {
             if (block_totals[k] != 0) atomicAdd(a.totals + k, static_cast<unsigned long long>(block_totals[k]));
         }
         if (a.partials != nullptr) {
-            a.partials[blockIdx.x] = values[0];
-            a.partials[gridDim.x + blockIdx.x] = values[1];
+            a.partials[block] = values[0];
+            a.partials[grid + block] = values[1];
         }
     }
+}
 
+__global__ void __launch_bounds__(kThreads) scatterKernel(ScatterArgs a) {
+    releaseNext();
+    waitForPrior();
+    scatterBlock(a, static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x));
+}
+
+__global__ void __launch_bounds__(kThreads) scatterBatchKernel(const ScatterArgs* args, const int* offsets,
+                                                               int count) {
+    releaseNext();
+    waitForPrior();
+    const int3 slot = batchSlot(offsets, count, static_cast<int>(blockIdx.x));
+    const ScatterArgs a = args[slot.x];
+    scatterBlock(a, slot.y, slot.z);
 }
 
 // One bin's metric terms (DensityBin::chargeArea / normalizationArea, Metrics.hpp:25-35).
@@ -227,9 +239,7 @@ __global__ void __launch_bounds__(kThreads) metricsKernel(MetricsArgs a) {
 // per bin row forms the row's sources in registers (they are never stored),
 // takes the row maximum for the row's plane exponent (splitSourceKernel's rule)
 // and writes the fp16 hi / lo planes of the first contraction's operand.
-__global__ void __launch_bounds__(kThreads) metricsSplitKernel(MetricsArgs a) {
-    releaseNext();
-    waitForPrior();
+__device__ __forceinline__ void metricsSplitBlock(const MetricsArgs& a, int block, int grid) {
     BinTerms terms;
     terms.t = a.target_density;
     terms.unit = a.bin_area * kFixedUnit;
@@ -241,12 +251,12 @@ __global__ void __launch_bounds__(kThreads) metricsSplitKernel(MetricsArgs a) {
     const double charge_total =
         movable_sum + terms.t * (a.static_fixed_sum + macro_sum + a.static_dark_sum + filler_sum);
     terms.mean = charge_total / (a.bin_area * static_cast<double>(a.bin_count)) - terms.t;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (block == 0 && threadIdx.x == 0) {
         a.scales->max_x = 0u;
         a.scales->max_phi = 0u;
     }
 
-    const int row = blockIdx.x;
+    const int row = block;
     const int cols = a.columns;
     const size_t base = static_cast<size_t>(row) * cols;
     const int bins = a.bin_count;
@@ -333,8 +343,23 @@ __global__ void __launch_bounds__(kThreads) metricsSplitKernel(MetricsArgs a) {
     blockReduce<9>(v, is_max);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k) a.partials[k * gridDim.x + blockIdx.x] = v[k];
+        for (int k = 0; k < 9; ++k) a.partials[k * grid + block] = v[k];
     }
+}
+
+__global__ void __launch_bounds__(kThreads) metricsSplitKernel(MetricsArgs a) {
+    releaseNext();
+    waitForPrior();
+    metricsSplitBlock(a, static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x));
+}
+
+__global__ void __launch_bounds__(kThreads) metricsSplitBatchKernel(const MetricsArgs* args, const int* offsets,
+                                                                    int count) {
+    releaseNext();
+    waitForPrior();
+    const int3 slot = batchSlot(offsets, count, static_cast<int>(blockIdx.x));
+    const MetricsArgs a = args[slot.x];
+    metricsSplitBlock(a, slot.y, slot.z);
 }
 
 __global__ void velocityKernel(const double2* next, const double2* previous, double2* velocity, int count) {
@@ -362,6 +387,19 @@ void launchMetricsSplit(const MetricsArgs& args, cudaStream_t stream) {
     if (args.rows <= 0) return;
     launchChained("Launch the density metrics and source split", metricsSplitKernel, dim3(args.rows),
                   dim3(kThreads), 0, stream, args);
+}
+
+void launchScatterBatch(const ScatterArgs* args, const int* offsets, int count, int blocks, cudaStream_t stream) {
+    if (blocks <= 0 || count <= 0) return;
+    launchChained("Launch the batched density scatter", scatterBatchKernel, dim3(blocks), dim3(kThreads), 0, stream,
+                  args, offsets, count);
+}
+
+void launchMetricsSplitBatch(const MetricsArgs* args, const int* offsets, int count, int blocks,
+                             cudaStream_t stream) {
+    if (blocks <= 0 || count <= 0) return;
+    launchChained("Launch the batched density metrics and source split", metricsSplitBatchKernel, dim3(blocks),
+                  dim3(kThreads), 0, stream, args, offsets, count);
 }
 
 void launchVelocity(const double2* next, const double2* previous, double2* velocity, int count, cudaStream_t stream) {

@@ -19,6 +19,7 @@
 #include <atomic>
 #include <thread>
 
+#include "batch.hpp"
 #include "common.cuh"
 #include "ingest.cuh"
 
@@ -59,10 +60,17 @@ void upload(T* device, const std::vector<T>& host, cudaStream_t stream) {
 
 }  // namespace
 
-Engine::Engine(const Problem& p, int device, uint64_t budget_bytes) : device_(device), arena_(budget_bytes) {
+Engine::Engine(const Problem& p, int device, uint64_t budget_bytes, Batch* batch)
+    : device_(device), batch_(batch), arena_(budget_bytes) {
     checkCuda(cudaSetDevice(device_), "Select CUDA device");
-    checkCuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "Create engine stream");
-    checkCuda(cudaStreamCreateWithFlags(&stream_wl_, cudaStreamNonBlocking), "Create wirelength stream");
+    if (batch_ != nullptr) {
+        require(batch_->device() == device_, "A batch runs on one device.");
+        stream_ = batch_->stream();  // every engine of a batch works on the batch's stream
+        owns_stream_ = false;
+    } else {
+        checkCuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "Create engine stream");
+        checkCuda(cudaStreamCreateWithFlags(&stream_wl_, cudaStreamNonBlocking), "Create wirelength stream");
+    }
     checkCuda(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "Create fork event");
     checkCuda(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "Create join event");
     particle_count_ = p.particle_count;
@@ -91,12 +99,24 @@ Engine::Engine(const Problem& p, int device, uint64_t budget_bytes) : device_(de
               "pinned evaluation record");
     std::memset(host_slots_, 0, slot_bytes);
     checkCuda(cudaStreamSynchronize(stream_), "Engine setup");
+    if (batch_ != nullptr) {
+        batch_->attach(this);
+        attached_ = true;
+    }
+}
+
+void Engine::leaveBatch() {
+    if (batch_ != nullptr && attached_) {
+        attached_ = false;
+        batch_->detach(this);
+    }
 }
 
 Engine::~Engine() {
+    leaveBatch();
     if (stream_ != nullptr) {
         cudaStreamSynchronize(stream_);
-        cudaStreamDestroy(stream_);
+        if (owns_stream_) cudaStreamDestroy(stream_);
     }
     if (stream_wl_ != nullptr) {
         cudaStreamSynchronize(stream_wl_);
@@ -489,13 +509,14 @@ void Engine::runDct(bool gradient, bool potential, bool forward, bool split_sour
     }
 }
 
-void Engine::launch(const EvalRequest& q) {
+EvalPlan Engine::plan(const EvalRequest& q) {
     const int nx = bins_x_, ny = bins_y_;
     const double2* positions = q.mode == kGiven ? q.positions : q.out_positions;
     require(positions != nullptr, "An evaluation needs positions.");
     require(q.smoothing > 0.0 && std::isfinite(q.smoothing), "Global placement requires positive finite smoothing.");
+    EvalPlan p;
 
-    ScatterArgs sa{};
+    ScatterArgs& sa = p.scatter_args;
     sa.mode = q.mode;
     sa.particle_count = static_cast<int>(particle_count_);
     sa.positions = q.positions;
@@ -518,18 +539,13 @@ void Engine::launch(const EvalRequest& q) {
     sa.layers = layers_;
     sa.totals = totals_;
     sa.partials = partials_sc_;
-    if (q.mode == kGiven) checkCuda(cudaEventRecord(fork_, stream_), "fork");
-    if (!q.reuse_density) {
-        beginKernel(kKindScatter);
-        launchScatter(sa, particle_count_ > 0 ? scatter_blocks_ : 0, stream_);
-        endKernel();
-    }
+    p.scatter = !q.reuse_density && particle_count_ > 0;
+    p.scatter_blocks = scatter_blocks_;
     // The wirelength pass needs the positions only: it runs beside the density
     // chain on its own stream (after the scatter when the scatter forms them).
-    if (q.mode != kGiven) checkCuda(cudaEventRecord(fork_, stream_), "fork");
-    checkCuda(cudaStreamWaitEvent(stream_wl_, fork_, 0), "fork");
+    p.fork_first = q.mode == kGiven;
 
-    WirelengthArgs wa{};
+    WirelengthArgs& wa = p.wirelength_args;
     wa.positions = positions;
     wa.pin_particle = pin_particle_;
     wa.pin_offset = pin_offset_;
@@ -545,26 +561,17 @@ void Engine::launch(const EvalRequest& q) {
     wa.partials = partials_wl_;
     wa.group_partials = wl_group_;
     wa.group_counters = wl_counters_;
-    beginKernel(kKindWirelength, stream_wl_);
-    launchWirelength(wa, wl_blocks_, stream_wl_);
-    endKernel(stream_wl_);
+    p.wirelength_blocks = wl_blocks_;
     if (q.rudy) {
         // The routability term runs beside the density chain, after the wirelength pass.
         require(rudy_main_.columns > 0, "RUDY was not enabled for this engine.");
-        const RudyArgs ra = rudyArgs(rudy_main_, positions, true);
-        beginKernel(kKindRudy, stream_wl_);
-        launchRudyDeposit(ra, stream_wl_);
-        launchRudyPrefix(ra, stream_wl_);
-        launchRudyMetrics(ra, rudy_main_.blocks, stream_wl_);
-        if (q.gradient) {
-            launchRudyTables(ra, stream_wl_);
-            launchRudyGradient(ra, stream_wl_);
-        }
-        endKernel(stream_wl_);
+        p.rudy = true;
+        p.rudy_gradient = q.gradient;
+        p.rudy_args = rudyArgs(rudy_main_, positions, true);
+        p.rudy_blocks = rudy_main_.blocks;
     }
-    checkCuda(cudaEventRecord(join_, stream_wl_), "join");
 
-    MetricsArgs ma{};
+    MetricsArgs& ma = p.metrics_args;
     ma.layers = layers_;
     ma.totals = totals_;
     ma.static_charge = static_charge_;
@@ -577,7 +584,9 @@ void Engine::launch(const EvalRequest& q) {
     ma.partials = partials_m_;
     int kernels = 1;  // wirelength
     if (!q.reuse_density) {
-        beginKernel(kKindMetrics);
+        p.metrics = true;
+        p.metrics_fused = metrics_fused_;
+        p.metrics_blocks = metrics_blocks_;
         if (metrics_fused_) {
             ma.columns = nx;
             ma.rows = ny;
@@ -586,18 +595,15 @@ void Engine::launch(const EvalRequest& q) {
             ma.split_plane = tc_source_.plane();
             ma.row_exp = tc_row_exp_;
             ma.scales = tc_scales_;
-            launchMetricsSplit(ma, stream_);
-        } else {
-            launchMetrics(ma, metrics_blocks_, stream_);
         }
-        endKernel();
         kernels += 2;  // scatter, metrics
     }
+    p.forward = !q.reuse_density;
+    p.split_source = !metrics_fused_;
+    p.gradient = q.gradient;
+    p.potential = q.gradient && q.want_potential;
 
-    runDct(q.gradient, q.gradient && q.want_potential, !q.reuse_density, !metrics_fused_);
-    checkCuda(cudaStreamWaitEvent(stream_, join_, 0), "join");
-
-    ReduceArgs ra{};
+    ReduceArgs& ra = p.reduce_args;
     int s = 0;
     const auto add = [&](const double* partials, int rows, int stride, int column, bool is_max, int target) {
         ra.sources[s++] = ReduceSource{partials, rows, stride, column, is_max ? 1 : 0, target};
@@ -633,7 +639,7 @@ void Engine::launch(const EvalRequest& q) {
     expected_mask_ = 0;
     for (int k = 0; k < s; ++k) expected_mask_ |= 1U << ra.sources[k].target;
     if (gather) {
-        GatherArgs ga{};
+        GatherArgs& ga = p.gather_args;
         ga.particle_count = static_cast<int>(particle_count_);
         ga.movable_count = static_cast<int>(movable_count_);
         ga.positions = positions;
@@ -663,25 +669,104 @@ void Engine::launch(const EvalRequest& q) {
         ga.rudy_gradient = q.rudy ? rudy_pin_gradient_ : nullptr;
         ga.rudy_weight = q.rudy ? q.rudy_weight : 0.0;
         ga.partials = partials_g_;
-        beginKernel(kKindGather);
-        launchGather(ga, gather_blocks_, stream_);
-        endKernel();
+        p.gather = true;
+        p.gather_blocks = gather_blocks_;
         kernels += 1;
     }
-    beginKernel(kKindReduce);
-    launchReduce(ra, stream_);
-    endKernel();
-    kernels += 1;
-
-
-    d2h_bytes_ += static_cast<uint64_t>(s) * sizeof(double) + sizeof(int) + sizeof(unsigned long long);
+    kernels += 1;  // reduction
     if (q.rudy) kernels += q.gradient ? 7 : 4;
-    launches_ += kernels;
+    p.kernels = kernels;
+    d2h_bytes_ += static_cast<uint64_t>(s) * sizeof(double) + sizeof(int) + sizeof(unsigned long long);
     last_gradient_ = q.gradient;
     last_propose_ = q.mode == kPropose;
+    return p;
+}
+
+void Engine::run(const EvalPlan& p) {
+    if (p.fork_first) checkCuda(cudaEventRecord(fork_, stream_), "fork");
+    if (p.scatter) {
+        beginKernel(kKindScatter);
+        launchScatter(p.scatter_args, p.scatter_blocks, stream_);
+        endKernel();
+    }
+    if (!p.fork_first) checkCuda(cudaEventRecord(fork_, stream_), "fork");
+    checkCuda(cudaStreamWaitEvent(stream_wl_, fork_, 0), "fork");
+    beginKernel(kKindWirelength, stream_wl_);
+    launchWirelength(p.wirelength_args, p.wirelength_blocks, stream_wl_);
+    endKernel(stream_wl_);
+    if (p.rudy) {
+        beginKernel(kKindRudy, stream_wl_);
+        launchRudyDeposit(p.rudy_args, stream_wl_);
+        launchRudyPrefix(p.rudy_args, stream_wl_);
+        launchRudyMetrics(p.rudy_args, p.rudy_blocks, stream_wl_);
+        if (p.rudy_gradient) {
+            launchRudyTables(p.rudy_args, stream_wl_);
+            launchRudyGradient(p.rudy_args, stream_wl_);
+        }
+        endKernel(stream_wl_);
+    }
+    checkCuda(cudaEventRecord(join_, stream_wl_), "join");
+    if (p.metrics) {
+        beginKernel(kKindMetrics);
+        if (p.metrics_fused) {
+            launchMetricsSplit(p.metrics_args, stream_);
+        } else {
+            launchMetrics(p.metrics_args, p.metrics_blocks, stream_);
+        }
+        endKernel();
+    }
+    runDct(p.gradient, p.potential, p.forward, p.split_source);
+    checkCuda(cudaStreamWaitEvent(stream_, join_, 0), "join");
+    if (p.gather) {
+        beginKernel(kKindGather);
+        launchGather(p.gather_args, p.gather_blocks, stream_);
+        endKernel();
+    }
+    beginKernel(kKindReduce);
+    launchReduce(p.reduce_args, stream_);
+    endKernel();
+    launches_ += p.kernels;
+}
+
+void Engine::launch(const EvalRequest& q) {
+    EvalPlan p = plan(q);
+    if (batch_ != nullptr) {
+        require(!p.rudy && !p.potential && (p.metrics_fused || !p.metrics),
+                "A batched evaluation supports neither RUDY, the potential, nor grids wider than 2,048 bins.");
+        batched_plan_ = p;
+        has_pending_ = true;
+        return;
+    }
+    run(p);
+}
+
+const TcBatch* Engine::deviceBatches() {
+    if (device_batches_ == nullptr) {
+        device_batches_ = arena_.array<TcBatch>(4, "batched contraction descriptors");
+        const TcBatch host[4] = {tc_fwd1_, tc_fwd2_, tc_inv1_, tc_inv2_};
+        checkCuda(cudaMemcpyAsync(device_batches_, host, sizeof(host), cudaMemcpyHostToDevice, stream_),
+                  "Upload contraction descriptors");
+        checkCuda(cudaStreamSynchronize(stream_), "Upload contraction descriptors");  // `host` leaves scope
+    }
+    return device_batches_;
+}
+
+const TcBatch& Engine::contraction(int stage) const {
+    switch (stage) {
+        case 0: return tc_fwd1_;
+        case 1: return tc_fwd2_;
+        case 2: return tc_inv1_;
+        default: return tc_inv2_;
+    }
 }
 
 const EvalScalars& Engine::sync() {
+    if (has_pending_) {
+        // Batched: the evaluation runs in the batch's next round, which has completed
+        // on the device when this returns; the record below is then already complete.
+        has_pending_ = false;
+        batch_->evaluate(this, batched_plan_);
+    }
     // Poll the record until every scalar of this evaluation and the error flag carry
     // its sequence; now and then ask the stream for a fault, so an evaluation that
     // can no longer publish surfaces as an error instead of a hang.

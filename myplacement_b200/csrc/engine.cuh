@@ -83,6 +83,37 @@ struct EvalScalars {
     double v[kScalarCount];
 };
 
+// Everything one evaluation launches, with its arguments (Engine::plan).  A plain
+// engine launches it on its own streams (Engine::run); a Batch launches the plans
+// of many engines together, one batched launch per kernel family.
+struct EvalPlan {
+    bool scatter = false;
+    ScatterArgs scatter_args{};
+    int scatter_blocks = 0;
+    bool fork_first = false;  // the positions are given: the wirelength pass need not wait for the scatter
+    WirelengthArgs wirelength_args{};
+    int wirelength_blocks = 0;
+    bool rudy = false;
+    bool rudy_gradient = false;
+    RudyArgs rudy_args{};
+    int rudy_blocks = 0;
+    bool metrics = false;
+    bool metrics_fused = false;
+    MetricsArgs metrics_args{};
+    int metrics_blocks = 0;
+    bool forward = false;       // the two forward contractions (and the source split when not fused)
+    bool split_source = false;
+    bool gradient = false;      // the two inverse contraction launches
+    bool potential = false;
+    bool gather = false;
+    GatherArgs gather_args{};
+    int gather_blocks = 0;
+    ReduceArgs reduce_args{};
+    int kernels = 0;            // launches of the evaluation (the engine's launch count)
+};
+
+class Batch;
+
 // Kernel families timed by the engine's optional event profiler.
 enum KernelKind : int {
     kKindScatter = 0,
@@ -106,13 +137,27 @@ struct KernelStats {
 
 class Engine {
 public:
-    Engine(const Problem& problem, int device, uint64_t budget_bytes);
+    // With a batch, the engine runs on the batch's stream and its evaluations are
+    // launched together with the other engines of the batch (Batch).
+    Engine(const Problem& problem, int device, uint64_t budget_bytes, Batch* batch = nullptr);
     ~Engine();
     Engine(const Engine&) = delete;
     Engine& operator=(const Engine&) = delete;
 
     // Launches one evaluation on the engine stream; the scalars are valid after sync().
+    // In a batch the evaluation is handed to the batch at sync().
     void launch(const EvalRequest& request);
+    // The launches of one evaluation (the scalar record's sequence advances), and
+    // launching them on the engine's streams.
+    EvalPlan plan(const EvalRequest& request);
+    void run(const EvalPlan& plan);
+    // The engine's contraction batches (forward 1, forward 2, inverse 1, inverse 2)
+    // copied to device memory, for batched launches; uploaded on first use.
+    const TcBatch* deviceBatches();
+    [[nodiscard]] const TcBatch& contraction(int stage) const;
+    // Stops taking part in the batch's rounds (the placement has finished); a later
+    // evaluation still runs through the batch.
+    void leaveBatch();
     // Waits for the stream and returns the scalars of the last launched evaluation.
     const EvalScalars& sync();
     const EvalScalars& evaluate(const EvalRequest& request) {
@@ -206,6 +251,12 @@ private:
     void buildBasis();
 
     int device_ = 0;
+    Batch* batch_ = nullptr;
+    bool owns_stream_ = true;
+    bool attached_ = false;
+    bool has_pending_ = false;
+    EvalPlan batched_plan_{};
+    TcBatch* device_batches_ = nullptr;
     cudaStream_t stream_ = nullptr;
     cudaStream_t stream_wl_ = nullptr;  // the wirelength pass overlaps the density chain
     cudaEvent_t fork_ = nullptr;

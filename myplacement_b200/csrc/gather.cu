@@ -137,12 +137,10 @@ __device__ void reduceAllSources(const ReduceArgs& a) {
     finishReduce(a);
 }
 
-__global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
-    releaseNext();
-    waitForPrior();
+__device__ __forceinline__ void gatherBlock(const GatherArgs& a, int block, int grid) {
     double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     // Grid-stride over the particles (one resident wave), each thread in ascending order.
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.particle_count; i += gridDim.x * blockDim.x) {
+    for (int i = block * blockDim.x + threadIdx.x; i < a.particle_count; i += grid * blockDim.x) {
         double wx = 0.0, wy = 0.0, rx_rudy = 0.0, ry_rudy = 0.0;
         if (i < a.movable_count) {
             const int begin = a.particle_pin_start[i];
@@ -200,17 +198,29 @@ __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
     blockReduce<8>(v, is_max);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) a.partials[k * gridDim.x + blockIdx.x] = v[k];
+        for (int k = 0; k < 8; ++k) a.partials[k * grid + block] = v[k];
     }
+}
+
+__global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
+    releaseNext();
+    waitForPrior();
+    gatherBlock(a, static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x));
+}
+
+__global__ void __launch_bounds__(kThreads) gatherBatchKernel(const GatherArgs* args, const int* offsets, int count) {
+    releaseNext();
+    waitForPrior();
+    const int3 slot = batchSlot(offsets, count, static_cast<int>(blockIdx.x));
+    const GatherArgs a = args[slot.x];
+    gatherBlock(a, slot.y, slot.z);
 }
 
 // The scalar reduction as its own kernel: every partial of every source is
 // first staged in shared memory with all loads in flight together (eight per
 // thread at a time), then warp w sums sources w, w + 32, ... from shared memory,
 // lane l taking rows l, l + 32, ... in order and a fixed shuffle tree.
-__global__ void __launch_bounds__(kReduceThreads) reduceKernel(ReduceArgs a) {
-    releaseNext();
-    waitForPrior();
+__device__ __forceinline__ void reduceBlock(const ReduceArgs& a) {
     extern __shared__ double staged[];
     const int total = a.offsets[a.source_count];
     if (total > a.staged_capacity) {
@@ -268,6 +278,37 @@ __global__ void __launch_bounds__(kReduceThreads) reduceKernel(ReduceArgs a) {
     finishReduce(a);
 }
 
+__global__ void __launch_bounds__(kReduceThreads) reduceKernel(ReduceArgs a) {
+    releaseNext();
+    waitForPrior();
+    reduceBlock(a);
+}
+
+// One block per instance, each with the shared memory of the largest staging.
+__global__ void __launch_bounds__(kReduceThreads) reduceBatchKernel(const ReduceArgs* args) {
+    releaseNext();
+    waitForPrior();
+    reduceBlock(args[blockIdx.x]);
+}
+
+void configureReduce() {
+    constexpr int kMaxDevices = 64;
+    static std::once_flag once[kMaxDevices];
+    static cudaError_t attribute[kMaxDevices] = {};
+    int device = 0;
+    checkCuda(cudaGetDevice(&device), "Query the current device");
+    require(device >= 0 && device < kMaxDevices, "Device index out of range.");
+    std::call_once(once[device], [device] {
+        attribute[device] = cudaFuncSetAttribute(reduceKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 kReduceStaged * static_cast<int>(sizeof(double)));
+        if (attribute[device] == cudaSuccess) {
+            attribute[device] = cudaFuncSetAttribute(reduceBatchKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     kReduceStaged * static_cast<int>(sizeof(double)));
+        }
+    });
+    checkCuda(attribute[device], "Configure the scalar reduction");
+}
+
 }  // namespace
 
 int gatherBlocks(int particle_count) {
@@ -285,20 +326,24 @@ void launchGather(const GatherArgs& args, int blocks, cudaStream_t stream) {
 
 void launchReduce(const ReduceArgs& args, cudaStream_t stream) {
     if (args.source_count <= 0) return;
-    constexpr int kMaxDevices = 64;
-    static std::once_flag once[kMaxDevices];
-    static cudaError_t attribute[kMaxDevices] = {};
-    int device = 0;
-    checkCuda(cudaGetDevice(&device), "Query the current device");
-    require(device >= 0 && device < kMaxDevices, "Device index out of range.");
-    std::call_once(once[device], [device] {
-        attribute[device] = cudaFuncSetAttribute(reduceKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 kReduceStaged * static_cast<int>(sizeof(double)));
-    });
-    checkCuda(attribute[device], "Configure the scalar reduction");
+    configureReduce();
     const int total = args.offsets[args.source_count];
     const size_t smem = total <= args.staged_capacity ? static_cast<size_t>(total) * sizeof(double) : 0;
     launchChained("Launch the scalar reduction", reduceKernel, dim3(1), dim3(kReduceThreads), smem, stream, args);
+}
+
+void launchGatherBatch(const GatherArgs* args, const int* offsets, int count, int blocks, cudaStream_t stream) {
+    if (blocks <= 0 || count <= 0) return;
+    launchChained("Launch the batched field gather", gatherBatchKernel, dim3(blocks), dim3(kThreads), 0, stream, args,
+                  offsets, count);
+}
+
+void launchReduceBatch(const ReduceArgs* args, int count, int staged_doubles, cudaStream_t stream) {
+    if (count <= 0) return;
+    configureReduce();
+    const size_t smem = static_cast<size_t>(std::max(0, std::min(staged_doubles, kReduceStaged))) * sizeof(double);
+    launchChained("Launch the batched scalar reduction", reduceBatchKernel, dim3(count), dim3(kReduceThreads), smem,
+                  stream, args);
 }
 
 }  // namespace mpgp

@@ -61,6 +61,12 @@ struct WirelengthArgs {
     unsigned int* group_counters;
 };
 void launchWirelength(const WirelengthArgs& args, int blocks, cudaStream_t stream);
+// Batched launches (every family below has one): `count` instances' argument blocks
+// in device memory, instance k owning launch blocks [offsets[k], offsets[k + 1]) of
+// `blocks`; each block does exactly what block (b - offsets[k]) of the instance's own
+// launch of offsets[k + 1] - offsets[k] blocks does, so results are those of the plain launch.
+void launchWirelengthBatch(const WirelengthArgs* args, const int* offsets, int count, int blocks,
+                           cudaStream_t stream);
 
 // The allocation-free wirelength entry (mpgp_wirelength_noalloc): caller-owned
 // device arrays in, scratch in a fixed file-scope device array.
@@ -106,6 +112,7 @@ struct ScatterArgs {
     double* partials;           // per block: predicted, max displacement
 };
 void launchScatter(const ScatterArgs& args, int blocks, cudaStream_t stream);
+void launchScatterBatch(const ScatterArgs* args, const int* offsets, int count, int blocks, cudaStream_t stream);
 
 // ---- density metrics + DCT source --------------------------------------------------
 struct MetricsArgs {
@@ -134,6 +141,8 @@ void launchMetrics(const MetricsArgs& args, int blocks, cudaStream_t stream);
 constexpr int kMetricsSplitPerThread = 8;
 inline bool metricsSplitFits(int columns) { return columns > 0 && columns <= kMetricsSplitPerThread * 256; }
 void launchMetricsSplit(const MetricsArgs& args, cudaStream_t stream);
+void launchMetricsSplitBatch(const MetricsArgs* args, const int* offsets, int count, int blocks,
+                             cudaStream_t stream);
 
 // ---- RUDY routing-demand map (rudy.cu) -------------------------------------------------
 struct RudyArgs {
@@ -203,6 +212,8 @@ static_assert(kScalarCount < 32, "the expected-scalar mask is 32 bits wide");
 constexpr int kReduceThreads = 1024;
 constexpr int kReduceStaged = 24576;  // doubles staged in shared memory (192 KiB)
 void launchReduce(const ReduceArgs& args, cudaStream_t stream);
+// One block per instance; staged_doubles: the largest staging of the instances (shared memory).
+void launchReduceBatch(const ReduceArgs* args, int count, int staged_doubles, cudaStream_t stream);
 
 // ---- field gather + gradient combine (the fused update pass) ----------------------------
 struct GatherArgs {
@@ -233,6 +244,7 @@ struct GatherArgs {
     // (counted on reduce_counter, which is zero between launches).
 };
 void launchGather(const GatherArgs& args, int blocks, cudaStream_t stream);
+void launchGatherBatch(const GatherArgs* args, const int* offsets, int count, int blocks, cudaStream_t stream);
 // The gather's grid: one resident wave of blocks (grid-stride over the particles).
 int gatherBlocks(int particle_count);
 

@@ -7,6 +7,7 @@
 #include <chrono>
 #include <cstring>
 
+#include "batch.hpp"
 #include "common.cuh"
 #include "dct_tc.cuh"
 #include "session.hpp"
@@ -87,7 +88,7 @@ struct Server::Job {
     bool done = false;
 };
 
-Server::Server(int device, uint64_t memory_budget, int workers) : device_(device) {
+Server::Server(int device, uint64_t memory_budget, int workers, bool batched) : device_(device) {
     require(workers > 0 && workers <= 256, "A server needs between 1 and 256 workers.");
     int count = 0;
     const cudaError_t status = cudaGetDeviceCount(&count);
@@ -102,6 +103,8 @@ Server::Server(int device, uint64_t memory_budget, int workers) : device_(device
         memory_budget = static_cast<uint64_t>(static_cast<double>(free_bytes) * 0.9);
     }
     budget_ = memory_budget;
+    if (batched) batch_ = std::make_unique<Batch>(device);
+    stats_.batched = batched ? 1 : 0;
     stats_.workers = workers;
     stats_.memory_budget = budget_;
     started_ = nowSeconds();
@@ -116,6 +119,7 @@ Server::~Server() {
     }
     ready_.notify_all();
     for (std::thread& t : workers_) t.join();
+    batch_.reset();
 }
 
 int64_t Server::submit(const mpgp_design& d, const mpgp_options& o) {
@@ -209,7 +213,7 @@ void Server::work() {
         uint64_t reserved_bytes = 0;
         try {
             checkCuda(cudaSetDevice(device_), "Select CUDA device");
-            Session session(job->design, job->options);
+            Session session(job->design, job->options, batch_.get());
             reserved_bytes = session.engine() != nullptr ? session.engine()->reservedBytes() : 0;
             int completed = 0;
             while (!session.step(64, &completed)) {
@@ -287,6 +291,13 @@ mpgp_server_stats Server::stats() const {
     std::lock_guard<std::mutex> lock(mutex_);
     mpgp_server_stats s = stats_;
     s.seconds = nowSeconds() - started_;
+    if (batch_) {
+        const BatchStats b = batch_->stats();
+        s.batch_rounds = b.rounds;
+        s.batch_evaluations = b.evaluations;
+        s.batch_launches = b.launches;
+        s.batch_peak_round = b.peak_round;
+    }
     return s;
 }
 

@@ -5,12 +5,16 @@
 // from running many placements at the same time.  The Server keeps a FIFO of
 // submitted jobs (each a full adaptive global placement, as mpgp_global_place)
 // and a pool of worker threads; each worker runs one job at a time as a
-// device-resident Session on its own CUDA streams, so the jobs' kernels overlap
-// on the device.  A job is admitted when its estimated device footprint fits in
-// what the memory budget has left (continuous batching: a job that arrives
-// while others run starts as soon as a worker and the memory are free).  A
-// job's result does not depend on what else runs: every session owns its
-// buffers and its reductions run in a fixed order.
+// device-resident Session.  In the batched mode (the default) the running jobs'
+// evaluations are gathered into shared rounds (Batch): one launch per kernel
+// family carries the iteration of every running job.  Otherwise each session
+// launches on its own streams and the jobs' kernels merely overlap.  A job is
+// admitted when its estimated device footprint fits in what the memory budget
+// has left (continuous batching: a job that arrives while others run joins the
+// rounds as soon as a worker and the memory are free).  A job's result does not
+// depend on what else runs: every session owns its buffers, every block of a
+// batched launch does what the same block of the job's own launch does, and the
+// reductions run in a fixed order.
 #pragma once
 
 #include <condition_variable>
@@ -27,12 +31,16 @@
 
 namespace mpgp {
 
+class Batch;
+
 // Upper bound of the device bytes a Session for this design reserves.
 uint64_t estimateSessionBytes(const mpgp_design& design, const mpgp_options& options);
 
 class Server {
 public:
-    Server(int device, uint64_t memory_budget, int workers);
+    // batched: the running jobs' evaluations share batched launches (Batch);
+    // otherwise each job launches its own kernels on its own streams.
+    Server(int device, uint64_t memory_budget, int workers, bool batched = true);
     ~Server();
     Server(const Server&) = delete;
     Server& operator=(const Server&) = delete;
@@ -54,6 +62,7 @@ private:
 
     int device_;
     uint64_t budget_;
+    std::unique_ptr<Batch> batch_;
     mutable std::mutex mutex_;
     std::condition_variable ready_;  // queue or admission changed
     std::condition_variable done_;   // a job finished

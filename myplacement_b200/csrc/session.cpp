@@ -93,7 +93,7 @@ mpgp_history_row makeHistoryRow(int iteration, const ObjectiveMetrics& m, double
 
 }  // namespace
 
-Session::Session(const mpgp_design& design, const mpgp_options& options) : options_(options) {
+Session::Session(const mpgp_design& design, const mpgp_options& options, Batch* batch) : options_(options) {
     started_ = std::chrono::steady_clock::now();
     validateDesign(design);
     {
@@ -122,7 +122,8 @@ Session::Session(const mpgp_design& design, const mpgp_options& options) : optio
     }
     require(options_.cuda_device >= 0 && options_.cuda_device < device_count,
             "Requested CUDA device does not exist on this host.");
-    engine_ = std::make_unique<Engine>(problem, options_.cuda_device, options_.maximum_cuda_memory_bytes);
+    engine_ = std::make_unique<Engine>(problem, options_.cuda_device, options_.maximum_cuda_memory_bytes,
+                                       rudy_requested_ ? nullptr : batch);
     if (rudy_requested_) engine_->enableRudy(options_);
     result_.cuda_device_used = options_.cuda_device;
 
@@ -646,6 +647,7 @@ void Session::finish(double* module_x, double* module_y, mpgp_result* result, mp
             }
         }
         result_.cuda_reserved_memory_bytes = engine_->reservedBytes();
+        engine_->leaveBatch();
     }
     result_.elapsed_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - started_).count();
     result_.history_count = static_cast<int32_t>(history_.size());

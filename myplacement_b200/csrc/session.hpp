@@ -51,7 +51,9 @@ struct CheckpointState {
 
 class Session {
 public:
-    Session(const mpgp_design& design, const mpgp_options& options);
+    // With a batch, the session's evaluations run in the batch's shared rounds
+    // (a routability run, which the batched launches do not cover, runs on its own).
+    Session(const mpgp_design& design, const mpgp_options& options, Batch* batch = nullptr);
     // Runs up to `iterations` controller iterations; returns true once the run is done.
     bool step(int iterations, int* completed);
     void finish(double* module_x, double* module_y, mpgp_result* result, mpgp_history_row* history, int capacity);

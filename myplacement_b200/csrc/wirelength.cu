@@ -259,10 +259,10 @@ __device__ void netWarps(const WirelengthArgs& a, int first, int count, double& 
     }
 }
 
-__global__ void __launch_bounds__(kThreads) wirelengthKernel(WirelengthArgs a) {
-    releaseNext();
-    waitForPrior();
-    const int4 work = a.block_work[blockIdx.x];
+// One block of the pass: `block` of `grid` blocks (the launch's, or its instance's in
+// a batched launch).
+__device__ __forceinline__ void wirelengthBlock(const WirelengthArgs& a, int block, int grid) {
+    const int4 work = a.block_work[block];
     double values[2] = {0.0, 0.0};
     switch (work.x) {
         case 1: netPairs(a, work.y, work.z, values[0], values[1]); break;
@@ -275,10 +275,26 @@ __global__ void __launch_bounds__(kThreads) wirelengthKernel(WirelengthArgs a) {
     const bool is_max[2] = {false, false};
     blockReduce<2>(values, is_max);
     if (threadIdx.x == 0) {
-        a.partials[blockIdx.x] = values[0];
-        a.partials[gridDim.x + blockIdx.x] = values[1];
+        a.partials[block] = values[0];
+        a.partials[grid + block] = values[1];
     }
-    reduceGroups<2>(a.partials, a.group_partials, a.group_counters, is_max);
+    reduceGroups<2>(a.partials, a.group_partials, a.group_counters, is_max, static_cast<unsigned>(block),
+                    static_cast<unsigned>(grid));
+}
+
+__global__ void __launch_bounds__(kThreads) wirelengthKernel(WirelengthArgs a) {
+    releaseNext();
+    waitForPrior();
+    wirelengthBlock(a, static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x));
+}
+
+__global__ void __launch_bounds__(kThreads) wirelengthBatchKernel(const WirelengthArgs* args, const int* offsets,
+                                                                  int count) {
+    releaseNext();
+    waitForPrior();
+    const int3 slot = batchSlot(offsets, count, static_cast<int>(blockIdx.x));
+    const WirelengthArgs a = args[slot.x];  // a private copy: stores through its pointers cannot alias it
+    wirelengthBlock(a, slot.y, slot.z);
 }
 
 }  // namespace
@@ -286,6 +302,13 @@ __global__ void __launch_bounds__(kThreads) wirelengthKernel(WirelengthArgs a) {
 void launchWirelength(const WirelengthArgs& args, int blocks, cudaStream_t stream) {
     if (blocks <= 0) return;
     launchChained("Launch the wirelength pass", wirelengthKernel, dim3(blocks), dim3(kThreads), 0, stream, args);
+}
+
+void launchWirelengthBatch(const WirelengthArgs* args, const int* offsets, int count, int blocks,
+                           cudaStream_t stream) {
+    if (blocks <= 0 || count <= 0) return;
+    launchChained("Launch the batched wirelength pass", wirelengthBatchKernel, dim3(blocks), dim3(kThreads), 0,
+                  stream, args, offsets, count);
 }
 
 // ---- allocation-free variant --------------------------------------------------------

@@ -371,13 +371,16 @@ class PlacementServer:
     Each job is a full adaptive global placement (GlobalPlacer.run).  `workers`
     host threads each drive one device-resident session; a job starts when a
     worker is free and its estimated footprint fits in `memory_budget` (bytes;
-    0 = 90 % of the device's free memory).  Results do not depend on the mix.
+    0 = 90 % of the device's free memory).  With `batched` the running jobs'
+    evaluations share batched launches (one per kernel family and round);
+    otherwise every job launches its own kernels.  Results do not depend on the
+    mix or the mode.
     """
 
-    def __init__(self, device: int = 0, memory_budget: int = 0, workers: int = 8):
+    def __init__(self, device: int = 0, memory_budget: int = 0, workers: int = 8, batched: bool = True):
         self.lib = load_library()
         self.handle = C.c_void_p()
-        check(self.lib.mpgp_server_create(device, memory_budget, workers, C.byref(self.handle)))
+        check(self.lib.mpgp_server_create_mode(device, memory_budget, workers, int(batched), C.byref(self.handle)))
         self._modules: dict[int, int] = {}
         self._capacity: dict[int, int] = {}
 
@@ -428,8 +431,9 @@ class PlacementServer:
 
 
 def batch_place(designs: list[Design], options: list[_abi.Options], device: int = 0, workers: int = 16,
-                memory_budget: int = 0) -> tuple[list[PlacementResult], list[dict], dict]:
-    """The batched form (mpgp_batch_place): every design placed, many at once; (results, job stats, server stats)."""
+                memory_budget: int = 0, batched: bool = True) -> tuple[list[PlacementResult], list[dict], dict]:
+    """The batched form (mpgp_batch_place): every design placed, many at once (with `batched`, in shared
+    batched launches); (results, job stats, server stats)."""
     lib = load_library()
     count = len(designs)
     structs = (_abi.Design * count)(*[d.as_c() for d in designs])
@@ -441,7 +445,7 @@ def batch_place(designs: list[Design], options: list[_abi.Options], device: int 
     results = (_abi.Result * count)()
     job_stats = (_abi.JobStats * count)()
     server_stats = _abi.ServerStats()
-    check(lib.mpgp_batch_place(count, structs, opts, device, workers, memory_budget, px, py, results, job_stats,
-                               C.byref(server_stats)))
+    check(lib.mpgp_batch_place(count, structs, opts, device, workers, int(batched), memory_budget, px, py, results,
+                               job_stats, C.byref(server_stats)))
     placed = [PlacementResult(xs[i], ys[i], results[i].as_dict()) for i in range(count)]
     return placed, [job_stats[i].as_dict() for i in range(count)], server_stats.as_dict()

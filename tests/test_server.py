@@ -1,8 +1,11 @@
 """The batched and served forms: many placements at once on one GPU.
 
 A job is exactly one GlobalPlacer.run; running it in a mix with others must not
-change its result (every session owns its buffers and reduces in a fixed
-order), and admission must respect the memory budget.
+change its result, in either server mode: batched (the running jobs'
+evaluations share one launch per kernel family and round, and every block of a
+batched launch does what the same block of the job's own launch does) or
+concurrent (every job launches its own kernels).  Admission must respect the
+memory budget.
 """
 from __future__ import annotations
 
@@ -31,13 +34,14 @@ def test_footprint_estimate_grows_with_the_design():
 
 
 @pytest.mark.gpu
-def test_served_results_equal_alone(gpu):
+@pytest.mark.parametrize("batched", [True, False])
+def test_served_results_equal_alone(gpu, batched):
     """Three jobs give bit-identical placements alone and inside a mix of eight."""
     probes = [_job(2000, 11), _job(3500, 12), _job(1200, 13)]
     alone = [mp.GlobalPlacer().run(d, o) for d, o in probes]
     fillers = [_job(cells, 20 + k) for k, cells in enumerate((3000, 1500, 2500, 4000, 1800))]
     order = [fillers[0], probes[0], fillers[1], fillers[2], probes[1], fillers[3], probes[2], fillers[4]]
-    with mp.PlacementServer(device=0, workers=4) as server:
+    with mp.PlacementServer(device=0, workers=4, batched=batched) as server:
         ids = [server.submit(d, o) for d, o in order]
         results = []
         for job in ids:
@@ -46,6 +50,10 @@ def test_served_results_equal_alone(gpu):
         stats = server.stats()
     assert stats["completed"] == 8 and stats["failed"] == 0
     assert stats["peak_running"] >= 2  # the jobs did overlap on the device
+    assert stats["batched"] == int(batched)
+    if batched:  # iterations of several jobs went into shared launches
+        assert stats["batch_rounds"] > 0 and stats["batch_peak_round"] >= 2
+        assert stats["batch_evaluations"] > stats["batch_rounds"]
     mixed = [results[1], results[4], results[6]]
     for (placed, job_stats), reference in zip(mixed, alone):
         np.testing.assert_array_equal(placed.module_x, reference.module_x)
@@ -58,9 +66,13 @@ def test_served_results_equal_alone(gpu):
 
 
 @pytest.mark.gpu
-def test_batch_place_matches_global_place(gpu):
-    jobs = [_job(cells, 40 + k, iterations=40) for k, cells in enumerate((1000, 2600, 1700, 3100, 1300, 2200))]
-    placed, job_stats, server_stats = mp.batch_place([d for d, _ in jobs], [o for _, o in jobs], workers=3)
+@pytest.mark.parametrize("batched", [True, False])
+def test_batch_place_matches_global_place(gpu, batched):
+    """Instances of uneven sizes and bin grids (32 x 32 to 128 x 128 bins: contractions of
+    one and of two K splits in one round) match their plain runs bit for bit."""
+    jobs = [_job(cells, 40 + k, iterations=40) for k, cells in enumerate((1000, 2600, 1700, 3100, 1300, 2200, 9000))]
+    placed, job_stats, server_stats = mp.batch_place([d for d, _ in jobs], [o for _, o in jobs], workers=4,
+                                                     batched=batched)
     assert server_stats["completed"] == len(jobs)
     for (design, options), result in zip(jobs, placed):
         reference = mp.GlobalPlacer().run(design, options)
