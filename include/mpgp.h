@@ -584,6 +584,18 @@ int mpgp_server_stats_get(const mpgp_server* server, mpgp_server_stats* stats);
 /* Finishes the running jobs, abandons the queued ones, joins the workers. */
 void mpgp_server_destroy(mpgp_server* server);
 
+/* ---- autotuning --------------------------------------------------------------
+ *
+ * No counterpart in the reference.  The K split of the tcgen05 field
+ * contractions (how many CTAs of a cluster share one output tile's sum) per
+ * contracted length (bins along the summed axis).  The library starts with the
+ * table that myplacement_b200/tune.py measured on a B200 (tuned_splits.inc);
+ * set replaces it for engines created afterwards (splits 1 or 2; a split whose
+ * clusters do not all fit on the GPU at once is not used).  get copies up to
+ * `capacity` entries and returns the table's size in *count. */
+int mpgp_tuning_set_splits(const int32_t* sizes, const int32_t* splits, int32_t count);
+int mpgp_tuning_get_splits(int32_t* sizes, int32_t* splits, int32_t capacity, int32_t* count);
+
 /* The batched form: `count` placements through a server (submit all, take all),
  * in the server's batched mode when batched != 0.  module_x[i] / module_y[i]
  * receive design i's positions; history is not kept. */

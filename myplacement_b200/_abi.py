@@ -370,6 +370,8 @@ def _declare(lib: C.CDLL) -> C.CDLL:
         "mpgp_session_stream": (vp, [vp]),
         "mpgp_session_destroy": (None, [vp]),
         "mpgp_estimate_bytes": (C.c_int, [C.POINTER(Design), C.POINTER(Options), C.POINTER(C.c_uint64)]),
+        "mpgp_tuning_set_splits": (C.c_int, [_i32, _i32, C.c_int32]),
+        "mpgp_tuning_get_splits": (C.c_int, [_i32, _i32, C.c_int32, _i32]),
         "mpgp_server_create": (C.c_int, [C.c_int, C.c_uint64, C.c_int32, C.POINTER(vp)]),
         "mpgp_server_create_mode": (C.c_int, [C.c_int, C.c_uint64, C.c_int32, C.c_int32, C.POINTER(vp)]),
         "mpgp_server_submit": (C.c_int, [vp, C.POINTER(Design), C.POINTER(Options), C.POINTER(C.c_int64)]),

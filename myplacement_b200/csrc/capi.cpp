@@ -13,6 +13,7 @@
 
 #include "bookshelf.hpp"
 #include "common.cuh"
+#include "dct_tc.cuh"
 #include "detailed.hpp"
 #include "engine.cuh"
 #include "mpgp.h"
@@ -161,6 +162,7 @@ int mpgp_backend_evaluate(mpgp_backend* b, const double* positions, double smoot
         if (b->particles > 0) {
             mpgp::checkCuda(cudaMemcpyAsync(e.scratchPositions(), positions, bytes, cudaMemcpyHostToDevice, e.stream()),
                       "Upload CUDA particle positions");
+            e.rebucket(e.scratchPositions());  // the scatter's particle order for these positions
         }
         mpgp::EvalRequest q;
         q.mode = mpgp::kGiven;
@@ -589,6 +591,22 @@ int mpgp_server_stats_get(const mpgp_server* s, mpgp_server_stats* stats) {
 }
 
 void mpgp_server_destroy(mpgp_server* s) { delete s; }
+
+int mpgp_tuning_set_splits(const int32_t* sizes, const int32_t* splits, int32_t count) {
+    return guarded([&] {
+        mpgp::require(count >= 0 && (count == 0 || (sizes != nullptr && splits != nullptr)),
+                      "Sizes and splits are required.");
+        mpgp::setTunedSplits(sizes, splits, count);
+    });
+}
+
+int mpgp_tuning_get_splits(int32_t* sizes, int32_t* splits, int32_t capacity, int32_t* count) {
+    return guarded([&] {
+        mpgp::require(count != nullptr && capacity >= 0 && (capacity == 0 || (sizes != nullptr && splits != nullptr)),
+                      "Output arrays are required.");
+        *count = mpgp::tunedSplits(sizes, splits, capacity);
+    });
+}
 
 int mpgp_batch_place(int32_t count, const mpgp_design* designs, const mpgp_options* options, int device,
                      int32_t workers, int32_t batched, uint64_t memory_budget_bytes, double* const* module_x,

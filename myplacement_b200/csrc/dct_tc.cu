@@ -772,15 +772,58 @@ void makeOperandMap(CUtensorMap* map, const SplitMatrix& m, int box_rows) {
     }
 }
 
-void tcPlan(TcBatch& batch, int task_count) {
-    configureKernel();
-    const int tiles = batchTiles(batch, task_count) * task_count;
-    int k_blocks = 0;
-    for (int i = 0; i < task_count; ++i) {
-        const int kb = (batch.task[i].k + kBlockK - 1) / kBlockK;
-        k_blocks = i == 0 ? kb : std::min(k_blocks, kb);
+namespace {
+
+// The autotuned K splits (tuned_splits.inc), replaceable at run time (mpgp_tuning_set_splits).
+std::mutex g_split_mutex;
+std::vector<std::pair<int, int>>& splitTable() {
+    static std::vector<std::pair<int, int>> table = {
+        std::pair<int, int>{0, 0},  // (no tuned size is 0; keeps the initialiser list non-empty)
+#include "tuned_splits.inc"
+    };
+    return table;
+}
+
+// The tuned split for a contraction over k, or 0 when k is not in the table.
+int tunedSplit(int k) {
+    std::lock_guard<std::mutex> lock(g_split_mutex);
+    for (const auto& entry : splitTable()) {
+        if (entry.first == k && entry.first > 0) return entry.second;
     }
-    batch.ksplit = 1;
+    return 0;
+}
+
+}  // namespace
+
+void setTunedSplits(const int* sizes, const int* splits, int count) {
+    for (int i = 0; i < count; ++i) {
+        require(sizes[i] > 0 && (splits[i] == 1 || splits[i] == 2), "A tuned split is 1 or 2 for a positive size.");
+    }
+    std::lock_guard<std::mutex> lock(g_split_mutex);
+    auto& table = splitTable();
+    table.assign(1, std::pair<int, int>{0, 0});
+    for (int i = 0; i < count; ++i) table.emplace_back(sizes[i], splits[i]);
+}
+
+int tunedSplits(int* sizes, int* splits, int capacity) {
+    std::lock_guard<std::mutex> lock(g_split_mutex);
+    int count = 0;
+    for (const auto& entry : splitTable()) {
+        if (entry.first <= 0) continue;
+        if (count < capacity) {
+            sizes[count] = entry.first;
+            splits[count] = entry.second;
+        }
+        ++count;
+    }
+    return count;
+}
+
+namespace {
+
+// The largest split whose clusters of a batch of `tiles` tiles still fit on the GPU at once.
+int fittingSplit(int tiles, int k_blocks) {
+    int best = 1;
     for (int ksplit = 2; ksplit <= kMaxSplit && ksplit <= k_blocks; ksplit *= 2) {
         cudaLaunchAttribute attribute[2] = {};
         cudaLaunchConfig_t config =
@@ -791,8 +834,28 @@ void tcPlan(TcBatch& batch, int task_count) {
             break;
         }
         if (tiles > clusters) break;  // the split would no longer run in one wave
-        batch.ksplit = ksplit;
+        best = ksplit;
     }
+    return best;
+}
+
+}  // namespace
+
+void tcPlan(TcBatch& batch, int task_count) {
+    configureKernel();
+    const int tiles = batchTiles(batch, task_count) * task_count;
+    int k_blocks = 0;
+    int k = 0;
+    for (int i = 0; i < task_count; ++i) {
+        const int kb = (batch.task[i].k + kBlockK - 1) / kBlockK;
+        k_blocks = i == 0 ? kb : std::min(k_blocks, kb);
+        k = std::max(k, batch.task[i].k);
+    }
+    const int fitting = fittingSplit(tiles, k_blocks);
+    const int tuned = tunedSplit(k);
+    // The tuned split where it is allowed (it divides the K blocks among at most as
+    // many CTAs as fit in one wave), else the largest split that fits.
+    batch.ksplit = tuned > 0 && tuned <= fitting ? tuned : fitting;
 }
 
 int tcBlocks(const TcBatch& batch, int task_count) {

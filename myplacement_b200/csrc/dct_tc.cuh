@@ -112,9 +112,15 @@ int taskTiles(const TcBatch& batch, int task);
 void launchTcGemmBatch(const TcItem* items, int count, int ksplit, cudaStream_t stream);
 
 void makeOperandMap(CUtensorMap* map, const SplitMatrix& m, int box_rows);
-// Chooses the K split of a batch: the largest cluster size whose clusters all fit
-// on the GPU at once.  Call after the tasks are filled in.
+// Chooses the K split of a batch: the tuned split of its contracted length when
+// one is set and its clusters all fit on the GPU at once, else the largest cluster
+// size whose clusters all fit.  Call after the tasks are filled in.
 void tcPlan(TcBatch& batch, int task_count);
+// The tuned splits (contracted length -> split), compiled in from tuned_splits.inc;
+// set replaces the whole table (engines planned afterwards use it).
+void setTunedSplits(const int* sizes, const int* splits, int count);
+// Copies up to `capacity` entries out; returns the table's size.
+int tunedSplits(int* sizes, int* splits, int capacity);
 // CTAs of one task row of the launch (the count of energy partials a spectral task writes).
 int tcBlocks(const TcBatch& batch, int task_count);
 void launchTcGemm(const TcBatch& batch, int task_count, cudaStream_t stream);

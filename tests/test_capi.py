@@ -65,3 +65,19 @@ def test_no_cpu_fallback_without_gpu(golden_dir):
                              np.zeros(64), np.zeros(64))
     backend, reason = mp.try_create_backend(layout, 0)
     assert backend is None and reason
+
+
+def test_tuning_table_round_trip():
+    """The autotuned contraction splits can be read, replaced and restored; bad splits are refused."""
+    from myplacement_b200 import tune
+
+    original = tune.get_splits()
+    try:
+        tune.set_splits({256: 2, 512: 1, 1024: 2})
+        assert tune.get_splits() == {256: 2, 512: 1, 1024: 2}
+        with pytest.raises(mp.EngineError) as error:
+            tune.set_splits({512: 3})
+        assert error.value.status == mp._abi.MPGP_ERR_INVALID_ARGUMENT
+    finally:
+        tune.set_splits(original)
+    assert tune.get_splits() == original
