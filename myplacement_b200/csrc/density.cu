@@ -197,6 +197,10 @@ __device__ __forceinline__ void scatterBlock(const ScatterArgs& a, int block, in
             a.partials[grid + block] = values[1];
         }
     }
+    if (a.partials != nullptr && a.group_counters != nullptr) {
+        reduceGroups<2>(a.partials, a.group_partials, a.group_counters, is_max, static_cast<unsigned>(block),
+                        static_cast<unsigned>(grid));
+    }
 }
 
 // Bucket key of a particle: the 8 x 8-bin tile of its centre (clamped to the core),
@@ -307,6 +311,9 @@ __global__ void __launch_bounds__(kThreads) metricsKernel(MetricsArgs a) {
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) a.partials[k * gridDim.x + blockIdx.x] = v[k];
+    }
+    if (a.group_counters != nullptr) {
+        reduceGroups<9>(a.partials, a.group_partials, a.group_counters, is_max, blockIdx.x, gridDim.x);
     }
 }
 
@@ -419,6 +426,10 @@ __device__ __forceinline__ void metricsSplitBlock(const MetricsArgs& a, int bloc
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) a.partials[k * grid + block] = v[k];
+    }
+    if (a.group_counters != nullptr) {
+        reduceGroups<9>(a.partials, a.group_partials, a.group_counters, is_max, static_cast<unsigned>(block),
+                        static_cast<unsigned>(grid));
     }
 }
 

@@ -494,7 +494,20 @@ void Engine::collectTimings() {
 //   X = S * Cx^T, rho_hat = Cy * X, phi_hat = rho_hat .* scale (+ Parseval energy)
 //   gradient: T = Dy * phi_hat, U = phi_hat * Dx^T, Ex = T * (Sx diag(kx))^T, Ey = (Sy diag(ky)) * U
 //   potential (parity hook only): phi = T * Dx^T.
+Engine::Groups Engine::newGroups(int blocks, int values, const char* what) {
+    Groups g;
+    g.count = std::max(1, ceilDiv(std::max(1, blocks), 32));
+    g.partials = arena_.array<double>(static_cast<std::size_t>(values) * g.count, what);
+    const std::size_t counters = static_cast<std::size_t>(g.count) + 1;
+    g.counters = arena_.array<unsigned int>(counters, what);
+    checkCuda(cudaMemsetAsync(g.counters, 0, counters * sizeof(unsigned int), stream_), what);
+    return g;
+}
+
 void Engine::allocateGroups() {
+    sc_groups_ = newGroups(scatter_blocks_, 2, "scatter group partials");
+    m_groups_ = newGroups(metrics_blocks_, 9, "metric group partials");
+    g_groups_ = newGroups(gather_blocks_, 8, "gather group partials");
     wl_groups_ = std::max(1, ceilDiv(std::max(1, wl_blocks_), 32));
     wl_group_ = arena_.array<double>(2 * static_cast<std::size_t>(wl_groups_), "wirelength group partials");
     const std::size_t counters = static_cast<std::size_t>(wl_groups_) + 1;
@@ -566,6 +579,8 @@ EvalPlan Engine::plan(const EvalRequest& q) {
     sa.totals = totals_;
     sa.partials = partials_sc_;
     sa.order = bucketed_ ? bucket_order_ : nullptr;
+    sa.group_partials = sc_groups_.partials;
+    sa.group_counters = sc_groups_.counters;
     p.scatter = !q.reuse_density && particle_count_ > 0;
     p.scatter_blocks = scatter_blocks_;
     // The wirelength pass needs the positions only: it runs beside the density
@@ -609,6 +624,8 @@ EvalPlan Engine::plan(const EvalRequest& q) {
     ma.bin_count = bin_count_;
     ma.source = source_;
     ma.partials = partials_m_;
+    ma.group_partials = m_groups_.partials;
+    ma.group_counters = m_groups_.counters;
     int kernels = 1;  // wirelength
     if (!q.reuse_density) {
         p.metrics = true;
@@ -637,12 +654,13 @@ EvalPlan Engine::plan(const EvalRequest& q) {
     };
     add(wl_group_, wl_blocks_ > 0 ? wl_groups_ : 0, 1, 0, false, kSmooth);
     add(wl_group_, wl_blocks_ > 0 ? wl_groups_ : 0, 1, wl_groups_, false, kHpwl);
-    const int scatter_rows = particle_count_ > 0 && q.mode == kPropose ? scatter_blocks_ : 0;
+    // The scatter, metrics and gather partials, folded per 32 blocks by the producers.
+    const int scatter_rows = particle_count_ > 0 && q.mode == kPropose ? sc_groups_.count : 0;
     if (!q.reuse_density) {  // otherwise the density scalars of the previous evaluation stand
-        add(partials_sc_, scatter_rows, 1, 0, false, kPredicted);
-        add(partials_sc_, scatter_rows, 1, scatter_rows, true, kMaxDisplacement);
+        add(sc_groups_.partials, scatter_rows, 1, 0, false, kPredicted);
+        add(sc_groups_.partials, scatter_rows, 1, sc_groups_.count, true, kMaxDisplacement);
         for (int k = 0; k < 9; ++k) {
-            add(partials_m_, metrics_blocks_, 1, k * metrics_blocks_, k >= 7, kOverflowWith + k);
+            add(m_groups_.partials, m_groups_.count, 1, k * m_groups_.count, k >= 7, kOverflowWith + k);
         }
         add(partials_e_, energy_blocks_, 1, 0, false, kEnergy);
     }
@@ -651,7 +669,9 @@ EvalPlan Engine::plan(const EvalRequest& q) {
     }
     const bool gather = q.gradient && particle_count_ > 0;
     if (q.gradient) {
-        for (int k = 0; k < 8; ++k) add(partials_g_, gather ? gather_blocks_ : 0, 1, k * gather_blocks_, false, kWireL1 + k);
+        for (int k = 0; k < 8; ++k) {
+            add(g_groups_.partials, gather ? g_groups_.count : 0, 1, k * g_groups_.count, false, kWireL1 + k);
+        }
     }
     ra.source_count = s;
     ra.offsets[0] = 0;
@@ -696,6 +716,8 @@ EvalPlan Engine::plan(const EvalRequest& q) {
         ga.rudy_gradient = q.rudy ? rudy_pin_gradient_ : nullptr;
         ga.rudy_weight = q.rudy ? q.rudy_weight : 0.0;
         ga.partials = partials_g_;
+        ga.group_partials = g_groups_.partials;
+        ga.group_counters = g_groups_.counters;
         p.gather = true;
         p.gather_blocks = gather_blocks_;
         kernels += 1;
@@ -1040,6 +1062,8 @@ void Engine::depositLayers(const double2* positions, int64_t* movable, int64_t* 
     sa.layers = layers_;
     sa.totals = totals_;
     sa.partials = partials_sc_;
+    sa.group_partials = sc_groups_.partials;
+    sa.group_counters = sc_groups_.counters;
     beginKernel(kKindScatter);
     launchScatter(sa, particle_count_ > 0 ? scatter_blocks_ : 0, stream_);
     endKernel();

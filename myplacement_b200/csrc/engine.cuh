@@ -338,6 +338,14 @@ private:
     // Second-level (per 32 blocks) wirelength partials and their counters (reduceGroups).
     double* wl_group_ = nullptr;
     unsigned int* wl_counters_ = nullptr;
+    // The same second level for the scatter, metrics and gather partials.
+    struct Groups {
+        int count = 0;
+        double* partials = nullptr;
+        unsigned int* counters = nullptr;
+    };
+    Groups sc_groups_, m_groups_, g_groups_;
+    Groups newGroups(int blocks, int values, const char* what);
     int wl_groups_ = 0;
     void allocateGroups();
     double* partials_wl_ = nullptr;

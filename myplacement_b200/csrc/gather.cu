@@ -200,6 +200,10 @@ __device__ __forceinline__ void gatherBlock(const GatherArgs& a, int block, int 
 #pragma unroll
         for (int k = 0; k < 8; ++k) a.partials[k * grid + block] = v[k];
     }
+    if (a.group_counters != nullptr) {
+        reduceGroups<8>(a.partials, a.group_partials, a.group_counters, is_max, static_cast<unsigned>(block),
+                        static_cast<unsigned>(grid));
+    }
 }
 
 __global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {

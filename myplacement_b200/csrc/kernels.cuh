@@ -111,6 +111,8 @@ struct ScatterArgs {
     unsigned long long* totals; // 3 exact layer totals
     double* partials;           // per block: predicted, max displacement
     const int* order;           // P: the particles in bucket order (block b takes slots b * 256 ..), or null
+    double* group_partials;     // per 32 blocks (reduceGroups), when group_counters is set
+    unsigned int* group_counters;
 };
 void launchScatter(const ScatterArgs& args, int blocks, cudaStream_t stream);
 // The scatter's shared-memory window (bins of the three layers a block accumulates
@@ -142,6 +144,8 @@ struct MetricsArgs {
     size_t split_plane;
     int* row_exp;
     TcScales* scales;
+    double* group_partials;            // per 32 blocks (reduceGroups), when group_counters is set
+    unsigned int* group_counters;
 };
 void launchMetrics(const MetricsArgs& args, int blocks, cudaStream_t stream);
 // The fused metrics-and-split pass takes one block per bin row and keeps a
@@ -248,8 +252,8 @@ struct GatherArgs {
     const double2* rudy_gradient;   // optional: RUDY pin slots (particle order), added with rudy_weight
     double rudy_weight;
     double* partials;               // per block: 8 partials (kWireL1 .. kRudyL1)
-    // Optional fused reduction: the last block to finish reduces `reduce`
-    // (counted on reduce_counter, which is zero between launches).
+    double* group_partials;         // per 32 blocks (reduceGroups), when group_counters is set
+    unsigned int* group_counters;
 };
 void launchGather(const GatherArgs& args, int blocks, cudaStream_t stream);
 void launchGatherBatch(const GatherArgs* args, const int* offsets, int count, int blocks, cudaStream_t stream);
