@@ -227,6 +227,9 @@ void Engine::buildNetLayout(const Problem& p) {
     rudy_net_weight_ = layout.net_weight64;
     particle_pin_start_ = layout.particle_pin_start;
     pin_slot_ = layout.pin_slot;
+    slot_particle_ = layout.slot_particle;
+    slot_pin_ = layout.slot_pin;
+    slot_offset_ = layout.slot_offset;
     wl_net_count_ = layout.kept_nets;
     wl_pin_count_ = layout.kept_pins;
     // Degree buckets: one thread per two-pin net, G lanes per net for degree <= G,
@@ -247,6 +250,13 @@ void Engine::buildNetLayout(const Problem& p) {
     const std::size_t pins = std::max<std::size_t>(1, static_cast<std::size_t>(layout.kept_pins));
     block_work_ = arena_.array<int4>(std::max<std::size_t>(1, work.size()), "wirelength work");
     pin_gradient_ = arena_.array<float2>(pins, "pin gradients");
+    pin_position_ = arena_.array<double2>(pins, "pin positions");
+    // The movable pins' slots: the last entry of the particle pin offsets.
+    if (movable_count_ > 0) {
+        checkCuda(cudaMemcpyAsync(&movable_slots_, particle_pin_start_ + movable_count_, sizeof(int),
+                                  cudaMemcpyDeviceToHost, stream_),
+                  "Count the movable pins");
+    }
     partials_wl_ = arena_.array<double>(2 * std::max<std::size_t>(1, work.size()), "wirelength partials");
     upload(block_work_, work, stream_);
     checkCuda(cudaMemsetAsync(pin_gradient_, 0, pins * sizeof(float2), stream_), "clear pin gradients");
@@ -587,8 +597,15 @@ EvalPlan Engine::plan(const EvalRequest& q) {
     // chain on its own stream (after the scatter when the scatter forms them).
     p.fork_first = q.mode == kGiven;
 
+    // The movable pins' positions, in the wirelength pass's pin order: unless nothing
+    // moved since the last evaluation, whose pin positions are then still in place.
+    p.pin_positions = !q.reuse_density && movable_slots_ > 0;
+    p.pin_args = PinPositionArgs{positions, slot_particle_, slot_pin_, slot_offset_, movable_slots_, pin_position_};
+    p.pin_blocks = pinPositionBlocks(movable_slots_);
+
     WirelengthArgs& wa = p.wirelength_args;
     wa.positions = positions;
+    wa.pin_position = pin_position_;
     wa.pin_particle = pin_particle_;
     wa.pin_offset = pin_offset_;
     wa.static_pins = static_pins_;
@@ -626,7 +643,7 @@ EvalPlan Engine::plan(const EvalRequest& q) {
     ma.partials = partials_m_;
     ma.group_partials = m_groups_.partials;
     ma.group_counters = m_groups_.counters;
-    int kernels = 1;  // wirelength
+    int kernels = p.pin_positions ? 2 : 1;  // pin positions, wirelength
     if (!q.reuse_density) {
         p.metrics = true;
         p.metrics_fused = metrics_fused_;
@@ -741,6 +758,7 @@ void Engine::run(const EvalPlan& p) {
     if (!p.fork_first) checkCuda(cudaEventRecord(fork_, stream_), "fork");
     checkCuda(cudaStreamWaitEvent(stream_wl_, fork_, 0), "fork");
     beginKernel(kKindWirelength, stream_wl_);
+    if (p.pin_positions) launchPinPositions(p.pin_args, stream_wl_);
     launchWirelength(p.wirelength_args, p.wirelength_blocks, stream_wl_);
     endKernel(stream_wl_);
     if (p.rudy) {

@@ -91,6 +91,9 @@ struct EvalPlan {
     ScatterArgs scatter_args{};
     int scatter_blocks = 0;
     bool fork_first = false;  // the positions are given: the wirelength pass need not wait for the scatter
+    bool pin_positions = false;  // the pin position pass runs first on the wirelength stream
+    PinPositionArgs pin_args{};
+    int pin_blocks = 0;
     WirelengthArgs wirelength_args{};
     int wirelength_blocks = 0;
     bool rudy = false;
@@ -301,6 +304,11 @@ private:
     float2* pin_gradient_ = nullptr;
     int* particle_pin_start_ = nullptr;
     int* pin_slot_ = nullptr;
+    int* slot_particle_ = nullptr;
+    int* slot_pin_ = nullptr;
+    float2* slot_offset_ = nullptr;
+    int movable_slots_ = 0;
+    double2* pin_position_ = nullptr;  // movable pins' absolute positions (pin order)
 
     // density
     unsigned long long* layers_ = nullptr;
