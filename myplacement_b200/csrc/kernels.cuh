@@ -139,7 +139,7 @@ struct ScatterArgs {
 void launchScatter(const ScatterArgs& args, int blocks, cudaStream_t stream);
 // The scatter's shared-memory window (bins of the three layers a block accumulates
 // before flushing) and the bucket tile (bins per side) its particle order sorts by.
-constexpr int kScatterWindow = 1536;
+constexpr int kScatterWindow = 1024;
 constexpr int kScatterTile = 8;
 // Bucket keys (tile of the centre, row-major) and the identity index of `count` particles.
 void launchBucketKeys(const double2* positions, int count, double llx, double lly, double bin_w, double bin_h,
