@@ -186,7 +186,15 @@ void Batch::execute(const std::vector<Request*>& round) {
     const std::size_t at_metrics_offsets = layout.add<int>(metrics.size() + 1);
     const std::size_t at_gather = layout.add<GatherArgs>(gather.size());
     const std::size_t at_gather_offsets = layout.add<int>(gather.size() + 1);
-    const std::size_t at_reduce = layout.add<ReduceArgs>(static_cast<std::size_t>(n));
+    // Reductions: the instances with a gather reduce in its last block (their arguments
+    // and pointers to them), the others in the reduction launch.
+    std::vector<int> rest;
+    for (int i = 0; i < n; ++i) {
+        if (!round[i]->plan->gather) rest.push_back(i);
+    }
+    const std::size_t at_reduce_gather = layout.add<ReduceArgs>(gather.size());
+    const std::size_t at_reduce_pointers = layout.add<const ReduceArgs*>(gather.size());
+    const std::size_t at_reduce = layout.add<ReduceArgs>(rest.size());
     std::size_t at_items[kContractionStages][kMaxSplit];
     for (int stage = 0; stage < kContractionStages; ++stage) {
         for (int k = 0; k < kMaxSplit; ++k) at_items[stage][k] = layout.add<TcItem>(items[stage][k].size());
@@ -227,7 +235,13 @@ void Batch::execute(const std::vector<Request*>& round) {
         at_gather, gather, [](const EvalPlan& p) { return p.gather_args; },
         [](const EvalPlan& p) { return p.gather_blocks; }, at_gather_offsets);
     ReduceArgs* reduce = reinterpret_cast<ReduceArgs*>(host + at_reduce);
-    for (int i = 0; i < n; ++i) reduce[i] = round[i]->plan->reduce_args;
+    for (std::size_t j = 0; j < rest.size(); ++j) reduce[j] = round[rest[j]]->plan->reduce_args;
+    ReduceArgs* reduce_gather = reinterpret_cast<ReduceArgs*>(host + at_reduce_gather);
+    const ReduceArgs** reduce_pointers = reinterpret_cast<const ReduceArgs**>(host + at_reduce_pointers);
+    for (std::size_t j = 0; j < gather.size(); ++j) {
+        reduce_gather[j] = round[gather[j]]->plan->reduce_args;
+        reduce_pointers[j] = reinterpret_cast<const ReduceArgs*>(device_args_ + at_reduce_gather) + j;
+    }
     for (int stage = 0; stage < kContractionStages; ++stage) {
         for (int k = 0; k < kMaxSplit; ++k) {
             if (!items[stage][k].empty()) {
@@ -281,12 +295,16 @@ void Batch::execute(const std::vector<Request*>& round) {
     checkCuda(cudaStreamWaitEvent(stream_, join_, 0), "Batch join");
     if (!gather.empty()) {
         launchGatherBatch(reinterpret_cast<const GatherArgs*>(on_device(at_gather)),
+                          reinterpret_cast<const ReduceArgs* const*>(on_device(at_reduce_pointers)),
                           reinterpret_cast<const int*>(on_device(at_gather_offsets)), static_cast<int>(gather.size()),
                           gather_blocks, stream_);
         ++launches;
     }
-    launchReduceBatch(reinterpret_cast<const ReduceArgs*>(on_device(at_reduce)), n, staged, stream_);
-    ++launches;
+    if (!rest.empty()) {
+        launchReduceBatch(reinterpret_cast<const ReduceArgs*>(on_device(at_reduce)), static_cast<int>(rest.size()),
+                          staged, stream_);
+        ++launches;
+    }
     checkCuda(cudaEventRecord(done_, stream_), "Batch done");
     checkCuda(cudaEventSynchronize(done_), "Batched evaluation on the device");
     std::lock_guard<std::mutex> lock(mutex_);

@@ -739,7 +739,7 @@ EvalPlan Engine::plan(const EvalRequest& q) {
         p.gather_blocks = gather_blocks_;
         kernels += 1;
     }
-    kernels += 1;  // reduction
+    if (!gather) kernels += 1;  // the reduction (a gather reduces in its last block)
     if (q.rudy) kernels += q.gradient ? 7 : 4;
     p.kernels = kernels;
     d2h_bytes_ += static_cast<uint64_t>(s) * sizeof(double) + sizeof(int) + sizeof(unsigned long long);
@@ -785,13 +785,15 @@ void Engine::run(const EvalPlan& p) {
     runDct(p.gradient, p.potential, p.forward, p.split_source);
     checkCuda(cudaStreamWaitEvent(stream_, join_, 0), "join");
     if (p.gather) {
+        // The gather's last block also reduces and publishes the evaluation.
         beginKernel(kKindGather);
-        launchGather(p.gather_args, p.gather_blocks, stream_);
+        launchGather(p.gather_args, &p.reduce_args, p.gather_blocks, stream_);
+        endKernel();
+    } else {
+        beginKernel(kKindReduce);
+        launchReduce(p.reduce_args, stream_);
         endKernel();
     }
-    beginKernel(kKindReduce);
-    launchReduce(p.reduce_args, stream_);
-    endKernel();
     launches_ += p.kernels;
 }
 

@@ -137,7 +137,7 @@ __device__ void reduceAllSources(const ReduceArgs& a) {
     finishReduce(a);
 }
 
-__device__ __forceinline__ void gatherBlock(const GatherArgs& a, int block, int grid) {
+__device__ __forceinline__ void gatherBlock(const GatherArgs& a, const ReduceArgs* reduce, int block, int grid) {
     double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     // Grid-stride over the particles (one resident wave), each thread in ascending order.
     for (int i = block * blockDim.x + threadIdx.x; i < a.particle_count; i += grid * blockDim.x) {
@@ -201,23 +201,27 @@ __device__ __forceinline__ void gatherBlock(const GatherArgs& a, int block, int 
         for (int k = 0; k < 8; ++k) a.partials[k * grid + block] = v[k];
     }
     if (a.group_counters != nullptr) {
-        reduceGroups<8>(a.partials, a.group_partials, a.group_counters, is_max, static_cast<unsigned>(block),
-                        static_cast<unsigned>(grid));
+        const int state = reduceGroups<8>(a.partials, a.group_partials, a.group_counters, is_max,
+                                          static_cast<unsigned>(block), static_cast<unsigned>(grid));
+        // The block that folded the last group: every partial of the evaluation is in
+        // place (the gather runs last), so it reduces and publishes them itself.
+        if (state == 2 && reduce != nullptr) reduceAllSources(*reduce);
     }
 }
 
-__global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a) {
+__global__ void __launch_bounds__(kThreads) gatherKernel(GatherArgs a, ReduceArgs reduce, int with_reduce) {
     releaseNext();
     waitForPrior();
-    gatherBlock(a, static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x));
+    gatherBlock(a, with_reduce ? &reduce : nullptr, static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x));
 }
 
-__global__ void __launch_bounds__(kThreads) gatherBatchKernel(const GatherArgs* args, const int* offsets, int count) {
+__global__ void __launch_bounds__(kThreads) gatherBatchKernel(const GatherArgs* args, const ReduceArgs* const* reduces,
+                                                              const int* offsets, int count) {
     releaseNext();
     waitForPrior();
     const int3 slot = batchSlot(offsets, count, static_cast<int>(blockIdx.x));
     const GatherArgs a = args[slot.x];
-    gatherBlock(a, slot.y, slot.z);
+    gatherBlock(a, reduces != nullptr ? reduces[slot.x] : nullptr, slot.y, slot.z);
 }
 
 // The scalar reduction as its own kernel: every partial of every source is
@@ -323,9 +327,12 @@ int gatherBlocks(int particle_count) {
     return std::max(1, std::min(ceilDiv(std::max(1, particle_count), kThreads), std::max(1, per_sm) * sms));
 }
 
-void launchGather(const GatherArgs& args, int blocks, cudaStream_t stream) {
+void launchGather(const GatherArgs& args, const ReduceArgs* reduce, int blocks, cudaStream_t stream) {
     if (blocks <= 0) return;
-    launchChained("Launch the field gather", gatherKernel, dim3(blocks), dim3(kThreads), 0, stream, args);
+    require(reduce == nullptr || args.group_counters != nullptr, "A gather that reduces needs its group counters.");
+    const ReduceArgs empty{};
+    launchChained("Launch the field gather", gatherKernel, dim3(blocks), dim3(kThreads), 0, stream, args,
+                  reduce != nullptr ? *reduce : empty, reduce != nullptr ? 1 : 0);
 }
 
 void launchReduce(const ReduceArgs& args, cudaStream_t stream) {
@@ -336,10 +343,11 @@ void launchReduce(const ReduceArgs& args, cudaStream_t stream) {
     launchChained("Launch the scalar reduction", reduceKernel, dim3(1), dim3(kReduceThreads), smem, stream, args);
 }
 
-void launchGatherBatch(const GatherArgs* args, const int* offsets, int count, int blocks, cudaStream_t stream) {
+void launchGatherBatch(const GatherArgs* args, const ReduceArgs* const* reduces, const int* offsets, int count,
+                       int blocks, cudaStream_t stream) {
     if (blocks <= 0 || count <= 0) return;
     launchChained("Launch the batched field gather", gatherBatchKernel, dim3(blocks), dim3(kThreads), 0, stream, args,
-                  offsets, count);
+                  reduces, offsets, count);
 }
 
 void launchReduceBatch(const ReduceArgs* args, int count, int staged_doubles, cudaStream_t stream) {

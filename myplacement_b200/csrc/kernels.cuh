@@ -277,8 +277,13 @@ struct GatherArgs {
     double* group_partials;         // per 32 blocks (reduceGroups), when group_counters is set
     unsigned int* group_counters;
 };
-void launchGather(const GatherArgs& args, int blocks, cudaStream_t stream);
-void launchGatherBatch(const GatherArgs* args, const int* offsets, int count, int blocks, cudaStream_t stream);
+// With `reduce`, the block that completes the last group fold also reduces the
+// evaluation's partials (every source of `reduce`) and publishes them: the gather is
+// the evaluation's last kernel, and no reduction launch follows it.
+void launchGather(const GatherArgs& args, const ReduceArgs* reduce, int blocks, cudaStream_t stream);
+// reduces[k]: instance k's reduction (device memory), or null (a null array: none reduce).
+void launchGatherBatch(const GatherArgs* args, const ReduceArgs* const* reduces, const int* offsets, int count,
+                       int blocks, cudaStream_t stream);
 // The gather's grid: one resident wave of blocks (grid-stride over the particles).
 int gatherBlocks(int particle_count);
 
