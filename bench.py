@@ -110,6 +110,21 @@ class ClockSampler:
                 self.proc.kill()
             self.out.close()
 
+    def samples(self) -> int:
+        try:
+            return sum(1 for line in self.path.read_text().splitlines() if line.count(",") >= 8)
+        except OSError:
+            return 0
+
+    def hold(self, load, minimum: int = 3, limit_s: float = 3.0) -> None:
+        """Keeps the GPU busy with `load` until `minimum` samples exist (the timed steps are far
+        shorter than nvidia-smi's sampling interval), at most `limit_s` seconds."""
+        if self.proc is None:
+            return
+        deadline = time.perf_counter() + limit_s
+        while self.samples() < minimum and time.perf_counter() < deadline:
+            load()
+
     def summary(self) -> dict:
         if self.proc is None or not self.path.exists():
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -129,7 +144,9 @@ class ClockSampler:
                     reasons.add(name)
         self.path.unlink(missing_ok=True)
         return {"sm_mhz": statistics.median(clocks) if clocks else None, "sm_max_mhz": max_clock,
-                "reasons": sorted(reasons), "samples": len(clocks)}
+                "reasons": sorted(reasons), "samples": len(clocks),
+                "sampled": "nvidia-smi every 200 ms from the first timed step until a few samples exist "
+                           "(the steps, then the 256 MiB flush write as load)"}
 
 
 def algorithmic_units(design, particles: int, bins_x: int, bins_y: int) -> dict:
@@ -293,9 +310,18 @@ def run_mine(args) -> None:
             end.record(ext)
             end.synchronize()
             step_ms.append(start.elapsed_time(end))
+        wall_timed = time.perf_counter() - wall0
+
+        def load():
+            flush_l2(flush, stream_ptr)
+            torch.cuda.synchronize()
+
+        # The clocks right after the timed steps, under the flush write's load, until
+        # nvidia-smi has a few samples.
+        clocks.hold(load)
     torch.cuda.synchronize()
     replicas.barrier()
-    wall = time.perf_counter() - wall0
+    wall = wall_timed
     launches = session.kernel_launches - launches_before
     stats = session.kernel_stats()
     session.set_profiling(False)
@@ -537,6 +563,9 @@ def run_batched(args) -> None:
         "hpwl_total": sum(r.hpwl_after for r in placed), "hpwl_total_plain": sum(r.hpwl_after for r in plain),
         "peak_running": server_stats["peak_running"], "batch_rounds": server_stats["batch_rounds"],
         "evaluations_per_round": server_stats["batch_evaluations"] / max(1, server_stats["batch_rounds"]),
+        "round_busy_us": 1e6 * server_stats["batch_busy_seconds"] / max(1, server_stats["batch_rounds"]),
+        "round_us": 1e6 * batched_seconds / max(1, server_stats["batch_rounds"]),
+        "host_cpus": os.cpu_count(),
         "gpu_launches": server_stats["batch_launches"],
         "data": "synthetic: cells log-normal median 4k in 1k-20k, small-design net law, bins 32^2-256^2, "
                 "early stop on (280-iteration budget)",

@@ -318,6 +318,7 @@ class ServerStats(C.Structure):
         ("batch_rounds", C.c_int64),
         ("batch_evaluations", C.c_int64),
         ("batch_launches", C.c_int64),
+        ("batch_busy_seconds", C.c_double),
     ]
 
     def as_dict(self) -> dict:

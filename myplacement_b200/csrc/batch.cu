@@ -1,8 +1,13 @@
 // Batched rounds of many engines' evaluations (batch.hpp).
 #include "batch.hpp"
 
+#include <linux/futex.h>
+#include <sys/syscall.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cstring>
 
 #include "common.cuh"
@@ -26,6 +31,15 @@ struct RoundLayout {
 };
 
 constexpr int kContractionStages = 4;  // forward 1, forward 2, inverse 1, inverse 2
+
+// Sleeps while *word still holds `seen` (Linux futex; spurious returns are fine).
+void futexWait(std::atomic<uint32_t>* word, uint32_t seen) {
+    syscall(SYS_futex, reinterpret_cast<uint32_t*>(word), FUTEX_WAIT_PRIVATE, seen, nullptr, nullptr, 0);
+}
+
+void futexWakeAll(std::atomic<uint32_t>* word) {
+    syscall(SYS_futex, reinterpret_cast<uint32_t*>(word), FUTEX_WAKE_PRIVATE, INT_MAX, nullptr, nullptr, 0);
+}
 
 }  // namespace
 
@@ -90,13 +104,20 @@ void Batch::detach(Engine* /*engine*/) {
 }
 
 void Batch::evaluate(Engine* engine, const EvalPlan& plan) {
-    Request request{engine, &plan, false, std::string(), MPGP_OK};
+    Request request;
+    request.engine = engine;
+    request.plan = &plan;
     {
-        std::unique_lock<std::mutex> lock(mutex_);
+        std::lock_guard<std::mutex> lock(mutex_);
         require(!stopping_, "The batch is shutting down.");
         pending_.push_back(&request);
-        submitted_.notify_all();
-        finished_.wait(lock, [&] { return request.done; });
+    }
+    submitted_.notify_all();
+    // Sleep on the round counter until this request's round has completed.
+    for (;;) {
+        const uint32_t seen = completed_rounds_.load(std::memory_order_acquire);
+        if (request.done.load(std::memory_order_acquire) != 0) break;
+        futexWait(&completed_rounds_, seen);
     }
     if (request.status != MPGP_OK) fail(request.status, request.error);
 }
@@ -123,6 +144,7 @@ void Batch::loop() {
         }
         int status = MPGP_OK;
         std::string error;
+        const auto started = std::chrono::steady_clock::now();
         try {
             execute(round);
         } catch (const Error& e) {
@@ -132,18 +154,21 @@ void Batch::loop() {
             status = MPGP_ERR_RUNTIME;
             error = e.what();
         }
+        const double busy = std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count();
         {
             std::lock_guard<std::mutex> lock(mutex_);
-            for (Request* r : round) {
-                r->status = status;
-                r->error = error;
-                r->done = true;
-            }
             stats_.rounds += 1;
             stats_.evaluations += static_cast<int64_t>(round.size());
             stats_.peak_round = std::max(stats_.peak_round, static_cast<int>(round.size()));
+            stats_.busy_seconds += busy;
         }
-        finished_.notify_all();
+        for (Request* r : round) {
+            r->status = status;
+            r->error = error;
+            r->done.store(1, std::memory_order_release);  // the request may be gone after this
+        }
+        completed_rounds_.fetch_add(1, std::memory_order_acq_rel);
+        futexWakeAll(&completed_rounds_);
     }
 }
 

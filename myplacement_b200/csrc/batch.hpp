@@ -16,6 +16,7 @@
 // its plain run, whatever else is in the batch.
 #pragma once
 
+#include <atomic>
 #include <condition_variable>
 #include <cstdint>
 #include <mutex>
@@ -28,10 +29,11 @@
 namespace mpgp {
 
 struct BatchStats {
-    int64_t rounds = 0;       // batched rounds launched
-    int64_t evaluations = 0;  // evaluations they carried
-    int64_t launches = 0;     // kernel launches of all rounds
-    int peak_round = 0;       // most evaluations in one round
+    int64_t rounds = 0;        // batched rounds launched
+    int64_t evaluations = 0;   // evaluations they carried
+    int64_t launches = 0;      // kernel launches of all rounds
+    int peak_round = 0;        // most evaluations in one round
+    double busy_seconds = 0.0; // time from each round's first launch to its completion, summed
 };
 
 class Batch {
@@ -54,11 +56,11 @@ public:
 
 private:
     struct Request {
-        Engine* engine;
-        const EvalPlan* plan;
-        bool done;
+        Engine* engine = nullptr;
+        const EvalPlan* plan = nullptr;
+        std::atomic<int> done{0};  // set (release) after status and error
         std::string error;
-        int status;
+        int status = MPGP_OK;
     };
     void loop();
     void execute(const std::vector<Request*>& round);
@@ -75,7 +77,9 @@ private:
 
     mutable std::mutex mutex_;
     std::condition_variable submitted_;
-    std::condition_variable finished_;
+    // Completed rounds, also the futex word the waiting engines sleep on: one wake
+    // releases them all at once, and each checks its own request without a lock.
+    std::atomic<uint32_t> completed_rounds_{0};
     std::vector<Request*> pending_;
     int attached_ = 0;
     bool stopping_ = false;

@@ -300,6 +300,7 @@ mpgp_server_stats Server::stats() const {
         s.batch_evaluations = b.evaluations;
         s.batch_launches = b.launches;
         s.batch_peak_round = b.peak_round;
+        s.batch_busy_seconds = b.busy_seconds;
     }
     return s;
 }

@@ -124,8 +124,12 @@ def test_noalloc_matches_the_reference_session_on_many_nets(gpu, ref):
     smoothing = 0.75 * max(design.core[2] - design.core[0], design.core[3] - design.core[1]) / bins
     call = NoAlloc(torch, layout, design.net_pin_start, design.net_weight, session.positions.shape[0])
     rng = np.random.default_rng(5)
+    half = np.stack([session.width, session.height], 1) * 0.5
+    low, high = np.array(design.core[:2]) + half, np.array(design.core[2:]) - half
     for trial in range(2):
-        positions = session.positions + (rng.normal(0.0, 3.0, session.positions.shape) if trial else 0.0)
+        # Moved cells stay inside the core: the reference clamps centres to it first.
+        positions = np.clip(session.positions + (rng.normal(0.0, 3.0, session.positions.shape) if trial else 0.0),
+                            low, high)
         comp = session.components(positions, smoothing)
         _check(call(positions, smoothing), comp["wire_gradient"], comp["smooth_wirelength"], comp["hpwl"])
 
