@@ -564,6 +564,7 @@ def run_batched(args) -> None:
         "peak_running": server_stats["peak_running"], "batch_rounds": server_stats["batch_rounds"],
         "evaluations_per_round": server_stats["batch_evaluations"] / max(1, server_stats["batch_rounds"]),
         "round_busy_us": 1e6 * server_stats["batch_busy_seconds"] / max(1, server_stats["batch_rounds"]),
+        "round_device_us": 1e6 * server_stats["batch_device_seconds"] / max(1, server_stats["batch_rounds"]),
         "round_us": 1e6 * batched_seconds / max(1, server_stats["batch_rounds"]),
         "host_cpus": os.cpu_count(),
         "gpu_launches": server_stats["batch_launches"],

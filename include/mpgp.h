@@ -559,7 +559,8 @@ typedef struct mpgp_server_stats {
     int64_t batch_rounds;           /* batched rounds launched */
     int64_t batch_evaluations;      /* evaluations those rounds carried */
     int64_t batch_launches;         /* kernel launches of those rounds */
-    double batch_busy_seconds;      /* from each round's upload to its completion on the device, summed */
+    double batch_busy_seconds;      /* host time from each round's upload to its completion, summed */
+    double batch_device_seconds;    /* device time of the rounds (CUDA events around each), summed */
 } mpgp_server_stats;
 
 /* Upper bound of the device bytes one placement of `design` reserves. */

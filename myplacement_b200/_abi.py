@@ -319,6 +319,7 @@ class ServerStats(C.Structure):
         ("batch_evaluations", C.c_int64),
         ("batch_launches", C.c_int64),
         ("batch_busy_seconds", C.c_double),
+        ("batch_device_seconds", C.c_double),
     ]
 
     def as_dict(self) -> dict:

@@ -50,7 +50,8 @@ Batch::Batch(int device, double window_seconds) : device_(device), window_(windo
     checkCuda(cudaStreamCreateWithFlags(&wirelength_, cudaStreamNonBlocking), "Create batch wirelength stream");
     checkCuda(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "Create batch event");
     checkCuda(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "Create batch event");
-    checkCuda(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "Create batch event");
+    checkCuda(cudaEventCreate(&start_), "Create batch event");
+    checkCuda(cudaEventCreate(&done_), "Create batch event");
     reserve(std::size_t{1} << 20);
     thread_ = std::thread([this] { loop(); });
 }
@@ -68,6 +69,7 @@ Batch::~Batch() {
     if (fork_ != nullptr) cudaEventDestroy(fork_);
     if (join_ != nullptr) cudaEventDestroy(join_);
     if (done_ != nullptr) cudaEventDestroy(done_);
+    if (start_ != nullptr) cudaEventDestroy(start_);
     if (host_args_ != nullptr) cudaFreeHost(host_args_);
     if (device_args_ != nullptr) cudaFree(device_args_);
     if (wirelength_ != nullptr) cudaStreamDestroy(wirelength_);
@@ -277,6 +279,7 @@ void Batch::execute(const std::vector<Request*>& round) {
 
     unsigned char* dev = device_args_;
     const auto on_device = [&](std::size_t at) { return dev + at; };
+    checkCuda(cudaEventRecord(start_, stream_), "Batch start");
     checkCuda(cudaMemcpyAsync(dev, host, layout.bytes, cudaMemcpyHostToDevice, stream_), "Upload batch arguments");
     int64_t launches = 0;
     // The same order as one engine's evaluation (Engine::run): scatter (which forms
@@ -332,8 +335,11 @@ void Batch::execute(const std::vector<Request*>& round) {
     }
     checkCuda(cudaEventRecord(done_, stream_), "Batch done");
     checkCuda(cudaEventSynchronize(done_), "Batched evaluation on the device");
+    float milliseconds = 0.0f;
+    checkCuda(cudaEventElapsedTime(&milliseconds, start_, done_), "Batch device time");
     std::lock_guard<std::mutex> lock(mutex_);
     stats_.launches += launches;
+    stats_.device_seconds += 1e-3 * static_cast<double>(milliseconds);
 }
 
 }  // namespace mpgp

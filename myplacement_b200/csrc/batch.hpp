@@ -33,7 +33,8 @@ struct BatchStats {
     int64_t evaluations = 0;   // evaluations they carried
     int64_t launches = 0;      // kernel launches of all rounds
     int peak_round = 0;        // most evaluations in one round
-    double busy_seconds = 0.0; // time from each round's first launch to its completion, summed
+    double busy_seconds = 0.0;    // host time from each round's upload to its completion, summed
+    double device_seconds = 0.0;  // device time of the rounds (CUDA events around each round), summed
 };
 
 class Batch {
@@ -70,7 +71,8 @@ private:
     double window_;
     cudaStream_t stream_ = nullptr;       // the engines' stream: the density chain and the contractions
     cudaStream_t wirelength_ = nullptr;   // the wirelength pass beside it
-    cudaEvent_t fork_ = nullptr, join_ = nullptr, done_ = nullptr;
+    cudaEvent_t fork_ = nullptr, join_ = nullptr;
+    cudaEvent_t start_ = nullptr, done_ = nullptr;  // timed: the round's device time
     unsigned char* host_args_ = nullptr;  // pinned staging of a round's argument blocks
     unsigned char* device_args_ = nullptr;
     std::size_t capacity_ = 0;

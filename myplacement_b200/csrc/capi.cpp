@@ -162,7 +162,6 @@ int mpgp_backend_evaluate(mpgp_backend* b, const double* positions, double smoot
         if (b->particles > 0) {
             mpgp::checkCuda(cudaMemcpyAsync(e.scratchPositions(), positions, bytes, cudaMemcpyHostToDevice, e.stream()),
                       "Upload CUDA particle positions");
-            e.rebucket(e.scratchPositions());  // the scatter's particle order for these positions
         }
         mpgp::EvalRequest q;
         q.mode = mpgp::kGiven;

@@ -18,8 +18,6 @@
 // (Metrics.cpp:101-119), reads-and-clears the fixed-point layers and writes the
 // mean-free FP32 source of the Poisson solve (ElectrostaticField.cpp:119-133);
 // the mean comes from the exact integer layer totals of the scatter.
-#include <climits>
-
 #include "common.cuh"
 #include "dct_tc.cuh"
 #include "kernels.cuh"
@@ -38,25 +36,15 @@ __device__ __forceinline__ double clampCenter(double value, double size, double 
     return lo <= hi ? fmax(lo, fmin(value, hi)) : __dmul_rn(__dadd_rn(low, high), 0.5);
 }
 
-// One block of the scatter.  With a bucket order (particles sorted by the 8 x 8-bin
-// tile of their centre, Engine::rebucket) a block's particles lie close together:
-// the block accumulates their fixed-point overlaps in a shared-memory window over
-// the bins they cover and flushes each non-zero window entry with one integer
-// atomic.  A block whose bins do not fit the window (or an unsorted block) adds
-// straight to the map.  Integer addition is exact and associative, so the map is
-// the same bit for bit either way.
+// One block of the scatter: particles block * 256 .. of the launch (or of its
+// instance in a batched launch), each adding its fixed-point overlaps to the map
+// with integer atomics (the map is L2-resident, so the atomics stay in L2).
 __device__ __forceinline__ void scatterBlock(const ScatterArgs& a, int block, int grid) {
-    __shared__ unsigned long long window_sum[3 * kScatterWindow];
-    __shared__ int window[4];  // first row, first column, last row, last column of the block's bins
-    const int slot = block * static_cast<int>(blockDim.x) + static_cast<int>(threadIdx.x);
-    const int i = slot < a.particle_count ? (a.order != nullptr ? a.order[slot] : slot) : -1;
+    const int i = block * static_cast<int>(blockDim.x) + static_cast<int>(threadIdx.x);
     double predicted = 0.0;
     double displacement = 0.0;
     long long totals[3] = {0, 0, 0};
-    bool deposit = false;
-    int c0 = 0, c1 = -1, r0 = 0, r1 = -1, code = 0;
-    float fl = 0.0f, fr = 0.0f, fb = 0.0f, ft = 0.0f;
-    if (i >= 0) {
+    if (i < a.particle_count) {
         double2 c;
         const double2 size = a.size[i];
         if (a.mode == kGiven) {
@@ -101,76 +89,32 @@ __device__ __forceinline__ void scatterBlock(const ScatterArgs& a, int block, in
             const double gr = __ddiv_rn(__dsub_rn(r, a.llx), a.bin_w);
             const double gb = __ddiv_rn(__dsub_rn(b, a.lly), a.bin_h);
             const double gt = __ddiv_rn(__dsub_rn(t, a.lly), a.bin_h);
-            c0 = static_cast<int>(clampIndex(floor(gl), a.bins_x - 1));
-            c1 = static_cast<int>(clampIndex(__dsub_rn(ceil(gr), 1.0), a.bins_x - 1));
-            r0 = static_cast<int>(clampIndex(floor(gb), a.bins_y - 1));
-            r1 = static_cast<int>(clampIndex(__dsub_rn(ceil(gt), 1.0), a.bins_y - 1));
-            fl = __double2float_rn(__dsub_rn(gl, static_cast<double>(c0)));
-            fr = __double2float_rn(__dsub_rn(gr, static_cast<double>(c0)));
-            fb = __double2float_rn(__dsub_rn(gb, static_cast<double>(r0)));
-            ft = __double2float_rn(__dsub_rn(gt, static_cast<double>(r0)));
-            code = a.layer[i];
-            deposit = true;
-        }
-    }
-    // The block's window: the bounding box of the bins its particles cover.
-    if (threadIdx.x == 0) {
-        window[0] = INT_MAX;
-        window[1] = INT_MAX;
-        window[2] = -1;
-        window[3] = -1;
-    }
-    __syncthreads();
-    if (deposit && a.order != nullptr) {
-        atomicMin(&window[0], r0);
-        atomicMin(&window[1], c0);
-        atomicMax(&window[2], r1);
-        atomicMax(&window[3], c1);
-    }
-    __syncthreads();
-    const int wr0 = window[0], wc0 = window[1];
-    const int wh = window[2] - wr0 + 1, ww = window[3] - wc0 + 1;
-    const bool windowed = window[2] >= 0 && wh * ww <= kScatterWindow;
-    const int plane = windowed ? wh * ww : 0;
-    if (windowed) {
-        for (int e = threadIdx.x; e < 3 * plane; e += blockDim.x) window_sum[e] = 0ULL;
-        __syncthreads();
-    }
-    if (deposit) {
-        unsigned long long* target = a.layers + static_cast<size_t>(code) * a.bins_x * a.bins_y;
-        unsigned long long* local = window_sum + code * plane;
-        long long sum = 0;
-        for (int row = r0; row <= r1; ++row) {
-            const float fi = static_cast<float>(row - r0);
-            const float oy = fmaxf(0.0f, __fsub_rn(fminf(ft, __fadd_rn(fi, 1.0f)), fmaxf(fb, fi)));
-            for (int column = c0; column <= c1; ++column) {
-                const float fj = static_cast<float>(column - c0);
-                const float ox = fmaxf(0.0f, __fsub_rn(fminf(fr, __fadd_rn(fj, 1.0f)), fmaxf(fl, fj)));
-                const long long q = __float2ll_rn(__fmul_rn(__fmul_rn(ox, oy), kFixedOne));
-                if (q != 0) {
-                    if (windowed) {
-                        atomicAdd(local + (row - wr0) * ww + (column - wc0), static_cast<unsigned long long>(q));
-                    } else {
+            const int c0 = static_cast<int>(clampIndex(floor(gl), a.bins_x - 1));
+            const int c1 = static_cast<int>(clampIndex(__dsub_rn(ceil(gr), 1.0), a.bins_x - 1));
+            const int r0 = static_cast<int>(clampIndex(floor(gb), a.bins_y - 1));
+            const int r1 = static_cast<int>(clampIndex(__dsub_rn(ceil(gt), 1.0), a.bins_y - 1));
+            const float fl = __double2float_rn(__dsub_rn(gl, static_cast<double>(c0)));
+            const float fr = __double2float_rn(__dsub_rn(gr, static_cast<double>(c0)));
+            const float fb = __double2float_rn(__dsub_rn(gb, static_cast<double>(r0)));
+            const float ft = __double2float_rn(__dsub_rn(gt, static_cast<double>(r0)));
+            const int code = a.layer[i];
+            unsigned long long* target = a.layers + static_cast<size_t>(code) * a.bins_x * a.bins_y;
+            long long sum = 0;
+            for (int row = r0; row <= r1; ++row) {
+                const float fi = static_cast<float>(row - r0);
+                const float oy = fmaxf(0.0f, __fsub_rn(fminf(ft, __fadd_rn(fi, 1.0f)), fmaxf(fb, fi)));
+                for (int column = c0; column <= c1; ++column) {
+                    const float fj = static_cast<float>(column - c0);
+                    const float ox = fmaxf(0.0f, __fsub_rn(fminf(fr, __fadd_rn(fj, 1.0f)), fmaxf(fl, fj)));
+                    const long long q = __float2ll_rn(__fmul_rn(__fmul_rn(ox, oy), kFixedOne));
+                    if (q != 0) {
                         atomicAdd(target + static_cast<size_t>(row) * a.bins_x + column,
                                   static_cast<unsigned long long>(q));
+                        sum += q;
                     }
-                    sum += q;
                 }
             }
-        }
-        totals[code] = sum;
-    }
-    if (windowed) {
-        __syncthreads();
-        const size_t bins = static_cast<size_t>(a.bins_x) * a.bins_y;
-        for (int e = threadIdx.x; e < 3 * plane; e += blockDim.x) {
-            const unsigned long long v = window_sum[e];
-            if (v == 0ULL) continue;
-            const int layer = e / plane;
-            const int rest = e - layer * plane;
-            const int row = wr0 + rest / ww;
-            const int column = wc0 + rest % ww;
-            atomicAdd(a.layers + layer * bins + static_cast<size_t>(row) * a.bins_x + column, v);
+            totals[code] = sum;
         }
     }
     // Exact integer totals of each layer (for the mean removal) and the proposal scalars.
@@ -201,22 +145,6 @@ __device__ __forceinline__ void scatterBlock(const ScatterArgs& a, int block, in
         reduceGroups<2>(a.partials, a.group_partials, a.group_counters, is_max, static_cast<unsigned>(block),
                         static_cast<unsigned>(grid));
     }
-}
-
-// Bucket key of a particle: the 8 x 8-bin tile of its centre (clamped to the core),
-// in row-major tile order.
-__global__ void bucketKeysKernel(const double2* positions, int count, double llx, double lly, double bin_w,
-                                 double bin_h, int bins_x, int bins_y, int* keys, int* index) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) return;
-    const double2 c = positions[i];
-    const double gx = (c.x - llx) / bin_w;
-    const double gy = (c.y - lly) / bin_h;
-    const int column = static_cast<int>(clampIndex(floor(gx), bins_x - 1));
-    const int row = static_cast<int>(clampIndex(floor(gy), bins_y - 1));
-    const int tiles_x = (bins_x + kScatterTile - 1) / kScatterTile;
-    keys[i] = (row / kScatterTile) * tiles_x + column / kScatterTile;
-    index[i] = i;
 }
 
 __global__ void __launch_bounds__(kThreads) scatterKernel(ScatterArgs a) {
@@ -473,14 +401,6 @@ void launchMetricsSplit(const MetricsArgs& args, cudaStream_t stream) {
     if (args.rows <= 0) return;
     launchChained("Launch the density metrics and source split", metricsSplitKernel, dim3(args.rows),
                   dim3(kThreads), 0, stream, args);
-}
-
-void launchBucketKeys(const double2* positions, int count, double llx, double lly, double bin_w, double bin_h,
-                      int bins_x, int bins_y, int* keys, int* index, cudaStream_t stream) {
-    if (count <= 0) return;
-    bucketKeysKernel<<<ceilDiv(count, kThreads), kThreads, 0, stream>>>(positions, count, llx, lly, bin_w, bin_h,
-                                                                        bins_x, bins_y, keys, index);
-    checkCuda(cudaGetLastError(), "Launch the scatter bucket keys");
 }
 
 void launchScatterBatch(const ScatterArgs* args, const int* offsets, int count, int blocks, cudaStream_t stream) {

@@ -19,8 +19,6 @@
 #include <atomic>
 #include <thread>
 
-#include <cub/device/device_radix_sort.cuh>
-
 #include "batch.hpp"
 #include "common.cuh"
 #include "ingest.cuh"
@@ -193,14 +191,6 @@ void Engine::uploadStatic(const Problem& p) {
             static_placeable_sum_ += area - p.static_dark[b];
         }
     }
-    // The scatter's bucket order and the sort that makes it (CUB radix sort scratch).
-    bucket_order_ = arena_.array<int>(n, "scatter bucket order");
-    bucket_keys_ = arena_.array<int>(2 * n, "scatter bucket keys");
-    bucket_index_ = arena_.array<int>(n, "scatter bucket keys");
-    checkCuda(cub::DeviceRadixSort::SortPairs(nullptr, bucket_temp_bytes_, bucket_keys_, bucket_keys_ + n,
-                                              bucket_index_, bucket_order_, static_cast<int>(n), 0, 32, stream_),
-              "Size the scatter bucket sort");
-    bucket_temp_ = arena_.allocate(std::max<std::size_t>(bucket_temp_bytes_, 16), "scatter bucket sort scratch");
     scatter_blocks_ = ceilDiv(std::max<int64_t>(1, particle_count_), kThreads);
     gather_blocks_ = gatherBlocks(static_cast<int>(std::min<int64_t>(particle_count_, 1 << 30)));
     metrics_fused_ = metricsSplitFits(bins_x_);
@@ -438,22 +428,6 @@ void Engine::buildTensorCoreBasis(double max_scale) {
     tc_fwd2_.task[0].energy_partials = partials_e_;
 }
 
-void Engine::rebucket(const double2* positions) {
-    if (particle_count_ <= 0) return;
-    const int n = static_cast<int>(particle_count_);
-    const int tiles = ceilDiv(bins_x_, kScatterTile) * ceilDiv(bins_y_, kScatterTile);
-    int bits = 1;
-    while (bits < 31 && (1 << bits) < tiles) ++bits;
-    launchBucketKeys(positions, n, region_.llx, region_.lly, bin_w_, bin_h_, bins_x_, bins_y_, bucket_keys_,
-                     bucket_index_, stream_);
-    std::size_t bytes = bucket_temp_bytes_;
-    checkCuda(cub::DeviceRadixSort::SortPairs(bucket_temp_, bytes, bucket_keys_, bucket_keys_ + n, bucket_index_,
-                                              bucket_order_, n, 0, bits, stream_),
-              "Sort the particles by bucket");
-    launches_ += 5;  // keys, and the radix sort's passes
-    bucketed_ = true;
-}
-
 void Engine::setStallProbe(long long polls) {
     for (TcBatch* b : {&tc_fwd1_, &tc_fwd2_, &tc_inv1_, &tc_inv2_, &tc_pot_}) b->stall_polls = std::max(0LL, polls);
 }
@@ -588,7 +562,6 @@ EvalPlan Engine::plan(const EvalRequest& q) {
     sa.layers = layers_;
     sa.totals = totals_;
     sa.partials = partials_sc_;
-    sa.order = bucketed_ ? bucket_order_ : nullptr;
     sa.group_partials = sc_groups_.partials;
     sa.group_counters = sc_groups_.counters;
     p.scatter = !q.reuse_density && particle_count_ > 0;
@@ -1068,7 +1041,6 @@ void Engine::depositLayers(const double2* positions, int64_t* movable, int64_t* 
     sa.mode = kGiven;
     sa.particle_count = static_cast<int>(particle_count_);
     sa.positions = positions;
-    sa.order = bucketed_ ? bucket_order_ : nullptr;
     sa.size = size_;
     sa.layer = layer_;
     sa.llx = region_.llx;

@@ -187,10 +187,6 @@ public:
     // Runs the fixed-point scatter alone at `positions` and copies the three layers out (parity hook).
     void depositLayers(const double2* positions, int64_t* movable, int64_t* macro, int64_t* filler);
     [[nodiscard]] double2* scratchPositions() const { return scratch_positions_; }
-    // Sorts the particles by the bin tile of `positions` (a stable radix sort, so the
-    // order is deterministic); later scatters take the particles in that order and
-    // accumulate in shared memory.  The density map does not depend on the order.
-    void rebucket(const double2* positions);
     // Failure-detection probe: with polls > 0 every later field contraction waits on a
     // barrier that nothing completes for at most `polls` polls and raises the engine's
     // error flag (the evaluation then fails with MPGP_ERR_TIMEOUT); 0 turns it off.
@@ -281,12 +277,6 @@ private:
     double static_fixed_sum_ = 0.0, static_dark_sum_ = 0.0, static_placeable_sum_ = 0.0;
 
     // particles
-    int* bucket_order_ = nullptr;  // scatter order (bucket-sorted particle indices); valid once rebucketed
-    int* bucket_keys_ = nullptr;   // 2 x P keys (unsorted, sorted) and P identity indices
-    int* bucket_index_ = nullptr;
-    void* bucket_temp_ = nullptr;
-    std::size_t bucket_temp_bytes_ = 0;
-    bool bucketed_ = false;
     double2* size_ = nullptr;
     unsigned char* layer_ = nullptr;
     double* charge_ = nullptr;

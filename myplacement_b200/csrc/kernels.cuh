@@ -132,18 +132,10 @@ struct ScatterArgs {
     unsigned long long* layers; // 3 * B fixed-point accumulators (movable, macro, filler)
     unsigned long long* totals; // 3 exact layer totals
     double* partials;           // per block: predicted, max displacement
-    const int* order;           // P: the particles in bucket order (block b takes slots b * 256 ..), or null
     double* group_partials;     // per 32 blocks (reduceGroups), when group_counters is set
     unsigned int* group_counters;
 };
 void launchScatter(const ScatterArgs& args, int blocks, cudaStream_t stream);
-// The scatter's shared-memory window (bins of the three layers a block accumulates
-// before flushing) and the bucket tile (bins per side) its particle order sorts by.
-constexpr int kScatterWindow = 1024;
-constexpr int kScatterTile = 8;
-// Bucket keys (tile of the centre, row-major) and the identity index of `count` particles.
-void launchBucketKeys(const double2* positions, int count, double llx, double lly, double bin_w, double bin_h,
-                      int bins_x, int bins_y, int* keys, int* index, cudaStream_t stream);
 void launchScatterBatch(const ScatterArgs* args, const int* offsets, int count, int blocks, cudaStream_t stream);
 
 // ---- density metrics + DCT source --------------------------------------------------

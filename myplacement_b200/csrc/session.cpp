@@ -163,7 +163,6 @@ Session::Session(const mpgp_design& design, const mpgp_options& options, Batch* 
                               engine_->stream()),
               "Upload initial positions");
     engine_->addTransfer(particles * sizeof(double2), 0);
-    engine_->rebucket(cur_);  // the scatter's particle order; refreshed every kRebucketInterval iterations
 
     // Initial evaluations and the penalty normalisation (AdaptiveGlobalPlacer.cpp:672-733).
     smoothing_ = options_.initial_smoothing * max_bin_;
@@ -407,10 +406,6 @@ bool Session::step(int iterations, int* completed) {
 void Session::iterate() {
     const mpgp_options& o = options_;
     const int iteration = iteration_;
-    // Cells move less than a bin per iteration: re-sorting them by bin tile every few
-    // iterations keeps each scatter block's particles close together.
-    constexpr int kRebucketInterval = 8;
-    if (iteration > 0 && iteration % kRebucketInterval == 0) engine_->rebucket(cur_);
     StateEval current;
     if (iteration == 0) {
         current = initial_;
