@@ -48,6 +48,9 @@ Batch::Batch(int device, double window_seconds) : device_(device), window_(windo
     checkCuda(cudaSetDevice(device_), "Select CUDA device");
     checkCuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "Create batch stream");
     checkCuda(cudaStreamCreateWithFlags(&wirelength_, cudaStreamNonBlocking), "Create batch wirelength stream");
+    checkCuda(cudaStreamCreateWithFlags(&split_, cudaStreamNonBlocking), "Create batch contraction stream");
+    checkCuda(cudaEventCreateWithFlags(&split_fork_, cudaEventDisableTiming), "Create batch event");
+    checkCuda(cudaEventCreateWithFlags(&split_join_, cudaEventDisableTiming), "Create batch event");
     checkCuda(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "Create batch event");
     checkCuda(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "Create batch event");
     checkCuda(cudaEventCreate(&start_), "Create batch event");
@@ -66,6 +69,9 @@ Batch::~Batch() {
     cudaSetDevice(device_);
     if (stream_ != nullptr) cudaStreamSynchronize(stream_);
     if (wirelength_ != nullptr) cudaStreamSynchronize(wirelength_);
+    if (split_ != nullptr) cudaStreamSynchronize(split_);
+    if (split_fork_ != nullptr) cudaEventDestroy(split_fork_);
+    if (split_join_ != nullptr) cudaEventDestroy(split_join_);
     if (fork_ != nullptr) cudaEventDestroy(fork_);
     if (join_ != nullptr) cudaEventDestroy(join_);
     if (done_ != nullptr) cudaEventDestroy(done_);
@@ -73,6 +79,7 @@ Batch::~Batch() {
     if (host_args_ != nullptr) cudaFreeHost(host_args_);
     if (device_args_ != nullptr) cudaFree(device_args_);
     if (wirelength_ != nullptr) cudaStreamDestroy(wirelength_);
+    if (split_ != nullptr) cudaStreamDestroy(split_);
     if (stream_ != nullptr) cudaStreamDestroy(stream_);
 }
 
@@ -178,6 +185,7 @@ void Batch::execute(const std::vector<Request*>& round) {
     const int n = static_cast<int>(round.size());
     std::vector<int> scatter, pins, metrics, gather;
     std::vector<TcItem> items[kContractionStages][kMaxSplit];
+    bool mixed_split = false;  // an instance whose stages use different splits (its stages must share a stream)
     int staged = 0;
     for (int i = 0; i < n; ++i) {
         const EvalPlan& p = *round[i]->plan;
@@ -190,6 +198,7 @@ void Batch::execute(const std::vector<Request*>& round) {
         if (total <= p.reduce_args.staged_capacity) staged = std::max(staged, total);
         const TcBatch* device_batches = engine->deviceBatches();
         for (int stage = 0; stage < kContractionStages; ++stage) {
+            mixed_split = mixed_split || engine->contraction(stage).ksplit != engine->contraction(0).ksplit;
             if (stage < 2 ? !p.forward : !p.gradient) continue;
             const TcBatch& batch = engine->contraction(stage);
             const int tasks = stage < 2 ? 1 : 2;
@@ -312,13 +321,32 @@ void Batch::execute(const std::vector<Request*>& round) {
                                 static_cast<int>(metrics.size()), metrics_blocks, stream_);
         ++launches;
     }
+    // The contraction stages.  Instances of one K split and of the other are
+    // disjoint, so with both present the split-1 group runs on a stream of its own
+    // beside the split-2 group (each group's stages stay in order on its stream).
+    // Only when every instance uses one split for all its stages: otherwise an
+    // instance's stages could land on both streams, and they depend on each other.
+    bool both = false;
+    for (int stage = 0; stage < kContractionStages && !mixed_split; ++stage) {
+        for (int other = 0; other < kContractionStages; ++other) {
+            both = both || (!items[stage][0].empty() && !items[other][1].empty());
+        }
+    }
+    if (both) {
+        checkCuda(cudaEventRecord(split_fork_, stream_), "Batch split fork");
+        checkCuda(cudaStreamWaitEvent(split_, split_fork_, 0), "Batch split fork");
+    }
     for (int stage = 0; stage < kContractionStages; ++stage) {
         for (int k = 0; k < kMaxSplit; ++k) {
             if (items[stage][k].empty()) continue;
             launchTcGemmBatch(reinterpret_cast<const TcItem*>(on_device(at_items[stage][k])),
-                              static_cast<int>(items[stage][k].size()), k + 1, stream_);
+                              static_cast<int>(items[stage][k].size()), k + 1, both && k == 0 ? split_ : stream_);
             ++launches;
         }
+    }
+    if (both) {
+        checkCuda(cudaEventRecord(split_join_, split_), "Batch split join");
+        checkCuda(cudaStreamWaitEvent(stream_, split_join_, 0), "Batch split join");
     }
     checkCuda(cudaStreamWaitEvent(stream_, join_, 0), "Batch join");
     if (!gather.empty()) {

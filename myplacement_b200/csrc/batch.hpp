@@ -71,6 +71,8 @@ private:
     double window_;
     cudaStream_t stream_ = nullptr;       // the engines' stream: the density chain and the contractions
     cudaStream_t wirelength_ = nullptr;   // the wirelength pass beside it
+    cudaStream_t split_ = nullptr;        // the split-1 contraction group beside the split-2 group
+    cudaEvent_t split_fork_ = nullptr, split_join_ = nullptr;
     cudaEvent_t fork_ = nullptr, join_ = nullptr;
     cudaEvent_t start_ = nullptr, done_ = nullptr;  // timed: the round's device time
     unsigned char* host_args_ = nullptr;  // pinned staging of a round's argument blocks
