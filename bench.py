@@ -75,24 +75,6 @@ def parse_args():
     return p.parse_args()
 
 
-def family_groups(stats: dict) -> dict:
-    """Timed families grouped by the kernel they launch (the field contractions' forward and
-    inverse launches are one kernel, tcGemmKernel)."""
-    groups = {}
-    for name, (n, ms) in stats.items():
-        if n > 0:
-            groups.setdefault(KERNEL_OF_FAMILY.get(name, name), []).append(name)
-    return groups
-
-
-def dominant_families(stats: dict) -> list:
-    """The families of the kernel with the most device time."""
-    groups = family_groups(stats)
-    if not groups:
-        return ["dct_forward", "dct_inverse"]
-    return groups[max(groups, key=lambda g: sum(stats[f][1] for f in groups[g]))]
-
-
 def load_peaks() -> tuple[dict, str]:
     if PEAKS_FILE.is_file():
         try:
@@ -304,30 +286,26 @@ def run_mine(args) -> None:
     session = mp.Session(design, options)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     stream_ptr = session.stream
-    # Two warm-up steps time every kernel family (shares, the dominant kernel); the
-    # last warm-up step and the timed steps time only the dominant kernel's families,
-    # since every event pair costs time inside the step.  The engine replays each
-    # evaluation shape from a CUDA graph captured at its first use with the timing
-    # then in force, so the last warm-up step captures what the timed steps replay.
-    profiled_warmup = min(2, max(1, args.warmup - 1))
-    warm_stats = None
+    # The last warm-up steps time every kernel family (shares, dominant family);
+    # the timed steps time only the dominant family, since every event pair costs
+    # host time inside the step.
+    profiled_warmup = min(2, args.warmup)
     for i in range(args.warmup):
-        if i == args.warmup - profiled_warmup - 1 or (args.warmup == 1 and i == 0):
+        if i == args.warmup - profiled_warmup:
             session.set_profiling(True)
         session.step(1)
-        if i == args.warmup - 2 or args.warmup == 1:
-            torch.cuda.synchronize()
-            warm_stats = session.kernel_stats()
-            session.reset_kernel_stats()
-            families = dominant_families(warm_stats)
-            session.set_profiling(families)
-    if warm_stats is None:  # no warm-up steps
-        warm_stats, families = {}, ["dct_forward", "dct_inverse"]
-        session.set_profiling(families)
     torch.cuda.synchronize()
+    warm_stats = session.kernel_stats()
     session.reset_kernel_stats()
-    groups = family_groups(warm_stats)
-    dominant = KERNEL_OF_FAMILY.get(families[0], families[0])
+    # The dominant kernel: families that launch the same kernel are summed (the field
+    # contractions' forward and inverse launches are one kernel, tcGemmKernel).
+    groups = {}
+    for name, (n, ms) in warm_stats.items():
+        if n > 0:
+            groups.setdefault(KERNEL_OF_FAMILY.get(name, name), []).append(name)
+    dominant = max(groups, key=lambda g: sum(warm_stats[f][1] for f in groups[g])) if groups else "tcGemmKernel"
+    families = groups.get(dominant, ["dct_forward", "dct_inverse"])
+    session.set_profiling(families)
     launches_before = session.kernel_launches
     step_ms = []
     start = torch.cuda.Event(enable_timing=True)

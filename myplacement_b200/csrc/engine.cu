@@ -129,14 +129,6 @@ Engine::~Engine() {
     if (host_error_ != nullptr) cudaFreeHost(host_error_);
     if (host_slots_ != nullptr) cudaFreeHost(host_slots_);
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
-    for (CapturedEvaluation& g : graphs_) {
-        if (g.exec != nullptr) cudaGraphExecDestroy(g.exec);
-        for (TimedSpan& span : g.spans) {
-            if (span.start != nullptr) cudaEventDestroy(span.start);
-            if (span.end != nullptr) cudaEventDestroy(span.end);
-        }
-    }
-    if (graph_host_ != nullptr) cudaFreeHost(graph_host_);
 }
 
 void Engine::newParticleArrays(int count, double2** out, const char* what) {
@@ -438,16 +430,6 @@ void Engine::buildTensorCoreBasis(double max_scale) {
 
 void Engine::setStallProbe(long long polls) {
     for (TcBatch* b : {&tc_fwd1_, &tc_fwd2_, &tc_inv1_, &tc_inv2_, &tc_pot_}) b->stall_polls = std::max(0LL, polls);
-    // The captured graphs hold the contraction descriptors by value: capture again.
-    checkCuda(cudaStreamSynchronize(stream_), "Release the evaluation graphs");
-    for (CapturedEvaluation& g : graphs_) {
-        cudaGraphExecDestroy(g.exec);
-        for (TimedSpan& span : g.spans) {
-            cudaEventDestroy(span.start);
-            cudaEventDestroy(span.end);
-        }
-    }
-    graphs_.clear();
 }
 
 const char* kernelKindName(int kind) {
@@ -460,6 +442,7 @@ void Engine::setTiming(uint32_t families) {
     if (families != 0 && events_.empty()) {
         events_.resize(64);
         for (cudaEvent_t& e : events_) checkCuda(cudaEventCreate(&e), "Create profiling event");
+        pending_kind_.resize(32);
     }
     timing_mask_ = families;
 }
@@ -467,45 +450,28 @@ void Engine::setTiming(uint32_t families) {
 void Engine::beginKernel(int kind, cudaStream_t on) {
     open_ = ((timing_mask_ >> kind) & 1u) != 0;
     if (!open_) return;
-    const cudaStream_t stream = on != nullptr ? on : stream_;
-    if (capturing_) {
-        // A timing node of the graph being captured: the graph owns its events.
-        checkCuda(cudaEventCreate(&open_start_), "Create profiling event");
-        checkCuda(cudaEventRecordWithFlags(open_start_, stream, cudaEventRecordExternal), "Record profiling event");
-        captured_spans_.push_back(TimedSpan{open_start_, nullptr, kind});
-        return;
-    }
-    if (pool_next_ + 2 > events_.size()) collectTimings();
-    open_start_ = events_[pool_next_];
-    pending_spans_.push_back(TimedSpan{open_start_, events_[pool_next_ + 1], kind});
-    pool_next_ += 2;
-    checkCuda(cudaEventRecord(open_start_, stream), "Record profiling event");
+    if (pending_ >= static_cast<int>(pending_kind_.size())) collectTimings();
+    pending_kind_[pending_] = kind;
+    checkCuda(cudaEventRecord(events_[2 * pending_], on != nullptr ? on : stream_), "Record profiling event");
 }
 
 void Engine::endKernel(cudaStream_t on) {
     if (!open_) return;
     open_ = false;
-    const cudaStream_t stream = on != nullptr ? on : stream_;
-    if (capturing_) {
-        cudaEvent_t end = nullptr;
-        checkCuda(cudaEventCreate(&end), "Create profiling event");
-        checkCuda(cudaEventRecordWithFlags(end, stream, cudaEventRecordExternal), "Record profiling event");
-        captured_spans_.back().end = end;
-        return;
-    }
-    checkCuda(cudaEventRecord(pending_spans_.back().end, stream), "Record profiling event");
+    checkCuda(cudaEventRecord(events_[2 * pending_ + 1], on != nullptr ? on : stream_), "Record profiling event");
+    ++pending_;
 }
 
 void Engine::collectTimings() {
-    for (const TimedSpan& span : pending_spans_) {
+    if (pending_ == 0) return;
+    for (int i = 0; i < pending_; ++i) {
         float ms = 0.0f;
-        checkCuda(cudaEventSynchronize(span.end), "Profiling sync");
-        checkCuda(cudaEventElapsedTime(&ms, span.start, span.end), "Profiling elapsed");
-        stats_.launches[span.kind] += 1;
-        stats_.milliseconds[span.kind] += static_cast<double>(ms);
+        checkCuda(cudaEventSynchronize(events_[2 * i + 1]), "Profiling sync");
+        checkCuda(cudaEventElapsedTime(&ms, events_[2 * i], events_[2 * i + 1]), "Profiling elapsed");
+        stats_.launches[pending_kind_[i]] += 1;
+        stats_.milliseconds[pending_kind_[i]] += static_cast<double>(ms);
     }
-    pending_spans_.clear();
-    pool_next_ = 0;
+    pending_ = 0;
 }
 
 // The Neumann field as dense contractions (ElectrostaticField.cpp:205-237):
@@ -755,44 +721,18 @@ EvalPlan Engine::plan(const EvalRequest& q) {
     return p;
 }
 
-void Engine::launchFamilies(const EvalPlan& p, bool batched) {
-    // batched: the kernels read their arguments from the graph's device buffer (the
-    // batched kernels over this one engine), which the first node fills.
-    unsigned char* dev = graph_device_;
-    const auto at = [&](std::size_t offset) { return dev + offset; };
-    const auto offsets = [&](int family) { return reinterpret_cast<const int*>(at(at_offsets_)) + 2 * family; };
-    if (batched) {
-        checkCuda(cudaMemcpyAsync(graph_device_, graph_host_, graph_bytes_, cudaMemcpyHostToDevice, stream_),
-                  "Upload evaluation arguments");
-    }
+void Engine::run(const EvalPlan& p) {
     if (p.fork_first) checkCuda(cudaEventRecord(fork_, stream_), "fork");
     if (p.scatter) {
         beginKernel(kKindScatter);
-        if (batched) {
-            launchScatterBatch(reinterpret_cast<const ScatterArgs*>(at(at_scatter_)), offsets(0), 1, p.scatter_blocks,
-                               stream_);
-        } else {
-            launchScatter(p.scatter_args, p.scatter_blocks, stream_);
-        }
+        launchScatter(p.scatter_args, p.scatter_blocks, stream_);
         endKernel();
     }
     if (!p.fork_first) checkCuda(cudaEventRecord(fork_, stream_), "fork");
     checkCuda(cudaStreamWaitEvent(stream_wl_, fork_, 0), "fork");
     beginKernel(kKindWirelength, stream_wl_);
-    if (p.pin_positions) {
-        if (batched) {
-            launchPinPositionsBatch(reinterpret_cast<const PinPositionArgs*>(at(at_pins_)), offsets(1), 1, p.pin_blocks,
-                                    stream_wl_);
-        } else {
-            launchPinPositions(p.pin_args, stream_wl_);
-        }
-    }
-    if (batched) {
-        launchWirelengthBatch(reinterpret_cast<const WirelengthArgs*>(at(at_wirelength_)), offsets(2), 1,
-                              p.wirelength_blocks, stream_wl_);
-    } else {
-        launchWirelength(p.wirelength_args, p.wirelength_blocks, stream_wl_);
-    }
+    if (p.pin_positions) launchPinPositions(p.pin_args, stream_wl_);
+    launchWirelength(p.wirelength_args, p.wirelength_blocks, stream_wl_);
     endKernel(stream_wl_);
     if (p.rudy) {
         beginKernel(kKindRudy, stream_wl_);
@@ -808,10 +748,7 @@ void Engine::launchFamilies(const EvalPlan& p, bool batched) {
     checkCuda(cudaEventRecord(join_, stream_wl_), "join");
     if (p.metrics) {
         beginKernel(kKindMetrics);
-        if (batched) {
-            launchMetricsSplitBatch(reinterpret_cast<const MetricsArgs*>(at(at_metrics_)), offsets(3), 1,
-                                    p.metrics_blocks, stream_);
-        } else if (p.metrics_fused) {
+        if (p.metrics_fused) {
             launchMetricsSplit(p.metrics_args, stream_);
         } else {
             launchMetrics(p.metrics_args, p.metrics_blocks, stream_);
@@ -823,145 +760,13 @@ void Engine::launchFamilies(const EvalPlan& p, bool batched) {
     if (p.gather) {
         // The gather's last block also reduces and publishes the evaluation.
         beginKernel(kKindGather);
-        if (batched) {
-            launchGatherBatch(reinterpret_cast<const GatherArgs*>(at(at_gather_)),
-                              reinterpret_cast<const ReduceArgs* const*>(at(at_reduce_pointer_)), offsets(4), 1,
-                              p.gather_blocks, stream_);
-        } else {
-            launchGather(p.gather_args, &p.reduce_args, p.gather_blocks, stream_);
-        }
+        launchGather(p.gather_args, &p.reduce_args, p.gather_blocks, stream_);
         endKernel();
     } else {
         beginKernel(kKindReduce);
-        if (batched) {
-            const int total = p.reduce_args.offsets[p.reduce_args.source_count];
-            launchReduceBatch(reinterpret_cast<const ReduceArgs*>(at(at_reduce_)), 1,
-                              total <= p.reduce_args.staged_capacity ? total : 0, stream_);
-        } else {
-            launchReduce(p.reduce_args, stream_);
-        }
+        launchReduce(p.reduce_args, stream_);
         endKernel();
     }
-}
-
-uint32_t Engine::graphKey(const EvalPlan& p) {
-    return (p.scatter ? 1u : 0u) | (p.pin_positions ? 2u : 0u) | (p.metrics ? 4u : 0u) | (p.forward ? 8u : 0u) |
-           (p.gradient ? 16u : 0u) | (p.gather ? 32u : 0u) | (p.fork_first ? 64u : 0u) |
-           (static_cast<uint32_t>(p.scatter_args.mode) << 8) |
-           (static_cast<uint32_t>(p.reduce_args.offsets[p.reduce_args.source_count]) << 12);
-}
-
-bool Engine::graphable(const EvalPlan& p) {
-    return !p.rudy && !p.potential && !p.split_source && (!p.metrics || p.metrics_fused);
-}
-
-void Engine::prepareGraphs() {
-    if (graph_host_ != nullptr) return;
-    prepareReduceLaunch();  // one-time kernel attributes, before any capture
-    std::size_t bytes = 0;
-    const auto add = [&](std::size_t size) {
-        const std::size_t offset = (bytes + 255) / 256 * 256;
-        bytes = offset + size;
-        return offset;
-    };
-    at_scatter_ = add(sizeof(ScatterArgs));
-    at_pins_ = add(sizeof(PinPositionArgs));
-    at_wirelength_ = add(sizeof(WirelengthArgs));
-    at_metrics_ = add(sizeof(MetricsArgs));
-    at_gather_ = add(sizeof(GatherArgs));
-    at_reduce_gather_ = add(sizeof(ReduceArgs));
-    at_reduce_pointer_ = add(sizeof(const ReduceArgs*));
-    at_reduce_ = add(sizeof(ReduceArgs));
-    at_offsets_ = add(10 * sizeof(int));
-    graph_bytes_ = (bytes + 255) / 256 * 256;
-    graph_device_ = static_cast<unsigned char*>(arena_.allocate(graph_bytes_, "evaluation arguments"));
-    checkCuda(cudaMallocHost(reinterpret_cast<void**>(&graph_host_), graph_bytes_), "Evaluation argument staging");
-    std::memset(graph_host_, 0, graph_bytes_);
-    // Each family's launch covers blocks [0, n) of this one engine.
-    int* offsets = reinterpret_cast<int*>(graph_host_ + at_offsets_);
-    const int blocks[5] = {scatter_blocks_, pinPositionBlocks(movable_slots_), wl_blocks_, metrics_blocks_,
-                           gather_blocks_};
-    for (int f = 0; f < 5; ++f) {
-        offsets[2 * f] = 0;
-        offsets[2 * f + 1] = blocks[f];
-    }
-    *reinterpret_cast<const ReduceArgs**>(graph_host_ + at_reduce_pointer_) =
-        reinterpret_cast<const ReduceArgs*>(graph_device_ + at_reduce_gather_);
-}
-
-const Engine::CapturedEvaluation* Engine::capture(const EvalPlan& p, uint32_t key) {
-    const int64_t launches_before = launches_;
-    CapturedEvaluation g;
-    g.key = key;
-    g.timing = timing_mask_;
-    capturing_ = true;
-    captured_spans_.clear();
-    cudaGraph_t graph = nullptr;
-    bool ok = cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-    if (ok) {
-        try {
-            launchFamilies(p, true);
-        } catch (const Error&) {
-            ok = false;
-        }
-        ok = cudaStreamEndCapture(stream_, &graph) == cudaSuccess && ok;
-    }
-    capturing_ = false;
-    g.kernels = p.kernels + static_cast<int>(launches_ - launches_before);
-    launches_ = launches_before;
-    g.spans = captured_spans_;
-    captured_spans_.clear();
-    if (ok) ok = cudaGraphInstantiate(&g.exec, graph, 0) == cudaSuccess;
-    if (graph != nullptr) cudaGraphDestroy(graph);
-    if (!ok) {
-        (void)cudaGetLastError();
-        for (TimedSpan& span : g.spans) {
-            if (span.start != nullptr) cudaEventDestroy(span.start);
-            if (span.end != nullptr) cudaEventDestroy(span.end);
-        }
-        graphs_usable_ = false;  // this engine launches directly from now on
-        return nullptr;
-    }
-    graphs_.push_back(std::move(g));
-    return &graphs_.back();
-}
-
-void Engine::replay(const EvalPlan& p) {
-    prepareGraphs();
-    const uint32_t key = graphKey(p);
-    const CapturedEvaluation* graph = nullptr;
-    for (const CapturedEvaluation& g : graphs_) {
-        if (g.key == key && g.timing == timing_mask_) graph = &g;
-    }
-    if (graph == nullptr) graph = capture(p, key);
-    if (graph == nullptr) {  // the capture failed: launch directly
-        launchFamilies(p, false);
-        launches_ += p.kernels;
-        return;
-    }
-    // This evaluation's argument blocks; the previous replay has completed (every
-    // evaluation is synchronised before the next is planned), so the staging is free.
-    if (p.scatter) std::memcpy(graph_host_ + at_scatter_, &p.scatter_args, sizeof(ScatterArgs));
-    if (p.pin_positions) std::memcpy(graph_host_ + at_pins_, &p.pin_args, sizeof(PinPositionArgs));
-    std::memcpy(graph_host_ + at_wirelength_, &p.wirelength_args, sizeof(WirelengthArgs));
-    if (p.metrics) std::memcpy(graph_host_ + at_metrics_, &p.metrics_args, sizeof(MetricsArgs));
-    if (p.gather) {
-        std::memcpy(graph_host_ + at_gather_, &p.gather_args, sizeof(GatherArgs));
-        std::memcpy(graph_host_ + at_reduce_gather_, &p.reduce_args, sizeof(ReduceArgs));
-    } else {
-        std::memcpy(graph_host_ + at_reduce_, &p.reduce_args, sizeof(ReduceArgs));
-    }
-    checkCuda(cudaGraphLaunch(graph->exec, stream_), "Launch the evaluation graph");
-    for (const TimedSpan& span : graph->spans) pending_spans_.push_back(span);
-    launches_ += graph->kernels;
-}
-
-void Engine::run(const EvalPlan& p) {
-    if (graphs_usable_ && graphable(p)) {
-        replay(p);
-        return;
-    }
-    launchFamilies(p, false);
     launches_ += p.kernels;
 }
 

@@ -359,46 +359,9 @@ private:
     // profiling
     uint32_t timing_mask_ = 0;
     bool open_ = false;
-    // Timed spans not yet read: (start event, end event, family).  Direct launches
-    // take their events from a pool; a captured graph owns the events of its
-    // timing nodes and adds their spans after each replay.
-    struct TimedSpan {
-        cudaEvent_t start;
-        cudaEvent_t end;
-        int kind;
-    };
     std::vector<cudaEvent_t> events_;
-    std::size_t pool_next_ = 0;
-    cudaEvent_t open_start_ = nullptr;
-    std::vector<TimedSpan> pending_spans_;
-
-    // CUDA-graph replay of evaluations (one graph per evaluation shape and timing
-    // mask): the plan's argument blocks go into a pinned staging buffer that the
-    // graph's first node copies to the device; the kernels are the batched ones over
-    // this one engine (the same code a Batch runs) and the contractions with their
-    // fixed descriptors.
-    struct CapturedEvaluation {
-        uint32_t key = 0;
-        uint32_t timing = 0;
-        cudaGraphExec_t exec = nullptr;
-        std::vector<TimedSpan> spans;
-        int kernels = 0;
-    };
-    std::vector<CapturedEvaluation> graphs_;
-    bool graphs_usable_ = true;
-    unsigned char* graph_host_ = nullptr;
-    unsigned char* graph_device_ = nullptr;
-    std::size_t graph_bytes_ = 0;
-    std::size_t at_scatter_ = 0, at_pins_ = 0, at_wirelength_ = 0, at_metrics_ = 0, at_gather_ = 0;
-    std::size_t at_reduce_gather_ = 0, at_reduce_pointer_ = 0, at_reduce_ = 0, at_offsets_ = 0;
-    bool capturing_ = false;
-    std::vector<TimedSpan> captured_spans_;
-    void prepareGraphs();
-    [[nodiscard]] static uint32_t graphKey(const EvalPlan& p);
-    [[nodiscard]] static bool graphable(const EvalPlan& p);
-    const CapturedEvaluation* capture(const EvalPlan& p, uint32_t key);
-    void replay(const EvalPlan& p);
-    void launchFamilies(const EvalPlan& p, bool batched_kernels);
+    std::vector<int> pending_kind_;
+    int pending_ = 0;
     KernelStats stats_;
     uint64_t h2d_bytes_ = 0;
     uint64_t d2h_bytes_ = 0;

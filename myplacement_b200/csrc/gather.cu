@@ -350,8 +350,6 @@ void launchGatherBatch(const GatherArgs* args, const ReduceArgs* const* reduces,
                   reduces, offsets, count);
 }
 
-void prepareReduceLaunch() { configureReduce(); }
-
 void launchReduceBatch(const ReduceArgs* args, int count, int staged_doubles, cudaStream_t stream) {
     if (count <= 0) return;
     configureReduce();

@@ -240,8 +240,6 @@ constexpr int kReduceStaged = 24576;  // doubles staged in shared memory (192 Ki
 void launchReduce(const ReduceArgs& args, cudaStream_t stream);
 // One block per instance; staged_doubles: the largest staging of the instances (shared memory).
 void launchReduceBatch(const ReduceArgs* args, int count, int staged_doubles, cudaStream_t stream);
-// Sets the reduction kernels' shared-memory attribute (done on first launch otherwise).
-void prepareReduceLaunch();
 
 // ---- field gather + gradient combine (the fused update pass) ----------------------------
 struct GatherArgs {
