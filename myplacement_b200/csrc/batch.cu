@@ -12,6 +12,7 @@
 
 #include "common.cuh"
 #include "dct_tc.cuh"
+#include "field_tc.cuh"
 
 namespace mpgp {
 
@@ -31,6 +32,14 @@ struct RoundLayout {
 };
 
 constexpr int kContractionStages = 4;  // forward 1, forward 2, inverse 1, inverse 2
+constexpr int kInverseX = 4;           // the banded solve's inverse along x (Engine::contraction)
+
+// The banded field items of a round with one cluster size and share width.
+struct FieldGroup {
+    FieldShape shape;
+    std::vector<FieldItem> items;
+    std::size_t at = 0;
+};
 
 // Sleeps while *word still holds `seen` (Linux futex; spurious returns are fine).
 void futexWait(std::atomic<uint32_t>* word, uint32_t seen) {
@@ -100,6 +109,7 @@ void Batch::reserve(std::size_t bytes) {
 
 void Batch::attach(Engine* engine) {
     engine->deviceBatches();  // the contraction descriptors the batched launches read
+    if (engine->banded()) engine->deviceField();
     std::lock_guard<std::mutex> lock(mutex_);
     ++attached_;
 }
@@ -185,6 +195,7 @@ void Batch::execute(const std::vector<Request*>& round) {
     const int n = static_cast<int>(round.size());
     std::vector<int> scatter, pins, metrics, gather;
     std::vector<TcItem> items[kContractionStages][kMaxSplit];
+    std::vector<FieldGroup> fields;
     bool mixed_split = false;  // an instance whose stages use different splits (its stages must share a stream)
     int staged = 0;
     for (int i = 0; i < n; ++i) {
@@ -197,6 +208,30 @@ void Batch::execute(const std::vector<Request*>& round) {
         const int total = p.reduce_args.offsets[p.reduce_args.source_count];
         if (total <= p.reduce_args.staged_capacity) staged = std::max(staged, total);
         const TcBatch* device_batches = engine->deviceBatches();
+        if (engine->banded()) {
+            // The banded launch (as Engine::runDct), then the inverse along x with the
+            // last stage of the staged instances.
+            const FieldShape& shape = engine->fieldBand().shape;
+            if (p.forward || p.gradient) {
+                auto group = std::find_if(fields.begin(), fields.end(), [&](const FieldGroup& g) {
+                    return g.shape.cluster == shape.cluster && g.shape.share_n == shape.share_n;
+                });
+                if (group == fields.end()) group = fields.insert(fields.end(), FieldGroup{shape, {}, 0});
+                const FieldBand* field = engine->deviceField();
+                for (int b = 0; b < shape.bands; ++b) group->items.push_back(FieldItem{field, b, p.gradient ? 1 : 0});
+            }
+            if (p.gradient) {
+                const TcBatch& batch = engine->contraction(kInverseX);
+                for (int task = 0; task < 2; ++task) {
+                    const int tiles = taskTiles(batch, task);
+                    for (int tile = 0; tile < tiles; ++tile) {
+                        items[kContractionStages - 1][batch.ksplit - 1].push_back(
+                            TcItem{device_batches + kInverseX, task, tile});
+                    }
+                }
+            }
+            continue;
+        }
         for (int stage = 0; stage < kContractionStages; ++stage) {
             mixed_split = mixed_split || engine->contraction(stage).ksplit != engine->contraction(0).ksplit;
             if (stage < 2 ? !p.forward : !p.gradient) continue;
@@ -235,6 +270,7 @@ void Batch::execute(const std::vector<Request*>& round) {
     for (int stage = 0; stage < kContractionStages; ++stage) {
         for (int k = 0; k < kMaxSplit; ++k) at_items[stage][k] = layout.add<TcItem>(items[stage][k].size());
     }
+    for (FieldGroup& g : fields) g.at = layout.add<FieldItem>(g.items.size());
     reserve(layout.bytes);
 
     unsigned char* host = host_args_;
@@ -285,6 +321,7 @@ void Batch::execute(const std::vector<Request*>& round) {
             }
         }
     }
+    for (const FieldGroup& g : fields) std::memcpy(host + g.at, g.items.data(), g.items.size() * sizeof(FieldItem));
 
     unsigned char* dev = device_args_;
     const auto on_device = [&](std::size_t at) { return dev + at; };
@@ -319,6 +356,12 @@ void Batch::execute(const std::vector<Request*>& round) {
         launchMetricsSplitBatch(reinterpret_cast<const MetricsArgs*>(on_device(at_metrics)),
                                 reinterpret_cast<const int*>(on_device(at_metrics_offsets)),
                                 static_cast<int>(metrics.size()), metrics_blocks, stream_);
+        ++launches;
+    }
+    // The banded field solves, one launch per cluster shape.
+    for (const FieldGroup& g : fields) {
+        launchFieldBatch(reinterpret_cast<const FieldItem*>(on_device(g.at)), static_cast<int>(g.items.size()), g.shape,
+                         stream_);
         ++launches;
     }
     // The contraction stages.  Instances of one K split and of the other are

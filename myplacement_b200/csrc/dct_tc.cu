@@ -51,9 +51,12 @@
 #include "common.cuh"
 #include "split.cuh"
 #include "dct_tc.cuh"
+#include "tc_ptx.cuh"
 
 namespace mpgp {
 namespace {
+
+using namespace tc;
 
 constexpr int kTcThreads = 192;
 constexpr int kStageBytes = kSplit * (kTileM + kTileN) * kBlockK * 2;
@@ -65,162 +68,15 @@ constexpr int kStagedOffset = kParkBytes;
 constexpr int kReceiveOffset = kRingBytes;
 constexpr int kBarrierOffset = kReceiveOffset + kParkBytes;
 constexpr int kPrefetchOffset = kBarrierOffset + 256;  // epilogue inputs fetched right after the dependency wait
-constexpr int kPrefetchInts = 4 + kTileM;              // exp_a, exp_b, out_exp, -, then the tile's row exponents
+constexpr int kPrefetchInts = 4 + kTileM + kMaxKbExponents;  // exp_a, exp_b, out_exp, -, the tile's row exponents,
+                                                              // then A's per-K-block exponents
 constexpr int kSmemBytes = kPrefetchOffset + kPrefetchInts * 4 + 1024 /* alignment slack */;
 constexpr uint32_t kTmemColumns = 4 * kTileN;  // two buffers x (main, correction) accumulators
-constexpr long kSpinLimit = 1L << 22;
+constexpr uint32_t kInstrDescriptor = instrDescriptor(kTileN);
 static_assert(kStagedOffset + kTileM * kTilePitch * 4 <= kRingBytes, "the parked and staged tiles must fit in the ring");
 static_assert((kParkPitch * 8) % 16 == 0, "parked rows must keep 16-byte alignment for the bulk copies");
 static_assert(kTileM % (8 * kMaxSplit) == 0, "every split owns whole 8-row groups");
 
-__device__ __forceinline__ uint32_t smemAddress(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ uint32_t clusterRank() {
-    uint32_t rank;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
-    return rank;
-}
-
-// Address of the same shared-memory offset in cluster CTA `rank`.
-__device__ __forceinline__ uint32_t clusterAddress(uint32_t address, uint32_t rank) {
-    uint32_t out;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(address), "r"(rank));
-    return out;
-}
-
-__device__ __forceinline__ void clusterArrive() {
-    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
-}
-
-__device__ __forceinline__ void clusterWait() {
-    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbarInit(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbarExpectTx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void mbarArrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ bool mbarTryWait(uint32_t bar, uint32_t parity) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return done != 0;
-}
-
-// Bounded wait; false (and the error flag raised) after kSpinLimit polls.
-__device__ __forceinline__ bool mbarWait(uint32_t bar, uint32_t parity, int* error_flag) {
-    for (long i = 0; i < kSpinLimit; ++i) {
-        if (mbarTryWait(bar, parity)) return true;
-    }
-    if (error_flag != nullptr) atomicExch(error_flag, 1);
-    return false;
-}
-
-__device__ __forceinline__ void tmaLoad3d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y, int z) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
-        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y), "r"(z)
-        : "memory");
-}
-
-// Bulk copy of `bytes` from this CTA's shared memory into a peer's (cluster
-// addresses for the destination and its mbarrier).
-__device__ __forceinline__ void bulkToPeer(uint32_t dst, uint32_t src, uint32_t bytes, uint32_t bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-        ::"r"(dst), "r"(src), "r"(bytes), "r"(bar)
-        : "memory");
-}
-
-// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
-__device__ __forceinline__ uint64_t smemDescriptor(uint32_t address) {
-    return static_cast<uint64_t>((address >> 4) & 0x3FFFu) | (1ull << 16) | (64ull << 32) | (1ull << 46) |
-           (2ull << 61);
-}
-
-// Instruction descriptor: F16 x F16 -> F32, both K-major, M = 128, N = kTileN.
-constexpr uint32_t kInstrDescriptor =
-    (1u << 4) | (static_cast<uint32_t>(kTileN >> 3) << 17) | (static_cast<uint32_t>(kTileM >> 4) << 24);
-
-__device__ __forceinline__ void ummaF16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(tmem), "l"(a), "l"(b), "r"(kInstrDescriptor), "r"(accumulate));
-}
-
-__device__ __forceinline__ void ummaCommit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-                 : "memory");
-}
-
-// Issues a 16-column TMEM load into raw registers; they hold the values only
-// after tmemWait, which takes them as operands so that no use moves above it.
-__device__ __forceinline__ void tmemLoad16(uint32_t address, uint32_t (&r)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-        "%14, %15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(address));
-}
-
-__device__ __forceinline__ void tmemWait(uint32_t (&a)[16], uint32_t (&b)[16]) {
-    asm volatile("tcgen05.wait::ld.sync.aligned;"
-                 : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7]), "+r"(a[8]), "+r"(a[9]), "+r"(a[10]), "+r"(a[11]), "+r"(a[12]), "+r"(a[13]), "+r"(a[14]), "+r"(a[15]), "+r"(b[0]), "+r"(b[1]), "+r"(b[2]), "+r"(b[3]), "+r"(b[4]), "+r"(b[5]), "+r"(b[6]), "+r"(b[7]), "+r"(b[8]), "+r"(b[9]), "+r"(b[10]), "+r"(b[11]), "+r"(b[12]), "+r"(b[13]), "+r"(b[14]), "+r"(b[15])
-                 :
-                 : "memory");
-}
-
-// Plane exponent of an output bounded by ref_max * gain.
-__device__ __forceinline__ int planeExponent(const unsigned* ref_max, float gain) {
-    return min(120, max(-120, exponentOf(__uint_as_float(*ref_max) * gain) - kPlaneTop));
-}
-
-// Eight consecutive values as two 16-byte plane stores (dst 16-byte aligned).
-__device__ __forceinline__ void storeSplit8(const float (&v)[8], float inv_scale, __half* hi_dst, __half* lo_dst) {
-    __half hi[8], lo[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) splitScaled(v[i], inv_scale, hi[i], lo[i]);
-    *reinterpret_cast<uint4*>(hi_dst) = make_uint4(packHalves(hi[0], hi[1]), packHalves(hi[2], hi[3]),
-                                                   packHalves(hi[4], hi[5]), packHalves(hi[6], hi[7]));
-    *reinterpret_cast<uint4*>(lo_dst) = make_uint4(packHalves(lo[0], lo[1]), packHalves(lo[2], lo[3]),
-                                                   packHalves(lo[4], lo[5]), packHalves(lo[6], lo[7]));
-}
-
-__device__ __forceinline__ double2 loadShared2(uint32_t address) {
-    double2 v;
-    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(address));
-    return v;
-}
-
-__device__ __forceinline__ void storeShared(uint32_t address, float v) {
-    asm volatile("st.shared.f32 [%0], %1;" ::"r"(address), "f"(v) : "memory");
-}
-
-__device__ __forceinline__ float loadShared(uint32_t address) {
-    float v;
-    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(address) : "memory");
-    return v;
-}
-
-// Parseval weight of a DCT-II index: 1/2 for the DC term, 1 otherwise.
-__device__ __forceinline__ double parsevalWeight(int index) { return index == 0 ? 0.5 : 1.0; }
 
 // One CTA of the cluster that computes output tile `tile_index` of task `t`;
 // `local_block` = tile_index * ksplit + the CTA's rank (its energy partial and,
@@ -413,9 +269,9 @@ __device__ __forceinline__ void tcTile(const TcBatch& batch, const TcTask& t, in
                     const uint64_t a_lo = smemDescriptor(a_base + kTileM * kBlockK * 2 + kk * 32);
                     const uint64_t b_hi = smemDescriptor(b_base + kk * 32);
                     const uint64_t b_lo = smemDescriptor(b_base + kTileN * kBlockK * 2 + kk * 32);
-                    ummaF16(corr_acc, a_hi, b_lo, kk > 0 ? 1u : 0u);
-                    ummaF16(corr_acc, a_lo, b_hi, 1u);
-                    ummaF16(main_acc, a_hi, b_hi, kk > 0 ? 1u : 0u);
+                    ummaF16(corr_acc, a_hi, b_lo, kInstrDescriptor, kk > 0 ? 1u : 0u);
+                    ummaF16(corr_acc, a_lo, b_hi, kInstrDescriptor, 1u);
+                    ummaF16(main_acc, a_hi, b_hi, kInstrDescriptor, kk > 0 ? 1u : 0u);
                 }
                 ummaCommit(empty0 + 8 * s);
                 ummaCommit(partial0 + 8 * buffer);
@@ -430,6 +286,14 @@ __device__ __forceinline__ void tcTile(const TcBatch& batch, const TcTask& t, in
         const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tmem_slot);
         const int quarter = warp & 3;
         const uint32_t lane_base = tmem + (static_cast<uint32_t>(quarter * 32) << 16);
+        // A's per-K-block exponents, staged for the epilogue warps.
+        int* kb_exp = reinterpret_cast<int*>(smem + kPrefetchOffset) + 4 + kTileM;
+        if (t.kb_exp_a != nullptr) {
+            for (int kb = static_cast<int>(threadIdx.x) - 64; kb < k_blocks; kb += 128) {
+                kb_exp[kb] = t.kb_exp_a[kb_begin + kb];
+            }
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+        }
         double acc[kTileN];
 #pragma unroll
         for (int j = 0; j < kTileN; ++j) acc[j] = 0.0;
@@ -439,17 +303,36 @@ __device__ __forceinline__ void tcTile(const TcBatch& batch, const TcTask& t, in
             ok = __all_sync(0xffffffffu, mbarWait(partial0 + 8 * buffer, (kb >> 1) & 1, batch.error_flag) ? 1 : 0) != 0;
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (t.kb_exp_a != nullptr) {
+                // A K-block of A with an exponent of its own: its partial carries that scale.
+                const double k_scale = pow2(kb_exp[kb]);
 #pragma unroll
-            for (int c0 = 0; c0 < kTileN; c0 += 16) {
-                uint32_t main_part[16], corr_part[16];
-                tmemLoad16(lane_base + static_cast<uint32_t>(buffer * 2 * kTileN + c0), main_part);
-                tmemLoad16(lane_base + static_cast<uint32_t>(buffer * 2 * kTileN + kTileN + c0), corr_part);
-                tmemWait(main_part, corr_part);
+                for (int c0 = 0; c0 < kTileN; c0 += 16) {
+                    uint32_t main_part[16], corr_part[16];
+                    tmemLoad16(lane_base + static_cast<uint32_t>(buffer * 2 * kTileN + c0), main_part);
+                    tmemLoad16(lane_base + static_cast<uint32_t>(buffer * 2 * kTileN + kTileN + c0), corr_part);
+                    tmemWait(main_part, corr_part);
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    acc[c0 + j] += static_cast<double>(__uint_as_float(main_part[j])) +
-                                   static_cast<double>(__uint_as_float(corr_part[j])) *
-                                       (1.0 / static_cast<double>(kLoShift));
+                    for (int j = 0; j < 16; ++j) {
+                        const double part = static_cast<double>(__uint_as_float(main_part[j])) +
+                                            static_cast<double>(__uint_as_float(corr_part[j])) *
+                                                (1.0 / static_cast<double>(kLoShift));
+                        acc[c0 + j] += part * k_scale;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int c0 = 0; c0 < kTileN; c0 += 16) {
+                    uint32_t main_part[16], corr_part[16];
+                    tmemLoad16(lane_base + static_cast<uint32_t>(buffer * 2 * kTileN + c0), main_part);
+                    tmemLoad16(lane_base + static_cast<uint32_t>(buffer * 2 * kTileN + kTileN + c0), corr_part);
+                    tmemWait(main_part, corr_part);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        acc[c0 + j] += static_cast<double>(__uint_as_float(main_part[j])) +
+                                       static_cast<double>(__uint_as_float(corr_part[j])) *
+                                           (1.0 / static_cast<double>(kLoShift));
+                    }
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -821,19 +704,36 @@ int tunedSplits(int* sizes, int* splits, int capacity) {
 
 namespace {
 
+// Clusters of `ksplit` CTAs the GPU holds at once (-1 when the query fails); the
+// answer depends only on the device and the cluster size, so it is asked once.
+int activeClusters(int ksplit) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mutex;
+    static int known[kMaxDevices][kMaxSplit + 1] = {};  // 0: not asked yet
+    int device = 0;
+    checkCuda(cudaGetDevice(&device), "Query the current device");
+    require(device >= 0 && device < kMaxDevices && ksplit >= 1 && ksplit <= kMaxSplit, "Device index out of range.");
+    std::lock_guard<std::mutex> lock(mutex);
+    int& answer = known[device][ksplit];
+    if (answer == 0) {
+        cudaLaunchAttribute attribute[2] = {};
+        cudaLaunchConfig_t config = launchConfig(dim3(static_cast<unsigned>(ksplit)), ksplit, nullptr, attribute);
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, tcGemmKernel, &config) != cudaSuccess) {
+            (void)cudaGetLastError();
+            clusters = -1;
+        }
+        answer = clusters == 0 ? -1 : clusters;
+    }
+    return answer;
+}
+
 // The largest split whose clusters of a batch of `tiles` tiles still fit on the GPU at once.
 int fittingSplit(int tiles, int k_blocks) {
     int best = 1;
     for (int ksplit = 2; ksplit <= kMaxSplit && ksplit <= k_blocks; ksplit *= 2) {
-        cudaLaunchAttribute attribute[2] = {};
-        cudaLaunchConfig_t config =
-            launchConfig(dim3(static_cast<unsigned>(tiles * ksplit)), ksplit, nullptr, attribute);
-        int clusters = 0;
-        if (cudaOccupancyMaxActiveClusters(&clusters, tcGemmKernel, &config) != cudaSuccess) {
-            (void)cudaGetLastError();
-            break;
-        }
-        if (tiles > clusters) break;  // the split would no longer run in one wave
+        const int clusters = activeClusters(ksplit);
+        if (clusters < 0 || tiles > clusters) break;  // the split would no longer run in one wave
         best = ksplit;
     }
     return best;
@@ -850,6 +750,11 @@ void tcPlan(TcBatch& batch, int task_count) {
         const int kb = (batch.task[i].k + kBlockK - 1) / kBlockK;
         k_blocks = i == 0 ? kb : std::min(k_blocks, kb);
         k = std::max(k, batch.task[i].k);
+    }
+    for (int i = 0; i < task_count; ++i) {
+        const TcTask& t = batch.task[i];
+        require(t.kb_exp_a == nullptr || (t.k + kBlockK - 1) / kBlockK <= kMaxKbExponents,
+                "A contraction with per-K-block exponents has too many K-blocks.");
     }
     const int fitting = fittingSplit(tiles, k_blocks);
     const int tuned = tunedSplit(k);

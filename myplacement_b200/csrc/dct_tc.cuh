@@ -19,6 +19,7 @@ constexpr int kTileN = 64;     // UMMA N = accumulator columns per CTA
 constexpr int kBlockK = 64;    // fp16 elements per 128-byte swizzled row
 constexpr int kStages = 3;
 constexpr int kMaxSplit = 2;   // largest K split (cluster size)
+constexpr int kMaxKbExponents = 32;  // K-blocks of a contraction whose A carries one exponent per K-block
 
 // A row-major matrix stored as kSplit fp16 planes; ld is a multiple of kBlockK
 // and the padding columns are zero.
@@ -61,8 +62,9 @@ struct alignas(64) TcTask {
     int m, n, k;
     int mode;
     int constant_operand;  // 1: A, 2: B is a fixed basis matrix (loaded before the dependency wait); 0: none
-    const int* exp_a;      // exponent of A, or null when row_exp_a is given
+    const int* exp_a;      // exponent of A, or null when row_exp_a or kb_exp_a is given
     const int* row_exp_a;  // per-row exponents of A
+    const int* kb_exp_a;   // exponents of A per K-block (at most kMaxKbExponents), or null
     const int* exp_b;
     // Output planes: exponent = exponent_of(ref_max * gain) - kPlaneTop, published
     // in out_exp by block 0; the actual max |C| is folded into out_max.

@@ -423,18 +423,82 @@ void Engine::buildTensorCoreBasis(double max_scale) {
     tcPlan(tc_inv1_, 2);
     tcPlan(tc_inv2_, 2);
     tcPlan(tc_pot_, 1);
-    energy_blocks_ = tcBlocks(tc_fwd2_, 1);
+
+    // The banded solve (field_tc.cu): Q = S Cx^T, rho_hat = Cy Q, phi_hat, M1 = Dy phi_hat and
+    // M2 = Syw phi_hat per band of spectral columns, then Ex = M1 (Sx diag(kx))^T,
+    // Ey = M2 Dx^T and the potential M1 Dx^T over all bands.
+    // MPGP_FIELD_SOLVE=staged keeps the four-launch solve on every grid.
+    const char* solve = std::getenv("MPGP_FIELD_SOLVE");
+    const FieldShape shape = solve != nullptr && std::strcmp(solve, "staged") == 0 ? FieldShape{} : fieldShape(nx, ny);
+    banded_ = shape.cluster > 0;
+    if (banded_) {
+        tc_m1_ = newSplit(ny, nx, "banded field planes");
+        tc_m2_ = newSplit(ny, nx, "banded field planes");
+        int* band_exp = arena_.array<int>(static_cast<std::size_t>(2 * shape.bands), "banded field exponents");
+        FieldBand& f = field_band_;
+        makeOperandMap(&f.map_s, tc_source_, kTileM);
+        makeOperandMap(&f.map_cx, tc_cx_, shape.share_n);
+        makeOperandMap(&f.map_cy, tc_cy_, kTileM);
+        makeOperandMap(&f.map_dy, tc_dy_, kTileM);
+        makeOperandMap(&f.map_syw, tc_syw_, kTileM);
+        f.nx = nx;
+        f.ny = ny;
+        f.shape = shape;
+        f.row_exp = tc_row_exp_;
+        f.exp_basis = sc->exp_basis;
+        f.scale = spectral_scale_;
+        f.m1 = tc_m1_.data;
+        f.m2 = tc_m2_.data;
+        f.m_ld = tc_m1_.ld;
+        f.m_plane = tc_m1_.plane();
+        f.m1_exp = band_exp;
+        f.m2_exp = band_exp + shape.bands;
+        f.gain_dy = static_cast<float>(row_l1[kDy] * kMargin);
+        f.gain_syw = static_cast<float>(row_l1[kSyw] * kMargin);
+        f.clear = &sc->max_source;
+        f.error_flag = tc_error_;
+        task(tc_invx_.task[0], tc_m1_, tc_sxwt_, ny, nx, nx, kTcField);
+        tc_invx_.task[0].kb_exp_a = f.m1_exp;
+        tc_invx_.task[0].exp_b = &sc->exp_basis[kSxwt];
+        tc_invx_.task[0].out_f = reinterpret_cast<float*>(field_);
+        tc_invx_.task[0].out_f_ld = 2 * nx;
+        tc_invx_.task[0].out_f_step = 2;
+        task(tc_invx_.task[1], tc_m2_, tc_dxc_, ny, nx, nx, kTcField);
+        tc_invx_.task[1].kb_exp_a = f.m2_exp;
+        tc_invx_.task[1].exp_b = &sc->exp_basis[kDxc];
+        tc_invx_.task[1].out_f = reinterpret_cast<float*>(field_) + 1;
+        tc_invx_.task[1].out_f_ld = 2 * nx;
+        tc_invx_.task[1].out_f_step = 2;
+        task(tc_potx_.task[0], tc_m1_, tc_dxc_, ny, nx, nx, kTcField);
+        tc_potx_.task[0].kb_exp_a = f.m1_exp;
+        tc_potx_.task[0].exp_b = &sc->exp_basis[kDxc];
+        tc_potx_.task[0].out_f = potential_;
+        tc_potx_.task[0].out_f_ld = nx;
+        tc_potx_.task[0].out_f_step = 1;
+        for (TcBatch* b : {&tc_invx_, &tc_potx_}) {
+            b->error_flag = tc_error_;
+            for (TcTask& t : b->task) t.constant_operand = 2;
+        }
+        tcPlan(tc_invx_, 2);
+        tcPlan(tc_potx_, 1);
+    }
+    energy_blocks_ = banded_ ? shape.blocks() : tcBlocks(tc_fwd2_, 1);
     partials_e_ = arena_.array<double>(static_cast<std::size_t>(energy_blocks_), "energy partials");
     tc_fwd2_.task[0].energy_partials = partials_e_;
+    field_band_.energy_partials = partials_e_;
 }
 
 void Engine::setStallProbe(long long polls) {
-    for (TcBatch* b : {&tc_fwd1_, &tc_fwd2_, &tc_inv1_, &tc_inv2_, &tc_pot_}) b->stall_polls = std::max(0LL, polls);
+    for (TcBatch* b : {&tc_fwd1_, &tc_fwd2_, &tc_inv1_, &tc_inv2_, &tc_pot_, &tc_invx_, &tc_potx_}) {
+        b->stall_polls = std::max(0LL, polls);
+    }
+    field_band_.stall_polls = std::max(0LL, polls);
 }
 
 const char* kernelKindName(int kind) {
-    static const char* names[kKindCount] = {"scatter", "wirelength", "metrics", "dct_forward",
-                                            "dct_inverse", "gather", "reduce", "vector", "dct_split", "rudy"};
+    static const char* names[kKindCount] = {"scatter", "wirelength", "metrics",        "dct_forward",
+                                            "dct_inverse", "gather", "reduce", "vector", "dct_split",
+                                            "rudy", "field_forward", "field_gradient"};
     return kind >= 0 && kind < kKindCount ? names[kind] : "unknown";
 }
 
@@ -501,6 +565,34 @@ void Engine::allocateGroups() {
 
 void Engine::runDct(bool gradient, bool potential, bool forward, bool split_source) {
     const int nx = bins_x_;
+    if (banded_) {
+        if (forward && split_source) {
+            beginKernel(kKindDctSplit);
+            launchSplitSource(source_, tc_source_, nx, tc_row_exp_, tc_scales_, stream_);
+            endKernel();
+            launches_ += 1;
+        }
+        // Without the forward flag (the density is that of the previous evaluation) the
+        // banded launch recomputes the forward passes, which give the same bits.
+        if (forward || gradient) {
+            beginKernel(gradient ? kKindFieldGradient : kKindFieldForward);
+            launchField(field_band_, gradient ? 1 : 0, stream_);
+            endKernel();
+            launches_ += 1;
+        }
+        if (!gradient) return;
+        beginKernel(kKindDctInverse);
+        launchTcGemm(tc_invx_, 2, stream_);
+        endKernel();
+        launches_ += 1;
+        if (potential) {
+            beginKernel(kKindDctInverse);
+            launchTcGemm(tc_potx_, 1, stream_);
+            endKernel();
+            launches_ += 1;
+        }
+        return;
+    }
     if (forward) {
         if (split_source) {
             beginKernel(kKindDctSplit);
@@ -784,8 +876,8 @@ void Engine::launch(const EvalRequest& q) {
 
 const TcBatch* Engine::deviceBatches() {
     if (device_batches_ == nullptr) {
-        device_batches_ = arena_.array<TcBatch>(4, "batched contraction descriptors");
-        const TcBatch host[4] = {tc_fwd1_, tc_fwd2_, tc_inv1_, tc_inv2_};
+        device_batches_ = arena_.array<TcBatch>(5, "batched contraction descriptors");
+        const TcBatch host[5] = {tc_fwd1_, tc_fwd2_, tc_inv1_, tc_inv2_, tc_invx_};
         checkCuda(cudaMemcpyAsync(device_batches_, host, sizeof(host), cudaMemcpyHostToDevice, stream_),
                   "Upload contraction descriptors");
         checkCuda(cudaStreamSynchronize(stream_), "Upload contraction descriptors");  // `host` leaves scope
@@ -793,12 +885,23 @@ const TcBatch* Engine::deviceBatches() {
     return device_batches_;
 }
 
+const FieldBand* Engine::deviceField() {
+    if (device_field_ == nullptr) {
+        device_field_ = arena_.array<FieldBand>(1, "batched field descriptor");
+        checkCuda(cudaMemcpyAsync(device_field_, &field_band_, sizeof(FieldBand), cudaMemcpyHostToDevice, stream_),
+                  "Upload the field descriptor");
+        checkCuda(cudaStreamSynchronize(stream_), "Upload the field descriptor");
+    }
+    return device_field_;
+}
+
 const TcBatch& Engine::contraction(int stage) const {
     switch (stage) {
         case 0: return tc_fwd1_;
         case 1: return tc_fwd2_;
         case 2: return tc_inv1_;
-        default: return tc_inv2_;
+        case 3: return tc_inv2_;
+        default: return tc_invx_;
     }
 }
 

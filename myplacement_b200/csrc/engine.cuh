@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "dct_tc.cuh"
+#include "field_tc.cuh"
 #include "kernels.cuh"
 #include "setup.hpp"
 
@@ -129,6 +130,8 @@ enum KernelKind : int {
     kKindVector,
     kKindDctSplit,
     kKindRudy,
+    kKindFieldForward,   // the banded field solve without the inverse passes
+    kKindFieldGradient,  // the banded field solve with them
     kKindCount
 };
 const char* kernelKindName(int kind);
@@ -154,10 +157,15 @@ public:
     // launching them on the engine's streams.
     EvalPlan plan(const EvalRequest& request);
     void run(const EvalPlan& plan);
-    // The engine's contraction batches (forward 1, forward 2, inverse 1, inverse 2)
-    // copied to device memory, for batched launches; uploaded on first use.
+    // The engine's contraction batches (forward 1, forward 2, inverse 1, inverse 2 of
+    // the staged solve, then the inverse along x of the banded solve) and its banded
+    // solve's descriptor, copied to device memory for batched launches; uploaded on first use.
     const TcBatch* deviceBatches();
+    const FieldBand* deviceField();
     [[nodiscard]] const TcBatch& contraction(int stage) const;
+    // The field solve is banded (field_tc.cu) rather than staged (four contraction launches).
+    [[nodiscard]] bool banded() const { return banded_; }
+    [[nodiscard]] const FieldBand& fieldBand() const { return field_band_; }
     // Stops taking part in the batch's rounds (the placement has finished); a later
     // evaluation still runs through the batch.
     void leaveBatch();
@@ -317,6 +325,13 @@ private:
     SplitMatrix tc_source_, tc_cx_, tc_cy_, tc_dy_, tc_dxc_, tc_sxwt_, tc_syw_;
     SplitMatrix tc_x1t_, tc_phi_, tc_phit_, tc_t_, tc_ut_;
     TcBatch tc_fwd1_{}, tc_fwd2_{}, tc_inv1_{}, tc_inv2_{}, tc_pot_{};
+    // The banded solve where the grid allows it: one banded launch, then the inverse
+    // along x of M1 and M2 (tc_invx_) and the potential (tc_potx_).
+    bool banded_ = false;
+    FieldBand field_band_{};
+    FieldBand* device_field_ = nullptr;
+    SplitMatrix tc_m1_, tc_m2_;
+    TcBatch tc_invx_{}, tc_potx_{};
     int* tc_row_exp_ = nullptr;
     TcScales* tc_scales_ = nullptr;
     int* tc_error_ = nullptr;
