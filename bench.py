@@ -41,7 +41,7 @@ PROFILE_TRAFFIC = REPO / "profiles" / "traffic_mid_210k.md"
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 # The kernel behind each timed family (families of one kernel are summed for the roofline).
 KERNEL_OF_FAMILY = {"dct_forward": "tcGemmKernel", "dct_inverse": "tcGemmKernel",
-                    "field_forward": "fieldKernel", "field_gradient": "fieldKernel",
+                    "field_forward": "fieldKernel", "field_gradient": "fieldKernel", "field_inverse": "fieldKernel",
                     "wirelength": "wirelengthKernel + pinPositionKernel", "scatter": "scatterKernel",
                     "metrics": "metricsSplitKernel", "gather": "gatherKernel", "reduce": "reduceKernel",
                     "vector": "velocityKernel", "dct_split": "splitSourceKernel", "rudy": "rudy kernels"}
@@ -163,7 +163,8 @@ def algorithmic_units(design, particles: int, bins_x: int, bins_y: int) -> dict:
     36 B/bin; gather + update 80 B/particle.  A DCT launch is one (forward) or
     two (inverse) M x N x K contractions at 2 flops per multiply-add (the transform's
     own work, not the three tensor-core products of the split); a banded field launch
-    is the two forward contractions, and with a gradient the two inverse ones along y;
+    is the two forward contractions, and with a gradient the two inverse ones along y (an
+    inverse launch only those two);
     the source split reads 4 B and writes two 2-byte planes per bin.
     """
     pins, nets, bins = design.pin_count, design.net_count, bins_x * bins_y
@@ -178,6 +179,7 @@ def algorithmic_units(design, particles: int, bins_x: int, bins_y: int) -> dict:
         # The banded solve: Q = S Cx^T and rho_hat = Cy Q, then M1 and M2 (two m x n x m) with a gradient.
         "field_forward": ("tensor", 2.0 * m * n * (n + m)),
         "field_gradient": ("tensor", 2.0 * m * n * (n + m) + 2 * 2.0 * m * n * m),
+        "field_inverse": ("tensor", 2 * 2.0 * m * n * m),
         "reduce": ("hbm", 8 * 64),
         "vector": ("hbm", 48 * particles),
         "dct_split": ("hbm", 4 * bins + 4 * bins),

@@ -218,7 +218,8 @@ void Batch::execute(const std::vector<Request*>& round) {
                 });
                 if (group == fields.end()) group = fields.insert(fields.end(), FieldGroup{shape, {}, 0});
                 const FieldBand* field = engine->deviceField();
-                for (int b = 0; b < shape.bands; ++b) group->items.push_back(FieldItem{field, b, p.gradient ? 1 : 0});
+                const FieldMode mode = p.forward ? (p.gradient ? kFieldGradient : kFieldForward) : kFieldInverse;
+                for (int b = 0; b < shape.bands; ++b) group->items.push_back(FieldItem{field, b, mode});
             }
             if (p.gradient) {
                 const TcBatch& batch = engine->contraction(kInverseX);

@@ -73,6 +73,7 @@ constexpr int kPrefetchInts = 4 + kTileM + kMaxKbExponents;  // exp_a, exp_b, ou
 constexpr int kSmemBytes = kPrefetchOffset + kPrefetchInts * 4 + 1024 /* alignment slack */;
 constexpr uint32_t kTmemColumns = 4 * kTileN;  // two buffers x (main, correction) accumulators
 constexpr uint32_t kInstrDescriptor = instrDescriptor(kTileN);
+constexpr uint32_t kPairDescriptor = instrDescriptor(2 * kTileN);  // A x [B_hi; B_lo]
 static_assert(kStagedOffset + kTileM * kTilePitch * 4 <= kRingBytes, "the parked and staged tiles must fit in the ring");
 static_assert((kParkPitch * 8) % 16 == 0, "parked rows must keep 16-byte alignment for the bulk copies");
 static_assert(kTileM % (8 * kMaxSplit) == 0, "every split owns whole 8-row groups");
@@ -183,13 +184,10 @@ __device__ __forceinline__ void tcTile(const TcBatch& batch, const TcTask& t, in
             unsigned char* stage = smem + kb * kStageBytes;
             const int k0 = (kb_begin + kb) * kBlockK;
             mbarExpectTx(full0 + 8 * kb, kStageBytes);
-            for (int p = 0; p < kSplit; ++p) {
-                if (t.constant_operand == 1) {
-                    tmaLoad3d(smemAddress(stage + p * kTileM * kBlockK * 2), &t.map_a, full0 + 8 * kb, k0, m0, p);
-                } else {
-                    tmaLoad3d(smemAddress(stage + kSplit * kTileM * kBlockK * 2 + p * kTileN * kBlockK * 2),
-                              &t.map_b, full0 + 8 * kb, k0, n0, p);
-                }
+            if (t.constant_operand == 1) {
+                tmaLoad3d(smemAddress(stage), &t.map_a, full0 + 8 * kb, k0, m0, 0);
+            } else {
+                tmaLoad3d(smemAddress(stage + kSplit * kTileM * kBlockK * 2), &t.map_b, full0 + 8 * kb, k0, n0, 0);
             }
         }
     }
@@ -208,14 +206,13 @@ __device__ __forceinline__ void tcTile(const TcBatch& batch, const TcTask& t, in
                 const int k0 = (kb_begin + kb) * kBlockK;
                 const bool early = kb < prefetched;  // its basis tile is already on the way
                 if (!early) mbarExpectTx(full0 + 8 * s, kStageBytes);
-                for (int p = 0; p < kSplit; ++p) {
-                    if (!early || t.constant_operand != 1) {
-                        tmaLoad3d(smemAddress(stage + p * kTileM * kBlockK * 2), &t.map_a, full0 + 8 * s, k0, m0, p);
-                    }
-                    if (!early || t.constant_operand != 2) {
-                        tmaLoad3d(smemAddress(stage + kSplit * kTileM * kBlockK * 2 + p * kTileN * kBlockK * 2),
-                                  &t.map_b, full0 + 8 * s, k0, n0, p);
-                    }
+                // One box per operand carries both planes (a TMA instruction costs about the
+                // same whatever its size, so fewer and larger boxes stream faster).
+                if (!early || t.constant_operand != 1) {
+                    tmaLoad3d(smemAddress(stage), &t.map_a, full0 + 8 * s, k0, m0, 0);
+                }
+                if (!early || t.constant_operand != 2) {
+                    tmaLoad3d(smemAddress(stage + kSplit * kTileM * kBlockK * 2), &t.map_b, full0 + 8 * s, k0, n0, 0);
                 }
                 issued = kb + 1;
             }
@@ -265,13 +262,14 @@ __device__ __forceinline__ void tcTile(const TcBatch& batch, const TcTask& t, in
                 const uint32_t corr_acc = main_acc + kTileN;
 #pragma unroll
                 for (int kk = 0; kk < kBlockK / 16; ++kk) {
+                    // [B_hi; B_lo] are consecutive rows of the stage: one product of A_hi with
+                    // both (2 kTileN columns) writes main and the first correction term
+                    // (corr_acc follows main_acc); A_lo B_hi completes the correction.
                     const uint64_t a_hi = smemDescriptor(a_base + kk * 32);
                     const uint64_t a_lo = smemDescriptor(a_base + kTileM * kBlockK * 2 + kk * 32);
-                    const uint64_t b_hi = smemDescriptor(b_base + kk * 32);
-                    const uint64_t b_lo = smemDescriptor(b_base + kTileN * kBlockK * 2 + kk * 32);
-                    ummaF16(corr_acc, a_hi, b_lo, kInstrDescriptor, kk > 0 ? 1u : 0u);
-                    ummaF16(corr_acc, a_lo, b_hi, kInstrDescriptor, 1u);
-                    ummaF16(main_acc, a_hi, b_hi, kInstrDescriptor, kk > 0 ? 1u : 0u);
+                    const uint64_t b_both = smemDescriptor(b_base + kk * 32);
+                    ummaF16(main_acc, a_hi, b_both, kPairDescriptor, kk > 0 ? 1u : 0u);
+                    ummaF16(corr_acc, a_lo, b_both, kInstrDescriptor, 1u);
                 }
                 ummaCommit(empty0 + 8 * s);
                 ummaCommit(partial0 + 8 * buffer);
@@ -644,7 +642,8 @@ void makeOperandMap(CUtensorMap* map, const SplitMatrix& m, int box_rows) {
                                 static_cast<cuuint64_t>(kSplit)};
     const cuuint64_t strides[2] = {static_cast<cuuint64_t>(m.ld) * 2,
                                    static_cast<cuuint64_t>(m.ld) * static_cast<cuuint64_t>(m.rows) * 2};
-    const cuuint32_t box[3] = {static_cast<cuuint32_t>(kBlockK), static_cast<cuuint32_t>(box_rows), 1};
+    const cuuint32_t box[3] = {static_cast<cuuint32_t>(kBlockK), static_cast<cuuint32_t>(box_rows),
+                               static_cast<cuuint32_t>(kSplit)};  // both planes: [plane][row][64 halves]
     const cuuint32_t element_strides[3] = {1, 1, 1};
     const CUresult result =
         encoder()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, m.data, dims, strides, box, element_strides,

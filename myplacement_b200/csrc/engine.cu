@@ -457,6 +457,8 @@ void Engine::buildTensorCoreBasis(double max_scale) {
         f.gain_syw = static_cast<float>(row_l1[kSyw] * kMargin);
         f.clear = &sc->max_source;
         f.error_flag = tc_error_;
+        f.phi_store = arena_.array<unsigned char>(fieldStoreBytes(shape), "kept field coefficients");
+        f.phi_records = arena_.array<int>(fieldRecordInts(shape), "kept field coefficient records");
         task(tc_invx_.task[0], tc_m1_, tc_sxwt_, ny, nx, nx, kTcField);
         tc_invx_.task[0].kb_exp_a = f.m1_exp;
         tc_invx_.task[0].exp_b = &sc->exp_basis[kSxwt];
@@ -496,9 +498,10 @@ void Engine::setStallProbe(long long polls) {
 }
 
 const char* kernelKindName(int kind) {
-    static const char* names[kKindCount] = {"scatter", "wirelength", "metrics",        "dct_forward",
-                                            "dct_inverse", "gather", "reduce", "vector", "dct_split",
-                                            "rudy", "field_forward", "field_gradient"};
+    static const char* names[kKindCount] = {"scatter",     "wirelength",     "metrics",       "dct_forward",
+                                            "dct_inverse", "gather",         "reduce",        "vector",
+                                            "dct_split",   "rudy",           "field_forward", "field_gradient",
+                                            "field_inverse"};
     return kind >= 0 && kind < kKindCount ? names[kind] : "unknown";
 }
 
@@ -573,10 +576,13 @@ void Engine::runDct(bool gradient, bool potential, bool forward, bool split_sour
             launches_ += 1;
         }
         // Without the forward flag (the density is that of the previous evaluation) the
-        // banded launch recomputes the forward passes, which give the same bits.
+        // banded launch runs only the inverse passes, from the coefficients the previous
+        // evaluation's launch kept.
         if (forward || gradient) {
-            beginKernel(gradient ? kKindFieldGradient : kKindFieldForward);
-            launchField(field_band_, gradient ? 1 : 0, stream_);
+            const FieldMode mode = forward ? (gradient ? kFieldGradient : kFieldForward) : kFieldInverse;
+            beginKernel(mode == kFieldForward ? kKindFieldForward
+                                              : (mode == kFieldGradient ? kKindFieldGradient : kKindFieldInverse));
+            launchField(field_band_, mode, stream_);
             endKernel();
             launches_ += 1;
         }

@@ -132,6 +132,7 @@ enum KernelKind : int {
     kKindRudy,
     kKindFieldForward,   // the banded field solve without the inverse passes
     kKindFieldGradient,  // the banded field solve with them
+    kKindFieldInverse,   // the banded field solve's inverse passes alone
     kKindCount
 };
 const char* kernelKindName(int kind);

@@ -110,12 +110,13 @@ __device__ __forceinline__ void writeGathered(unsigned char* gathered, int i, in
     }
 }
 
-// One CTA of the cluster of band `band`; `local_block` indexes its energy partial.
-// The caller has released its successor.
+// One CTA of the cluster of band `band` in mode `mode` (FieldMode); `local_block`
+// indexes its energy partial.  The caller has released its successor.
 template <int N>
-__device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int gradient, int local_block) {
+__device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int mode, int local_block) {
     constexpr int kBTile = kSplit * N * kBlockK * 2;
     constexpr uint32_t kDescriptor = instrDescriptor(N);
+    constexpr uint32_t kPairDescriptor = instrDescriptor(2 * N);  // A x [B_hi; B_lo]: main and first correction
     constexpr uint32_t kTmemColumns = 4 * N < 32 ? 32 : 4 * N;
     const FieldShape& shape = f.shape;
     if (f.stall_polls > 0) {
@@ -144,8 +145,26 @@ __device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int grad
     const int lane = threadIdx.x & 31;
     const int s1 = (f.nx + kBlockK - 1) / kBlockK;  // pass 0 K-blocks (x)
     const int s2 = 2 * row_blocks;                   // pass 1-3 K-blocks (y, ky)
-    const int steps = s1 + s2 + (gradient ? 2 * s2 : 0);
+    const bool forward = mode != kFieldInverse;
+    const bool gradient = mode != kFieldForward;
+    // Ring steps: pass 0 (s1 K-blocks), then s2 per later pass; an inverse launch starts at pass 2.
+    const int steps = forward ? s1 + s2 + (gradient ? 2 * s2 : 0) : 2 * s2;
+    const int pass1_step = forward ? s1 : -1;
+    const int pass2_step = forward ? s1 + s2 : 0;
+    const auto decode = [&](int step, int& pass, int& kb) {
+        if (forward && step < s1) {
+            pass = 0;
+            kb = step;
+            return;
+        }
+        const int t = forward ? step - s1 : step + s2;
+        pass = 1 + t / s2;
+        kb = t % s2;
+    };
     const uint32_t push_bytes = static_cast<uint32_t>(2 * kBTile);
+    // This share's slot of the kept phi_hat^T and of its records.
+    unsigned char* const store = f.phi_store + static_cast<size_t>(band * shares + h) * s2 * kBTile;
+    int* const store_records = f.phi_records + static_cast<size_t>(band * shares + h) * row_blocks * 4;
 
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -180,43 +199,72 @@ __device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int grad
         const uint32_t incoming = static_cast<uint32_t>(row_blocks - 1) * (push_bytes + 16);
         mbarInit(received_q, 5);
         mbarExpectTx(received_q, incoming);
-        mbarInit(received_phi, 5);
-        mbarExpectTx(received_phi, incoming);
+        if (forward) {
+            mbarInit(received_phi, 5);
+            mbarExpectTx(received_phi, incoming);
+        } else {
+            mbarInit(received_phi, 1);  // the loader's arrival with the kept operand's bytes
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncthreads();
     clusterArrive();  // this CTA's barriers are initialised; peers wait for it before sending
 
-    // The first ring stages' basis tiles do not depend on the previous kernels.
-    const int prefetched = min(kFieldStages, s1);
+    // The first ring stages' basis tiles do not depend on the previous kernels: Cx
+    // (pass 0's B) for a forward launch, Dy (pass 2's A, whole stages) for an inverse one.
+    const int prefetched = min(kFieldStages, forward ? s1 : s2);
     if (warp == 0 && lane == 0) {
         for (int step = 0; step < prefetched; ++step) {
-            unsigned char* stage = smem + step * kFieldStageBytes;
-            mbarExpectTx(full0 + 8 * step, static_cast<uint32_t>(kATileBytes + kBTile));
-            for (int p = 0; p < kSplit; ++p) {
-                tmaLoad3d(smemAddress(stage + kATileBytes + p * N * 128), &f.map_cx, full0 + 8 * step,
-                          step * kBlockK, kx0, p);
+            const uint32_t stage = smemAddress(smem + step * kFieldStageBytes);
+            if (forward) {
+                mbarExpectTx(full0 + 8 * step, static_cast<uint32_t>(kATileBytes + kBTile));
+                tmaLoad3d(stage + kATileBytes, &f.map_cx, full0 + 8 * step, step * kBlockK, kx0, 0);
+            } else {
+                mbarExpectTx(full0 + 8 * step, static_cast<uint32_t>(kATileBytes));
+                tmaLoad3d(stage, &f.map_dy, full0 + 8 * step, step * kBlockK, i * kTileM, 0);
             }
         }
     }
-    // The spectral scale of each epilogue thread's row (a fixed table), staged in shared memory.
+    // The spectral scale of each epilogue thread's row (a fixed table), staged in shared
+    // memory: epilogue warp q loads rows 32 q .. 32 q + 31 of the tile, a row per
+    // 32 / N-lane group and pass, and reads back only its own rows.
     const int quarter = warp & 3;
     const int r = quarter * 32 + lane;
     const int row = i * kTileM + r;
     float* scale = reinterpret_cast<float*>(smem + kScaleOffset) + r * kScalePitch;
     if (warp >= 2) {
-#pragma unroll 8
-        for (int j = 0; j < N; ++j) {
-            scale[j] = row < f.ny && kx0 + j < f.nx ? __ldg(f.scale + static_cast<size_t>(row) * f.nx + kx0 + j) : 0.0f;
+        constexpr int kRowsPerPass = 32 / N;
+        const int j = lane % N;
+        const int kx = kx0 + j;
+        float v[32 / kRowsPerPass];
+#pragma unroll
+        for (int k = 0; k < 32 / kRowsPerPass; ++k) {
+            const int rr = k * kRowsPerPass + lane / N;
+            const int grow = i * kTileM + quarter * 32 + rr;
+            v[k] = grow < f.ny && kx < f.nx ? __ldg(f.scale + static_cast<size_t>(grow) * f.nx + kx) : 0.0f;
         }
+        float* tile = reinterpret_cast<float*>(smem + kScaleOffset);
+#pragma unroll
+        for (int k = 0; k < 32 / kRowsPerPass; ++k) {
+            const int rr = k * kRowsPerPass + lane / N;
+            tile[(quarter * 32 + rr) * kScalePitch + j] = v[k];
+        }
+        __syncwarp();
     }
     waitForPrior();  // the source planes and their row exponents come from the previous kernels
     clusterWait();
-    if (gradient && warp < 2) clusterArrive();  // the second cluster barrier: see the spectral epilogue
+    if (forward && gradient && warp < 2) clusterArrive();  // the second cluster barrier: see the spectral epilogue
 
     if (warp == 0) {
         if (lane == 0) {
+            if (!forward) {
+                // The kept phi_hat^T of this share (every row block's K-blocks) and its records.
+                mbarExpectTx(received_phi, static_cast<uint32_t>(s2 * kBTile + row_blocks * 16));
+                bulkFromGlobal(gathered_s, store, static_cast<uint32_t>(s2 * kBTile), received_phi);
+                bulkFromGlobal(records_s + 16 * kMaxRowBlocks, store_records, static_cast<uint32_t>(row_blocks * 16),
+                               received_phi);
+            }
             bool ok = true;
             int issued = 0;
             for (int step = 0; step < steps && ok; ++step) {
@@ -225,24 +273,19 @@ __device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int grad
                 if (!ok) break;
                 const uint32_t stage = smemAddress(smem + slot * kFieldStageBytes);
                 const uint32_t full = full0 + 8 * slot;
-                if (step < s1) {
-                    if (step >= prefetched) {
+                const bool early = step < prefetched;  // its basis tile is already on the way
+                int pass, kb;
+                decode(step, pass, kb);
+                if (pass == 0) {
+                    if (!early) {
                         mbarExpectTx(full, static_cast<uint32_t>(kATileBytes + kBTile));
-                        for (int p = 0; p < kSplit; ++p) {
-                            tmaLoad3d(stage + kATileBytes + p * N * 128, &f.map_cx, full, step * kBlockK, kx0, p);
-                        }
+                        tmaLoad3d(stage + kATileBytes, &f.map_cx, full, step * kBlockK, kx0, 0);
                     }
-                    for (int p = 0; p < kSplit; ++p) {
-                        tmaLoad3d(stage + p * kAPlaneBytes, &f.map_s, full, step * kBlockK, i * kTileM, p);
-                    }
-                } else {
-                    const int pass = step < s1 + s2 ? 1 : (step < s1 + 2 * s2 ? 2 : 3);
-                    const int kb = (step - s1) % s2;
+                    tmaLoad3d(stage, &f.map_s, full, step * kBlockK, i * kTileM, 0);
+                } else if (!early) {
                     const CUtensorMap* map = pass == 1 ? &f.map_cy : (pass == 2 ? &f.map_dy : &f.map_syw);
                     mbarExpectTx(full, static_cast<uint32_t>(kATileBytes));
-                    for (int p = 0; p < kSplit; ++p) {
-                        tmaLoad3d(stage + p * kAPlaneBytes, map, full, kb * kBlockK, i * kTileM, p);
-                    }
+                    tmaLoad3d(stage, map, full, kb * kBlockK, i * kTileM, 0);
                 }
                 issued = step + 1;
             }
@@ -263,31 +306,46 @@ __device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int grad
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tmem_slot);
         if (lane == 0) {
+            // A partial covers a pair of K-blocks (2 p, 2 p + 1) of a pass: one producer's
+            // tile of a gathered operand, so one exponent.
+            int partial = 0;
             for (int step = 0; step < steps; ++step) {
                 const int slot = step % kFieldStages;
-                const int buffer = step & 1;
-                if (step >= 2 && !mbarWait(consumed0 + 8 * buffer, ((step >> 1) - 1) & 1, f.error_flag)) break;
+                int pass, kb;
+                decode(step, pass, kb);
+                const int count = pass == 0 ? s1 : s2;
+                const bool opens = (kb & 1) == 0;
+                const bool closes = (kb & 1) == 1 || kb == count - 1;
+                const int buffer = partial & 1;
+                if (opens && partial >= 2 &&
+                    !mbarWait(consumed0 + 8 * buffer, ((partial >> 1) - 1) & 1, f.error_flag)) {
+                    break;
+                }
                 if (!mbarWait(full0 + 8 * slot, (step / kFieldStages) & 1, f.error_flag)) break;
-                if (step == s1 && !mbarWait(received_q, 0, f.error_flag)) break;
-                if (step == s1 + s2 && !mbarWait(received_phi, 0, f.error_flag)) break;
+                if (step == pass1_step && !mbarWait(received_q, 0, f.error_flag)) break;
+                if (step == pass2_step && !mbarWait(received_phi, 0, f.error_flag)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t a_base = smemAddress(smem + slot * kFieldStageBytes);
-                const uint32_t b_base = step < s1 ? a_base + kATileBytes
-                                                  : gathered_s + static_cast<uint32_t>(((step - s1) % s2) * kBTile);
+                const uint32_t b_base = pass == 0 ? a_base + kATileBytes : gathered_s + static_cast<uint32_t>(kb * kBTile);
                 const uint32_t main_acc = tmem + static_cast<uint32_t>(buffer * 2 * N);
                 const uint32_t corr_acc = main_acc + N;
 #pragma unroll
                 for (int kk = 0; kk < kBlockK / 16; ++kk) {
+                    // The B tile's planes are consecutive rows, [B_hi; B_lo], so one product of
+                    // A_hi with both (2N columns) writes main and the first correction term
+                    // (corr_acc follows main_acc); A_lo B_hi completes the correction.
                     const uint64_t a_hi = smemDescriptor(a_base + kk * 32);
                     const uint64_t a_lo = smemDescriptor(a_base + kAPlaneBytes + kk * 32);
-                    const uint64_t b_hi = smemDescriptor(b_base + kk * 32);
-                    const uint64_t b_lo = smemDescriptor(b_base + N * 128 + kk * 32);
-                    ummaF16(corr_acc, a_hi, b_lo, kDescriptor, kk > 0 ? 1u : 0u);
-                    ummaF16(corr_acc, a_lo, b_hi, kDescriptor, 1u);
-                    ummaF16(main_acc, a_hi, b_hi, kDescriptor, kk > 0 ? 1u : 0u);
+                    const uint64_t b_both = smemDescriptor(b_base + kk * 32);
+                    const uint32_t accumulate = kk > 0 || !opens ? 1u : 0u;
+                    ummaF16(main_acc, a_hi, b_both, kPairDescriptor, accumulate);
+                    ummaF16(corr_acc, a_lo, b_both, kDescriptor, 1u);
                 }
                 ummaCommit(empty0 + 8 * slot);
-                ummaCommit(partial0 + 8 * buffer);
+                if (closes) {
+                    ummaCommit(partial0 + 8 * buffer);
+                    ++partial;
+                }
             }
         }
         __syncwarp();
@@ -302,11 +360,18 @@ __device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int grad
         const int exp_row = row_in ? f.row_exp[row] : 0;
         float top_phi = 0.0f;
         int exp_m1 = 0, exp_m2 = 0;
+        if (!forward) {
+            // The band's maximum |phi_hat| from the records the forward launch kept.
+            const int* band_records = f.phi_records + static_cast<size_t>(band) * shares * row_blocks * 4;
+            float band_top = 0.0f;
+            for (int k = 0; k < shares * row_blocks; ++k) band_top = fmaxf(band_top, __int_as_float(band_records[k * 4 + 1]));
+            exp_m1 = planeExponentOf(band_top * f.gain_dy);
+            exp_m2 = planeExponentOf(band_top * f.gain_syw);
+        }
         bool ok = true;
-        int step = 0;
-        const int passes = gradient ? 4 : 2;
+        int partial = 0;
 #pragma unroll 1
-        for (int pass = 0; pass < passes; ++pass) {
+        for (int pass = forward ? 0 : 2; pass < (gradient ? 4 : 2); ++pass) {
             double acc[N];
 #pragma unroll
             for (int j = 0; j < N; ++j) acc[j] = 0.0;
@@ -318,14 +383,15 @@ __device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int grad
                 ok = ok && got;
             }
             const int* exps = records + (pass == 1 ? 0 : kMaxRowBlocks * 4);
-            const int count = pass == 0 ? s1 : s2;
-            for (int kb = 0; kb < count; ++kb, ++step) {
+            const int pairs = ((pass == 0 ? s1 : s2) + 1) / 2;
+            for (int pair = 0; pair < pairs; ++pair, ++partial) {
                 if (!ok) continue;
-                const int buffer = step & 1;
-                ok = __all_sync(0xffffffffu, mbarWait(partial0 + 8 * buffer, (step >> 1) & 1, f.error_flag) ? 1 : 0) != 0;
+                const int buffer = partial & 1;
+                ok = __all_sync(0xffffffffu, mbarWait(partial0 + 8 * buffer, (partial >> 1) & 1, f.error_flag) ? 1 : 0) !=
+                     0;
                 if (!ok) continue;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const double k_scale = pass == 0 ? 1.0 : pow2(exps[(kb >> 1) * 4]);
+                const double k_scale = pass == 0 ? 1.0 : pow2(exps[pair * 4]);
 #pragma unroll
                 for (int c0 = 0; c0 < N; c0 += 16) {
                     uint32_t main_part[16], corr_part[16];
@@ -334,10 +400,11 @@ __device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int grad
                     tmemWait(main_part, corr_part);
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
-                        const double part = static_cast<double>(__uint_as_float(main_part[j])) +
-                                            static_cast<double>(__uint_as_float(corr_part[j])) *
-                                                (1.0 / static_cast<double>(kLoShift));
-                        acc[c0 + j] += part * k_scale;
+                        // main + 2^-11 corr rounds once in FP32 (the product is exact), then
+                        // joins the FP64 sum with the producer's scale (a power of two).
+                        const float part = __fmaf_rn(__uint_as_float(corr_part[j]), 1.0f / kLoShift,
+                                                     __uint_as_float(main_part[j]));
+                        acc[c0 + j] = __fma_rn(static_cast<double>(part), k_scale, acc[c0 + j]);
                     }
                 }
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -398,8 +465,8 @@ __device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int grad
                 if (et == 0 && f.energy_partials != nullptr) {
                     f.energy_partials[local_block] = ((reduce_d[0] + reduce_d[1]) + reduce_d[2]) + reduce_d[3];
                 }
+                top_phi = epilogueMax(top_phi, reduce_f + 4, quarter);
                 if (gradient) {
-                    top_phi = epilogueMax(top_phi, reduce_f + 4, quarter);
                     if (et == 0) {
                         // This tile's max |phi_hat| to every CTA of the cluster: the band's maximum
                         // bounds M1 and M2, whose planes share one exponent per band.
@@ -410,18 +477,31 @@ __device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int grad
                     // Every CTA's pass-1 operand reads are complete (its last partial is in):
                     // from now on the peers may overwrite its gathered operand.
                     clusterArrive();
-                    const int e = planeExponentOf(top_phi);
-                    writeGathered<N>(gathered, i, r, phi, static_cast<float>(pow2(-e)));
-                    if (et == 0) records[kMaxRowBlocks * 4 + i * 4] = e;
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    __syncwarp();
-                    if (lane == 0) mbarArrive(received_phi);
+                }
+                // phi_hat^T into the gathered operand (its own K-blocks), and kept in global
+                // memory with its exponent and maximum for a later inverse launch.
+                const int e = planeExponentOf(top_phi);
+                writeGathered<N>(gathered, i, r, phi, static_cast<float>(pow2(-e)));
+                if (et == 0) {
+                    records[kMaxRowBlocks * 4 + i * 4] = e;
+                    records[kMaxRowBlocks * 4 + i * 4 + 1] = __float_as_int(top_phi);
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (gradient && lane == 0) mbarArrive(received_phi);
+                epilogueSync();
+                if (et == 0) {
+                    const uint32_t own = gathered_s + static_cast<uint32_t>(2 * i * kBTile);
+                    bulkToGlobal(store + static_cast<size_t>(2 * i) * kBTile, own, push_bytes);
+                    bulkToGlobal(store_records + i * 4, records_s + static_cast<uint32_t>(16 * (kMaxRowBlocks + i)), 16);
+                    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                }
+                if (gradient) {
                     clusterWait();
                     float band_top = 0.0f;
                     for (int peer = 0; peer < shape.cluster; ++peer) band_top = fmaxf(band_top, phi_max[peer]);
                     exp_m1 = planeExponentOf(band_top * f.gain_dy);
                     exp_m2 = planeExponentOf(band_top * f.gain_syw);
-                    epilogueSync();
                     if (et == 0 && row_blocks > 1) {
                         const uint32_t src = gathered_s + static_cast<uint32_t>(2 * i * kBTile);
                         const uint32_t record = records_s + static_cast<uint32_t>(16 * (kMaxRowBlocks + i));
@@ -456,7 +536,9 @@ __device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int grad
             }
         }
     }
-    if (gradient && warp < 2) clusterWait();
+    if (forward && gradient && warp < 2) clusterWait();
+    // The kept phi_hat^T has reached global memory before the grid completes.
+    if (threadIdx.x == 64) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     if (local_block == 0 && threadIdx.x == 0 && f.clear != nullptr) *f.clear = 0u;
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -467,10 +549,10 @@ __device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int grad
 }
 
 template <int N>
-__global__ void __launch_bounds__(kFieldThreads, 1) fieldKernel(const __grid_constant__ FieldBand band, int gradient) {
+__global__ void __launch_bounds__(kFieldThreads, 1) fieldKernel(const __grid_constant__ FieldBand band, int mode) {
     releaseNext();
     const int cluster = band.shape.cluster;
-    fieldBand<N>(band, static_cast<int>(blockIdx.x) / cluster, gradient, static_cast<int>(blockIdx.x));
+    fieldBand<N>(band, static_cast<int>(blockIdx.x) / cluster, mode, static_cast<int>(blockIdx.x));
 }
 
 // Batched: cluster c computes band items[c].band of the grid items[c].field (a
@@ -487,7 +569,7 @@ __global__ void __launch_bounds__(kFieldThreads, 1) fieldBatchKernel(const Field
             asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
         }
     }
-    fieldBand<N>(band, item.band, item.gradient,
+    fieldBand<N>(band, item.band, item.mode,
                  item.band * cluster + static_cast<int>(blockIdx.x % static_cast<unsigned>(cluster)));
 }
 
@@ -535,11 +617,11 @@ void checkShape(const FieldShape& s) {
 }
 
 template <int N>
-void launchFieldN(const FieldBand& band, int gradient, cudaStream_t stream) {
+void launchFieldN(const FieldBand& band, int mode, cudaStream_t stream) {
     configureField<N>();
     cudaLaunchAttribute attribute[2] = {};
     const cudaLaunchConfig_t config = fieldConfig(band.shape.blocks(), band.shape.cluster, stream, attribute);
-    checkCuda(cudaLaunchKernelEx(&config, fieldKernel<N>, band, gradient), "Launch the banded field kernel");
+    checkCuda(cudaLaunchKernelEx(&config, fieldKernel<N>, band, mode), "Launch the banded field kernel");
 }
 
 template <int N>
@@ -563,12 +645,22 @@ FieldShape fieldShape(int nx, int ny) {
     return s;
 }
 
-void launchField(const FieldBand& band, int gradient, cudaStream_t stream) {
+size_t fieldStoreBytes(const FieldShape& shape) {
+    // Per band and share: 2 m_blocks K-blocks of share_n x 64 halves, both planes.
+    return static_cast<size_t>(shape.bands) * shape.shares * 2 * shape.m_blocks * kSplit * shape.share_n * kBlockK * 2;
+}
+
+size_t fieldRecordInts(const FieldShape& shape) {
+    return static_cast<size_t>(shape.bands) * shape.shares * shape.m_blocks * 4;
+}
+
+void launchField(const FieldBand& band, FieldMode mode, cudaStream_t stream) {
     checkShape(band.shape);
+    require(band.phi_store != nullptr && band.phi_records != nullptr, "The banded field solve needs its phi_hat store.");
     if (band.shape.share_n == 16) {
-        launchFieldN<16>(band, gradient, stream);
+        launchFieldN<16>(band, mode, stream);
     } else {
-        launchFieldN<32>(band, gradient, stream);
+        launchFieldN<32>(band, mode, stream);
     }
 }
 

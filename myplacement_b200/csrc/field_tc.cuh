@@ -28,6 +28,13 @@ struct FieldShape {
 // The banded solve's shape for an nx x ny grid (cluster 0 beyond kFieldMaxRows x kFieldMaxColumns).
 FieldShape fieldShape(int nx, int ny);
 
+// What a banded launch runs.
+enum FieldMode : int {
+    kFieldForward = 0,   // passes 0-1: phi_hat (kept in phi_store) and the energy partials
+    kFieldGradient = 1,  // passes 0-3: also M1 and M2
+    kFieldInverse = 2,   // passes 2-3 only, from the phi_hat the last forward launch kept
+};
+
 // One grid's banded solve.  With S the split source (ny x nx), Cx, Cy the DCT-II
 // bases, Dy the DCT-III basis and Syw the wave-number-weighted DST-III basis along
 // y (dct_tc.cuh), the cluster of band b computes for kx in b:
@@ -52,6 +59,11 @@ struct alignas(64) FieldBand {
     size_t m_plane = 0;
     int* m1_exp = nullptr;
     int* m2_exp = nullptr;
+    // phi_hat^T of the last forward launch, per band and share in the layout the
+    // inverse passes read it in (fieldStoreBytes), and per producing CTA its plane
+    // exponent and tile maximum ([band][share][row block][4] ints).
+    unsigned char* phi_store = nullptr;
+    int* phi_records = nullptr;
     float gain_dy = 0.0f;   // bounds |Dy x| <= gain_dy max |x| (row L1 norm with a margin)
     float gain_syw = 0.0f;
     unsigned* clear = nullptr;  // a magnitude block 0 zeroes (chain bookkeeping), or null
@@ -60,14 +72,18 @@ struct alignas(64) FieldBand {
     long long stall_polls = 0;
 };
 
-void launchField(const FieldBand& band, int gradient, cudaStream_t stream);
+// Bytes of FieldBand::phi_store and ints of FieldBand::phi_records for a shape.
+size_t fieldStoreBytes(const FieldShape& shape);
+size_t fieldRecordInts(const FieldShape& shape);
+
+void launchField(const FieldBand& band, FieldMode mode, cudaStream_t stream);
 
 // One cluster's work in a batched launch: band `band` of the grid `field` (a
-// FieldBand in device memory), with or without the inverse passes.
+// FieldBand in device memory) in mode `mode` (a FieldMode).
 struct FieldItem {
     const FieldBand* field;
     int band;
-    int gradient;
+    int mode;
 };
 // Launches `count` items, all of grids of one shape's cluster size and share
 // width (`shape`), from device memory.

@@ -92,6 +92,19 @@ __device__ __forceinline__ void bulkToPeer(uint32_t dst, uint32_t src, uint32_t 
         : "memory");
 }
 
+// Bulk copy of `bytes` from global memory into this CTA's shared memory (completion on `bar`).
+__device__ __forceinline__ void bulkFromGlobal(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// Bulk copy of `bytes` from this CTA's shared memory to global memory (bulk async group).
+__device__ __forceinline__ void bulkToGlobal(void* dst, uint32_t src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes)
+                 : "memory");
+}
+
 // UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
 __device__ __forceinline__ uint64_t smemDescriptor(uint32_t address) {
     return static_cast<uint64_t>((address >> 4) & 0x3FFFu) | (1ull << 16) | (64ull << 32) | (1ull << 46) |
