@@ -427,9 +427,13 @@ void Engine::buildTensorCoreBasis(double max_scale) {
     // The banded solve (field_tc.cu): Q = S Cx^T, rho_hat = Cy Q, phi_hat, M1 = Dy phi_hat and
     // M2 = Syw phi_hat per band of spectral columns, then Ex = M1 (Sx diag(kx))^T,
     // Ey = M2 Dx^T and the potential M1 Dx^T over all bands.
-    // MPGP_FIELD_SOLVE=staged keeps the four-launch solve on every grid.
+    // The banded solve for grids taller than kFieldBandedMinRows rows (up to its limits);
+    // MPGP_FIELD_SOLVE=staged or =banded chooses for every grid the banded solve takes.
     const char* solve = std::getenv("MPGP_FIELD_SOLVE");
-    const FieldShape shape = solve != nullptr && std::strcmp(solve, "staged") == 0 ? FieldShape{} : fieldShape(nx, ny);
+    bool banded = ny > kFieldBandedMinRows;
+    if (solve != nullptr && std::strcmp(solve, "staged") == 0) banded = false;
+    if (solve != nullptr && std::strcmp(solve, "banded") == 0) banded = true;
+    const FieldShape shape = banded ? fieldShape(nx, ny) : FieldShape{};
     banded_ = shape.cluster > 0;
     if (banded_) {
         tc_m1_ = newSplit(ny, nx, "banded field planes");

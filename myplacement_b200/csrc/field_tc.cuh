@@ -16,6 +16,10 @@ namespace mpgp {
 constexpr int kFieldMaxRows = 512;
 // The widest: the inverse along x carries one exponent per band (kMaxKbExponents).
 constexpr int kFieldMaxColumns = kBlockK * kMaxKbExponents;
+// By default only grids taller than this take the banded solve: on smaller grids its
+// clusters hold whole SMs for little work, and batched rounds of many small
+// placements ran faster with the staged solve.
+constexpr int kFieldBandedMinRows = 256;
 
 struct FieldShape {
     int m_blocks = 0;  // 128-row blocks of the y range

@@ -108,3 +108,29 @@ def test_server_needs_a_gpu():
         pytest.skip("a GPU is present")
     with pytest.raises(mp.EngineError):
         mp.PlacementServer(device=0, workers=2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("solve", ["default", "banded"])
+def test_batched_banded_field_solve_matches_plain(gpu, monkeypatch, solve):
+    """Grids taller than 256 rows take the banded field solve: in a batched round one
+    launch per cluster shape, and inverse-only launches for the evaluations that reuse
+    the last density.  With MPGP_FIELD_SOLVE=banded the small grids take it too (clusters
+    of four and eight CTAs of 16 columns).  Batched results equal the plain runs."""
+    if solve == "banded":
+        monkeypatch.setenv("MPGP_FIELD_SOLVE", "banded")
+    else:
+        monkeypatch.delenv("MPGP_FIELD_SOLVE", raising=False)
+    jobs = []
+    for cells, bins, seed in ((2500, 320, 81), (1800, 448, 82), (1200, 64, 83), (3000, 128, 84), (2200, 256, 85)):
+        design, _ = small_instance(cells, seed)
+        x, y = mp.random_placement(design, seed)
+        design = design.copy_with_positions(x, y)
+        jobs.append((design, mp.default_options(bins_x=bins, bins_y=bins, target_density=0.9, iterations=30)))
+    placed, _, server_stats = mp.batch_place([d for d, _ in jobs], [o for _, o in jobs], workers=5, batched=True)
+    assert server_stats["completed"] == len(jobs)
+    for (design, options), result in zip(jobs, placed):
+        reference = mp.GlobalPlacer().run(design, options)
+        np.testing.assert_array_equal(result.module_x, reference.module_x)
+        np.testing.assert_array_equal(result.module_y, reference.module_y)
+        assert result.hpwl_after == reference.hpwl_after
