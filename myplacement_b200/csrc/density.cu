@@ -18,6 +18,8 @@
 // (Metrics.cpp:101-119), reads-and-clears the fixed-point layers and writes the
 // mean-free FP32 source of the Poisson solve (ElectrostaticField.cpp:119-133);
 // the mean comes from the exact integer layer totals of the scatter.
+#include <algorithm>
+
 #include "common.cuh"
 #include "dct_tc.cuh"
 #include "kernels.cuh"
@@ -386,6 +388,15 @@ __global__ void velocityKernel(const double2* next, const double2* previous, dou
     velocity[i] = make_double2(n.x - p.x, n.y - p.y);
 }
 
+// Copies `count` positions (a checkpoint of the controller's placement).
+__global__ void copyPositionsKernel(const double2* source, double2* destination, int count) {
+    releaseNext();
+    waitForPrior();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        destination[i] = source[i];
+    }
+}
+
 }  // namespace
 
 void launchScatter(const ScatterArgs& args, int blocks, cudaStream_t stream) {
@@ -414,6 +425,16 @@ void launchMetricsSplitBatch(const MetricsArgs* args, const int* offsets, int co
     if (blocks <= 0 || count <= 0) return;
     launchChained("Launch the batched density metrics and source split", metricsSplitBatchKernel, dim3(blocks),
                   dim3(kThreads), 0, stream, args, offsets, count);
+}
+
+void launchCopyPositions(const double2* source, double2* destination, int count, cudaStream_t stream) {
+    if (count <= 0) return;
+    int device = 0, sms = 0;
+    checkCuda(cudaGetDevice(&device), "Query the current device");
+    checkCuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "Query the SM count");
+    const int blocks = std::max(1, std::min(ceilDiv(count, kThreads), 4 * sms));
+    launchChained("Launch the checkpoint copy", copyPositionsKernel, dim3(blocks), dim3(kThreads), 0, stream, source,
+                  destination, count);
 }
 
 void launchVelocity(const double2* next, const double2* previous, double2* velocity, int count, cudaStream_t stream) {

@@ -280,6 +280,8 @@ void launchGatherBatch(const GatherArgs* args, const ReduceArgs* const* reduces,
 int gatherBlocks(int particle_count);
 
 // ---- small vector kernels ---------------------------------------------------------
+// A device-to-device copy of positions as a chained kernel (programmatic launch, no copy engine).
+void launchCopyPositions(const double2* source, double2* destination, int count, cudaStream_t stream);
 void launchVelocity(const double2* next, const double2* previous, double2* velocity, int count,
                     cudaStream_t stream);
 

@@ -362,12 +362,10 @@ void Session::considerCheckpoint(double2* positions, const ObjectiveMetrics& m, 
     const double overflow = m.design.normalized_overflow;
     const bool feasible = overflow <= options_.maximum_bin_overflow;
     const double score = m.hpwl + rudy_target_weight_ * m.rudy_energy;
-    const std::size_t bytes = sizeof(double2) * static_cast<std::size_t>(engine_->particleCount());
     if (feasible && (!best_feasible_.found || score < best_feasible_.selection_score - 1e-10 ||
                      (std::abs(score - best_feasible_.selection_score) <= 1e-10 && m.hpwl < best_feasible_.hpwl))) {
-        checkCuda(cudaMemcpyAsync(best_feasible_.positions, positions, bytes, cudaMemcpyDeviceToDevice,
-                                  engine_->stream()),
-                  "Store checkpoint");
+        launchCopyPositions(positions, best_feasible_.positions, static_cast<int>(engine_->particleCount()), engine_->stream());
+        engine_->countLaunches(1);
         best_feasible_.iteration = iteration;
         best_feasible_.hpwl = m.hpwl;
         best_feasible_.overflow = overflow;
@@ -379,9 +377,8 @@ void Session::considerCheckpoint(double2* positions, const ObjectiveMetrics& m, 
     if (!best_feasible_.found &&
         (!best_fallback_.found || overflow < best_fallback_.overflow - 1e-12 ||
          (std::abs(overflow - best_fallback_.overflow) <= 1e-12 && m.hpwl < best_fallback_.hpwl))) {
-        checkCuda(cudaMemcpyAsync(best_fallback_.positions, positions, bytes, cudaMemcpyDeviceToDevice,
-                                  engine_->stream()),
-                  "Store checkpoint");
+        launchCopyPositions(positions, best_fallback_.positions, static_cast<int>(engine_->particleCount()), engine_->stream());
+        engine_->countLaunches(1);
         best_fallback_.iteration = iteration;
         best_fallback_.hpwl = m.hpwl;
         best_fallback_.overflow = overflow;
