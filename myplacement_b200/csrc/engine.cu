@@ -571,38 +571,51 @@ void Engine::allocateGroups() {
 }
 
 void Engine::runDct(bool gradient, bool potential, bool forward, bool split_source) {
-    const int nx = bins_x_;
     if (banded_) {
-        if (forward && split_source) {
-            beginKernel(kKindDctSplit);
-            launchSplitSource(source_, tc_source_, nx, tc_row_exp_, tc_scales_, stream_);
-            endKernel();
-            launches_ += 1;
-        }
-        // Without the forward flag (the density is that of the previous evaluation) the
-        // banded launch runs only the inverse passes, from the coefficients the previous
-        // evaluation's launch kept.
-        if (forward || gradient) {
-            const FieldMode mode = forward ? (gradient ? kFieldGradient : kFieldForward) : kFieldInverse;
-            beginKernel(mode == kFieldForward ? kKindFieldForward
-                                              : (mode == kFieldGradient ? kKindFieldGradient : kKindFieldInverse));
-            launchField(field_band_, mode, stream_);
-            endKernel();
-            launches_ += 1;
-        }
-        if (!gradient) return;
-        beginKernel(kKindDctInverse);
-        launchTcGemm(tc_invx_, 2, stream_);
-        endKernel();
-        launches_ += 1;
-        if (potential) {
-            beginKernel(kKindDctInverse);
-            launchTcGemm(tc_potx_, 1, stream_);
-            endKernel();
-            launches_ += 1;
-        }
+        runBandedField(gradient, forward, split_source);
+        runBandedInverseX(gradient, potential);
         return;
     }
+    runStagedField(gradient, potential, forward, split_source);
+}
+
+void Engine::runBandedField(bool gradient, bool forward, bool split_source) {
+    const int nx = bins_x_;
+    if (forward && split_source) {
+        beginKernel(kKindDctSplit);
+        launchSplitSource(source_, tc_source_, nx, tc_row_exp_, tc_scales_, stream_);
+        endKernel();
+        launches_ += 1;
+    }
+    // Without the forward flag (the density is that of the previous evaluation) the
+    // banded launch runs only the inverse passes, from the coefficients the previous
+    // evaluation's launch kept.
+    if (forward || gradient) {
+        const FieldMode mode = forward ? (gradient ? kFieldGradient : kFieldForward) : kFieldInverse;
+        beginKernel(mode == kFieldForward ? kKindFieldForward
+                                          : (mode == kFieldGradient ? kKindFieldGradient : kKindFieldInverse));
+        launchField(field_band_, mode, stream_);
+        endKernel();
+        launches_ += 1;
+    }
+}
+
+void Engine::runBandedInverseX(bool gradient, bool potential) {
+    if (!gradient) return;
+    beginKernel(kKindDctInverse);
+    launchTcGemm(tc_invx_, 2, stream_);
+    endKernel();
+    launches_ += 1;
+    if (potential) {
+        beginKernel(kKindDctInverse);
+        launchTcGemm(tc_potx_, 1, stream_);
+        endKernel();
+        launches_ += 1;
+    }
+}
+
+void Engine::runStagedField(bool gradient, bool potential, bool forward, bool split_source) {
+    const int nx = bins_x_;
     if (forward) {
         if (split_source) {
             beginKernel(kKindDctSplit);
@@ -831,6 +844,43 @@ void Engine::run(const EvalPlan& p) {
         endKernel();
     }
     if (!p.fork_first) checkCuda(cudaEventRecord(fork_, stream_), "fork");
+    // With the banded field solve the wirelength pass is launched after the banded kernel:
+    // blocks start in launch order, and the banded kernel's clusters (whole SMs each)
+    // would otherwise wait for the wirelength pass's blocks to drain.
+    if (!banded_) runWirelengthPass(p);
+    if (p.metrics) {
+        beginKernel(kKindMetrics);
+        if (p.metrics_fused) {
+            launchMetricsSplit(p.metrics_args, stream_);
+        } else {
+            launchMetrics(p.metrics_args, p.metrics_blocks, stream_);
+        }
+        endKernel();
+    }
+    if (banded_) {
+        runBandedField(p.gradient, p.forward, p.split_source);
+        runWirelengthPass(p);
+        runBandedInverseX(p.gradient, p.potential);
+    } else {
+        runStagedField(p.gradient, p.potential, p.forward, p.split_source);
+    }
+    checkCuda(cudaStreamWaitEvent(stream_, join_, 0), "join");
+    if (p.gather) {
+        // The gather's last block also reduces and publishes the evaluation.
+        beginKernel(kKindGather);
+        launchGather(p.gather_args, &p.reduce_args, p.gather_blocks, stream_);
+        endKernel();
+    } else {
+        beginKernel(kKindReduce);
+        launchReduce(p.reduce_args, stream_);
+        endKernel();
+    }
+    launches_ += p.kernels;
+}
+
+// The wirelength stream's part of an evaluation (after the fork event): pin positions,
+// the wirelength pass and the RUDY kernels, then the join event.
+void Engine::runWirelengthPass(const EvalPlan& p) {
     checkCuda(cudaStreamWaitEvent(stream_wl_, fork_, 0), "fork");
     beginKernel(kKindWirelength, stream_wl_);
     if (p.pin_positions) launchPinPositions(p.pin_args, stream_wl_);
@@ -848,28 +898,6 @@ void Engine::run(const EvalPlan& p) {
         endKernel(stream_wl_);
     }
     checkCuda(cudaEventRecord(join_, stream_wl_), "join");
-    if (p.metrics) {
-        beginKernel(kKindMetrics);
-        if (p.metrics_fused) {
-            launchMetricsSplit(p.metrics_args, stream_);
-        } else {
-            launchMetrics(p.metrics_args, p.metrics_blocks, stream_);
-        }
-        endKernel();
-    }
-    runDct(p.gradient, p.potential, p.forward, p.split_source);
-    checkCuda(cudaStreamWaitEvent(stream_, join_, 0), "join");
-    if (p.gather) {
-        // The gather's last block also reduces and publishes the evaluation.
-        beginKernel(kKindGather);
-        launchGather(p.gather_args, &p.reduce_args, p.gather_blocks, stream_);
-        endKernel();
-    } else {
-        beginKernel(kKindReduce);
-        launchReduce(p.reduce_args, stream_);
-        endKernel();
-    }
-    launches_ += p.kernels;
 }
 
 void Engine::launch(const EvalRequest& q) {

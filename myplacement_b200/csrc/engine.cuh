@@ -258,6 +258,10 @@ private:
 
     void collectTimings();
     void runDct(bool gradient, bool potential, bool forward, bool split_source = true);
+    void runBandedField(bool gradient, bool forward, bool split_source);
+    void runBandedInverseX(bool gradient, bool potential);
+    void runStagedField(bool gradient, bool potential, bool forward, bool split_source);
+    void runWirelengthPass(const EvalPlan& p);
     void uploadStatic(const Problem& problem);
     void buildNetLayout(const Problem& problem);
     void buildBasis();
