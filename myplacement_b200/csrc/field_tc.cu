@@ -440,9 +440,12 @@ __device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int mode
                         bulkToPeer(clusterAddress(records_s + 16 * i, peer), records_s + 16 * i, 16, bar);
                     }
                     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-                    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
                 }
             } else if (pass == 1) {
+                // The copies of pass 0 have read this CTA's Q^T K-blocks long ago (their peers'
+                // pass 1 needed them); phi_hat^T overwrites them below, after the energy
+                // reduction's barrier orders every writer after this wait.
+                if (et == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
                 // rho_hat = Cy Q; phi_hat = rho_hat .* scale (ElectrostaticField.cpp:212-221);
                 // the Parseval energy sum_{ky,kx} w(ky) w(kx) phi_hat rho_hat.
                 float phi[N];
@@ -513,7 +516,6 @@ __device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int mode
                             bulkToPeer(clusterAddress(record, peer), record, 16, bar);
                         }
                         asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-                        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
                     }
                 }
             } else {
@@ -537,7 +539,8 @@ __device__ __forceinline__ void fieldBand(const FieldBand& f, int band, int mode
         }
     }
     if (forward && gradient && warp < 2) clusterWait();
-    // The kept phi_hat^T has reached global memory before the grid completes.
+    // Every bulk copy this CTA issued has read its source and written its destination
+    // (the kept phi_hat^T reaches global memory) before the grid completes.
     if (threadIdx.x == 64) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     if (local_block == 0 && threadIdx.x == 0 && f.clear != nullptr) *f.clear = 0u;
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
