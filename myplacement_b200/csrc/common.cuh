@@ -40,6 +40,12 @@ inline void require(bool condition, const char* message) {
     if (!condition) fail(MPGP_ERR_INVALID_ARGUMENT, message);
 }
 
+// The library's device-memory pool of `device` (created once per device): the
+// engines' arrays and set-up scratch are sub-allocated from it with stream-ordered
+// allocation, and memory a finished session frees stays in the pool for the next
+// session, instead of a cudaMalloc and cudaFree per array (each about 0.15 ms).
+cudaMemPool_t devicePool(int device);
+
 constexpr double kEpsilon = 1e-9;  // Geometry.hpp:8
 constexpr double kPi = 3.141592653589793238462643383279502884;
 constexpr int kThreads = 256;

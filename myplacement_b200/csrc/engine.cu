@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <atomic>
 #include <thread>
@@ -25,8 +26,44 @@
 
 namespace mpgp {
 
+cudaMemPool_t devicePool(int device) {
+    constexpr int kMaxDevices = 64;
+    static std::once_flag once[kMaxDevices];
+    static cudaMemPool_t pools[kMaxDevices] = {};
+    static cudaError_t status[kMaxDevices] = {};
+    require(device >= 0 && device < kMaxDevices, "Device index out of range.");
+    std::call_once(once[device], [device] {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        status[device] = cudaMemPoolCreate(&pools[device], &props);
+        if (status[device] == cudaSuccess) {
+            // Keep freed memory for the next session rather than returning it at every
+            // synchronisation.
+            uint64_t threshold = ~0ULL;
+            status[device] = cudaMemPoolSetAttribute(pools[device], cudaMemPoolAttrReleaseThreshold, &threshold);
+        }
+    });
+    checkCuda(status[device], "Create the device memory pool");
+    return pools[device];
+}
+
 DeviceArena::~DeviceArena() {
-    for (void* p : blocks_) cudaFree(p);
+    // The owner has synchronised every stream that used the arrays; the frees are
+    // ordered on the legacy stream, which waits for no other non-blocking stream.
+    for (void* p : blocks_) {
+        if (pool_ != nullptr) {
+            cudaFreeAsync(p, nullptr);
+        } else {
+            cudaFree(p);
+        }
+    }
+}
+
+void DeviceArena::bind(int device, cudaStream_t stream) {
+    pool_ = devicePool(device);
+    stream_ = stream;
 }
 
 void* DeviceArena::allocate(std::size_t bytes, const char* what) {
@@ -38,7 +75,11 @@ void* DeviceArena::allocate(std::size_t bytes, const char* what) {
                                   std::to_string(reserved_) + " bytes, limit " + std::to_string(limit_) + " bytes).");
     }
     void* p = nullptr;
-    checkCuda(cudaMalloc(&p, bytes), what);
+    if (pool_ != nullptr) {
+        checkCuda(cudaMallocFromPoolAsync(&p, bytes, pool_, stream_), what);
+    } else {
+        checkCuda(cudaMalloc(&p, bytes), what);
+    }
     blocks_.push_back(p);
     reserved_ += bytes;
     return p;
@@ -71,6 +112,7 @@ Engine::Engine(const Problem& p, int device, uint64_t budget_bytes, Batch* batch
         checkCuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "Create engine stream");
         checkCuda(cudaStreamCreateWithFlags(&stream_wl_, cudaStreamNonBlocking), "Create wirelength stream");
     }
+    arena_.bind(device_, stream_);
     checkCuda(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "Create fork event");
     checkCuda(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "Create join event");
     particle_count_ = p.particle_count;

@@ -24,6 +24,9 @@ public:
     DeviceArena(const DeviceArena&) = delete;
     DeviceArena& operator=(const DeviceArena&) = delete;
 
+    // Allocations are taken from the device's pool on `stream` (devicePool) once bound;
+    // before that, and for an unbound arena, with cudaMalloc.
+    void bind(int device, cudaStream_t stream);
     void* allocate(std::size_t bytes, const char* what);
     template <typename T>
     T* array(std::size_t count, const char* what) {
@@ -36,6 +39,8 @@ private:
     uint64_t limit_;
     uint64_t reserved_ = 0;
     std::vector<void*> blocks_;
+    cudaMemPool_t pool_ = nullptr;
+    cudaStream_t stream_ = nullptr;
 };
 
 struct EvalRequest {

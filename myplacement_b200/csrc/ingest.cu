@@ -137,7 +137,9 @@ public:
         const std::size_t bytes = std::max<std::size_t>(1, count) * sizeof(T);
         check(bytes);
         void* p = nullptr;
-        checkCuda(cudaMallocAsync(&p, bytes, stream_), "ingest scratch");
+        int device = 0;
+        checkCuda(cudaGetDevice(&device), "Query the current device");
+        checkCuda(cudaMallocFromPoolAsync(&p, bytes, devicePool(device), stream_), "ingest scratch");
         blocks_.push_back(p);
         held_ += bytes;
         return static_cast<T*>(p);
