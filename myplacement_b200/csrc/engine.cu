@@ -102,6 +102,11 @@ void upload(T* device, const std::vector<T>& host, cudaStream_t stream) {
 }  // namespace
 
 Engine::Engine(const Problem& p, int device, uint64_t budget_bytes, Batch* batch)
+    : Engine(Grid{p.bins_x, p.bins_y, p.region, p.target_density}, device, budget_bytes, batch) {
+    load(p);
+}
+
+Engine::Engine(const Grid& grid, int device, uint64_t budget_bytes, Batch* batch)
     : device_(device), batch_(batch), arena_(budget_bytes) {
     checkCuda(cudaSetDevice(device_), "Select CUDA device");
     if (batch_ != nullptr) {
@@ -115,20 +120,26 @@ Engine::Engine(const Problem& p, int device, uint64_t budget_bytes, Batch* batch
     arena_.bind(device_, stream_);
     checkCuda(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "Create fork event");
     checkCuda(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "Create join event");
-    particle_count_ = p.particle_count;
-    movable_count_ = p.movable_count;
-    bins_x_ = p.bins_x;
-    bins_y_ = p.bins_y;
+    bins_x_ = grid.bins_x;
+    bins_y_ = grid.bins_y;
     bin_count_ = bins_x_ * bins_y_;
-    region_ = p.region;
-    target_density_ = p.target_density;
+    region_ = grid.region;
+    target_density_ = grid.target_density;
     bin_w_ = region_.width() / static_cast<double>(bins_x_);
     bin_h_ = region_.height() / static_cast<double>(bins_y_);
     bin_area_ = (std::max(0.0, region_.width()) * std::max(0.0, region_.height())) / static_cast<double>(bin_count_);
     const uint64_t uploaded_before = g_uploaded_bytes;
+    buildBasis();
+    h2d_bytes_ += g_uploaded_bytes - uploaded_before;
+}
+
+void Engine::load(const Problem& p) {
+    require(p.bins_x == bins_x_ && p.bins_y == bins_y_, "The problem's grid is not the engine's.");
+    particle_count_ = p.particle_count;
+    movable_count_ = p.movable_count;
+    const uint64_t uploaded_before = g_uploaded_bytes;
     uploadStatic(p);
     buildNetLayout(p);
-    buildBasis();
     allocateGroups();
     h2d_bytes_ += g_uploaded_bytes - uploaded_before;
     // The reduction publishes the scalars and the error flag into mapped pinned

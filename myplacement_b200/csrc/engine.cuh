@@ -152,6 +152,16 @@ public:
     // With a batch, the engine runs on the batch's stream and its evaluations are
     // launched together with the other engines of the batch (Batch).
     Engine(const Problem& problem, int device, uint64_t budget_bytes, Batch* batch = nullptr);
+    // Two-phase construction: the grid's part (streams, the field solve's bases and
+    // buffers) needs only the grid, so it can run while the host builds the particles;
+    // load() then uploads the problem (whose grid must be this one).
+    struct Grid {
+        int bins_x = 0, bins_y = 0;
+        Rect2 region;
+        double target_density = 0.0;
+    };
+    Engine(const Grid& grid, int device, uint64_t budget_bytes, Batch* batch = nullptr);
+    void load(const Problem& problem);
     ~Engine();
     Engine(const Engine&) = delete;
     Engine& operator=(const Engine&) = delete;

@@ -16,6 +16,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <exception>
+#include <thread>
 
 #include "common.cuh"
 
@@ -113,8 +115,23 @@ Session::Session(const mpgp_design& design, const mpgp_options& options, Batch* 
         result_ = mpgp_result{};
         return;
     }
-    problem_ = buildProblem(design, derived_, options_, fillers_);
-    const Problem& problem = problem_;
+    // The host problem (static layers, fillers, particle and pin arrays) is built on a
+    // second thread while this one sets up the engine's grid part on the device (the
+    // field solve's bases and buffers need only the grid).
+    std::exception_ptr problem_error;
+    std::thread problem_thread([&] {
+        try {
+            problem_ = buildProblem(design, derived_, options_, fillers_);
+        } catch (...) {
+            problem_error = std::current_exception();
+        }
+    });
+    struct Join {
+        std::thread& t;
+        ~Join() {
+            if (t.joinable()) t.join();
+        }
+    } join{problem_thread};
     int device_count = 0;
     const cudaError_t count_status = cudaGetDeviceCount(&device_count);
     if (count_status != cudaSuccess || device_count <= 0) {
@@ -122,8 +139,13 @@ Session::Session(const mpgp_design& design, const mpgp_options& options, Batch* 
     }
     require(options_.cuda_device >= 0 && options_.cuda_device < device_count,
             "Requested CUDA device does not exist on this host.");
-    engine_ = std::make_unique<Engine>(problem, options_.cuda_device, options_.maximum_cuda_memory_bytes,
+    const Engine::Grid grid{options_.bins_x, options_.bins_y, derived_.core, options_.target_density};
+    engine_ = std::make_unique<Engine>(grid, options_.cuda_device, options_.maximum_cuda_memory_bytes,
                                        rudy_requested_ ? nullptr : batch);
+    problem_thread.join();
+    if (problem_error) std::rethrow_exception(problem_error);
+    const Problem& problem = problem_;
+    engine_->load(problem);
     if (rudy_requested_) engine_->enableRudy(options_);
     result_.cuda_device_used = options_.cuda_device;
 
