@@ -42,7 +42,7 @@ FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustain
 # The kernel behind each timed family (families of one kernel are summed for the roofline).
 KERNEL_OF_FAMILY = {"dct_forward": "tcGemmKernel", "dct_inverse": "tcGemmKernel",
                     "field_forward": "fieldKernel", "field_gradient": "fieldKernel", "field_inverse": "fieldKernel",
-                    "wirelength": "wirelengthKernel + pinPositionKernel", "scatter": "scatterKernel",
+                    "wirelength": "wirelengthKernel", "scatter": "scatterKernel",
                     "metrics": "metricsSplitKernel", "gather": "gatherKernel", "reduce": "reduceKernel",
                     "vector": "velocityKernel", "dct_split": "splitSourceKernel", "rudy": "rudy kernels"}
 # Iteration budget of the end-to-end runs (early stop on): large enough that the run stops on its

@@ -193,7 +193,7 @@ void Batch::loop() {
 
 void Batch::execute(const std::vector<Request*>& round) {
     const int n = static_cast<int>(round.size());
-    std::vector<int> scatter, pins, metrics, gather;
+    std::vector<int> scatter, metrics, gather;
     std::vector<TcItem> items[kContractionStages][kMaxSplit];
     std::vector<FieldGroup> fields;
     bool mixed_split = false;  // an instance whose stages use different splits (its stages must share a stream)
@@ -202,7 +202,6 @@ void Batch::execute(const std::vector<Request*>& round) {
         const EvalPlan& p = *round[i]->plan;
         Engine* engine = round[i]->engine;
         if (p.scatter) scatter.push_back(i);
-        if (p.pin_positions) pins.push_back(i);
         if (p.metrics) metrics.push_back(i);
         if (p.gather) gather.push_back(i);
         const int total = p.reduce_args.offsets[p.reduce_args.source_count];
@@ -250,8 +249,6 @@ void Batch::execute(const std::vector<Request*>& round) {
     RoundLayout layout;
     const std::size_t at_scatter = layout.add<ScatterArgs>(scatter.size());
     const std::size_t at_scatter_offsets = layout.add<int>(scatter.size() + 1);
-    const std::size_t at_pins = layout.add<PinPositionArgs>(pins.size());
-    const std::size_t at_pins_offsets = layout.add<int>(pins.size() + 1);
     const std::size_t at_wirelength = layout.add<WirelengthArgs>(static_cast<std::size_t>(n));
     const std::size_t at_wirelength_offsets = layout.add<int>(static_cast<std::size_t>(n) + 1);
     const std::size_t at_metrics = layout.add<MetricsArgs>(metrics.size());
@@ -295,9 +292,6 @@ void Batch::execute(const std::vector<Request*>& round) {
     const int scatter_blocks = fill(
         at_scatter, scatter, [](const EvalPlan& p) { return p.scatter_args; },
         [](const EvalPlan& p) { return p.scatter_blocks; }, at_scatter_offsets);
-    const int pin_blocks = fill(
-        at_pins, pins, [](const EvalPlan& p) { return p.pin_args; }, [](const EvalPlan& p) { return p.pin_blocks; },
-        at_pins_offsets);
     const int wirelength_blocks = fill(
         at_wirelength, everyone, [](const EvalPlan& p) { return p.wirelength_args; },
         [](const EvalPlan& p) { return p.wirelength_blocks; }, at_wirelength_offsets);
@@ -340,12 +334,6 @@ void Batch::execute(const std::vector<Request*>& round) {
     }
     checkCuda(cudaEventRecord(fork_, stream_), "Batch fork");
     checkCuda(cudaStreamWaitEvent(wirelength_, fork_, 0), "Batch fork");
-    if (pin_blocks > 0) {
-        launchPinPositionsBatch(reinterpret_cast<const PinPositionArgs*>(on_device(at_pins)),
-                                reinterpret_cast<const int*>(on_device(at_pins_offsets)), static_cast<int>(pins.size()),
-                                pin_blocks, wirelength_);
-        ++launches;
-    }
     if (wirelength_blocks > 0) {
         launchWirelengthBatch(reinterpret_cast<const WirelengthArgs*>(on_device(at_wirelength)),
                               reinterpret_cast<const int*>(on_device(at_wirelength_offsets)), n, wirelength_blocks,

@@ -147,7 +147,7 @@ void Engine::load(const Problem& p) {
     // evaluation's critical path.
     checkCuda(cudaMallocHost(reinterpret_cast<void**>(&host_scalars_), sizeof(EvalScalars)), "pinned scalars");
     std::memset(host_scalars_, 0, sizeof(EvalScalars));
-    const std::size_t slot_bytes = 2 * (static_cast<std::size_t>(kScalarCount) + 1) * sizeof(unsigned long long);
+    const std::size_t slot_bytes = 2 * static_cast<std::size_t>(kRecordSlots) * sizeof(unsigned long long);
     checkCuda(cudaHostAlloc(reinterpret_cast<void**>(&host_slots_), slot_bytes, cudaHostAllocMapped),
               "pinned evaluation record");
     std::memset(host_slots_, 0, slot_bytes);
@@ -270,9 +270,6 @@ void Engine::buildNetLayout(const Problem& p) {
     rudy_net_weight_ = layout.net_weight64;
     particle_pin_start_ = layout.particle_pin_start;
     pin_slot_ = layout.pin_slot;
-    slot_particle_ = layout.slot_particle;
-    slot_pin_ = layout.slot_pin;
-    slot_offset_ = layout.slot_offset;
     wl_net_count_ = layout.kept_nets;
     wl_pin_count_ = layout.kept_pins;
     // Degree buckets: one thread per two-pin net, G lanes per net for degree <= G,
@@ -293,13 +290,6 @@ void Engine::buildNetLayout(const Problem& p) {
     const std::size_t pins = std::max<std::size_t>(1, static_cast<std::size_t>(layout.kept_pins));
     block_work_ = arena_.array<int4>(std::max<std::size_t>(1, work.size()), "wirelength work");
     pin_gradient_ = arena_.array<float2>(pins, "pin gradients");
-    pin_position_ = arena_.array<double2>(pins, "pin positions");
-    // The movable pins' slots: the last entry of the particle pin offsets.
-    if (movable_count_ > 0) {
-        checkCuda(cudaMemcpyAsync(&movable_slots_, particle_pin_start_ + movable_count_, sizeof(int),
-                                  cudaMemcpyDeviceToHost, stream_),
-                  "Count the movable pins");
-    }
     partials_wl_ = arena_.array<double>(2 * std::max<std::size_t>(1, work.size()), "wirelength partials");
     upload(block_work_, work, stream_);
     checkCuda(cudaMemsetAsync(pin_gradient_, 0, pins * sizeof(float2), stream_), "clear pin gradients");
@@ -738,15 +728,8 @@ EvalPlan Engine::plan(const EvalRequest& q) {
     // chain on its own stream (after the scatter when the scatter forms them).
     p.fork_first = q.mode == kGiven;
 
-    // The movable pins' positions, in the wirelength pass's pin order: unless nothing
-    // moved since the last evaluation, whose pin positions are then still in place.
-    p.pin_positions = !q.reuse_density && movable_slots_ > 0;
-    p.pin_args = PinPositionArgs{positions, slot_particle_, slot_pin_, slot_offset_, movable_slots_, pin_position_};
-    p.pin_blocks = pinPositionBlocks(movable_slots_);
-
     WirelengthArgs& wa = p.wirelength_args;
     wa.positions = positions;
-    wa.pin_position = pin_position_;
     wa.pin_particle = pin_particle_;
     wa.pin_offset = pin_offset_;
     wa.static_pins = static_pins_;
@@ -784,7 +767,7 @@ EvalPlan Engine::plan(const EvalRequest& q) {
     ma.partials = partials_m_;
     ma.group_partials = m_groups_.partials;
     ma.group_counters = m_groups_.counters;
-    int kernels = p.pin_positions ? 2 : 1;  // pin positions, wirelength
+    int kernels = 1;  // the wirelength pass
     if (!q.reuse_density) {
         p.metrics = true;
         p.metrics_fused = metrics_fused_;
@@ -837,12 +820,16 @@ EvalPlan Engine::plan(const EvalRequest& q) {
     ra.staged_capacity = kReduceStaged;
     ra.scalars = scalars_;
     ra.totals = totals_;
-    ra.host_slots = host_slots_;
+    const uint64_t ticket = ++launches_issued_;
+    const int record = static_cast<int>(ticket & 1U);
+    ra.host_slots = host_slots_ + static_cast<std::size_t>(record) * kRecordSlots;
     ra.device_error = tc_error_;
     ra.sequence = static_cast<unsigned int>(++sequence_);
     if (ra.sequence == 0) ra.sequence = static_cast<unsigned int>(++sequence_);  // 0 marks an empty record
-    expected_mask_ = 0;
-    for (int k = 0; k < s; ++k) expected_mask_ |= 1U << ra.sources[k].target;
+    record_sequence_[record] = ra.sequence;
+    record_ticket_[record] = ticket;
+    record_mask_[record] = 0;
+    for (int k = 0; k < s; ++k) record_mask_[record] |= 1U << ra.sources[k].target;
     if (gather) {
         GatherArgs& ga = p.gather_args;
         ga.particle_count = static_cast<int>(particle_count_);
@@ -931,12 +918,11 @@ void Engine::run(const EvalPlan& p) {
     launches_ += p.kernels;
 }
 
-// The wirelength stream's part of an evaluation (after the fork event): pin positions,
-// the wirelength pass and the RUDY kernels, then the join event.
+// The wirelength stream's part of an evaluation (after the fork event): the wirelength
+// pass and the RUDY kernels, then the join event.
 void Engine::runWirelengthPass(const EvalPlan& p) {
     checkCuda(cudaStreamWaitEvent(stream_wl_, fork_, 0), "fork");
     beginKernel(kKindWirelength, stream_wl_);
-    if (p.pin_positions) launchPinPositions(p.pin_args, stream_wl_);
     launchWirelength(p.wirelength_args, p.wirelength_blocks, stream_wl_);
     endKernel(stream_wl_);
     if (p.rudy) {
@@ -953,16 +939,18 @@ void Engine::runWirelengthPass(const EvalPlan& p) {
     checkCuda(cudaEventRecord(join_, stream_wl_), "join");
 }
 
-void Engine::launch(const EvalRequest& q) {
+uint64_t Engine::launch(const EvalRequest& q) {
+    if (batch_ != nullptr) require(!has_pending_, "A batched engine takes one evaluation at a time.");
     EvalPlan p = plan(q);
     if (batch_ != nullptr) {
         require(!p.rudy && !p.potential && (p.metrics_fused || !p.metrics),
                 "A batched evaluation supports neither RUDY, the potential, nor grids wider than 2,048 bins.");
         batched_plan_ = p;
         has_pending_ = true;
-        return;
+        return launches_issued_;
     }
     run(p);
+    return launches_issued_;
 }
 
 const TcBatch* Engine::deviceBatches() {
@@ -996,7 +984,10 @@ const TcBatch& Engine::contraction(int stage) const {
     }
 }
 
-const EvalScalars& Engine::sync() {
+const EvalScalars& Engine::sync(uint64_t ticket) {
+    const int record = static_cast<int>(ticket & 1U);
+    require(ticket > synced_ticket_ || ticket == launches_issued_, "This evaluation was already read.");
+    require(record_ticket_[record] == ticket, "This evaluation's record was reused by a later launch.");
     if (has_pending_) {
         // Batched: the evaluation runs in the batch's next round, which has completed
         // on the device when this returns; the record below is then already complete.
@@ -1006,12 +997,13 @@ const EvalScalars& Engine::sync() {
     // Poll the record until every scalar of this evaluation and the error flag carry
     // its sequence; now and then ask the stream for a fault, so an evaluation that
     // can no longer publish surfaces as an error instead of a hang.
-    const unsigned long long tag = static_cast<unsigned long long>(static_cast<unsigned int>(sequence_)) << 32;
-    const volatile unsigned long long* slots = host_slots_;
+    const unsigned long long tag = static_cast<unsigned long long>(record_sequence_[record]) << 32;
+    const uint32_t expected_mask = record_mask_[record];
+    const volatile unsigned long long* slots = host_slots_ + static_cast<std::size_t>(record) * kRecordSlots;
     const auto current = [&](int index) { return (slots[index] & 0xffffffff00000000ULL) == tag; };
     const auto complete = [&]() {
         if (!current(2 * kScalarCount)) return false;
-        for (uint32_t m = expected_mask_; m != 0; m &= m - 1) {
+        for (uint32_t m = expected_mask; m != 0; m &= m - 1) {
             const int k = __builtin_ctz(m);
             if (!current(2 * k) || !current(2 * k + 1)) return false;
         }
@@ -1030,12 +1022,15 @@ const EvalScalars& Engine::sync() {
         if (polls > 4096) std::this_thread::yield();
     }
     std::atomic_thread_fence(std::memory_order_acquire);
-    for (uint32_t m = expected_mask_; m != 0; m &= m - 1) {
+    for (uint32_t m = expected_mask; m != 0; m &= m - 1) {
         const int k = __builtin_ctz(m);
         const unsigned long long bits = (slots[2 * k] & 0xffffffffULL) | ((slots[2 * k + 1] & 0xffffffffULL) << 32);
         std::memcpy(&host_scalars_->v[k], &bits, sizeof(double));
     }
-    collectTimings();
+    synced_ticket_ = std::max(synced_ticket_, ticket);
+    // Profiling events are read once no later evaluation is in flight (reading them
+    // waits for every recorded event).
+    if (ticket == launches_issued_) collectTimings();
     if ((slots[2 * kScalarCount] & 0xffffffffULL) != 0) {
         fail(MPGP_ERR_TIMEOUT, "A tcgen05 field contraction timed out waiting on its pipeline.");
     }

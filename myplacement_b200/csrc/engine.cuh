@@ -97,9 +97,6 @@ struct EvalPlan {
     ScatterArgs scatter_args{};
     int scatter_blocks = 0;
     bool fork_first = false;  // the positions are given: the wirelength pass need not wait for the scatter
-    bool pin_positions = false;  // the pin position pass runs first on the wirelength stream
-    PinPositionArgs pin_args{};
-    int pin_blocks = 0;
     WirelengthArgs wirelength_args{};
     int wirelength_blocks = 0;
     bool rudy = false;
@@ -166,9 +163,12 @@ public:
     Engine(const Engine&) = delete;
     Engine& operator=(const Engine&) = delete;
 
-    // Launches one evaluation on the engine stream; the scalars are valid after sync().
-    // In a batch the evaluation is handed to the batch at sync().
-    void launch(const EvalRequest& request);
+    // Launches one evaluation on the engine stream and returns its ticket; its scalars
+    // are valid after sync(ticket).  Two evaluations may be in flight: each publishes
+    // into one of two records, so the later launch does not overwrite the earlier's
+    // record before the host has read it.  In a batch the evaluation is handed to the
+    // batch at sync(), and only one may be in flight.
+    uint64_t launch(const EvalRequest& request);
     // The launches of one evaluation (the scalar record's sequence advances), and
     // launching them on the engine's streams.
     EvalPlan plan(const EvalRequest& request);
@@ -185,12 +185,13 @@ public:
     // Stops taking part in the batch's rounds (the placement has finished); a later
     // evaluation still runs through the batch.
     void leaveBatch();
-    // Waits for the stream and returns the scalars of the last launched evaluation.
-    const EvalScalars& sync();
-    const EvalScalars& evaluate(const EvalRequest& request) {
-        launch(request);
-        return sync();
-    }
+    // Waits for the evaluation `ticket` (at most one launch old) and returns its scalars
+    // (scalars it does not compute keep the value of the last evaluation synced before).
+    const EvalScalars& sync(uint64_t ticket);
+    const EvalScalars& sync() { return sync(launches_issued_); }
+    const EvalScalars& evaluate(const EvalRequest& request) { return sync(launch(request)); }
+    // Two evaluations may be in flight (not in a batch).
+    [[nodiscard]] bool overlapsEvaluations() const { return batch_ == nullptr; }
     // Evaluation results in the reference's structures.
     void densityMetrics(const EvalScalars& s, bool with_fillers, mpgp_density_metrics& out) const;
     [[nodiscard]] double energy(const EvalScalars& s) const;
@@ -322,11 +323,6 @@ private:
     float2* pin_gradient_ = nullptr;
     int* particle_pin_start_ = nullptr;
     int* pin_slot_ = nullptr;
-    int* slot_particle_ = nullptr;
-    int* slot_pin_ = nullptr;
-    float2* slot_offset_ = nullptr;
-    int movable_slots_ = 0;
-    double2* pin_position_ = nullptr;  // movable pins' absolute positions (pin order)
 
     // density
     unsigned long long* layers_ = nullptr;
@@ -359,8 +355,14 @@ private:
     // Evaluation results published by the reduction into mapped pinned memory
     // (ReduceArgs::host_slots), the scalars the current evaluation writes, and
     // the cache of the latest value of every scalar.
+    // Two records of kRecordSlots slots; launch k publishes into record k % 2.
+    static constexpr int kRecordSlots = 2 * (kScalarCount + 1);
     unsigned long long* host_slots_ = nullptr;
-    uint32_t expected_mask_ = 0;
+    uint32_t record_mask_[2] = {0, 0};       // the scalars the record's evaluation writes
+    uint32_t record_sequence_[2] = {0, 0};   // its sequence (the record's tag)
+    uint64_t record_ticket_[2] = {0, 0};     // its ticket
+    uint64_t launches_issued_ = 0;
+    uint64_t synced_ticket_ = 0;
     unsigned long long sequence_ = 0;
     void buildTensorCoreBasis(double max_scale);
     SplitMatrix newSplit(int rows, int cols, const char* what);

@@ -97,17 +97,11 @@ __global__ void numberStaticKernel(int pins, const int* is_static, const int* st
     pin_index[i] = i;
 }
 
-__global__ void slotsKernel(int pins, const int* sorted_keys, const int* sorted_pins, int movable, int* slot,
-                            const float2* pin_offset, int* slot_particle, int* slot_pin, float2* slot_offset) {
+__global__ void slotsKernel(int pins, const int* sorted_keys, const int* sorted_pins, int movable, int* slot) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pins) return;
-    const bool moves = sorted_keys[i] < movable;
-    slot[sorted_pins[i]] = moves ? i : -1;
-    if (moves) {  // the movable pins take slots 0 .. (movable pins - 1), in particle order
-        slot_particle[i] = sorted_keys[i];
-        slot_pin[i] = sorted_pins[i];
-        slot_offset[i] = pin_offset[sorted_pins[i]];
-    }
+    // The movable pins take slots 0 .. (movable pins - 1), in particle order.
+    slot[sorted_pins[i]] = sorted_keys[i] < movable ? i : -1;
 }
 
 int blocksFor(long long count) { return std::max(1, ceilDiv(std::max(1LL, count), kThreads)); }
@@ -277,9 +271,6 @@ NetLayout buildNetLayoutOnDevice(const Problem& p, int movable, const DeviceAllo
     out.particle_pin_start =
         static_cast<int*>(allocate((static_cast<std::size_t>(movable) + 1) * sizeof(int), "particle pin offsets"));
     out.pin_slot = static_cast<int*>(allocate(pins * sizeof(int), "pin gradient slots"));
-    out.slot_particle = static_cast<int*>(allocate(pins * sizeof(int), "pin slots"));
-    out.slot_pin = static_cast<int*>(allocate(pins * sizeof(int), "pin slots"));
-    out.slot_offset = static_cast<float2*>(allocate(pins * sizeof(float2), "pin slots"));
     int* particle_keys = scratch.array<int>(pins);
     int* pin_index = scratch.array<int>(pins);
     int* sorted_particles = scratch.array<int>(pins);
@@ -301,9 +292,7 @@ NetLayout buildNetLayoutOnDevice(const Problem& p, int movable, const DeviceAllo
                                                   out.kept_pins, 0, bits, stream),
                   "pin sort");
         slotsKernel<<<blocksFor(out.kept_pins), kThreads, 0, stream>>>(out.kept_pins, sorted_particles, sorted_pins,
-                                                                       movable, out.pin_slot, out.pin_offset,
-                                                                       out.slot_particle, out.slot_pin,
-                                                                       out.slot_offset);
+                                                                       movable, out.pin_slot);
         checkCuda(cudaGetLastError(), "Launch the slot assignment");
     }
     {

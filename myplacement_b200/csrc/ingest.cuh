@@ -29,11 +29,6 @@ struct NetLayout {
     double* net_weight64 = nullptr;  // FP64 (RUDY)
     int* particle_pin_start = nullptr;  // movable + 1
     int* pin_slot = nullptr;      // a pin's slot in its particle's range, -1 for static pins
-    // Per slot of a movable pin (slots in particle order; particle_pin_start[movable] of them):
-    // its particle, its pin (in bucket order) and its offset from the particle's centre.
-    int* slot_particle = nullptr;
-    int* slot_pin = nullptr;
-    float2* slot_offset = nullptr;
 };
 
 NetLayout buildNetLayoutOnDevice(const Problem& problem, int movable, const DeviceAllocator& allocate,

@@ -59,30 +59,9 @@ struct WirelengthArgs {
     double* partials;             // per block: smooth, hpwl
     double* group_partials;       // per 32 blocks: smooth, hpwl (reduceGroups)
     unsigned int* group_counters;
-    // I': the absolute position of every movable pin (pin order), written by the pin
-    // position pass; when set, movable pins are read from it instead of the particle
-    // centre plus the offset (the same FP64 sum, so the same values).
-    const double2* pin_position;
 };
 void launchWirelength(const WirelengthArgs& args, int blocks, cudaStream_t stream);
 
-// ---- pin positions (the wirelength pass's streamed input) ------------------------------
-// One thread per movable pin slot (particle order): pin_position[slot_pin[j]] =
-// positions[slot_particle[j]] + slot_offset[j], in FP64.  Reads are coalesced and the
-// scattered stores do not stall, so the wirelength pass streams its pins' positions
-// instead of gathering particle centres pin by pin.
-struct PinPositionArgs {
-    const double2* positions;
-    const int* slot_particle;
-    const int* slot_pin;
-    const float2* slot_offset;
-    int slots;
-    double2* pin_position;
-};
-int pinPositionBlocks(int slots);
-void launchPinPositions(const PinPositionArgs& args, cudaStream_t stream);
-void launchPinPositionsBatch(const PinPositionArgs* args, const int* offsets, int count, int blocks,
-                             cudaStream_t stream);
 // Batched launches (every family below has one): `count` instances' argument blocks
 // in device memory, instance k owning launch blocks [offsets[k], offsets[k + 1]) of
 // `blocks`; each block does exactly what block (b - offsets[k]) of the instance's own

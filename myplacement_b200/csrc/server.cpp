@@ -60,14 +60,12 @@ uint64_t estimateSessionBytes(const mpgp_design& design, const mpgp_options& opt
     // Twelve split matrices of two fp16 planes: six nx-row and six ny-row ones.
     const uint64_t split = 4ull * 3ull * (nx * ldx + ny * ldy + ny * ldx + nx * ldy);
     // 12 session vectors + sizes, charge, preconditioner, layer, upload scratch (per
-    // particle); particle, offset, slot,
-    // gradient, a possible static copy, the slot-ordered particle / pin / offset and the
-    // pin position (per pin); CSR, weight, work and partials (per net); layers, static
-    // charge, source, scale, field, potential (per bin); and the set-up's transient
-    // sorting and scanning scratch (per pin and per net), which is freed before the
-    // iterations start but must fit while it lives.
-    const uint64_t bytes =
-        256ull * particles + (40ull + 32ull + 80ull) * pins + (16ull + 48ull) * nets + 64ull * bins + split;
+    // particle); particle, offset, slot, gradient and a possible static copy (per pin);
+    // CSR, weight, work and partials (per net); layers, static charge, source, scale,
+    // field, potential (per bin); and the set-up's transient sorting and scanning
+    // scratch (per pin and per net), which is freed before the iterations start but
+    // must fit while it lives.
+    const uint64_t bytes = 256ull * particles + (40ull + 80ull) * pins + (16ull + 48ull) * nets + 64ull * bins + split;
     return bytes + (256ull << 10) /* partials, scalars, rounding of ~60 allocations */;
 }
 

@@ -247,8 +247,9 @@ void Session::fillMetrics(const EvalScalars& s, double penalty, double rudy_weig
     out.max_displacement = s.v[kMaxDisplacement];
 }
 
-StateEval Session::evaluateGiven(double2* positions, bool gradient, double penalty, double2* raw, double2* pre,
-                                 bool with_prev, bool with_velocity, bool reuse_density, double rudy_weight_override) {
+EvalRequest Session::givenRequest(double2* positions, bool gradient, double penalty, double2* raw, double2* pre,
+                                  bool with_prev, bool with_velocity, bool reuse_density,
+                                  double rudy_weight_override) {
     EvalRequest q;
     q.mode = kGiven;
     q.rudy = rudy_active_;
@@ -267,16 +268,10 @@ StateEval Session::evaluateGiven(double2* positions, bool gradient, double penal
         q.prev_gradient = prev_grad_;
     }
     if (with_velocity) q.velocity = velocity_;
-    const EvalScalars& s = engine_->evaluate(q);
-    ++result_.evaluations;
-    StateEval out;
-    fillMetrics(s, penalty, q.rudy ? q.rudy_weight : 0.0, out);
-    out.raw = raw;
-    out.pre = pre;
-    return out;
+    return q;
 }
 
-StateEval Session::evaluateLookahead(double momentum, double penalty, double2* raw, double2* pre) {
+EvalRequest Session::lookaheadRequest(double momentum, double penalty, double2* raw, double2* pre) {
     density_cached_ = false;
     EvalRequest q;
     q.mode = kLookahead;
@@ -296,13 +291,29 @@ StateEval Session::evaluateLookahead(double momentum, double penalty, double2* r
         q.prev_positions = prev_pos_;
         q.prev_gradient = prev_grad_;
     }
-    const EvalScalars& s = engine_->evaluate(q);
+    return q;
+}
+
+StateEval Session::collect(uint64_t ticket, const EvalRequest& q, double penalty) {
+    const EvalScalars& s = engine_->sync(ticket);
     ++result_.evaluations;
     StateEval out;
     fillMetrics(s, penalty, q.rudy ? q.rudy_weight : 0.0, out);
-    out.raw = raw;
-    out.pre = pre;
+    out.raw = q.raw;
+    out.pre = q.pre;
     return out;
+}
+
+StateEval Session::evaluateGiven(double2* positions, bool gradient, double penalty, double2* raw, double2* pre,
+                                 bool with_prev, bool with_velocity, bool reuse_density, double rudy_weight_override) {
+    const EvalRequest q =
+        givenRequest(positions, gradient, penalty, raw, pre, with_prev, with_velocity, reuse_density, rudy_weight_override);
+    return collect(engine_->launch(q), q, penalty);
+}
+
+StateEval Session::evaluateLookahead(double momentum, double penalty, double2* raw, double2* pre) {
+    const EvalRequest q = lookaheadRequest(momentum, penalty, raw, pre);
+    return collect(engine_->launch(q), q, penalty);
 }
 
 StateEval Session::evaluateProposal(const double2* base, const StateEval& base_eval, double step, double max_disp,
@@ -426,13 +437,31 @@ void Session::iterate() {
     const mpgp_options& o = options_;
     const int iteration = iteration_;
     StateEval current;
+    // The momentum lookahead (below) needs nothing from the current evaluation but the
+    // go-ahead: when it is likely to run, it is launched right behind the current
+    // evaluation, before the host reads that one, and dropped unread if the current
+    // evaluation calls for a restart.  Its request and results are those of the
+    // sequential order, since no state it reads changes in between.
+    const auto momentumOf = [&](int age) {
+        return std::min(o.maximum_momentum, static_cast<double>(age) / static_cast<double>(age + 3));
+    };
+    uint64_t lookahead_ticket = 0;
+    EvalRequest lookahead_request;
     if (iteration == 0) {
         current = initial_;
     } else {
         smoothing_ = smoothingFromOverflow(last_optimizer_overflow_);
         if (rudy_active_ && refreshRudyWeight()) has_previous_gradient_ = false;
-        current = evaluateGiven(cur_, true, penalty_, raw_cur_, pre_cur_, has_previous_gradient_, true,
-                                density_cached_);
+        const EvalRequest q = givenRequest(cur_, true, penalty_, raw_cur_, pre_cur_, has_previous_gradient_, true,
+                                           density_cached_, -1.0);
+        const uint64_t ticket = engine_->launch(q);
+        const bool speculate = engine_->overlapsEvaluations() && !rudy_requested_ && !rudy_active_ &&
+                               objective_worse_streak_ < 2 && momentum_age_ > 0 && !velocity_zero_;
+        if (speculate) {
+            lookahead_request = lookaheadRequest(momentumOf(momentum_age_), penalty_, raw_look_, pre_look_);
+            lookahead_ticket = engine_->launch(lookahead_request);
+        }
+        current = collect(ticket, q, penalty_);
     }
     bool rudy_just_activated = false;
     if (rudy_requested_ && !rudy_active_ &&
@@ -453,13 +482,13 @@ void Session::iterate() {
     const StateEval* base = &current;
     StateEval lookahead;
     if (!restarted && momentum_age_ > 0) {
-        const double momentum =
-            std::min(o.maximum_momentum, static_cast<double>(momentum_age_) / static_cast<double>(momentum_age_ + 3));
+        const double momentum = momentumOf(momentum_age_);
         const double alignment = velocity_zero_ ? 0.0 : -current.alignment;  // momentumAlignment (:610-617)
         if (alignment <= 0.0) {
             restarted = true;
         } else {
-            lookahead = evaluateLookahead(momentum, penalty_, raw_look_, pre_look_);
+            lookahead = lookahead_ticket != 0 ? collect(lookahead_ticket, lookahead_request, penalty_)
+                                              : evaluateLookahead(momentum, penalty_, raw_look_, pre_look_);
             if (lookahead.m.objective > current.m.objective * (1.0 + o.hpwl_growth_restart_threshold)) {
                 restarted = true;
             } else {

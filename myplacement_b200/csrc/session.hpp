@@ -71,6 +71,12 @@ private:
                             bool with_prev, bool with_velocity, bool reuse_density = false,
                             double rudy_weight_override = -1.0);
     StateEval evaluateLookahead(double momentum, double penalty, double2* raw, double2* pre);
+    // The requests behind evaluateGiven and evaluateLookahead, and the reading of an
+    // evaluation launched earlier (so that two can be in flight).
+    EvalRequest givenRequest(double2* positions, bool gradient, double penalty, double2* raw, double2* pre,
+                             bool with_prev, bool with_velocity, bool reuse_density, double rudy_weight_override);
+    EvalRequest lookaheadRequest(double momentum, double penalty, double2* raw, double2* pre);
+    StateEval collect(uint64_t ticket, const EvalRequest& request, double penalty);
     StateEval evaluateProposal(const double2* base, const StateEval& base_eval, double step, double max_disp,
                                double penalty);
     void fillMetrics(const EvalScalars& s, double penalty, double rudy_weight, StateEval& out) const;

@@ -41,16 +41,10 @@ __device__ __forceinline__ PinPoint loadPin(const WirelengthArgs& a, int pin) {
     PinPoint p;
     p.particle = a.pin_particle[pin];
     if (p.particle >= 0) {
-        if (a.pin_position != nullptr) {
-            const double2 q = a.pin_position[pin];
-            p.x = q.x;
-            p.y = q.y;
-        } else {
-            const double2 c = a.positions[p.particle];
-            const float2 o = a.pin_offset[pin];
-            p.x = c.x + static_cast<double>(o.x);
-            p.y = c.y + static_cast<double>(o.y);
-        }
+        const double2 c = a.positions[p.particle];
+        const float2 o = a.pin_offset[pin];
+        p.x = c.x + static_cast<double>(o.x);
+        p.y = c.y + static_cast<double>(o.y);
     } else {
         const double2 s = a.static_pins[-p.particle - 1];
         p.x = s.x;
@@ -92,46 +86,25 @@ __device__ void netPairs(const WirelengthArgs& a, int first, int count, double& 
     // Two-pin nets lead the layout: net k's pins are 2k and 2k + 1, so each of the
     // pin arrays is read as one vector (the arrays start 256-byte aligned).
     const int2 particle = reinterpret_cast<const int2*>(a.pin_particle)[net];
+    const float4 offset = reinterpret_cast<const float4*>(a.pin_offset)[net];
     const int2 slot = a.gradient ? reinterpret_cast<const int2*>(a.pin_slot)[net] : make_int2(0, 0);
     const float weight = a.net_weight[net];
-    PinPoint p, q;
-    if (a.pin_position != nullptr) {
-        // The pair's two positions as one 32-byte load (the array starts 256-byte aligned).
-        const double4 pair = reinterpret_cast<const double4*>(a.pin_position)[net];
-        const auto place = [&](int index, double x, double y) {
-            PinPoint pin;
-            pin.particle = index;
-            if (index >= 0) {
-                pin.x = x;
-                pin.y = y;
-            } else {
-                const double2 s = a.static_pins[-index - 1];
-                pin.x = s.x;
-                pin.y = s.y;
-            }
-            return pin;
-        };
-        p = place(particle.x, pair.x, pair.y);
-        q = place(particle.y, pair.z, pair.w);
-    } else {
-        const float4 offset = reinterpret_cast<const float4*>(a.pin_offset)[net];
-        const auto place = [&](int index, float ox, float oy) {
-            PinPoint pin;
-            pin.particle = index;
-            if (index >= 0) {
-                const double2 c = a.positions[index];
-                pin.x = c.x + static_cast<double>(ox);
-                pin.y = c.y + static_cast<double>(oy);
-            } else {
-                const double2 s = a.static_pins[-index - 1];
-                pin.x = s.x;
-                pin.y = s.y;
-            }
-            return pin;
-        };
-        p = place(particle.x, offset.x, offset.y);
-        q = place(particle.y, offset.z, offset.w);
-    }
+    const auto place = [&](int index, float ox, float oy) {
+        PinPoint pin;
+        pin.particle = index;
+        if (index >= 0) {
+            const double2 c = a.positions[index];
+            pin.x = c.x + static_cast<double>(ox);
+            pin.y = c.y + static_cast<double>(oy);
+        } else {
+            const double2 s = a.static_pins[-index - 1];
+            pin.x = s.x;
+            pin.y = s.y;
+        }
+        return pin;
+    };
+    const PinPoint p = place(particle.x, offset.x, offset.y);
+    const PinPoint q = place(particle.y, offset.z, offset.w);
     const float dx = static_cast<float>(p.x - q.x);
     const float dy = static_cast<float>(p.y - q.y);
     const float ax = fabsf(dx), ay = fabsf(dy);
@@ -286,15 +259,6 @@ __device__ void netWarps(const WirelengthArgs& a, int first, int count, double& 
     }
 }
 
-// One block of the pin position pass.
-__device__ __forceinline__ void pinPositionBlock(const PinPositionArgs& a, int block) {
-    const int j = block * static_cast<int>(blockDim.x) + static_cast<int>(threadIdx.x);
-    if (j >= a.slots) return;
-    const double2 c = a.positions[a.slot_particle[j]];
-    const float2 o = a.slot_offset[j];
-    a.pin_position[a.slot_pin[j]] = make_double2(c.x + static_cast<double>(o.x), c.y + static_cast<double>(o.y));
-}
-
 // One block of the pass: `block` of `grid` blocks (the launch's, or its instance's in
 // a batched launch).
 __device__ __forceinline__ void wirelengthBlock(const WirelengthArgs& a, int block, int grid) {
@@ -333,21 +297,6 @@ __global__ void __launch_bounds__(kThreads) wirelengthBatchKernel(const Wireleng
     wirelengthBlock(a, slot.y, slot.z);
 }
 
-__global__ void __launch_bounds__(kThreads) pinPositionKernel(PinPositionArgs a) {
-    releaseNext();
-    waitForPrior();
-    pinPositionBlock(a, static_cast<int>(blockIdx.x));
-}
-
-__global__ void __launch_bounds__(kThreads) pinPositionBatchKernel(const PinPositionArgs* args, const int* offsets,
-                                                                   int count) {
-    releaseNext();
-    waitForPrior();
-    const int3 slot = batchSlot(offsets, count, static_cast<int>(blockIdx.x));
-    const PinPositionArgs a = args[slot.x];
-    pinPositionBlock(a, slot.y);
-}
-
 }  // namespace
 
 void launchWirelength(const WirelengthArgs& args, int blocks, cudaStream_t stream) {
@@ -360,21 +309,6 @@ void launchWirelengthBatch(const WirelengthArgs* args, const int* offsets, int c
     if (blocks <= 0 || count <= 0) return;
     launchChained("Launch the batched wirelength pass", wirelengthBatchKernel, dim3(blocks), dim3(kThreads), 0,
                   stream, args, offsets, count);
-}
-
-int pinPositionBlocks(int slots) { return slots > 0 ? ceilDiv(slots, kThreads) : 0; }
-
-void launchPinPositions(const PinPositionArgs& args, cudaStream_t stream) {
-    const int blocks = pinPositionBlocks(args.slots);
-    if (blocks <= 0) return;
-    launchChained("Launch the pin positions", pinPositionKernel, dim3(blocks), dim3(kThreads), 0, stream, args);
-}
-
-void launchPinPositionsBatch(const PinPositionArgs* args, const int* offsets, int count, int blocks,
-                             cudaStream_t stream) {
-    if (blocks <= 0 || count <= 0) return;
-    launchChained("Launch the batched pin positions", pinPositionBatchKernel, dim3(blocks), dim3(kThreads), 0, stream,
-                  args, offsets, count);
 }
 
 // ---- allocation-free variant --------------------------------------------------------
