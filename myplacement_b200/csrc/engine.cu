@@ -147,7 +147,7 @@ void Engine::load(const Problem& p) {
     // evaluation's critical path.
     checkCuda(cudaMallocHost(reinterpret_cast<void**>(&host_scalars_), sizeof(EvalScalars)), "pinned scalars");
     std::memset(host_scalars_, 0, sizeof(EvalScalars));
-    const std::size_t slot_bytes = 2 * static_cast<std::size_t>(kRecordSlots) * sizeof(unsigned long long);
+    const std::size_t slot_bytes = static_cast<std::size_t>(kRecords) * kRecordSlots * sizeof(unsigned long long);
     checkCuda(cudaHostAlloc(reinterpret_cast<void**>(&host_slots_), slot_bytes, cudaHostAllocMapped),
               "pinned evaluation record");
     std::memset(host_slots_, 0, slot_bytes);
@@ -273,13 +273,18 @@ void Engine::buildNetLayout(const Problem& p) {
     wl_net_count_ = layout.kept_nets;
     wl_pin_count_ = layout.kept_pins;
     // Degree buckets: one thread per two-pin net, G lanes per net for degree <= G,
-    // a warp loop above 32.  The blocks run heaviest bucket first (one round of the
-    // block's lanes each), so the long warp-loop nets do not form the kernel's tail.
+    // a warp loop above 32.  The blocks run heaviest bucket first, so the long
+    // warp-loop nets do not form the kernel's tail.  Each block takes two rounds of
+    // its lanes: half the blocks of one round each, and so half the block-end
+    // reductions, measured 4% faster a warm iteration (the pass shares the SMs with
+    // the field solve, and its blocks' fixed costs held them).
+    constexpr int kRounds = 2;
     const int kGroups[6] = {1, 4, 8, 16, 32, 0};
     std::vector<int4> work;
     for (int b = 5; b >= 0; --b) {
         const int group = kGroups[b];
-        const int nets_per_block = group == 0 ? kThreads / 32 : group == 1 ? kThreads : kThreads / group;
+        const int nets_per_block =
+            kRounds * (group == 0 ? kThreads / 32 : group == 1 ? kThreads : kThreads / group);
         const int first_net = layout.bucket_first[b];
         const int count = layout.bucket_first[b + 1] - layout.bucket_first[b];
         for (int off = 0; off < count; off += nets_per_block) {
@@ -695,6 +700,10 @@ EvalPlan Engine::plan(const EvalRequest& q) {
     const double2* positions = q.mode == kGiven ? q.positions : q.out_positions;
     require(positions != nullptr, "An evaluation needs positions.");
     require(q.smoothing > 0.0 && std::isfinite(q.smoothing), "Global placement requires positive finite smoothing.");
+    const bool folds = q.velocity_base != nullptr || q.checkpoint_out != nullptr;
+    require(!folds || (q.mode == kGiven && q.gradient && particle_count_ > 0), "Only an evaluation with a gather at "
+            "given positions takes the previous step's velocity update and checkpoint copy.");
+    require((q.velocity_base == nullptr) == (q.velocity_out == nullptr), "A velocity update needs its output.");
     EvalPlan p;
 
     ScatterArgs& sa = p.scatter_args;
@@ -821,7 +830,7 @@ EvalPlan Engine::plan(const EvalRequest& q) {
     ra.scalars = scalars_;
     ra.totals = totals_;
     const uint64_t ticket = ++launches_issued_;
-    const int record = static_cast<int>(ticket & 1U);
+    const int record = static_cast<int>(ticket % kRecords);
     ra.host_slots = host_slots_ + static_cast<std::size_t>(record) * kRecordSlots;
     ra.device_error = tc_error_;
     ra.sequence = static_cast<unsigned int>(++sequence_);
@@ -858,6 +867,9 @@ EvalPlan Engine::plan(const EvalRequest& q) {
         ga.prev_positions = q.prev_positions;
         ga.prev_gradient = q.prev_gradient;
         ga.velocity = q.velocity;
+        ga.velocity_base = q.velocity_base;
+        ga.velocity_out = q.velocity_out;
+        ga.checkpoint_out = q.checkpoint_out;
         ga.rudy_gradient = q.rudy ? rudy_pin_gradient_ : nullptr;
         ga.rudy_weight = q.rudy ? q.rudy_weight : 0.0;
         ga.partials = partials_g_;
@@ -985,7 +997,7 @@ const TcBatch& Engine::contraction(int stage) const {
 }
 
 const EvalScalars& Engine::sync(uint64_t ticket) {
-    const int record = static_cast<int>(ticket & 1U);
+    const int record = static_cast<int>(ticket % kRecords);
     require(ticket > synced_ticket_ || ticket == launches_issued_, "This evaluation was already read.");
     require(record_ticket_[record] == ticket, "This evaluation's record was reused by a later launch.");
     if (has_pending_) {

@@ -66,6 +66,12 @@ struct EvalRequest {
     const double2* prev_positions = nullptr;
     const double2* prev_gradient = nullptr;
     const double2* velocity = nullptr;
+    // Work of the previous step folded into this evaluation's gather (kGiven with a
+    // gradient): velocity_out = positions - velocity_base (the step just taken; the
+    // momentum alignment then uses it) and checkpoint_out = positions.
+    const double2* velocity_base = nullptr;
+    double2* velocity_out = nullptr;
+    double2* checkpoint_out = nullptr;
     bool want_potential = false;
     // The density map, forward field coefficients and energy of the previous
     // evaluation are those of these positions (nothing moved since): keep them and
@@ -164,10 +170,10 @@ public:
     Engine& operator=(const Engine&) = delete;
 
     // Launches one evaluation on the engine stream and returns its ticket; its scalars
-    // are valid after sync(ticket).  Two evaluations may be in flight: each publishes
-    // into one of two records, so the later launch does not overwrite the earlier's
-    // record before the host has read it.  In a batch the evaluation is handed to the
-    // batch at sync(), and only one may be in flight.
+    // are valid after sync(ticket).  Up to kRecords evaluations may be in flight: each
+    // publishes into its own record, so a later launch does not overwrite an earlier
+    // one's record before the host has read it.  In a batch the evaluation is handed to
+    // the batch at sync(), and only one may be in flight.
     uint64_t launch(const EvalRequest& request);
     // The launches of one evaluation (the scalar record's sequence advances), and
     // launching them on the engine's streams.
@@ -185,12 +191,12 @@ public:
     // Stops taking part in the batch's rounds (the placement has finished); a later
     // evaluation still runs through the batch.
     void leaveBatch();
-    // Waits for the evaluation `ticket` (at most one launch old) and returns its scalars
+    // Waits for the evaluation `ticket` (fewer than kRecords launches old) and returns its scalars
     // (scalars it does not compute keep the value of the last evaluation synced before).
     const EvalScalars& sync(uint64_t ticket);
     const EvalScalars& sync() { return sync(launches_issued_); }
     const EvalScalars& evaluate(const EvalRequest& request) { return sync(launch(request)); }
-    // Two evaluations may be in flight (not in a batch).
+    // Evaluations may be in flight together (not in a batch), up to kRecords.
     [[nodiscard]] bool overlapsEvaluations() const { return batch_ == nullptr; }
     // Evaluation results in the reference's structures.
     void densityMetrics(const EvalScalars& s, bool with_fillers, mpgp_density_metrics& out) const;
@@ -355,12 +361,13 @@ private:
     // Evaluation results published by the reduction into mapped pinned memory
     // (ReduceArgs::host_slots), the scalars the current evaluation writes, and
     // the cache of the latest value of every scalar.
-    // Two records of kRecordSlots slots; launch k publishes into record k % 2.
+    // kRecords records of kRecordSlots slots; launch k publishes into record k % kRecords.
+    static constexpr int kRecords = 2;
     static constexpr int kRecordSlots = 2 * (kScalarCount + 1);
     unsigned long long* host_slots_ = nullptr;
-    uint32_t record_mask_[2] = {0, 0};       // the scalars the record's evaluation writes
-    uint32_t record_sequence_[2] = {0, 0};   // its sequence (the record's tag)
-    uint64_t record_ticket_[2] = {0, 0};     // its ticket
+    uint32_t record_mask_[kRecords] = {};       // the scalars the record's evaluation writes
+    uint32_t record_sequence_[kRecords] = {};   // its sequence (the record's tag)
+    uint64_t record_ticket_[kRecords] = {};     // its ticket
     uint64_t launches_issued_ = 0;
     uint64_t synced_ticket_ = 0;
     unsigned long long sequence_ = 0;

@@ -160,6 +160,13 @@ __device__ __forceinline__ void gatherBlock(const GatherArgs& a, const ReduceArg
             }
         }
         const double2 p = a.positions[i];
+        if (a.checkpoint_out != nullptr) a.checkpoint_out[i] = p;
+        double2 step = make_double2(0.0, 0.0);
+        if (a.velocity_base != nullptr) {
+            const double2 b = a.velocity_base[i];
+            step = make_double2(p.x - b.x, p.y - b.y);
+            a.velocity_out[i] = step;
+        }
         const double2 e = sampleField(a, p.x, p.y);
         const double q = a.charge[i];
         const double dx = -q * e.x;
@@ -189,7 +196,7 @@ __device__ __forceinline__ void gatherBlock(const GatherArgs& a, const ReduceArg
                 v[5] += gx * gx + gy * gy;
             }
             if (a.velocity != nullptr) {
-                const double2 vel = a.velocity[i];
+                const double2 vel = a.velocity_base != nullptr ? step : a.velocity[i];
                 v[6] += vel.x * px + vel.y * py;
             }
         }

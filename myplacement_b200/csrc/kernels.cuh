@@ -242,6 +242,9 @@ struct GatherArgs {
     const double2* prev_positions;  // optional (step estimate)
     const double2* prev_gradient;
     const double2* velocity;        // optional (momentum alignment)
+    const double2* velocity_base;   // optional: velocity_out = positions - velocity_base (the alignment uses it)
+    double2* velocity_out;
+    double2* checkpoint_out;        // optional: a copy of the positions
     const double2* rudy_gradient;   // optional: RUDY pin slots (particle order), added with rudy_weight
     double rudy_weight;
     double* partials;               // per block: 8 partials (kWireL1 .. kRudyL1)

@@ -306,36 +306,72 @@ StateEval Session::collect(uint64_t ticket, const EvalRequest& q, double penalty
 
 StateEval Session::evaluateGiven(double2* positions, bool gradient, double penalty, double2* raw, double2* pre,
                                  bool with_prev, bool with_velocity, bool reuse_density, double rudy_weight_override) {
-    const EvalRequest q =
+    EvalRequest q =
         givenRequest(positions, gradient, penalty, raw, pre, with_prev, with_velocity, reuse_density, rudy_weight_override);
-    return collect(engine_->launch(q), q, penalty);
+    const uint64_t ticket = launchEvaluation(q);
+    return collect(ticket, q, penalty);
 }
 
 StateEval Session::evaluateLookahead(double momentum, double penalty, double2* raw, double2* pre) {
-    const EvalRequest q = lookaheadRequest(momentum, penalty, raw, pre);
-    return collect(engine_->launch(q), q, penalty);
+    EvalRequest q = lookaheadRequest(momentum, penalty, raw, pre);
+    const uint64_t ticket = launchEvaluation(q);
+    return collect(ticket, q, penalty);
 }
 
-StateEval Session::evaluateProposal(const double2* base, const StateEval& base_eval, double step, double max_disp,
-                                    double penalty) {
+uint64_t Session::launchEvaluation(EvalRequest& q) {
+    if (pending_velocity_base_ != nullptr || pending_checkpoint_ != nullptr) {
+        if (q.mode == kGiven && q.positions == cur_ && q.gradient && engine_->particleCount() > 0) {
+            q.velocity_base = pending_velocity_base_;
+            q.velocity_out = pending_velocity_base_ != nullptr ? velocity_ : nullptr;
+            q.checkpoint_out = pending_checkpoint_;
+            pending_velocity_base_ = nullptr;
+            pending_checkpoint_ = nullptr;
+        } else {
+            flushPending();
+        }
+    }
+    return engine_->launch(q);
+}
+
+void Session::flushPending() {
+    const int count = static_cast<int>(engine_->particleCount());
+    if (pending_velocity_base_ != nullptr) {
+        engine_->beginKernel(kKindVector);
+        launchVelocity(cur_, pending_velocity_base_, velocity_, count, engine_->stream());
+        engine_->endKernel();
+        engine_->countLaunches(1);
+        pending_velocity_base_ = nullptr;
+    }
+    if (pending_checkpoint_ != nullptr) {
+        launchCopyPositions(cur_, pending_checkpoint_, count, engine_->stream());
+        engine_->countLaunches(1);
+        pending_checkpoint_ = nullptr;
+    }
+}
+
+EvalRequest Session::proposalRequest(const double2* base, const double2* pre, const double2* raw, double step,
+                                     double max_disp) {
     density_cached_ = false;
     EvalRequest q;
     q.mode = kPropose;
     q.rudy = rudy_active_;
     q.rudy_weight = rudy_weight_;
     q.base = base;
-    q.direction = base_eval.pre;
-    q.raw_direction = base_eval.raw;
+    q.direction = pre;
+    q.raw_direction = raw;
     q.step = step;
     q.max_displacement = max_disp;
     q.out_positions = cand_;
     q.smoothing = smoothing_;
     q.gradient = false;
-    const EvalScalars& s = engine_->evaluate(q);
-    ++result_.evaluations;
-    StateEval out;
-    fillMetrics(s, penalty, q.rudy ? q.rudy_weight : 0.0, out);
-    return out;
+    return q;
+}
+
+StateEval Session::evaluateProposal(const double2* base, const StateEval& base_eval, double step, double max_disp,
+                                    double penalty) {
+    EvalRequest q = proposalRequest(base, base_eval.pre, base_eval.raw, step, max_disp);
+    const uint64_t ticket = launchEvaluation(q);
+    return collect(ticket, q, penalty);
 }
 
 // refreshRudyWeight (AdaptiveGlobalPlacer.cpp:689-698): the weight ramps to its
@@ -388,6 +424,18 @@ void Session::refreshCheckpointRudyScore(CheckpointState& checkpoint) {
     checkpoint.selection_score = e.m.hpwl + rudy_target_weight_ * e.m.rudy_energy;
 }
 
+// A checkpoint of the current positions is copied by the next evaluation's gather;
+// any other copy is a kernel of its own.
+void Session::copyCheckpoint(double2* positions, double2* destination) {
+    if (positions == cur_ && pending_checkpoint_ == nullptr) {
+        pending_checkpoint_ = destination;
+        return;
+    }
+    if (pending_checkpoint_ == destination) pending_checkpoint_ = nullptr;  // superseded
+    launchCopyPositions(positions, destination, static_cast<int>(engine_->particleCount()), engine_->stream());
+    engine_->countLaunches(1);
+}
+
 // considerCheckpoint (AdaptiveGlobalPlacer.cpp:559-596); the score adds the routability
 // target weight times the RUDY energy.
 void Session::considerCheckpoint(double2* positions, const ObjectiveMetrics& m, int iteration, bool& is_new_best) {
@@ -397,8 +445,7 @@ void Session::considerCheckpoint(double2* positions, const ObjectiveMetrics& m, 
     const double score = m.hpwl + rudy_target_weight_ * m.rudy_energy;
     if (feasible && (!best_feasible_.found || score < best_feasible_.selection_score - 1e-10 ||
                      (std::abs(score - best_feasible_.selection_score) <= 1e-10 && m.hpwl < best_feasible_.hpwl))) {
-        launchCopyPositions(positions, best_feasible_.positions, static_cast<int>(engine_->particleCount()), engine_->stream());
-        engine_->countLaunches(1);
+        copyCheckpoint(positions, best_feasible_.positions);
         best_feasible_.iteration = iteration;
         best_feasible_.hpwl = m.hpwl;
         best_feasible_.overflow = overflow;
@@ -410,8 +457,7 @@ void Session::considerCheckpoint(double2* positions, const ObjectiveMetrics& m, 
     if (!best_feasible_.found &&
         (!best_fallback_.found || overflow < best_fallback_.overflow - 1e-12 ||
          (std::abs(overflow - best_fallback_.overflow) <= 1e-12 && m.hpwl < best_fallback_.hpwl))) {
-        launchCopyPositions(positions, best_fallback_.positions, static_cast<int>(engine_->particleCount()), engine_->stream());
-        engine_->countLaunches(1);
+        copyCheckpoint(positions, best_fallback_.positions);
         best_fallback_.iteration = iteration;
         best_fallback_.hpwl = m.hpwl;
         best_fallback_.overflow = overflow;
@@ -452,14 +498,14 @@ void Session::iterate() {
     } else {
         smoothing_ = smoothingFromOverflow(last_optimizer_overflow_);
         if (rudy_active_ && refreshRudyWeight()) has_previous_gradient_ = false;
-        const EvalRequest q = givenRequest(cur_, true, penalty_, raw_cur_, pre_cur_, has_previous_gradient_, true,
-                                           density_cached_, -1.0);
-        const uint64_t ticket = engine_->launch(q);
+        EvalRequest q = givenRequest(cur_, true, penalty_, raw_cur_, pre_cur_, has_previous_gradient_, true,
+                                     density_cached_, -1.0);
+        const uint64_t ticket = launchEvaluation(q);
         const bool speculate = engine_->overlapsEvaluations() && !rudy_requested_ && !rudy_active_ &&
                                objective_worse_streak_ < 2 && momentum_age_ > 0 && !velocity_zero_;
         if (speculate) {
             lookahead_request = lookaheadRequest(momentumOf(momentum_age_), penalty_, raw_look_, pre_look_);
-            lookahead_ticket = engine_->launch(lookahead_request);
+            lookahead_ticket = launchEvaluation(lookahead_request);
         }
         current = collect(ticket, q, penalty_);
     }
@@ -469,6 +515,7 @@ void Session::iterate() {
         activateRudy(current, has_previous_gradient_, true);
         refreshCheckpointRudyScore(best_feasible_);
         has_previous_gradient_ = false;
+        pending_velocity_base_ = nullptr;  // the velocity restarts from zero
         checkCuda(cudaMemsetAsync(velocity_, 0, sizeof(double2) * static_cast<std::size_t>(engine_->particleCount()),
                                   engine_->stream()),
                   "Clear velocity");
@@ -555,10 +602,9 @@ void Session::iterate() {
 
     const double penalty_used = penalty_;
     if (accepted) {
-        engine_->beginKernel(kKindVector);
-        launchVelocity(cand_, cur_, velocity_, static_cast<int>(engine_->particleCount()), engine_->stream());
-        engine_->endKernel();
-        engine_->countLaunches(1);
+        // velocity = accepted - current positions, done by the next evaluation (the
+        // buffer of the current positions is left alone until then).
+        const double2* stepped_from = cur_;
         velocity_zero_ = false;
         last_step_size_ = used_step_size;
         momentum_age_ = restarted ? 0 : momentum_age_ + 1;
@@ -585,6 +631,7 @@ void Session::iterate() {
             has_previous_gradient_ = true;
         }
         std::swap(cur_, cand_);  // current_positions = accepted positions
+        pending_velocity_base_ = stepped_from;
         density_cached_ = true;  // the accepted candidate was the last evaluation
         last_optimizer_overflow_ = accepted_eval.m.optimizer.normalized_overflow;
         considerCheckpoint(cur_, accepted_eval.m, iteration + 1, new_best_checkpoint);
@@ -599,6 +646,7 @@ void Session::iterate() {
                                           used_maximum_displacement, base_pre_norm, used_curvature, backtracks,
                                           restarted, true, new_best_checkpoint, rudy_weight_, rudy_active_));
     } else {
+        pending_velocity_base_ = nullptr;  // the velocity restarts from zero
         checkCuda(cudaMemsetAsync(velocity_, 0, sizeof(double2) * static_cast<std::size_t>(engine_->particleCount()),
                                   engine_->stream()),
                   "Clear velocity");
@@ -639,6 +687,7 @@ void Session::currentPositions(double* xy) const {
 void Session::finish(double* module_x, double* module_y, mpgp_result* result, mpgp_history_row* history,
                      int capacity) {
     if (!empty_) {
+        flushPending();
         const CheckpointState& chosen = best_feasible_.found ? best_feasible_ : best_fallback_;
         double2* final_positions = chosen.found ? chosen.positions : cur_;
         if (chosen.found) {

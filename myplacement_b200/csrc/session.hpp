@@ -76,7 +76,16 @@ private:
     EvalRequest givenRequest(double2* positions, bool gradient, double penalty, double2* raw, double2* pre,
                              bool with_prev, bool with_velocity, bool reuse_density, double rudy_weight_override);
     EvalRequest lookaheadRequest(double momentum, double penalty, double2* raw, double2* pre);
+    EvalRequest proposalRequest(const double2* base, const double2* pre, const double2* raw, double step,
+                                double max_disp);
     StateEval collect(uint64_t ticket, const EvalRequest& request, double penalty);
+    // The accepted step's velocity update and checkpoint copy wait for the next
+    // evaluation: one at the current positions with a gradient does them in its gather
+    // (settlePending hands them to it); before any other evaluation, and before the
+    // host reads a checkpoint, flushPending launches them as kernels.
+    uint64_t launchEvaluation(EvalRequest& request);
+    void flushPending();
+    void copyCheckpoint(double2* positions, double2* destination);
     StateEval evaluateProposal(const double2* base, const StateEval& base_eval, double step, double max_disp,
                                double penalty);
     void fillMetrics(const EvalScalars& s, double penalty, double rudy_weight, StateEval& out) const;
@@ -131,6 +140,8 @@ private:
     int iteration_ = 0;
     StateEval initial_;
     bool velocity_zero_ = true;
+    const double2* pending_velocity_base_ = nullptr;  // velocity_ = cur_ - this, not yet done
+    double2* pending_checkpoint_ = nullptr;           // a checkpoint of cur_ not yet copied
     // The last evaluation was the accepted candidate now held in cur_, so its
     // density map, field coefficients and energy are still on the device.
     bool density_cached_ = false;

@@ -78,13 +78,9 @@ __device__ __forceinline__ float groupSum(float v) {
 __device__ __forceinline__ float fastExp(float v) { return __expf(v); }
 __device__ __forceinline__ float fastLog(float v) { return __logf(v); }
 
-// Two-pin nets, one thread per net; the bucket's pins are consecutive pairs.
-__device__ void netPairs(const WirelengthArgs& a, int first, int count, double& smooth, double& hpwl) {
-    const int local = static_cast<int>(threadIdx.x);
-    if (local >= count) return;  // the caller's block reduction follows; every thread still reaches it
-    const int net = first + local;
-    // Two-pin nets lead the layout: net k's pins are 2k and 2k + 1, so each of the
-    // pin arrays is read as one vector (the arrays start 256-byte aligned).
+// One two-pin net.  Two-pin nets lead the layout: net k's pins are 2k and 2k + 1,
+// so each of the pin arrays is read as one vector (the arrays start 256-byte aligned).
+__device__ __forceinline__ void netPair(const WirelengthArgs& a, int net, double& smooth, double& hpwl) {
     const int2 particle = reinterpret_cast<const int2*>(a.pin_particle)[net];
     const float4 offset = reinterpret_cast<const float4*>(a.pin_offset)[net];
     const int2 slot = a.gradient ? reinterpret_cast<const int2*>(a.pin_slot)[net] : make_int2(0, 0);
@@ -119,6 +115,13 @@ __device__ void netPairs(const WirelengthArgs& a, int first, int count, double& 
         const float gy = copysignf(weight * __fdividef(1.0f - ty, 1.0f + ty), dy);
         if (p.particle >= 0) a.pin_gradient[slot.x] = make_float2(gx, gy);
         if (q.particle >= 0) a.pin_gradient[slot.y] = make_float2(-gx, -gy);
+    }
+}
+
+// Two-pin nets, one thread per net and round; the bucket's pins are consecutive pairs.
+__device__ void netPairs(const WirelengthArgs& a, int first, int count, double& smooth, double& hpwl) {
+    for (int local = static_cast<int>(threadIdx.x); local < count; local += static_cast<int>(blockDim.x)) {
+        netPair(a, first + local, smooth, hpwl);
     }
 }
 
