@@ -131,17 +131,6 @@ Engine::Engine(const Grid& grid, int device, uint64_t budget_bytes, Batch* batch
     const uint64_t uploaded_before = g_uploaded_bytes;
     buildBasis();
     h2d_bytes_ += g_uploaded_bytes - uploaded_before;
-}
-
-void Engine::load(const Problem& p) {
-    require(p.bins_x == bins_x_ && p.bins_y == bins_y_, "The problem's grid is not the engine's.");
-    particle_count_ = p.particle_count;
-    movable_count_ = p.movable_count;
-    const uint64_t uploaded_before = g_uploaded_bytes;
-    uploadStatic(p);
-    buildNetLayout(p);
-    allocateGroups();
-    h2d_bytes_ += g_uploaded_bytes - uploaded_before;
     // The reduction publishes the scalars and the error flag into mapped pinned
     // memory; the host polls it, with no copy or stream synchronisation on the
     // evaluation's critical path.
@@ -151,6 +140,31 @@ void Engine::load(const Problem& p) {
     checkCuda(cudaHostAlloc(reinterpret_cast<void**>(&host_slots_), slot_bytes, cudaHostAllocMapped),
               "pinned evaluation record");
     std::memset(host_slots_, 0, slot_bytes);
+}
+
+void Engine::load(const Problem& p) {
+    loadNets(p, p.movable_count);
+    loadParticles(p);
+}
+
+void Engine::loadNets(const Problem& p, int64_t movable_count) {
+    require(!nets_loaded_, "The engine's nets are loaded once.");
+    movable_count_ = movable_count;
+    const uint64_t uploaded_before = g_uploaded_bytes;
+    buildNetLayout(p);
+    h2d_bytes_ += g_uploaded_bytes - uploaded_before;
+    nets_loaded_ = true;
+}
+
+void Engine::loadParticles(const Problem& p) {
+    require(nets_loaded_, "The engine's nets are loaded before its particles.");
+    require(p.bins_x == bins_x_ && p.bins_y == bins_y_, "The problem's grid is not the engine's.");
+    require(p.movable_count == movable_count_, "The problem's movable count is not the one its nets were laid out for.");
+    particle_count_ = p.particle_count;
+    const uint64_t uploaded_before = g_uploaded_bytes;
+    uploadStatic(p);
+    allocateGroups();
+    h2d_bytes_ += g_uploaded_bytes - uploaded_before;
     checkCuda(cudaStreamSynchronize(stream_), "Engine setup");
     if (batch_ != nullptr) {
         batch_->attach(this);

@@ -164,7 +164,11 @@ public:
         double target_density = 0.0;
     };
     Engine(const Grid& grid, int device, uint64_t budget_bytes, Batch* batch = nullptr);
+    // The problem's upload and device layout, all at once or in two steps: the nets
+    // (needing only the pin and net arrays and the movable count), then the particles.
     void load(const Problem& problem);
+    void loadNets(const Problem& problem, int64_t movable_count);
+    void loadParticles(const Problem& problem);
     ~Engine();
     Engine(const Engine&) = delete;
     Engine& operator=(const Engine&) = delete;
@@ -369,6 +373,7 @@ private:
     uint32_t record_sequence_[kRecords] = {};   // its sequence (the record's tag)
     uint64_t record_ticket_[kRecords] = {};     // its ticket
     uint64_t launches_issued_ = 0;
+    bool nets_loaded_ = false;
     uint64_t synced_ticket_ = 0;
     unsigned long long sequence_ = 0;
     void buildTensorCoreBasis(double max_scale);

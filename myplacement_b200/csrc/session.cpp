@@ -115,15 +115,23 @@ Session::Session(const mpgp_design& design, const mpgp_options& options, Batch* 
         result_ = mpgp_result{};
         return;
     }
-    // The host problem (static layers, fillers, particle and pin arrays) is built on a
-    // second thread while this one sets up the engine's grid part on the device (the
-    // field solve's bases and buffers need only the grid).
-    std::exception_ptr problem_error;
-    std::thread problem_thread([&] {
+    // The host problem is built on two threads while this one sets up the engine's grid
+    // part on the device (the field solve's bases and buffers need only the grid): the
+    // pin and net arrays, whose device layout then starts at once, and the static
+    // layers, fillers and particle arrays, which are uploaded last.
+    std::exception_ptr pins_error, particles_error;
+    std::thread pins_thread([&] {
         try {
-            problem_ = buildProblem(design, derived_, options_, fillers_);
+            buildProblemPins(design, derived_, problem_);
         } catch (...) {
-            problem_error = std::current_exception();
+            pins_error = std::current_exception();
+        }
+    });
+    std::thread particles_thread([&] {
+        try {
+            buildProblemParticles(design, derived_, options_, problem_, fillers_);
+        } catch (...) {
+            particles_error = std::current_exception();
         }
     });
     struct Join {
@@ -131,7 +139,7 @@ Session::Session(const mpgp_design& design, const mpgp_options& options, Batch* 
         ~Join() {
             if (t.joinable()) t.join();
         }
-    } join{problem_thread};
+    } join_pins{pins_thread}, join_particles{particles_thread};
     int device_count = 0;
     const cudaError_t count_status = cudaGetDeviceCount(&device_count);
     if (count_status != cudaSuccess || device_count <= 0) {
@@ -142,10 +150,12 @@ Session::Session(const mpgp_design& design, const mpgp_options& options, Batch* 
     const Engine::Grid grid{options_.bins_x, options_.bins_y, derived_.core, options_.target_density};
     engine_ = std::make_unique<Engine>(grid, options_.cuda_device, options_.maximum_cuda_memory_bytes,
                                        rudy_requested_ ? nullptr : batch);
-    problem_thread.join();
-    if (problem_error) std::rethrow_exception(problem_error);
-    const Problem& problem = problem_;
-    engine_->load(problem);
+    pins_thread.join();
+    if (pins_error) std::rethrow_exception(pins_error);
+    engine_->loadNets(problem_, static_cast<int64_t>(derived_.movable.size()));
+    particles_thread.join();
+    if (particles_error) std::rethrow_exception(particles_error);
+    engine_->loadParticles(problem_);
     if (rudy_requested_) engine_->enableRudy(options_);
     result_.cuda_device_used = options_.cuda_device;
 

@@ -410,55 +410,43 @@ std::vector<Filler> createFillers(const mpgp_design& d, const DerivedDesign& der
     return fillers;
 }
 
-Problem buildProblem(const mpgp_design& d, const DerivedDesign& derived, const mpgp_options& options,
-                     std::vector<Filler>& fillers) {
-    Problem problem;
-    problem.bins_x = options.bins_x;
-    problem.bins_y = options.bins_y;
-    problem.region = derived.core;
-    problem.target_density = options.target_density;
-    // The pin CSR (buildHostLayout, CudaPlacementBackend.cu:815-837) depends only on
-    // the movable list, so a second thread forms it while this one builds the static
-    // layers, the fillers and the particle arrays.
+// The pin CSR (buildHostLayout, CudaPlacementBackend.cu:815-837): movable pins keep
+// their transformed offsets, static pins their absolute positions.
+void buildProblemPins(const mpgp_design& d, const DerivedDesign& derived, Problem& problem) {
     std::vector<int32_t> module_particle(static_cast<std::size_t>(d.module_count), -1);
     for (std::size_t index = 0; index < derived.movable.size(); ++index) {
         module_particle[derived.movable[index]] = static_cast<int32_t>(index);
     }
-    std::exception_ptr pins_error;
-    std::thread pins([&] {
-        try {
-            problem.net_weight.assign(d.net_weight, d.net_weight + d.net_count);
-            problem.net_pin_start.assign(d.net_pin_start, d.net_pin_start + d.net_count + 1);
-            const std::size_t count = static_cast<std::size_t>(d.pin_count);
-            problem.pin_particle.resize(count);
-            problem.pin_x.resize(count);
-            problem.pin_y.resize(count);
-            setupWorkers(count).blocks(count, 65536, [&](std::size_t b, std::size_t e) {
-                for (std::size_t p = b; p < e; ++p) {
-                    const int32_t m = d.pin_module[p];
-                    double ox, oy;
-                    transformOffset(d.pin_offset_x[p], d.pin_offset_y[p], orientationOf(d, m), ox, oy);
-                    const int32_t particle = module_particle[m];
-                    problem.pin_particle[p] = particle;
-                    if (particle >= 0) {
-                        problem.pin_x[p] = ox;
-                        problem.pin_y[p] = oy;
-                    } else {
-                        problem.pin_x[p] = d.module_x[m] + ox;  // pinPosition (PlacementDatabase.cpp:138-142)
-                        problem.pin_y[p] = d.module_y[m] + oy;
-                    }
-                }
-            });
-        } catch (...) {
-            pins_error = std::current_exception();
+    problem.net_weight.assign(d.net_weight, d.net_weight + d.net_count);
+    problem.net_pin_start.assign(d.net_pin_start, d.net_pin_start + d.net_count + 1);
+    const std::size_t count = static_cast<std::size_t>(d.pin_count);
+    problem.pin_particle.resize(count);
+    problem.pin_x.resize(count);
+    problem.pin_y.resize(count);
+    setupWorkers(count).blocks(count, 65536, [&](std::size_t b, std::size_t e) {
+        for (std::size_t p = b; p < e; ++p) {
+            const int32_t m = d.pin_module[p];
+            double ox, oy;
+            transformOffset(d.pin_offset_x[p], d.pin_offset_y[p], orientationOf(d, m), ox, oy);
+            const int32_t particle = module_particle[m];
+            problem.pin_particle[p] = particle;
+            if (particle >= 0) {
+                problem.pin_x[p] = ox;
+                problem.pin_y[p] = oy;
+            } else {
+                problem.pin_x[p] = d.module_x[m] + ox;  // pinPosition (PlacementDatabase.cpp:138-142)
+                problem.pin_y[p] = d.module_y[m] + oy;
+            }
         }
     });
-    struct Join {
-        std::thread& t;
-        ~Join() {
-            if (t.joinable()) t.join();
-        }
-    } join{pins};
+}
+
+void buildProblemParticles(const mpgp_design& d, const DerivedDesign& derived, const mpgp_options& options,
+                           Problem& problem, std::vector<Filler>& fillers) {
+    problem.bins_x = options.bins_x;
+    problem.bins_y = options.bins_y;
+    problem.region = derived.core;
+    problem.target_density = options.target_density;
     staticDensity(d, derived, options.bins_x, options.bins_y, options.target_density, problem.static_fixed,
                   problem.static_dark);
     fillers = createFillers(d, derived, problem.static_fixed, problem.static_dark, options.bins_x, options.bins_y,
@@ -507,7 +495,28 @@ Problem buildProblem(const mpgp_design& d, const DerivedDesign& derived, const m
             problem.precond_base[index] = 1.0 / (pin_factor * area_factor);
         }
     });
+}
 
+Problem buildProblem(const mpgp_design& d, const DerivedDesign& derived, const mpgp_options& options,
+                     std::vector<Filler>& fillers) {
+    // The pin CSR depends only on the movable list, so a second thread forms it while
+    // this one builds the static layers, the fillers and the particle arrays.
+    Problem problem;
+    std::exception_ptr pins_error;
+    std::thread pins([&] {
+        try {
+            buildProblemPins(d, derived, problem);
+        } catch (...) {
+            pins_error = std::current_exception();
+        }
+    });
+    struct Join {
+        std::thread& t;
+        ~Join() {
+            if (t.joinable()) t.join();
+        }
+    } join{pins};
+    buildProblemParticles(d, derived, options, problem, fillers);
     pins.join();
     if (pins_error) std::rethrow_exception(pins_error);
     return problem;

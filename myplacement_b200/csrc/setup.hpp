@@ -81,6 +81,12 @@ std::vector<Filler> createFillers(const mpgp_design& design, const DerivedDesign
 // CudaPlacementBackend.cu:784-839).  `fillers` receives the filler geometry.
 Problem buildProblem(const mpgp_design& design, const DerivedDesign& derived, const mpgp_options& options,
                      std::vector<Filler>& fillers);
+// Its two independent parts, which write disjoint members of `problem` and may run
+// on two threads at once: the net and pin arrays (buildHostLayout's CSR part), and
+// the grid, the static layers, the fillers and the particle arrays.
+void buildProblemPins(const mpgp_design& design, const DerivedDesign& derived, Problem& problem);
+void buildProblemParticles(const mpgp_design& design, const DerivedDesign& derived, const mpgp_options& options,
+                           Problem& problem, std::vector<Filler>& fillers);
 
 // The drop-in path: a Problem from an mpgp_layout.
 Problem problemFromLayout(const mpgp_layout& layout);
