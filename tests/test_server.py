@@ -69,7 +69,11 @@ def test_served_results_equal_alone(gpu, batched):
 @pytest.mark.parametrize("batched", [True, False])
 def test_batch_place_matches_global_place(gpu, batched):
     """Instances of uneven sizes and bin grids (32 x 32 to 128 x 128 bins: contractions of
-    one and of two K splits in one round) match their plain runs bit for bit."""
+    one and of two K splits in one round) match their plain runs bit for bit.  A plain
+    run launches the momentum lookahead behind the current evaluation and hands the
+    accepted step's velocity update and checkpoint copy to the next gather; a batched
+    instance takes one evaluation at a time, so equal results also show that the
+    overlap changes nothing."""
     jobs = [_job(cells, 40 + k, iterations=40) for k, cells in enumerate((1000, 2600, 1700, 3100, 1300, 2200, 9000))]
     placed, job_stats, server_stats = mp.batch_place([d for d, _ in jobs], [o for _, o in jobs], workers=4,
                                                      batched=batched)
