@@ -279,20 +279,57 @@ DerivedDesign deriveDesign(const mpgp_design& d) {
         }
         out.core = {core.llx, core.lly, core.urx, core.ury};
     }
-    out.is_fixed.resize(static_cast<std::size_t>(d.module_count));
-    out.is_macro.resize(static_cast<std::size_t>(d.module_count));
-    out.pin_count.assign(static_cast<std::size_t>(d.module_count), 0);
-    for (int32_t m = 0; m < d.module_count; ++m) {
-        const bool terminal = (d.module_flags[m] & MPGP_MODULE_TERMINAL) != 0;
-        const bool fixed = terminal || (d.module_flags[m] & MPGP_MODULE_FIXED) != 0;
-        out.is_fixed[m] = fixed ? 1 : 0;
-        out.is_macro[m] = (!terminal && out.nominal_row_height > kEpsilon &&
-                           std::abs(d.module_height[m] - out.nominal_row_height) > kEpsilon)
-                              ? 1
-                              : 0;
-        if (!fixed) out.movable.push_back(m);
+    const std::size_t modules = static_cast<std::size_t>(d.module_count);
+    const std::size_t pins = static_cast<std::size_t>(d.pin_count);
+    out.is_fixed.resize(modules);
+    out.is_macro.resize(modules);
+    out.pin_count.assign(modules, 0);
+    // Module flags and the movable list (in module order: each piece's movable
+    // modules go after those of the pieces before it), then the pin counts (integer
+    // sums, so the pieces' order does not matter), on up to eight host threads.
+    const Workers workers = setupWorkers(modules + pins);
+    const std::size_t pieces = static_cast<std::size_t>(workers.threads());
+    const auto bound = [&](std::size_t k, std::size_t n) { return n * k / pieces; };
+    std::vector<std::size_t> movable_in(pieces + 1, 0);
+    workers.run(pieces, [&](std::size_t k) {
+        std::size_t count = 0;
+        for (std::size_t m = bound(k, modules); m < bound(k + 1, modules); ++m) {
+            const bool terminal = (d.module_flags[m] & MPGP_MODULE_TERMINAL) != 0;
+            const bool fixed = terminal || (d.module_flags[m] & MPGP_MODULE_FIXED) != 0;
+            out.is_fixed[m] = fixed ? 1 : 0;
+            out.is_macro[m] = (!terminal && out.nominal_row_height > kEpsilon &&
+                               std::abs(d.module_height[m] - out.nominal_row_height) > kEpsilon)
+                                  ? 1
+                                  : 0;
+            if (!fixed) ++count;
+        }
+        movable_in[k + 1] = count;
+    });
+    for (std::size_t k = 0; k < pieces; ++k) movable_in[k + 1] += movable_in[k];
+    out.movable.resize(movable_in[pieces]);
+    std::vector<std::vector<int32_t>> counts(pieces > 1 ? pieces : 0);
+    workers.run(pieces, [&](std::size_t k) {
+        std::size_t at = movable_in[k];
+        for (std::size_t m = bound(k, modules); m < bound(k + 1, modules); ++m) {
+            if (!out.is_fixed[m]) out.movable[at++] = static_cast<int32_t>(m);
+        }
+        if (pieces > 1) {
+            std::vector<int32_t>& mine = counts[k];
+            mine.assign(modules, 0);
+            for (std::size_t p = bound(k, pins); p < bound(k + 1, pins); ++p) ++mine[d.pin_module[p]];
+        }
+    });
+    if (pieces <= 1) {
+        for (std::size_t p = 0; p < pins; ++p) ++out.pin_count[d.pin_module[p]];
+    } else {
+        workers.run(pieces, [&](std::size_t k) {
+            for (std::size_t m = bound(k, modules); m < bound(k + 1, modules); ++m) {
+                int32_t sum = 0;
+                for (std::size_t j = 0; j < pieces; ++j) sum += counts[j][m];
+                out.pin_count[m] = sum;
+            }
+        });
     }
-    for (int64_t p = 0; p < d.pin_count; ++p) ++out.pin_count[d.pin_module[p]];
     return out;
 }
 
